@@ -1,0 +1,323 @@
+#!/usr/bin/env python
+"""Benchmark: plain-FP32 elastic2d_batch, 32 shots on a 1000x500 grid (padded
+1170x670), dh 5 m, dt 0.5 ms, nt 3000, fd_order 10, nbc 80, 12 seeded layers.
+
+One "step" is one full elastic2d_batch run of the 32-shot batch (3000 time
+steps).  `value` is shots/s with model, acquisition and outputs resident in
+HBM (device entry point); `e2e` is the same metric through the public API
+with pinned host inputs, the H2D copies and the seismogram D2H inside the
+timed region.  Multi-GPU (torchrun): every rank runs its own 32 shots (shots
+are independent, no data-path collective), time = max over ranks.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+for _p in (ROOT, ROOT / "fomo.jl_b200"):
+    if str(_p) not in sys.path:
+        sys.path.insert(0, str(_p))
+
+METRIC = "shots/s"
+WORKLOAD = ("elastic2d_batch fp32: 32 shots, 1000x500 grid (padded 1170x670), dh 5 m, dt 0.5 ms, "
+            "nt 3000, fd_order 10, nbc 80, 12 seeded layers, 500 receivers, 20 Hz Ricker")
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.out, stderr=subprocess.DEVNULL)
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        self.out.flush()
+        rows = []
+        try:
+            for line in Path(self.out.name).read_text().splitlines():
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9:
+                    rows.append(f)
+        finally:
+            os.unlink(self.out.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline(cfg, target_s=12.0, threads=None):
+    """The FP32 CPU oracle (OpenMP, all host threads) on a bounded sample:
+    all 32 shots for a reduced number of time steps, scaled linearly to nt."""
+    from oracle import oracle as O
+
+    O.build()
+    if threads:
+        O.set_threads(threads)
+    cores = O.max_threads()
+    ns = cfg["sx"].size
+    w = np.asarray(__import__("fomo_b200").ricker_wavelet(cfg["f0"], cfg["dt"], cfg["nt"]))
+
+    def run(nt_s):
+        t0 = time.perf_counter()
+        O.elastic2d(cfg["vp"], cfg["vs"], cfg["rho"], cfg["dh"], cfg["dt"], nt_s,
+                    sx=cfg["sx"].reshape(1, -1), sz=cfg["sz"].reshape(1, -1), rx=cfg["rx"],
+                    rz=cfg["rz"], wavelet=w[:nt_s].reshape(1, -1), nbc=cfg["nbc"],
+                    fd_order=cfg["fd_order"], n_shots=ns)
+        return time.perf_counter() - t0
+
+    t = run(2)
+    nt_s = int(max(2, min(cfg["nt"], round(2 * target_s / max(t, 1e-6)))))
+    return nt_s, cores, run
+
+
+def reference_arm(args, cfg):
+    world, rank, _ = _dist()
+    if rank != 0:
+        return
+    nt_s, cores, run = cpu_baseline(cfg, target_s=6.0)
+    ns = cfg["sx"].size
+    for _ in range(args.warmup):
+        run(nt_s)
+    times = [run(nt_s) for _ in range(args.steps)]
+    t = float(np.mean(times))
+    value = ns / (t * cfg["nt"] / nt_s)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "shots/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t * cfg["nt"] / nt_s * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_shots": int(ns), "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": "shots/s", "cores": cores, "kind": "port",
+                         "sample": f"{ns} shots x {nt_s} of {cfg['nt']} time steps per step, "
+                                   "scaled linearly; FP32 C++/OpenMP restatement of Fomo's kernels "
+                                   "(Julia reference not runnable on this box)"},
+        "e2e": {"value": value, "unit": "shots/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def ours(args, cfg):
+    import torch
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    import fomo_b200 as F
+    from fomo_b200 import _lib as L
+    from fomo_b200 import device as D
+    from fomo_b200.api import _check_numerics, _min_pos
+
+    ns = cfg["sx"].size
+    nt = cfg["nt"]
+    _check_numerics(cfg["vp"].max(), _min_pos(cfg["vp"]), np.float32(cfg["dh"]),
+                    np.float32(cfg["dt"]), np.float32(cfg["f0"]), cfg["fd_order"])
+    v_ref = float(_min_pos(cfg["vp"]))
+    w = F.ricker_wavelet(cfg["f0"], cfg["dt"], nt)
+
+    def dev_f32(a2d):  # (nx, nz) Fortran == (nz, nx) row-major
+        return torch.from_numpy(np.ascontiguousarray(np.asarray(a2d, np.float32).T)).to(dev)
+
+    d_vp, d_vs, d_rho = dev_f32(cfg["vp"]), dev_f32(cfg["vs"]), dev_f32(cfg["rho"])
+    d_sx = torch.tensor(cfg["sx"].reshape(ns, 1), dtype=torch.int32, device=dev)
+    d_sz = torch.tensor(cfg["sz"].reshape(ns, 1), dtype=torch.int32, device=dev)
+    d_w = torch.from_numpy(w.reshape(nt, 1).copy()).to(dev)
+    d_rx = torch.tensor(cfg["rx"], dtype=torch.int32, device=dev)
+    d_rz = torch.tensor(cfg["rz"], dtype=torch.int32, device=dev)
+    nrec = cfg["rx"].size
+    d_svx = torch.empty((ns, nt, nrec), dtype=torch.float32, device=dev)
+    d_svz = torch.empty_like(d_svx)
+    kernel = int(os.environ.get("FOMO_BENCH_KERNEL", "0"))
+
+    def step(flags=0):
+        return D.elastic2d_batch(d_vp, d_vs, d_rho, dh=cfg["dh"], dt=cfg["dt"], nt=nt,
+                                 nbc=cfg["nbc"], fd_order=cfg["fd_order"], v_ref=v_ref, sx=d_sx,
+                                 sz=d_sz, wavelet=d_w, rx=d_rx, rz=d_rz, seis_vx=d_svx,
+                                 seis_vz=d_svz, kernel=kernel, device=local, flags=flags)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        st = step()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches = 0
+    sweep_ms = []
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            st = step(flags=D.PROFILE)
+            launches += st.gpu_launches + 1  # + the medium-preparation kernel
+            sweep_ms.append(st.sweep_ms)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    clocks = clk.summary()
+    value = ns * world / (ms * 1e-3)
+    cells = st.cell_updates
+    gcell = cells * world / (ms * 1e-3) / 1e9
+    alg_step = st.alg_bytes / nt  # bytes per time step of the 32-shot batch
+    sweep = float(np.mean(sweep_ms))
+    peak, peak_kind = _peaks()
+    achieved = alg_step / (sweep * 1e-3) / 1e9 if sweep > 0 else None
+    finite = bool(torch.isfinite(d_svz).all().item())
+
+    # ---- e2e through the public API: pinned host inputs, D2H of the seismograms
+    def pinned(a):
+        t = torch.empty(a.shape[::-1], dtype=torch.float32, pin_memory=True)
+        t.copy_(torch.from_numpy(np.ascontiguousarray(np.asarray(a, np.float32).T)))
+        return t.numpy().T  # Fortran-ordered (nx, nz) view of pinned memory
+
+    h_vp, h_vs, h_rho = pinned(cfg["vp"]), pinned(cfg["vs"]), pinned(cfg["rho"])
+    ctx = L.context(local)
+    ctx.set_stream(stream.cuda_stream)
+    kw = dict(sx=cfg["sx"], sz=cfg["sz"], rx=cfg["rx"], rz=cfg["rz"], nbc=cfg["nbc"],
+              fd_order=cfg["fd_order"], device=local, kernel=kernel)
+    import warnings
+
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")  # the config is below 4 points per wavelength by design
+        F.elastic2d_batch(h_vp, h_vs, h_rho, cfg["dh"], cfg["dt"], nt, cfg["f0"], **kw)
+        torch.cuda.synchronize()
+        barrier()
+        e2 = torch.cuda.Event(enable_timing=True)
+        e3 = torch.cuda.Event(enable_timing=True)
+        e2.record(stream)
+        for _ in range(args.steps):
+            r = F.elastic2d_batch(h_vp, h_vs, h_rho, cfg["dh"], cfg["dt"], nt, cfg["f0"], **kw)
+        e3.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(e2.elapsed_time(e3) / args.steps)
+    h2d = 3 * cfg["vp"].size * 4 + nt * 4 + 4 * 2 * (ns + nrec)
+    d2h = r.seis_vx.nbytes + r.seis_vz.nbytes
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "shots/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_shots_per_gpu": int(ns), "global_shots": int(ns * world),
+                   "padded_grid": [1170, 670], "nt": nt, "parallelism": f"shots sharded x{world}",
+                   "l2": "inputs larger than L2 (1.0 GB wavefield state per GPU)",
+                   "kernel_family": {1: "two-phase", 2: "single-sweep"}.get(st.kernel, str(st.kernel))},
+        "gcell_updates_per_s": gcell,
+        "e2e": {"value": ns * world / (e2e_ms * 1e-3), "unit": "shots/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": None,
+                     "peak_kind": peak_kind,
+                     "kernel": f"time-step sweep ({st.sweep_launches} kernel(s)/step)",
+                     "alg_bytes_per_launch": alg_step / max(st.sweep_launches, 1),
+                     "sweep_ms_per_step": sweep},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "finite": finite,
+    }
+    if rank == 0 and world == 1 and not os.environ.get("FOMO_BENCH_NO_CPU"):
+        nt_s, cores, run = cpu_baseline(cfg)
+        t = run(nt_s)
+        cv = ns / (t * nt / nt_s)
+        line["cpu_baseline"] = {"value": cv, "unit": "shots/s", "cores": cores, "kind": "port",
+                                "sample": f"{ns} shots x {nt_s} of {nt} time steps ({t:.1f} s), "
+                                          "scaled linearly; FP32 C++/OpenMP oracle"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    args = ap.parse_args()
+    from fomo_b200.synthetic import elastic_batch_config
+
+    cfg = elastic_batch_config()
+    if args.impl == "reference":
+        reference_arm(args, cfg)
+    else:
+        ours(args, cfg)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,466 @@
+// solver2d.cu -- host drivers of the 2D solvers (acoustic2d, elastic2d,
+// scalar2d and the _batch variants): validation, workspace layout, device
+// medium preparation, the time loop and the result download.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "solver2d_kernels.cuh"
+#include "sweep2d.cuh"
+
+namespace fomo {
+namespace {
+
+enum Phys { kAcoustic = 0, kElastic = 1, kScalar = 2 };
+
+struct Plan2 {
+  Phys phys;
+  int nx, nz, nt, nbc, fd_order, N, M, pad, nxp, nzp;
+  long long plane;
+  float dh, dt, v_ref;
+  int ns, n_src, n_rec;
+  bool dev;
+  int snap_interval, nsnap;
+  int kernel;
+};
+
+int check_indices(fomo_ctx* ctx, const char* what, const int32_t* ix, const int32_t* iz,
+                  long long n, int nx, int nz) {
+  for (long long k = 0; k < n; ++k)
+    if (ix[k] < 1 || ix[k] > nx || iz[k] < 1 || iz[k] > nz)
+      return fail(ctx, FOMO_EARG,
+                  std::string(what) + " index out of range: need 1 <= x <= " + std::to_string(nx) +
+                      ", 1 <= z <= " + std::to_string(nz) + " (got " + std::to_string(ix[k]) + ", " +
+                      std::to_string(iz[k]) + ")");
+  return FOMO_OK;
+}
+
+// Copies a small index/value array to the host when the caller passed device
+// pointers (validation and linear-index construction happen on the host).
+template <class T>
+int host_copy(fomo_ctx* ctx, const T* src, long long n, bool dev, std::vector<T>& out) {
+  out.resize((size_t)std::max<long long>(n, 0));
+  if (n <= 0) return FOMO_OK;
+  if (dev) {
+    FOMO_CU(ctx, cudaMemcpy(out.data(), src, sizeof(T) * n, cudaMemcpyDeviceToHost));
+  } else {
+    std::memcpy(out.data(), src, sizeof(T) * n);
+  }
+  return FOMO_OK;
+}
+
+int make_plan(fomo_ctx* ctx, Phys phys, const fomo_grid2d* g, const fomo_acq* acq,
+              int snap_interval, const fomo_opts* opts, bool batch, Plan2& P) {
+  if (!ctx) return FOMO_EARG;
+  if (!g || !acq) return fail(ctx, FOMO_EARG, "grid and acquisition descriptors are required");
+  P.phys = phys;
+  P.nx = g->nx;
+  P.nz = g->nz;
+  P.nt = g->nt;
+  P.nbc = g->nbc;
+  P.fd_order = g->fd_order;
+  P.dh = g->dh;
+  P.dt = g->dt;
+  P.v_ref = g->v_ref;
+  P.N = order_to_N(g->fd_order);
+  if (P.N < 0) return fail(ctx, FOMO_EARG, "Unsupported FD order: " + std::to_string(g->fd_order));
+  if (P.nx < 1 || P.nz < 1) return fail(ctx, FOMO_EARG, "grid must be at least 1x1");
+  if (P.nt < 1) return fail(ctx, FOMO_EARG, "nt must be >= 1");
+  if (!(P.dh > 0.0f) || !(P.dt > 0.0f)) return fail(ctx, FOMO_EARG, "dh and dt must be > 0");
+  if (P.nbc < 0) return fail(ctx, FOMO_EARG, "nbc must be >= 0");
+  P.M = P.N;
+  P.pad = P.nbc + P.M;
+  if (P.pad < 2) return fail(ctx, FOMO_EARG, "nbc + fd_order/2 must be >= 2");
+  P.nxp = P.nx + 2 * P.pad;
+  P.nzp = P.nz + 2 * P.pad;
+  P.plane = (long long)P.nxp * P.nzp;
+  P.ns = acq->n_shots;
+  P.n_src = acq->n_src;
+  P.n_rec = acq->n_rec;
+  if (P.ns < 1) return fail(ctx, FOMO_EARG, "at least 1 shot is required");
+  if (!batch && P.ns != 1) return fail(ctx, FOMO_EARG, "single-shot solver takes n_shots == 1");
+  if (P.n_src < 0 || P.n_rec < 0) return fail(ctx, FOMO_EARG, "negative source/receiver count");
+  if (P.n_src > 0 && (!acq->sx || !acq->sz || !acq->wavelet))
+    return fail(ctx, FOMO_EARG, "sources need sx, sz and a wavelet matrix");
+  if (P.n_rec > 0 && (!acq->rx || !acq->rz)) return fail(ctx, FOMO_EARG, "receivers need rx, rz");
+  if (snap_interval < 0) return fail(ctx, FOMO_EARG, "snap_interval must be >= 0");
+  P.snap_interval = snap_interval;
+  P.nsnap = snap_interval > 0 ? P.nt / snap_interval : 0;
+  P.dev = opts && (opts->flags & FOMO_F_DEVICE_PTRS);
+  P.kernel = opts ? opts->kernel : FOMO_KERNEL_AUTO;
+  if (opts && opts->precision != FOMO_FP32)
+    return fail(ctx, FOMO_EUNSUPPORTED, "this solver stores FP32 only");
+  if ((long long)P.nxp * P.nzp > (1LL << 31))
+    return fail(ctx, FOMO_EARG, "padded grid exceeds 2^31 cells");
+  return FOMO_OK;
+}
+
+float min_positive(const std::vector<float>& v) {
+  float m = INFINITY;
+  for (float x : v)
+    if (x > 0.0f && x < m) m = x;
+  return m;
+}
+
+struct Outs {
+  float* seis[3];
+  int nseis;
+  float* snaps;
+};
+
+// Common run: model (vp, vs, rho per phys), acquisition, outputs.
+int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float* rho,
+          const fomo_acq* acq, Outs outs, const fomo_opts* opts, fomo_stats* stats) {
+  FOMO_CU(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const long long nint = (long long)P.nx * P.nz;
+  if (!vp || (P.phys != kScalar && !rho) || (P.phys == kElastic && !vs))
+    return fail(ctx, FOMO_EARG, "model arrays are required");
+
+  // ---- indices: validate (utils/checks.jl:8-13) and pad (source.jl:18-28) ----
+  std::vector<int32_t> hsx, hsz, hrx, hrz;
+  long long nsrc_all = (long long)P.n_src * P.ns;
+  int rc;
+  if ((rc = host_copy(ctx, acq->sx, nsrc_all, P.dev, hsx)) ||
+      (rc = host_copy(ctx, acq->sz, nsrc_all, P.dev, hsz)) ||
+      (rc = host_copy(ctx, acq->rx, (long long)P.n_rec, P.dev, hrx)) ||
+      (rc = host_copy(ctx, acq->rz, (long long)P.n_rec, P.dev, hrz)))
+    return rc;
+  if ((rc = check_indices(ctx, "source", hsx.data(), hsz.data(), nsrc_all, P.nx, P.nz)) ||
+      (rc = check_indices(ctx, "receiver", hrx.data(), hrz.data(), P.n_rec, P.nx, P.nz)))
+    return rc;
+  std::vector<int32_t> src_lin(nsrc_all), rec_lin(P.n_rec);
+  for (long long k = 0; k < nsrc_all; ++k)
+    src_lin[k] = (hsx[k] - 1 + P.pad) + P.nxp * (hsz[k] - 1 + P.pad);
+  for (int r = 0; r < P.n_rec; ++r) rec_lin[r] = (hrx[r] - 1 + P.pad) + P.nxp * (hrz[r] - 1 + P.pad);
+
+  // ---- v_ref default: minimum(vp > 0) (acoustic2d.jl:55) ----
+  if (!(P.v_ref > 0.0f)) {
+    std::vector<float> hvp;
+    if ((rc = host_copy(ctx, vp, nint, P.dev, hvp))) return rc;
+    P.v_ref = min_positive(hvp);
+    if (!std::isfinite(P.v_ref)) return fail(ctx, FOMO_EARG, "vp has no positive value for v_ref");
+  }
+  HabcHost hh = make_habc(P.pad, P.v_ref, P.dt, P.dh);
+
+  // ---- workspace layout ----
+  const int nmat = P.phys == kElastic ? 5 : (P.phys == kAcoustic ? 3 : 1);
+  const int nfield = P.phys == kElastic ? 5 : (P.phys == kAcoustic ? 3 : 1);
+  const int nsets = P.phys == kScalar ? 3 : 2;
+  const long long seis_n = (long long)P.n_rec * P.nt * P.ns;
+  Arena ar;
+  size_t o_model = P.dev ? 0 : ar.take<float>(3 * nint);
+  size_t o_mat = ar.take<float>(nmat * P.plane);
+  size_t o_state = ar.take<float>((long long)nsets * nfield * P.ns * P.plane);
+  size_t o_w = ar.take<float>(hh.wtab.size());
+  size_t o_src = ar.take<int32_t>(std::max<long long>(nsrc_all, 1));
+  size_t o_rec = ar.take<int32_t>(std::max(P.n_rec, 1));
+  size_t o_wav = P.dev ? 0 : ar.take<float>(std::max<long long>((long long)P.n_src * P.nt, 1));
+  size_t o_seis = P.dev ? 0 : ar.take<float>(std::max<long long>(outs.nseis * seis_n, 1));
+  size_t o_snap = (!P.dev && outs.snaps && P.nsnap) ? ar.take<float>(P.nsnap * nint) : 0;
+  if ((rc = ensure_workspace(ctx, ar.off))) return rc;
+
+  const float* d_vp = vp;
+  const float* d_vs = vs;
+  const float* d_rho = rho;
+  const float* d_wav = acq->wavelet;
+  if (!P.dev) {
+    float* m = ws_ptr<float>(ctx, o_model);
+    FOMO_CU(ctx, cudaMemcpyAsync(m, vp, sizeof(float) * nint, cudaMemcpyHostToDevice, st));
+    d_vp = m;
+    if (vs) {
+      FOMO_CU(ctx, cudaMemcpyAsync(m + nint, vs, sizeof(float) * nint, cudaMemcpyHostToDevice, st));
+      d_vs = m + nint;
+    }
+    if (rho) {
+      FOMO_CU(ctx,
+              cudaMemcpyAsync(m + 2 * nint, rho, sizeof(float) * nint, cudaMemcpyHostToDevice, st));
+      d_rho = m + 2 * nint;
+    }
+    if (P.n_src > 0) {
+      float* w = ws_ptr<float>(ctx, o_wav);
+      FOMO_CU(ctx, cudaMemcpyAsync(w, acq->wavelet, sizeof(float) * P.n_src * P.nt,
+                                   cudaMemcpyHostToDevice, st));
+      d_wav = w;
+    }
+  }
+  float* d_mat = ws_ptr<float>(ctx, o_mat);
+  float* d_state = ws_ptr<float>(ctx, o_state);
+  float* d_w = ws_ptr<float>(ctx, o_w);
+  int32_t* d_src = ws_ptr<int32_t>(ctx, o_src);
+  int32_t* d_rec = ws_ptr<int32_t>(ctx, o_rec);
+  FOMO_CU(ctx, cudaMemcpyAsync(d_w, hh.wtab.data(), sizeof(float) * hh.wtab.size(),
+                               cudaMemcpyHostToDevice, st));
+  if (nsrc_all)
+    FOMO_CU(ctx, cudaMemcpyAsync(d_src, src_lin.data(), sizeof(int32_t) * nsrc_all,
+                                 cudaMemcpyHostToDevice, st));
+  if (P.n_rec)
+    FOMO_CU(ctx, cudaMemcpyAsync(d_rec, rec_lin.data(), sizeof(int32_t) * P.n_rec,
+                                 cudaMemcpyHostToDevice, st));
+  float* d_seis[3] = {nullptr, nullptr, nullptr};
+  for (int k = 0; k < outs.nseis; ++k)
+    d_seis[k] = P.dev ? outs.seis[k] : (outs.seis[k] ? ws_ptr<float>(ctx, o_seis) + k * seis_n : nullptr);
+  float* d_snap = P.dev ? outs.snaps : (o_snap ? ws_ptr<float>(ctx, o_snap) : nullptr);
+  if (!outs.snaps) d_snap = nullptr;
+
+  // ---- medium (device) ----
+  float dtdh = P.dt / P.dh;  // Float32(dt / dh)
+  FOMO_CU(ctx, launch_medium2d(st, P.phys == kElastic ? 0 : (P.phys == kAcoustic ? 1 : 2), P.nx,
+                               P.nz, P.pad, dtdh, d_vp, d_vs, d_rho, d_mat, d_mat + P.plane,
+                               d_mat + 2 * P.plane, d_mat + 3 * P.plane, d_mat + 4 * P.plane));
+  // ---- zero state (reset!, batch.jl:30-35) ----
+  FOMO_CU(ctx, cudaMemsetAsync(d_state, 0, sizeof(float) * nsets * nfield * P.ns * P.plane, st));
+  if (!P.dev)
+    for (int k = 0; k < outs.nseis; ++k)
+      if (d_seis[k]) FOMO_CU(ctx, cudaMemsetAsync(d_seis[k], 0, sizeof(float) * seis_n, st));
+
+  Geo2 g{P.nxp, P.nzp, P.M, hh.nbc, P.plane};
+  Coef c;
+  for (int l = 0; l < 5; ++l) c.a[l] = kFD[P.N][l];
+  HabcDev h{hh.q, hh.qt, hh.qxt, hh.nbc, hh.wstride, d_w};
+  const float dtx = dtdh, dtz = dtdh;
+  auto field = [&](int set, int f) { return d_state + ((long long)set * nfield + f) * P.ns * P.plane; };
+
+  int kernel = P.kernel;
+  if (kernel == FOMO_KERNEL_AUTO) kernel = pick_kernel_2d((int)P.phys, P.N, P.nxp, P.nzp, P.ns);
+  if (kernel == FOMO_KERNEL_SINGLE_SWEEP && !sweep2d_supported((int)P.phys, P.N))
+    kernel = FOMO_KERNEL_TWO_PHASE;
+
+  dim3 blk(32, 8), grd(cdiv(P.nxp, 32), cdiv(P.nzp, 8), P.ns);
+  int launches = 0;
+  // FOMO_F_PROFILE: event pairs around the sweep kernel(s) of a window of steps
+  const bool prof = opts && (opts->flags & FOMO_F_PROFILE) && P.nt >= 2;
+  const int w0 = P.nt / 2, nw = prof ? std::min(16, P.nt - w0) : 0;
+  std::vector<cudaEvent_t> pev(2 * nw, nullptr);
+  for (auto& e : pev) FOMO_CU(ctx, cudaEventCreate(&e));
+  auto prof_mark = [&](int it, int which) -> cudaError_t {
+    int k = it - 1 - w0;
+    if (k < 0 || k >= nw) return cudaSuccess;
+    return cudaEventRecord(pev[2 * k + which], st);
+  };
+  int sweeps_per_step = 0;
+  FOMO_CU(ctx, cudaEventRecord(ctx->ev0, st));
+  int A = 0, B = 1, C2 = 2;  // scalar: A = u^{n-1}, B = u^n, C2 = u^{n+1}
+  for (int it = 1; it <= P.nt; ++it) {
+    FOMO_CU(ctx, prof_mark(it, 0));
+    if (P.phys == kElastic) {
+      ElFields a{field(A, 0), field(A, 1), field(A, 2), field(A, 3), field(A, 4)};
+      ElMat m{d_mat, d_mat + P.plane, d_mat + 2 * P.plane, d_mat + 3 * P.plane, d_mat + 4 * P.plane};
+      if (kernel == FOMO_KERNEL_SINGLE_SWEEP) {
+        ElOut o{field(B, 0), field(B, 1), field(B, 2), field(B, 3), field(B, 4)};
+        FOMO_CU(ctx, launch_sweep_elastic(st, P.N, g, c, dtx, dtz, h, a, m, o, P.ns));
+        launches += 1;
+        sweeps_per_step = 1;
+      } else {
+#define FOMO_EL_CASE(NN)                                                                       \
+  case NN:                                                                                     \
+    k_el_vel<NN><<<grd, blk, 0, st>>>(g, c, dtx, dtz, h, a, m, field(B, 0), field(B, 1));      \
+    k_el_str<NN><<<grd, blk, 0, st>>>(g, c, dtx, dtz, h, a, field(B, 0), field(B, 1), m,       \
+                                      field(B, 2), field(B, 3), field(B, 4));                  \
+    break;
+        switch (P.N) { FOMO_EL_CASE(1) FOMO_EL_CASE(2) FOMO_EL_CASE(3) FOMO_EL_CASE(4) FOMO_EL_CASE(5) }
+#undef FOMO_EL_CASE
+        launches += 2;
+        sweeps_per_step = 2;
+      }
+      FOMO_CU(ctx, prof_mark(it, 1));
+      k_inject_record<<<P.ns, 256, 0, st>>>(it, P.nt, P.plane, P.n_src, d_src, d_wav, field(B, 2),
+                                            field(B, 3), P.n_rec, d_rec, field(B, 0), field(B, 1),
+                                            nullptr, d_seis[0], d_seis[1], nullptr);
+      launches += 1;
+    } else if (P.phys == kAcoustic) {
+      const float* p0 = field(A, 2);
+      const float* vx0 = field(A, 0);
+      const float* vz0 = field(A, 1);
+      const float* bx = d_mat;
+      const float* bz = d_mat + P.plane;
+      const float* kap = d_mat + 2 * P.plane;
+#define FOMO_AC_CASE(NN)                                                                          \
+  case NN:                                                                                        \
+    k_ac_vel<NN><<<grd, blk, 0, st>>>(g, c, dtx, dtz, h, p0, vx0, vz0, bx, bz, field(B, 0),      \
+                                      field(B, 1));                                               \
+    k_ac_prs<NN><<<grd, blk, 0, st>>>(g, c, dtx, dtz, h, p0, field(B, 0), field(B, 1), kap,      \
+                                      field(B, 2));                                               \
+    break;
+      switch (P.N) { FOMO_AC_CASE(1) FOMO_AC_CASE(2) FOMO_AC_CASE(3) FOMO_AC_CASE(4) FOMO_AC_CASE(5) }
+#undef FOMO_AC_CASE
+      sweeps_per_step = 2;
+      FOMO_CU(ctx, prof_mark(it, 1));
+      k_inject_record<<<P.ns, 256, 0, st>>>(it, P.nt, P.plane, P.n_src, d_src, d_wav, field(B, 2),
+                                            nullptr, P.n_rec, d_rec, field(B, 2), field(B, 0),
+                                            field(B, 1), d_seis[0], d_seis[1], d_seis[2]);
+      launches += 3;
+    } else {
+      D2Coef dc;
+      dc.two_c0 = 2.0f * kD2C0[P.N];
+      for (int l = 0; l < 5; ++l) dc.d[l] = kD2[P.N][l];
+#define FOMO_SC_CASE(NN)                                                                      \
+  case NN:                                                                                    \
+    k_sc_step<NN><<<grd, blk, 0, st>>>(g, dc, h, field(B, 0), field(A, 0), d_mat, field(C2, 0)); \
+    break;
+      switch (P.N) { FOMO_SC_CASE(1) FOMO_SC_CASE(2) FOMO_SC_CASE(3) FOMO_SC_CASE(4) FOMO_SC_CASE(5) }
+#undef FOMO_SC_CASE
+      sweeps_per_step = 1;
+      FOMO_CU(ctx, prof_mark(it, 1));
+      k_inject_record<<<1, 256, 0, st>>>(it, P.nt, P.plane, P.n_src, d_src, d_wav, field(C2, 0),
+                                         nullptr, P.n_rec, d_rec, field(C2, 0), nullptr, nullptr,
+                                         d_seis[0], nullptr, nullptr);
+      launches += 2;
+    }
+    FOMO_CU(ctx, cudaGetLastError());
+    // snapshot of the interior (fused_kernels.jl:192-195): p (acoustic), vz (elastic)
+    if (d_snap && P.snap_interval > 0 && it % P.snap_interval == 0) {
+      int k = it / P.snap_interval - 1;
+      const float* src = (P.phys == kAcoustic ? field(B, 2) : field(B, 1)) + P.pad + (long long)P.pad * P.nxp;
+      FOMO_CU(ctx, cudaMemcpy2DAsync(d_snap + (long long)k * nint, sizeof(float) * P.nx, src,
+                                     sizeof(float) * P.nxp, sizeof(float) * P.nx, P.nz,
+                                     cudaMemcpyDeviceToDevice, st));
+    }
+    if (P.phys == kScalar) {
+      int t = A;
+      A = B;
+      B = C2;
+      C2 = t;
+    } else {
+      std::swap(A, B);
+    }
+  }
+  FOMO_CU(ctx, cudaEventRecord(ctx->ev1, st));
+
+  // ---- results ----
+  if (!P.dev) {
+    for (int k = 0; k < outs.nseis; ++k)
+      if (outs.seis[k] && seis_n)
+        FOMO_CU(ctx, cudaMemcpyAsync(outs.seis[k], d_seis[k], sizeof(float) * seis_n,
+                                     cudaMemcpyDeviceToHost, st));
+    if (d_snap && P.nsnap)
+      FOMO_CU(ctx, cudaMemcpyAsync(outs.snaps, d_snap, sizeof(float) * P.nsnap * nint,
+                                   cudaMemcpyDeviceToHost, st));
+  }
+  if (opts && opts->final_state) {
+    // (nxp, nzp, nfield, ns) host layout; scalar returns (u^n, u^{n-1})
+    for (int s = 0; s < P.ns; ++s)
+      for (int f = 0; f < nfield; ++f) {
+        int set = P.phys == kScalar ? (f == 0 ? B : A) : A;
+        const float* src = P.phys == kScalar ? field(set, 0) : field(A, f) + (long long)s * P.plane;
+        FOMO_CU(ctx, cudaMemcpyAsync(opts->final_state + ((long long)s * nfield + f) * P.plane, src,
+                                     sizeof(float) * P.plane, cudaMemcpyDeviceToHost, st));
+      }
+    if (P.phys == kScalar)
+      FOMO_CU(ctx, cudaMemcpyAsync(opts->final_state + P.plane, field(A, 0),
+                                   sizeof(float) * P.plane, cudaMemcpyDeviceToHost, st));
+  }
+  FOMO_CU(ctx, cudaStreamSynchronize(st));
+  float ms = 0.0f;
+  FOMO_CU(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  double sweep_ms = 0.0;
+  for (int k = 0; k < nw; ++k) {
+    float t = 0.0f;
+    FOMO_CU(ctx, cudaEventElapsedTime(&t, pev[2 * k], pev[2 * k + 1]));
+    sweep_ms += t;
+  }
+  for (auto& e : pev) cudaEventDestroy(e);
+  if (nw) sweep_ms /= nw;
+  if (stats) {
+    stats->kernel_time_s = ms * 1e-3;
+    stats->cell_updates = (double)P.plane * P.nt * P.ns;
+    double wpc = P.phys == kElastic ? 10.0 : (P.phys == kAcoustic ? 6.0 : 3.0);
+    double wm = P.phys == kElastic ? 5.0 : (P.phys == kAcoustic ? 3.0 : 1.0);
+    stats->alg_bytes = 4.0 * (double)P.plane * P.nt * (wpc * P.ns + wm);
+    stats->n_shots = P.ns;
+    stats->gpu_launches = launches;
+    stats->kernel = kernel;
+    stats->status = FOMO_OK;
+    stats->sweep_ms = sweep_ms;
+    stats->sweep_launches = sweeps_per_step;
+  }
+  return FOMO_OK;
+}
+
+}  // namespace
+}  // namespace fomo
+
+using namespace fomo;
+
+extern "C" {
+
+int fomo_acoustic2d(fomo_ctx* ctx, const fomo_grid2d* g, const float* vp, const float* rho,
+                    const fomo_acq* acq, int32_t snap_interval, float* seis_p, float* seis_vx,
+                    float* seis_vz, float* snaps, const fomo_opts* opts, fomo_stats* stats) {
+  Plan2 P;
+  int rc = make_plan(ctx, kAcoustic, g, acq, snap_interval, opts, false, P);
+  if (rc) return rc;
+  Outs o{{seis_p, seis_vx, seis_vz}, 3, snaps};
+  return run2d(ctx, P, vp, nullptr, rho, acq, o, opts, stats);
+}
+
+int fomo_acoustic2d_batch(fomo_ctx* ctx, const fomo_grid2d* g, const float* vp, const float* rho,
+                          const fomo_acq* acq, float* seis_p, float* seis_vx, float* seis_vz,
+                          const fomo_opts* opts, fomo_stats* stats) {
+  Plan2 P;
+  int rc = make_plan(ctx, kAcoustic, g, acq, 0, opts, true, P);
+  if (rc) return rc;
+  Outs o{{seis_p, seis_vx, seis_vz}, 3, nullptr};
+  return run2d(ctx, P, vp, nullptr, rho, acq, o, opts, stats);
+}
+
+int fomo_elastic2d(fomo_ctx* ctx, const fomo_grid2d* g, const float* vp, const float* vs,
+                   const float* rho, const fomo_acq* acq, int32_t snap_interval, float* seis_vx,
+                   float* seis_vz, float* snaps, const fomo_opts* opts, fomo_stats* stats) {
+  Plan2 P;
+  int rc = make_plan(ctx, kElastic, g, acq, snap_interval, opts, false, P);
+  if (rc) return rc;
+  Outs o{{seis_vx, seis_vz, nullptr}, 2, snaps};
+  return run2d(ctx, P, vp, vs, rho, acq, o, opts, stats);
+}
+
+int fomo_elastic2d_batch(fomo_ctx* ctx, const fomo_grid2d* g, const float* vp, const float* vs,
+                         const float* rho, const fomo_acq* acq, float* seis_vx, float* seis_vz,
+                         const fomo_opts* opts, fomo_stats* stats) {
+  Plan2 P;
+  int rc = make_plan(ctx, kElastic, g, acq, 0, opts, true, P);
+  if (rc) return rc;
+  Outs o{{seis_vx, seis_vz, nullptr}, 2, nullptr};
+  return run2d(ctx, P, vp, vs, rho, acq, o, opts, stats);
+}
+
+int fomo_scalar2d(fomo_ctx* ctx, const fomo_grid2d* g, const float* vp, const fomo_acq* acq,
+                  float* seis_u, const fomo_opts* opts, fomo_stats* stats) {
+  Plan2 P;
+  int rc = make_plan(ctx, kScalar, g, acq, 0, opts, false, P);
+  if (rc) return rc;
+  Outs o{{seis_u, nullptr, nullptr}, 1, nullptr};
+  return run2d(ctx, P, vp, nullptr, nullptr, acq, o, opts, stats);
+}
+
+int fomo_debug_medium2d(fomo_ctx* ctx, int32_t kind, int32_t nx, int32_t nz, int32_t pad,
+                        float dt, float dh, const float* vp, const float* vs, const float* rho,
+                        float* out) {
+  if (!ctx || !vp || !out || nx < 1 || nz < 1 || pad < 1 || kind < 0 || kind > 2)
+    return fail(ctx, FOMO_EARG, "bad debug_medium2d arguments");
+  if ((kind == 0 && (!vs || !rho)) || (kind == 1 && !rho))
+    return fail(ctx, FOMO_EARG, "model arrays missing");
+  FOMO_CU(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  long long nint = (long long)nx * nz, plane = (long long)(nx + 2 * pad) * (nz + 2 * pad);
+  int nf = kind == 0 ? 5 : (kind == 1 ? 3 : 1);
+  Arena ar;
+  size_t om = ar.take<float>(3 * nint), oo = ar.take<float>(nf * plane);
+  int rc = ensure_workspace(ctx, ar.off);
+  if (rc) return rc;
+  float* m = ws_ptr<float>(ctx, om);
+  float* o = ws_ptr<float>(ctx, oo);
+  FOMO_CU(ctx, cudaMemcpyAsync(m, vp, sizeof(float) * nint, cudaMemcpyHostToDevice, st));
+  if (vs) FOMO_CU(ctx, cudaMemcpyAsync(m + nint, vs, sizeof(float) * nint, cudaMemcpyHostToDevice, st));
+  if (rho)
+    FOMO_CU(ctx, cudaMemcpyAsync(m + 2 * nint, rho, sizeof(float) * nint, cudaMemcpyHostToDevice, st));
+  FOMO_CU(ctx, launch_medium2d(st, kind, nx, nz, pad, dt / dh, m, vs ? m + nint : nullptr,
+                               rho ? m + 2 * nint : nullptr, o, o + plane, o + 2 * plane,
+                               o + 3 * plane, o + 4 * plane));
+  FOMO_CU(ctx, cudaMemcpyAsync(out, o, sizeof(float) * nf * plane, cudaMemcpyDeviceToHost, st));
+  FOMO_CU(ctx, cudaStreamSynchronize(st));
+  return FOMO_OK;
+}
+
+}  // extern "C"

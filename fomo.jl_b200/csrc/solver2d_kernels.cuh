@@ -1,0 +1,377 @@
+// solver2d_kernels.cuh -- two-phase time-step kernels for the 2D solvers.
+//
+// One step = velocity sweep (A -> B) + stress/pressure sweep (A,B -> B) +
+// inject/record, on ping-pong buffers A (time n) and B (time n+1).  The
+// deterministic two-pass HABC of boundary/habc/kernels_det.jl:22-172 is fused
+// into each sweep: a frame cell evaluates the Higdon value from the
+// pre-correction field, recomputing the one inward neighbour's update from A
+// (a pure function), so no scratch frame buffer and no second pass exist.
+#pragma once
+#include "fomo_internal.cuh"
+
+namespace fomo {
+
+// ---------------------------------------------------------------------------
+// elastic2d velocity / stress updates (elastic2d/fused_kernels.jl:21-124,
+// batch.jl:278-378).  Materials are shared by all shots; fields carry the
+// shot offset already.
+// ---------------------------------------------------------------------------
+struct ElFields {
+  const float* vx;
+  const float* vz;
+  const float* txx;
+  const float* tzz;
+  const float* txz;
+};
+struct ElOut {
+  float* vx;
+  float* vz;
+  float* txx;
+  float* tzz;
+  float* txz;
+};
+struct ElMat {
+  const float* bx;
+  const float* bz;
+  const float* lam;
+  const float* l2m;
+  const float* mut;
+};
+
+template <int N>
+__device__ __forceinline__ void el_vel_at(const Geo2& g, const Coef& c, float dtx, float dtz,
+                                          const ElFields& a, const ElMat& m, int x, int z,
+                                          float& ux, float& uz) {
+  long long p = (long long)z * g.nx + x;
+  float vx = __ldg(a.vx + p), vz = __ldg(a.vz + p);
+  if (interior2(g, x, z)) {
+    const long long sz = g.nx;
+    float dxx = dm<N>(a.txx, p, 1, c);
+    float dxzz = dm<N>(a.txz, p, sz, c);
+    float dxzx = dp<N>(a.txz, p, 1, c);
+    float dzz = dp<N>(a.tzz, p, sz, c);
+    vx = __fmaf_rn(__ldg(m.bx + p), __fmaf_rn(dtx, dxx, __fmul_rn(dtz, dxzz)), vx);
+    vz = __fmaf_rn(__ldg(m.bz + p), __fmaf_rn(dtx, dxzx, __fmul_rn(dtz, dzz)), vz);
+  }
+  ux = vx;
+  uz = vz;
+}
+
+template <int N>
+__global__ void __launch_bounds__(256) k_el_vel(Geo2 g, Coef c, float dtx, float dtz, HabcDev h,
+                                                ElFields a, ElMat m, float* __restrict__ vx1,
+                                                float* __restrict__ vz1) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int z = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= g.nx || z >= g.nz) return;
+  const long long so = (long long)blockIdx.z * g.plane;
+  a.vx += so; a.vz += so; a.txx += so; a.tzz += so; a.txz += so;
+  float ux, uz;
+  el_vel_at<N>(g, c, dtx, dtz, a, m, x, z, ux, uz);
+  long long p = (long long)z * g.nx + x;
+  int sx, sz, dist;
+  if (frame2(g, x, z, sx, sz, dist)) {
+    float wx = habc_weight(h, 0, dist), wz = habc_weight(h, 1, dist);
+    float fox = __ldg(a.vx + p), foz = __ldg(a.vz + p);
+    if (sx != 0 && sz != 0) {
+      long long px = p + sx, pz = p + (long long)sz * g.nx;
+      float ax, az, bx, bz;
+      el_vel_at<N>(g, c, dtx, dtz, a, m, x + sx, z, ax, az);
+      el_vel_at<N>(g, c, dtx, dtz, a, m, x, z + sz, bx, bz);
+      ux = higdon_corner(wx, ux, higdon_side(h, ax, fox, __ldg(a.vx + px)),
+                         higdon_side(h, bx, fox, __ldg(a.vx + pz)));
+      uz = higdon_corner(wz, uz, higdon_side(h, az, foz, __ldg(a.vz + px)),
+                         higdon_side(h, bz, foz, __ldg(a.vz + pz)));
+    } else {
+      int nxp = x + sx, nzp = z + sz;
+      long long pn = (long long)nzp * g.nx + nxp;
+      float nx_, nz_;
+      el_vel_at<N>(g, c, dtx, dtz, a, m, nxp, nzp, nx_, nz_);
+      ux = higdon_edge(wx, ux, higdon_side(h, nx_, fox, __ldg(a.vx + pn)));
+      uz = higdon_edge(wz, uz, higdon_side(h, nz_, foz, __ldg(a.vz + pn)));
+    }
+  }
+  vx1[so + p] = ux;
+  vz1[so + p] = uz;
+}
+
+template <int N>
+__device__ __forceinline__ void el_str_at(const Geo2& g, const Coef& c, float dtx, float dtz,
+                                          const float* __restrict__ vx, const float* __restrict__ vz,
+                                          const ElFields& a, const ElMat& m, int x, int z,
+                                          float& sxx, float& szz, float& sxz) {
+  long long p = (long long)z * g.nx + x;
+  sxx = __ldg(a.txx + p);
+  szz = __ldg(a.tzz + p);
+  sxz = __ldg(a.txz + p);
+  if (interior2(g, x, z)) {
+    const long long sz = g.nx;
+    float dvxdx = dp<N>(vx, p, 1, c);
+    float dvzdz = dm<N>(vz, p, sz, c);
+    float dvxdz = dp<N>(vx, p, sz, c);
+    float dvzdx = dm<N>(vz, p, 1, c);
+    float lam = __ldg(m.lam + p), l2m = __ldg(m.l2m + p);
+    float ex = __fmul_rn(dvxdx, dtx), ez = __fmul_rn(dvzdz, dtz);
+    sxx = __fadd_rn(sxx, __fmaf_rn(l2m, ex, __fmul_rn(lam, ez)));
+    szz = __fadd_rn(szz, __fmaf_rn(lam, ex, __fmul_rn(l2m, ez)));
+    sxz = __fmaf_rn(__ldg(m.mut + p), __fmaf_rn(dvxdz, dtz, __fmul_rn(dvzdx, dtx)), sxz);
+  }
+}
+
+template <int N>
+__global__ void __launch_bounds__(256) k_el_str(Geo2 g, Coef c, float dtx, float dtz, HabcDev h,
+                                                ElFields a, const float* __restrict__ vx1,
+                                                const float* __restrict__ vz1, ElMat m,
+                                                float* __restrict__ txx1, float* __restrict__ tzz1,
+                                                float* __restrict__ txz1) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int z = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= g.nx || z >= g.nz) return;
+  const long long so = (long long)blockIdx.z * g.plane;
+  a.txx += so; a.tzz += so; a.txz += so;
+  const float* vx = vx1 + so;
+  const float* vz = vz1 + so;
+  float sxx, szz, sxz;
+  el_str_at<N>(g, c, dtx, dtz, vx, vz, a, m, x, z, sxx, szz, sxz);
+  long long p = (long long)z * g.nx + x;
+  int sx, sz, dist;
+  if (frame2(g, x, z, sx, sz, dist)) {
+    float w = habc_weight(h, 2, dist);
+    float o1 = __ldg(a.txx + p), o2 = __ldg(a.tzz + p), o3 = __ldg(a.txz + p);
+    if (sx != 0 && sz != 0) {
+      long long px = p + sx, pz = p + (long long)sz * g.nx;
+      float a1, a2, a3, b1, b2, b3;
+      el_str_at<N>(g, c, dtx, dtz, vx, vz, a, m, x + sx, z, a1, a2, a3);
+      el_str_at<N>(g, c, dtx, dtz, vx, vz, a, m, x, z + sz, b1, b2, b3);
+      sxx = higdon_corner(w, sxx, higdon_side(h, a1, o1, __ldg(a.txx + px)),
+                          higdon_side(h, b1, o1, __ldg(a.txx + pz)));
+      szz = higdon_corner(w, szz, higdon_side(h, a2, o2, __ldg(a.tzz + px)),
+                          higdon_side(h, b2, o2, __ldg(a.tzz + pz)));
+      sxz = higdon_corner(w, sxz, higdon_side(h, a3, o3, __ldg(a.txz + px)),
+                          higdon_side(h, b3, o3, __ldg(a.txz + pz)));
+    } else {
+      int xn = x + sx, zn = z + sz;
+      long long pn = (long long)zn * g.nx + xn;
+      float n1, n2, n3;
+      el_str_at<N>(g, c, dtx, dtz, vx, vz, a, m, xn, zn, n1, n2, n3);
+      sxx = higdon_edge(w, sxx, higdon_side(h, n1, o1, __ldg(a.txx + pn)));
+      szz = higdon_edge(w, szz, higdon_side(h, n2, o2, __ldg(a.tzz + pn)));
+      sxz = higdon_edge(w, sxz, higdon_side(h, n3, o3, __ldg(a.txz + pn)));
+    }
+  }
+  txx1[so + p] = sxx;
+  tzz1[so + p] = szz;
+  txz1[so + p] = sxz;
+}
+
+// ---------------------------------------------------------------------------
+// acoustic2d velocity / pressure (acoustic2d/fused_kernels.jl:27-114,
+// batch.jl:38-120)
+// ---------------------------------------------------------------------------
+template <int N>
+__device__ __forceinline__ void ac_vel_at(const Geo2& g, const Coef& c, float dtx, float dtz,
+                                          const float* __restrict__ pr, const float* __restrict__ vx0,
+                                          const float* __restrict__ vz0, const float* __restrict__ bx,
+                                          const float* __restrict__ bz, int x, int z, float& ux,
+                                          float& uz) {
+  long long p = (long long)z * g.nx + x;
+  float vx = __ldg(vx0 + p), vz = __ldg(vz0 + p);
+  if (interior2(g, x, z)) {
+    float dpdx = dm<N>(pr, p, 1, c);
+    float dpdz = dp<N>(pr, p, g.nx, c);
+    vx = __fmaf_rn(__fmul_rn(__ldg(bx + p), dtx), dpdx, vx);
+    vz = __fmaf_rn(__fmul_rn(__ldg(bz + p), dtz), dpdz, vz);
+  }
+  ux = vx;
+  uz = vz;
+}
+
+template <int N>
+__global__ void __launch_bounds__(256) k_ac_vel(Geo2 g, Coef c, float dtx, float dtz, HabcDev h,
+                                                const float* __restrict__ p0,
+                                                const float* __restrict__ vx0,
+                                                const float* __restrict__ vz0,
+                                                const float* __restrict__ bx,
+                                                const float* __restrict__ bz,
+                                                float* __restrict__ vx1, float* __restrict__ vz1) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int z = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= g.nx || z >= g.nz) return;
+  const long long so = (long long)blockIdx.z * g.plane;
+  p0 += so; vx0 += so; vz0 += so;
+  float ux, uz;
+  ac_vel_at<N>(g, c, dtx, dtz, p0, vx0, vz0, bx, bz, x, z, ux, uz);
+  long long p = (long long)z * g.nx + x;
+  int sx, sz, dist;
+  if (frame2(g, x, z, sx, sz, dist)) {
+    float wx = habc_weight(h, 0, dist), wz = habc_weight(h, 1, dist);
+    float fox = __ldg(vx0 + p), foz = __ldg(vz0 + p);
+    if (sx != 0 && sz != 0) {
+      long long px = p + sx, pz = p + (long long)sz * g.nx;
+      float ax, az, bxv, bzv;
+      ac_vel_at<N>(g, c, dtx, dtz, p0, vx0, vz0, bx, bz, x + sx, z, ax, az);
+      ac_vel_at<N>(g, c, dtx, dtz, p0, vx0, vz0, bx, bz, x, z + sz, bxv, bzv);
+      ux = higdon_corner(wx, ux, higdon_side(h, ax, fox, __ldg(vx0 + px)),
+                         higdon_side(h, bxv, fox, __ldg(vx0 + pz)));
+      uz = higdon_corner(wz, uz, higdon_side(h, az, foz, __ldg(vz0 + px)),
+                         higdon_side(h, bzv, foz, __ldg(vz0 + pz)));
+    } else {
+      int xn = x + sx, zn = z + sz;
+      long long pn = (long long)zn * g.nx + xn;
+      float nx_, nz_;
+      ac_vel_at<N>(g, c, dtx, dtz, p0, vx0, vz0, bx, bz, xn, zn, nx_, nz_);
+      ux = higdon_edge(wx, ux, higdon_side(h, nx_, fox, __ldg(vx0 + pn)));
+      uz = higdon_edge(wz, uz, higdon_side(h, nz_, foz, __ldg(vz0 + pn)));
+    }
+  }
+  vx1[so + p] = ux;
+  vz1[so + p] = uz;
+}
+
+template <int N>
+__device__ __forceinline__ float ac_prs_at(const Geo2& g, const Coef& c, float dtx, float dtz,
+                                           const float* __restrict__ vx, const float* __restrict__ vz,
+                                           const float* __restrict__ p0,
+                                           const float* __restrict__ kappa, int x, int z) {
+  long long p = (long long)z * g.nx + x;
+  float v = __ldg(p0 + p);
+  if (interior2(g, x, z)) {
+    float dvxdx = dp<N>(vx, p, 1, c);
+    float dvzdz = dm<N>(vz, p, g.nx, c);
+    v = __fmaf_rn(__ldg(kappa + p), __fmaf_rn(dvxdx, dtx, __fmul_rn(dvzdz, dtz)), v);
+  }
+  return v;
+}
+
+template <int N>
+__global__ void __launch_bounds__(256) k_ac_prs(Geo2 g, Coef c, float dtx, float dtz, HabcDev h,
+                                                const float* __restrict__ p0,
+                                                const float* __restrict__ vx1,
+                                                const float* __restrict__ vz1,
+                                                const float* __restrict__ kappa,
+                                                float* __restrict__ p1) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int z = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= g.nx || z >= g.nz) return;
+  const long long so = (long long)blockIdx.z * g.plane;
+  p0 += so;
+  const float* vx = vx1 + so;
+  const float* vz = vz1 + so;
+  float u = ac_prs_at<N>(g, c, dtx, dtz, vx, vz, p0, kappa, x, z);
+  long long p = (long long)z * g.nx + x;
+  int sx, sz, dist;
+  if (frame2(g, x, z, sx, sz, dist)) {
+    float w = habc_weight(h, 2, dist);
+    float fo = __ldg(p0 + p);
+    if (sx != 0 && sz != 0) {
+      long long px = p + sx, pz = p + (long long)sz * g.nx;
+      float a = ac_prs_at<N>(g, c, dtx, dtz, vx, vz, p0, kappa, x + sx, z);
+      float b = ac_prs_at<N>(g, c, dtx, dtz, vx, vz, p0, kappa, x, z + sz);
+      u = higdon_corner(w, u, higdon_side(h, a, fo, __ldg(p0 + px)),
+                        higdon_side(h, b, fo, __ldg(p0 + pz)));
+    } else {
+      int xn = x + sx, zn = z + sz;
+      long long pn = (long long)zn * g.nx + xn;
+      float a = ac_prs_at<N>(g, c, dtx, dtz, vx, vz, p0, kappa, xn, zn);
+      u = higdon_edge(w, u, higdon_side(h, a, fo, __ldg(p0 + pn)));
+    }
+  }
+  p1[so + p] = u;
+}
+
+// ---------------------------------------------------------------------------
+// scalar2d leapfrog (scalar2d/scalar2d.jl:29-84): u2 = update(u1, u0), then
+// HABC with f_old = u1; three rotating buffers keep every read race-free.
+// ---------------------------------------------------------------------------
+struct D2Coef {
+  float two_c0;
+  float d[5];
+};
+
+template <int N>
+__device__ __forceinline__ float sc_at(const Geo2& g, const D2Coef& c, const float* __restrict__ u1,
+                                       const float* __restrict__ u0, const float* __restrict__ c2,
+                                       int x, int z) {
+  long long p = (long long)z * g.nx + x;
+  float uc = __ldg(u1 + p);
+  if (!interior2(g, x, z)) return uc;
+  float lap = __fmul_rn(c.two_c0, uc);
+  const long long s = g.nx;
+#pragma unroll
+  for (int l = 1; l <= N; ++l) {
+    float nb = __fadd_rn(__fadd_rn(__fadd_rn(__ldg(u1 + p + l), __ldg(u1 + p - l)),
+                                   __ldg(u1 + p + l * s)),
+                         __ldg(u1 + p - l * s));
+    lap = __fmaf_rn(c.d[l - 1], nb, lap);
+  }
+  return __fmaf_rn(__ldg(c2 + p), lap, __fsub_rn(__fmul_rn(2.0f, uc), __ldg(u0 + p)));
+}
+
+template <int N>
+__global__ void __launch_bounds__(256) k_sc_step(Geo2 g, D2Coef c, HabcDev h,
+                                                 const float* __restrict__ u1,
+                                                 const float* __restrict__ u0,
+                                                 const float* __restrict__ c2,
+                                                 float* __restrict__ u2) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int z = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= g.nx || z >= g.nz) return;
+  float u = sc_at<N>(g, c, u1, u0, c2, x, z);
+  long long p = (long long)z * g.nx + x;
+  int sx, sz, dist;
+  if (frame2(g, x, z, sx, sz, dist)) {
+    float w = habc_weight(h, 2, dist);
+    float fo = __ldg(u1 + p);
+    if (sx != 0 && sz != 0) {
+      long long px = p + sx, pz = p + (long long)sz * g.nx;
+      float a = sc_at<N>(g, c, u1, u0, c2, x + sx, z);
+      float b = sc_at<N>(g, c, u1, u0, c2, x, z + sz);
+      u = higdon_corner(w, u, higdon_side(h, a, fo, __ldg(u1 + px)),
+                        higdon_side(h, b, fo, __ldg(u1 + pz)));
+    } else {
+      int xn = x + sx, zn = z + sz;
+      long long pn = (long long)zn * g.nx + xn;
+      float a = sc_at<N>(g, c, u1, u0, c2, xn, zn);
+      u = higdon_edge(w, u, higdon_side(h, a, fo, __ldg(u1 + pn)));
+    }
+  }
+  u2[p] = u;
+}
+
+// ---------------------------------------------------------------------------
+// Injection then recording, one block per shot (inject_source.jl:4-24,
+// batch_acq.jl:40-130, record_receiver.jl:3-18).  Sources are added by one
+// thread in source order, so coincident sources sum deterministically (the
+// reference's concurrent `+=` races there); recording follows a barrier so a
+// receiver on a source cell sees the injected value, as the reference's
+// launch order does.
+//   inj0/inj1: fields receiving the wavelet (acoustic p; elastic txx,tzz;
+//              scalar u).  rec0..2: recorded fields (null = skip).
+// ---------------------------------------------------------------------------
+static __global__ void k_inject_record(int it, int nt, long long plane, int n_src,
+                                const int* __restrict__ src_lin, const float* __restrict__ wav,
+                                float* inj0, float* inj1, int n_rec,
+                                const int* __restrict__ rec_lin, const float* rec0,
+                                const float* rec1, const float* rec2, float* __restrict__ s0,
+                                float* __restrict__ s1, float* __restrict__ s2) {
+  const int s = blockIdx.x;
+  const long long so = (long long)s * plane;
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < n_src; ++q) {
+      long long p = so + src_lin[(long long)s * n_src + q];
+      float w = wav[(long long)(it - 1) * n_src + q];
+      inj0[p] = __fadd_rn(inj0[p], w);
+      if (inj1) inj1[p] = __fadd_rn(inj1[p], w);
+    }
+  }
+  __syncthreads();
+  const long long ob = (long long)n_rec * ((long long)(it - 1) + (long long)nt * s);
+  for (int r = threadIdx.x; r < n_rec; r += blockDim.x) {
+    long long p = so + rec_lin[r];
+    if (rec0) s0[ob + r] = rec0[p];
+    if (rec1) s1[ob + r] = rec1[p];
+    if (rec2) s2[ob + r] = rec2[p];
+  }
+}
+
+}  // namespace fomo

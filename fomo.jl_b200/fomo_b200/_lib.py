@@ -1,0 +1,145 @@
+"""ctypes binding of libfomo_b200.so (the C ABI declared in include/fomo_b200.h).
+
+The library is the only compute path: if it is missing or no CUDA device is
+present, every solver raises instead of falling back to anything else.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+from pathlib import Path
+
+PKG_ROOT = Path(__file__).resolve().parent.parent  # fomo.jl_b200/
+LIB_PATH = Path(os.environ.get("FOMO_B200_LIB", PKG_ROOT / "lib" / "libfomo_b200.so"))
+
+FOMO_OK = 0
+FOMO_EARG = -1
+FOMO_ECUDA = -2
+FOMO_ENOMEM = -3
+FOMO_ENONFINITE = -4
+FOMO_EUNSUPPORTED = -5
+
+FOMO_F_DEVICE_PTRS = 1
+FOMO_F_PROFILE = 2
+FOMO_FP32, FOMO_FP16, FOMO_BF16 = 0, 1, 2
+FOMO_KERNEL_AUTO, FOMO_KERNEL_TWO_PHASE, FOMO_KERNEL_SINGLE_SWEEP = 0, 1, 2
+
+# Every symbol include/fomo_b200.h declares (checked by the ABI tests).
+EXPORTS = (
+    "fomo_version", "fomo_create", "fomo_destroy", "fomo_last_error", "fomo_set_stream",
+    "fomo_trim", "fomo_check_numerics", "fomo_acoustic2d", "fomo_acoustic2d_batch",
+    "fomo_elastic2d", "fomo_elastic2d_batch", "fomo_scalar2d", "fomo_debug_medium2d",
+)
+
+
+class Grid2D(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("nz", C.c_int32), ("dh", C.c_float), ("dt", C.c_float),
+                ("nt", C.c_int32), ("nbc", C.c_int32), ("fd_order", C.c_int32),
+                ("v_ref", C.c_float)]
+
+
+class Acq(C.Structure):
+    _fields_ = [("n_shots", C.c_int32), ("n_src", C.c_int32), ("sx", C.c_void_p),
+                ("sz", C.c_void_p), ("wavelet", C.c_void_p), ("n_rec", C.c_int32),
+                ("rx", C.c_void_p), ("rz", C.c_void_p)]
+
+
+class Opts(C.Structure):
+    _fields_ = [("flags", C.c_uint32), ("precision", C.c_int32), ("kernel", C.c_int32),
+                ("check_every", C.c_int32), ("final_state", C.c_void_p)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("kernel_time_s", C.c_double), ("cell_updates", C.c_double),
+                ("alg_bytes", C.c_double), ("n_shots", C.c_int32), ("gpu_launches", C.c_int32),
+                ("kernel", C.c_int32), ("status", C.c_int32), ("sweep_ms", C.c_double),
+                ("sweep_launches", C.c_int32), ("reserved", C.c_int32)]
+
+
+class FomoError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"libfomo_b200 error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+_lock = threading.Lock()
+
+
+def lib() -> C.CDLL:
+    """Load the library (raises OSError when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not LIB_PATH.exists():
+                raise OSError(f"libfomo_b200.so not built at {LIB_PATH} (run `make -C fomo.jl_b200`)")
+            L = C.CDLL(str(LIB_PATH))
+            vp, i32, f32 = C.c_void_p, C.c_int32, C.c_float
+            L.fomo_version.restype = C.c_int
+            L.fomo_create.argtypes = [C.POINTER(C.c_void_p), C.c_int]
+            L.fomo_create.restype = C.c_int
+            L.fomo_destroy.argtypes = [vp]
+            L.fomo_destroy.restype = None
+            L.fomo_last_error.argtypes = [vp]
+            L.fomo_last_error.restype = C.c_char_p
+            L.fomo_set_stream.argtypes = [vp, vp]
+            L.fomo_trim.argtypes = [vp]
+            L.fomo_check_numerics.argtypes = [f32, f32, f32, i32, i32, C.POINTER(C.c_float)]
+            L.fomo_check_numerics.restype = C.c_int
+            g, a, o, s = C.POINTER(Grid2D), C.POINTER(Acq), C.POINTER(Opts), C.POINTER(Stats)
+            L.fomo_acoustic2d.argtypes = [vp, g, vp, vp, a, i32, vp, vp, vp, vp, o, s]
+            L.fomo_acoustic2d_batch.argtypes = [vp, g, vp, vp, a, vp, vp, vp, o, s]
+            L.fomo_elastic2d.argtypes = [vp, g, vp, vp, vp, a, i32, vp, vp, vp, o, s]
+            L.fomo_elastic2d_batch.argtypes = [vp, g, vp, vp, vp, a, vp, vp, o, s]
+            L.fomo_scalar2d.argtypes = [vp, g, vp, a, vp, o, s]
+            L.fomo_debug_medium2d.argtypes = [vp, i32, i32, i32, i32, f32, f32, vp, vp, vp, vp]
+            for name in ("fomo_acoustic2d", "fomo_acoustic2d_batch", "fomo_elastic2d",
+                         "fomo_elastic2d_batch", "fomo_scalar2d", "fomo_debug_medium2d",
+                         "fomo_set_stream", "fomo_trim"):
+                getattr(L, name).restype = C.c_int
+            _lib = L
+    return _lib
+
+
+class Context:
+    """One libfomo_b200 context (a stream and a reusable device workspace)."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        rc = lib().fomo_create(C.byref(h), int(device))
+        if rc != FOMO_OK:
+            raise FomoError(rc, f"fomo_create(device={device}) failed (no usable CUDA device?)")
+        self.handle = h
+        self.device = device
+
+    def check(self, rc: int) -> None:
+        if rc != FOMO_OK:
+            msg = lib().fomo_last_error(self.handle)
+            raise FomoError(rc, msg.decode() if msg else "")
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        self.check(lib().fomo_set_stream(self.handle, C.c_void_p(stream_ptr or 0)))
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib().fomo_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):  # pragma: no cover - interpreter shutdown order varies
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_ctx: dict[int, Context] = {}
+
+
+def context(device: int = 0) -> Context:
+    c = _ctx.get(device)
+    if c is None:
+        c = _ctx[device] = Context(device)
+    return c

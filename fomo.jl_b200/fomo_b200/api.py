@@ -1,0 +1,418 @@
+"""Fomo.jl's public solvers over libfomo_b200 (same names, keywords, errors, results).
+
+Each function validates its inputs exactly where the Julia reference does
+(utils/checks.jl), builds the wavelet matrix as the reference's L5 code does,
+then calls one C-ABI entry point; all stepping happens in the CUDA library.
+Arrays follow the reference: models are ``(nx, nz)`` with x first, indices
+1-based, seismograms ``(n_rec, nt[, n_shots])``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import warnings
+from typing import NamedTuple, Optional, Sequence
+
+import numpy as np
+
+from . import _lib as L
+
+__all__ = [
+    "ArgumentError", "acoustic2d", "acoustic2d_batch", "elastic2d", "elastic2d_batch",
+    "scalar2d", "ricker_wavelet", "get_fd_coefficients", "get_centered_d2",
+]
+
+
+class ArgumentError(ValueError):
+    """Invalid input, raised before any launch (Julia's ArgumentError)."""
+
+
+# utils/FD_utils.jl:5-11 (Float32 values of the reference's literals)
+_FD = {
+    2: [1.0],
+    4: [1.125, -0.041666667],
+    6: [1.171875, -0.065104167, 0.0046875],
+    8: [1.1962890625, -0.079752604167, 0.0095703125, -0.000697544643],
+    10: [1.2115478515625, -0.089721679687, 0.0138427734375, -0.00176565987723, 0.0001186795166],
+}
+# utils/FD_centered.jl:27-41
+_D2C0 = {2: -2.0, 4: -5 / 2, 6: -49 / 18, 8: -205 / 72, 10: -5269 / 1800}
+_D2 = {
+    2: [1.0], 4: [4 / 3, -1 / 12], 6: [3 / 2, -3 / 20, 1 / 90],
+    8: [8 / 5, -1 / 5, 8 / 315, -1 / 560], 10: [5 / 3, -5 / 21, 5 / 126, -5 / 1008, 1 / 3150],
+}
+
+
+def get_fd_coefficients(order: int) -> np.ndarray:
+    if order not in _FD:
+        raise ValueError(f"Unsupported FD order: {order}")
+    return np.asarray(_FD[order], dtype=np.float64).astype(np.float32)
+
+
+def get_centered_d2(order: int):
+    if order not in _D2:
+        raise ValueError(f"Unsupported FD order: {order} (centered d2)")
+    return np.float32(_D2C0[order]), np.asarray(_D2[order], dtype=np.float64).astype(np.float32)
+
+
+def ricker_wavelet(f0, dt, nt) -> np.ndarray:
+    """Ricker wavelet (utils/ricker_wavelet.jl:6-12), evaluated in float64, returned as float32."""
+    f0 = float(np.float32(f0))
+    t = np.arange(int(nt), dtype=np.float64) * float(np.float32(dt))
+    tau = t - 1.5 / f0
+    a = (np.pi * f0 * tau) ** 2
+    return ((1.0 - 2.0 * a) * np.exp(-a)).astype(np.float32)
+
+
+class Stats(NamedTuple):
+    kernel_time_s: float
+
+
+class BatchStats(NamedTuple):
+    kernel_time_s: float
+    n_shots: int
+
+
+class Acoustic2DResult(NamedTuple):
+    seis_p: np.ndarray
+    seis_vx: np.ndarray
+    seis_vz: np.ndarray
+    snaps: list
+    stats: Stats
+
+
+class Elastic2DResult(NamedTuple):
+    seis_vx: np.ndarray
+    seis_vz: np.ndarray
+    snaps: list
+    stats: Stats
+
+
+class Acoustic2DBatchResult(NamedTuple):
+    seis_p: np.ndarray
+    seis_vx: np.ndarray
+    seis_vz: np.ndarray
+    stats: BatchStats
+
+
+class Elastic2DBatchResult(NamedTuple):
+    seis_vx: np.ndarray
+    seis_vz: np.ndarray
+    stats: BatchStats
+
+
+class Scalar2DResult(NamedTuple):
+    seis_u: np.ndarray
+    stats: Stats
+
+
+# ---------------------------------------------------------------------------
+# checks (utils/checks.jl)
+# ---------------------------------------------------------------------------
+def _check_geometry(nx, nz, sx, sz, rx, rz):
+    sx, sz, rx, rz = (np.asarray(a).ravel() for a in (sx, sz, rx, rz))
+    if not (np.all((1 <= sx) & (sx <= nx)) and np.all((1 <= sz) & (sz <= nz))):
+        raise ArgumentError(f"source index out of range: need 1 <= sx <= {nx}, 1 <= sz <= {nz}")
+    if not (np.all((1 <= rx) & (rx <= nx)) and np.all((1 <= rz) & (rz <= nz))):
+        raise ArgumentError(f"receiver index out of range: need 1 <= rx <= {nx}, 1 <= rz <= {nz}")
+
+
+def _warn_dispersion(vmin_disp, f0, dh, ppw_min=4.0):
+    fmax = np.float32(2.5) * np.float32(f0)
+    ppw = float(vmin_disp) / float(fmax) / float(dh)
+    if ppw < ppw_min:
+        warnings.warn(f"dispersion risk: shortest wavelength has only {ppw:.1f} grid points "
+                      f"(vmin={vmin_disp}, fmax~{float(fmax):.1f} Hz); reduce dh or f0",
+                      stacklevel=3)
+
+
+def _check_numerics(vmax, vmin_disp, dh, dt, f0, fd_order, centered=False):
+    if fd_order not in _FD:
+        raise ValueError(f"Unsupported FD order: {fd_order}")
+    dmax = C.c_float()
+    rc = L.lib().fomo_check_numerics(float(vmax), float(dh), float(dt), int(fd_order),
+                                     1 if centered else 0, C.byref(dmax))
+    if rc != L.FOMO_OK:
+        kind = "CFL unstable (centered)" if centered else "CFL unstable"
+        raise ArgumentError(f"{kind}: dt={dt} > dt_max={dmax.value:.4g} "
+                            f"(vmax={vmax}, dh={dh}, fd_order={fd_order})")
+    _warn_dispersion(vmin_disp, f0, dh)
+
+
+def _min_pos(a) -> np.float32:
+    a = np.asarray(a, dtype=np.float32)
+    pos = a[a > 0]
+    if pos.size == 0:
+        raise ArgumentError("model has no positive velocity")
+    return np.float32(pos.min())
+
+
+def _f32F(a) -> np.ndarray:
+    return np.asfortranarray(np.asarray(a, dtype=np.float32))
+
+
+def _i32F(a) -> np.ndarray:
+    return np.asfortranarray(np.asarray(a, dtype=np.int32))
+
+
+def _ptr(a) -> Optional[int]:
+    return None if a is None else a.ctypes.data
+
+
+def _wavelet_row(wavelet, f0, dt, nt) -> np.ndarray:
+    w = ricker_wavelet(f0, dt, nt) if wavelet is None else np.asarray(wavelet, dtype=np.float32).ravel()
+    if w.size != nt:
+        raise ArgumentError(f"wavelet length {w.size} != nt={nt}")
+    return w
+
+
+def _opts(kernel: int = 0, final_state: Optional[np.ndarray] = None, precision: int = 0):
+    o = L.Opts()
+    o.flags = 0
+    o.precision = precision
+    o.kernel = kernel
+    o.check_every = 0
+    o.final_state = _ptr(final_state)
+    return o
+
+
+def _grid(nx, nz, dh, dt, nt, nbc, fd_order, v_ref) -> L.Grid2D:
+    return L.Grid2D(int(nx), int(nz), float(dh), float(dt), int(nt), int(nbc), int(fd_order),
+                    float(v_ref))
+
+
+def _acq(sxm: np.ndarray, szm: np.ndarray, wm: np.ndarray, rx: np.ndarray, rz: np.ndarray):
+    n_src, ns = sxm.shape
+    return L.Acq(ns, n_src, _ptr(sxm), _ptr(szm), _ptr(wm), rx.size, _ptr(rx), _ptr(rz))
+
+
+def _check_boundary(boundary):
+    b = str(boundary).lstrip(":")
+    if b not in ("habc", "sponge"):
+        raise ArgumentError(f"boundary must be :habc or :sponge, got {boundary}")
+    if b == "sponge":
+        raise NotImplementedError("boundary=:sponge is not provided by libfomo_b200 (HABC only)")
+
+
+def _snap_list(snaps: Optional[np.ndarray]) -> list:
+    if snaps is None:
+        return []
+    return [np.asfortranarray(snaps[:, :, k]) for k in range(snaps.shape[2])]
+
+
+# ---------------------------------------------------------------------------
+# acoustic2d / elastic2d (single shot, n_src sources firing together)
+# ---------------------------------------------------------------------------
+def acoustic2d(vp, rho, dh, dt, nt, f0, *, sx: Sequence[int], sz: Sequence[int], rx, rz,
+               nbc: int = 50, fd_order: int = 8, snap_interval: int = 0, boundary="habc",
+               v_ref=None, sponge_factor=0.015, wavelet=None, scale_source_by_dt: bool = False,
+               use_cuda_graph: bool = True, verbose: bool = True, device: int = 0,
+               kernel: int = 0, final_state: Optional[np.ndarray] = None) -> Acoustic2DResult:
+    """2D acoustic velocity-pressure simulation (equations/acoustic2d/acoustic2d.jl:47-192)."""
+    _check_boundary(boundary)
+    vp, rho = _f32F(vp), _f32F(rho)
+    nx, nz = vp.shape
+    dh, dt, f0 = np.float32(dh), np.float32(dt), np.float32(f0)
+    _check_geometry(nx, nz, sx, sz, rx, rz)
+    _check_numerics(vp.max(), _min_pos(vp), dh, dt, f0, fd_order)
+    v_ref = _min_pos(vp) if v_ref is None else np.float32(v_ref)
+    w = _wavelet_row(wavelet, f0, dt, nt)
+    sxv, szv = _i32F(sx).ravel(), _i32F(sz).ravel()
+    if sxv.size != szv.size:
+        raise ArgumentError("sx and sz lengths differ")
+    wm = np.asfortranarray(np.repeat(w[None, :], sxv.size, axis=0))
+    if scale_source_by_dt:
+        wm = np.asfortranarray((wm * dt).astype(np.float32))
+    rxv, rzv = _i32F(rx).ravel(), _i32F(rz).ravel()
+    nrec = rxv.size
+    seis = [np.zeros((nrec, nt), dtype=np.float32, order="F") for _ in range(3)]
+    nsnap = nt // snap_interval if snap_interval > 0 else 0
+    snaps = np.zeros((nx, nz, nsnap), dtype=np.float32, order="F") if nsnap else None
+    st = L.Stats()
+    ctx = L.context(device)
+    g = _grid(nx, nz, dh, dt, nt, nbc, fd_order, v_ref)
+    acq = _acq(sxv.reshape(-1, 1, order="F"), szv.reshape(-1, 1, order="F"), wm, rxv, rzv)
+    o = _opts(kernel, final_state)
+    ctx.check(L.lib().fomo_acoustic2d(ctx.handle, C.byref(g), _ptr(vp), _ptr(rho), C.byref(acq),
+                                      int(snap_interval), _ptr(seis[0]), _ptr(seis[1]),
+                                      _ptr(seis[2]), _ptr(snaps), C.byref(o), C.byref(st)))
+    return Acoustic2DResult(seis[0], seis[1], seis[2], _snap_list(snaps), Stats(st.kernel_time_s))
+
+
+def elastic2d(vp, vs, rho, dh, dt, nt, f0, *, sx: Sequence[int], sz: Sequence[int], rx, rz,
+              nbc: int = 50, fd_order: int = 8, snap_interval: int = 0, boundary="habc",
+              v_ref=None, sponge_factor=0.015, wavelet=None, scale_source_by_dt: bool = False,
+              use_cuda_graph: bool = True, verbose: bool = True, device: int = 0,
+              kernel: int = 0, final_state: Optional[np.ndarray] = None) -> Elastic2DResult:
+    """2D elastic velocity-stress simulation (equations/elastic2d/elastic2d.jl:45-163)."""
+    _check_boundary(boundary)
+    vp, vs, rho = _f32F(vp), _f32F(vs), _f32F(rho)
+    nx, nz = vp.shape
+    dh, dt, f0 = np.float32(dh), np.float32(dt), np.float32(f0)
+    _check_geometry(nx, nz, sx, sz, rx, rz)
+    vmin_disp = _min_pos(vs) if np.any(vs > 0) else _min_pos(vp)  # elastic2d.jl:69-71
+    _check_numerics(vp.max(), vmin_disp, dh, dt, f0, fd_order)
+    v_ref = _min_pos(vp) if v_ref is None else np.float32(v_ref)
+    w = _wavelet_row(wavelet, f0, dt, nt)
+    sxv, szv = _i32F(sx).ravel(), _i32F(sz).ravel()
+    if sxv.size != szv.size:
+        raise ArgumentError("sx and sz lengths differ")
+    wm = np.asfortranarray(np.repeat(w[None, :], sxv.size, axis=0))
+    if scale_source_by_dt:
+        wm = np.asfortranarray((wm * dt).astype(np.float32))
+    rxv, rzv = _i32F(rx).ravel(), _i32F(rz).ravel()
+    nrec = rxv.size
+    seis = [np.zeros((nrec, nt), dtype=np.float32, order="F") for _ in range(2)]
+    nsnap = nt // snap_interval if snap_interval > 0 else 0
+    snaps = np.zeros((nx, nz, nsnap), dtype=np.float32, order="F") if nsnap else None
+    st = L.Stats()
+    ctx = L.context(device)
+    g = _grid(nx, nz, dh, dt, nt, nbc, fd_order, v_ref)
+    acq = _acq(sxv.reshape(-1, 1, order="F"), szv.reshape(-1, 1, order="F"), wm, rxv, rzv)
+    o = _opts(kernel, final_state)
+    ctx.check(L.lib().fomo_elastic2d(ctx.handle, C.byref(g), _ptr(vp), _ptr(vs), _ptr(rho),
+                                     C.byref(acq), int(snap_interval), _ptr(seis[0]),
+                                     _ptr(seis[1]), _ptr(snaps), C.byref(o), C.byref(st)))
+    return Elastic2DResult(seis[0], seis[1], _snap_list(snaps), Stats(st.kernel_time_s))
+
+
+# ---------------------------------------------------------------------------
+# batch variants: sx/sz are (n_shots x n_src) (a vector = one source per shot)
+# ---------------------------------------------------------------------------
+def _shot_matrix(sx, sz):
+    sxm = np.asarray(sx, dtype=np.int64)
+    szm = np.asarray(sz, dtype=np.int64)
+    if sxm.ndim == 1:
+        sxm = sxm.reshape(-1, 1)
+    if szm.ndim == 1:
+        szm = szm.reshape(-1, 1)
+    if sxm.shape != szm.shape:
+        raise ArgumentError(f"sx and sz shapes differ: {sxm.shape} vs {szm.shape}")
+    if sxm.shape[0] < 1:
+        raise ArgumentError("at least 1 shot is required")
+    return sxm, szm
+
+
+def _batch_common(vp, dh, dt, nt, f0, sx, sz, rx, rz, fd_order, v_ref, wavelet,
+                  scale_source_by_dt):
+    nx, nz = vp.shape
+    sxm, szm = _shot_matrix(sx, sz)
+    ns, n_src = sxm.shape
+    for s in range(ns):  # batch.jl:201-206
+        _check_geometry(nx, nz, sxm[s], szm[s], rx, rz)
+    _check_numerics(vp.max(), _min_pos(vp), dh, dt, f0, fd_order)
+    v_ref = _min_pos(vp) if v_ref is None else np.float32(v_ref)
+    w = _wavelet_row(wavelet, f0, dt, nt)
+    wm = np.asfortranarray(np.repeat(w[None, :], n_src, axis=0))
+    if scale_source_by_dt:
+        wm = np.asfortranarray((wm * dt).astype(np.float32))
+    # device layout (n_src, n_shots) (batch.jl:219-220)
+    sxd, szd = _i32F(sxm.T), _i32F(szm.T)
+    rxv, rzv = _i32F(rx).ravel(), _i32F(rz).ravel()
+    return v_ref, wm, sxd, szd, rxv, rzv, ns
+
+
+def acoustic2d_batch(vp, rho, dh, dt, nt, f0, *, sx, sz, rx, rz, nbc: int = 50,
+                     fd_order: int = 8, v_ref=None, wavelet=None,
+                     scale_source_by_dt: bool = False, verbose: bool = True, device: int = 0,
+                     kernel: int = 0, final_state=None) -> Acoustic2DBatchResult:
+    """Multi-shot acoustic run on one shared model (equations/acoustic2d/batch.jl:180-261)."""
+    vp, rho = _f32F(vp), _f32F(rho)
+    nx, nz = vp.shape
+    dh, dt, f0 = np.float32(dh), np.float32(dt), np.float32(f0)
+    v_ref, wm, sxd, szd, rxv, rzv, ns = _batch_common(vp, dh, dt, nt, f0, sx, sz, rx, rz,
+                                                      fd_order, v_ref, wavelet, scale_source_by_dt)
+    nrec = rxv.size
+    seis = [np.zeros((nrec, nt, ns), dtype=np.float32, order="F") for _ in range(3)]
+    st = L.Stats()
+    ctx = L.context(device)
+    g = _grid(nx, nz, dh, dt, nt, nbc, fd_order, v_ref)
+    acq = _acq(sxd, szd, wm, rxv, rzv)
+    o = _opts(kernel, final_state)
+    ctx.check(L.lib().fomo_acoustic2d_batch(ctx.handle, C.byref(g), _ptr(vp), _ptr(rho),
+                                            C.byref(acq), _ptr(seis[0]), _ptr(seis[1]),
+                                            _ptr(seis[2]), C.byref(o), C.byref(st)))
+    return Acoustic2DBatchResult(seis[0], seis[1], seis[2], BatchStats(st.kernel_time_s, ns))
+
+
+def elastic2d_batch(vp, vs, rho, dh, dt, nt, f0, *, sx, sz, rx, rz, nbc: int = 50,
+                    fd_order: int = 8, v_ref=None, wavelet=None,
+                    scale_source_by_dt: bool = False, verbose: bool = True, device: int = 0,
+                    kernel: int = 0, final_state=None) -> Elastic2DBatchResult:
+    """Multi-shot elastic run on one shared model (equations/elastic2d/batch.jl:197-261)."""
+    vp, vs, rho = _f32F(vp), _f32F(vs), _f32F(rho)
+    nx, nz = vp.shape
+    dh, dt, f0 = np.float32(dh), np.float32(dt), np.float32(f0)
+    v_ref, wm, sxd, szd, rxv, rzv, ns = _batch_common(vp, dh, dt, nt, f0, sx, sz, rx, rz,
+                                                      fd_order, v_ref, wavelet, scale_source_by_dt)
+    nrec = rxv.size
+    seis = [np.zeros((nrec, nt, ns), dtype=np.float32, order="F") for _ in range(2)]
+    st = L.Stats()
+    ctx = L.context(device)
+    g = _grid(nx, nz, dh, dt, nt, nbc, fd_order, v_ref)
+    acq = _acq(sxd, szd, wm, rxv, rzv)
+    o = _opts(kernel, final_state)
+    ctx.check(L.lib().fomo_elastic2d_batch(ctx.handle, C.byref(g), _ptr(vp), _ptr(vs), _ptr(rho),
+                                           C.byref(acq), _ptr(seis[0]), _ptr(seis[1]),
+                                           C.byref(o), C.byref(st)))
+    return Elastic2DBatchResult(seis[0], seis[1], BatchStats(st.kernel_time_s, ns))
+
+
+# ---------------------------------------------------------------------------
+# scalar2d (equations/scalar2d/scalar2d.jl:104-189)
+# ---------------------------------------------------------------------------
+def scalar_wavelet_matrix(w, vp, dt, sx, sz, source_scale):
+    """Rows of the wavelet scaled per source as scalar2d.jl:141-147 does."""
+    n_src = len(sx)
+    wm = np.repeat(np.asarray(w, dtype=np.float32)[None, :], n_src, axis=0)
+    dt = np.float32(dt)
+    if source_scale == "v2dt2":
+        for q in range(n_src):
+            v = np.float32(vp[sx[q] - 1, sz[q] - 1])
+            wm[q, :] = (wm[q, :] * np.float32((v * v) * (dt * dt))).astype(np.float32)
+    elif source_scale == "dt":
+        wm = (wm * dt).astype(np.float32)
+    return np.asfortranarray(wm)
+
+
+def scalar2d(vp, dh, dt, nt, f0, *, sx, sz, rx, rz, nbc: int = 50, fd_order: int = 8,
+             v_ref=None, wavelet=None, source_scale="v2dt2", verbose: bool = True,
+             device: int = 0, kernel: int = 0, final_state=None) -> Scalar2DResult:
+    """Second-order constant-density scalar wave (equations/scalar2d/scalar2d.jl:104-189)."""
+    source_scale = str(source_scale).lstrip(":")
+    if source_scale not in ("v2dt2", "dt", "none"):
+        raise ArgumentError(f"source_scale must be :v2dt2 / :dt / :none, got {source_scale}")
+    vp = _f32F(vp)
+    nx, nz = vp.shape
+    dh, dt, f0 = np.float32(dh), np.float32(dt), np.float32(f0)
+    _check_geometry(nx, nz, sx, sz, rx, rz)
+    _check_numerics(vp.max(), _min_pos(vp), dh, dt, f0, fd_order, centered=True)
+    v_ref = _min_pos(vp) if v_ref is None else np.float32(v_ref)
+    w = _wavelet_row(wavelet, f0, dt, nt)
+    sxv, szv = _i32F(sx).ravel(), _i32F(sz).ravel()
+    wm = scalar_wavelet_matrix(w, vp, dt, sxv, szv, source_scale)
+    rxv, rzv = _i32F(rx).ravel(), _i32F(rz).ravel()
+    seis = np.zeros((rxv.size, nt), dtype=np.float32, order="F")
+    st = L.Stats()
+    ctx = L.context(device)
+    g = _grid(nx, nz, dh, dt, nt, nbc, fd_order, v_ref)
+    acq = _acq(sxv.reshape(-1, 1, order="F"), szv.reshape(-1, 1, order="F"), wm, rxv, rzv)
+    o = _opts(kernel, final_state)
+    ctx.check(L.lib().fomo_scalar2d(ctx.handle, C.byref(g), _ptr(vp), C.byref(acq), _ptr(seis),
+                                    C.byref(o), C.byref(st)))
+    return Scalar2DResult(seis, Stats(st.kernel_time_s))
+
+
+def debug_medium2d(kind: str, vp, vs, rho, pad: int, dt=1.0, dh=1.0, device: int = 0):
+    """Device-prepared padded materials (diagnostics): elastic/acoustic/scalar."""
+    k = {"elastic": 0, "acoustic": 1, "scalar": 2}[kind]
+    vp = _f32F(vp)
+    vs = _f32F(vs) if vs is not None else None
+    rho = _f32F(rho) if rho is not None else None
+    nx, nz = vp.shape
+    nf = {0: 5, 1: 3, 2: 1}[k]
+    out = np.zeros((nx + 2 * pad, nz + 2 * pad, nf), dtype=np.float32, order="F")
+    ctx = L.context(device)
+    ctx.check(L.lib().fomo_debug_medium2d(ctx.handle, k, nx, nz, pad, float(np.float32(dt)),
+                                          float(np.float32(dh)), _ptr(vp), _ptr(vs), _ptr(rho),
+                                          _ptr(out)))
+    return out

@@ -1,0 +1,175 @@
+/*
+ * fomo_b200.h -- C ABI of libfomo_b200.so, the B200 (sm_100a) time-stepping
+ * engine behind Fomo.jl's public solvers.
+ *
+ * Each entry point replaces one Fomo.jl public function (and the device loop it
+ * drives); the Julia host code keeps the reference's signatures and result
+ * NamedTuples and `ccall`s these symbols instead of launching CUDA.jl kernels.
+ *
+ * Conventions (identical to the reference):
+ *  - grids are column-major with x fastest: vp[(i-1) + nx*(j-1)] is vp[i, j];
+ *  - source / receiver indices are 1-based and UNPADDED, exactly as the user
+ *    passes them to Fomo (the library adds the pad offset,
+ *    acquisition/source.jl:18-28, receiver.jl:15-19);
+ *  - padded sizes are nx + 2*pad with pad = nbc + fd_order/2
+ *    (elastic2d/medium.jl:21-26); the HABC zone is pad-1 (habc.jl:38);
+ *  - seismograms are (n_rec, nt[, n_shots]) column-major, snapshots are
+ *    (nx, nz, nt/snap_interval) interior slices;
+ *  - all arithmetic is FP32 unless fomo_opts.precision selects a 16-bit
+ *    storage format (FP32 accumulation always).
+ *
+ * Errors: every call returns FOMO_OK (0) or a negative FOMO_E* code and never
+ * aborts; fomo_last_error() gives the message.  FOMO_EARG corresponds to the
+ * reference's ArgumentError (utils/checks.jl:8-71).
+ *
+ * Threading: a fomo_ctx is used by one host thread at a time; it owns a CUDA
+ * stream (or borrows the caller's via fomo_set_stream) and a device
+ * workspace that grows on demand and is reused across calls.
+ */
+#ifndef FOMO_B200_H
+#define FOMO_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FOMO_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define FOMO_API __attribute__((visibility("default")))
+#else
+#define FOMO_API
+#endif
+
+#define FOMO_OK 0
+#define FOMO_EARG (-1)        /* invalid argument (reference: ArgumentError)      */
+#define FOMO_ECUDA (-2)       /* CUDA runtime error                                */
+#define FOMO_ENOMEM (-3)      /* device allocation failed                          */
+#define FOMO_ENONFINITE (-4)  /* NaN/Inf sentinel tripped (fomo_opts.check_every) */
+#define FOMO_EUNSUPPORTED (-5)
+
+/* fomo_opts.flags */
+#define FOMO_F_DEVICE_PTRS 1u /* every array argument is a device pointer */
+#define FOMO_F_PROFILE 2u     /* time the sweep kernels of a window of steps  */
+
+/* fomo_opts.precision: storage format of wavefields and material arrays */
+#define FOMO_FP32 0
+#define FOMO_FP16 1
+#define FOMO_BF16 2
+
+/* fomo_opts.kernel: time-step kernel family (0 lets the autotuner pick) */
+#define FOMO_KERNEL_AUTO 0
+#define FOMO_KERNEL_TWO_PHASE 1    /* velocity sweep + stress sweep per step      */
+#define FOMO_KERNEL_SINGLE_SWEEP 2 /* one fused sweep per step (z-marching tiles) */
+
+typedef struct fomo_ctx fomo_ctx;
+
+/* Grid and run parameters shared by the 2D solvers. */
+typedef struct fomo_grid2d {
+  int32_t nx, nz;    /* interior (unpadded) grid                                */
+  float dh, dt;      /* spacing (m), time step (s)                              */
+  int32_t nt;        /* time steps                                              */
+  int32_t nbc;       /* absorbing layers (reference keyword nbc, default 50)    */
+  int32_t fd_order;  /* 2, 4, 6, 8 or 10                                        */
+  float v_ref;       /* HABC reference velocity; <= 0 selects min(vp > 0)       */
+} fomo_grid2d;
+
+/* Acquisition: sources per shot and a receiver spread shared by all shots. */
+typedef struct fomo_acq {
+  int32_t n_shots;      /* 1 for the single-shot solvers                        */
+  int32_t n_src;        /* sources per shot                                     */
+  const int32_t* sx;    /* (n_src, n_shots), 1-based interior indices           */
+  const int32_t* sz;
+  const float* wavelet; /* (n_src, nt): injected raw (`f += w[q, it]`)          */
+  int32_t n_rec;
+  const int32_t* rx;    /* (n_rec), 1-based interior indices                    */
+  const int32_t* rz;
+} fomo_acq;
+
+typedef struct fomo_opts {
+  uint32_t flags;       /* FOMO_F_* */
+  int32_t precision;    /* FOMO_FP32 / FOMO_FP16 / FOMO_BF16                    */
+  int32_t kernel;       /* FOMO_KERNEL_*                                        */
+  int32_t check_every;  /* NaN/Inf sentinel every K steps, 0 = off              */
+  float* final_state;   /* optional HOST buffer: padded end-of-run wavefields   */
+} fomo_opts;
+
+typedef struct fomo_stats {
+  double kernel_time_s; /* CUDA-event time of the time loop (stats.kernel_time_s) */
+  double cell_updates;  /* padded cells x nt x shots                              */
+  double alg_bytes;     /* algorithmic HBM bytes of the loop                      */
+  int32_t n_shots;
+  int32_t gpu_launches; /* kernels launched inside the timed loop                 */
+  int32_t kernel;       /* kernel family that ran                                 */
+  int32_t status;
+  double sweep_ms;      /* FOMO_F_PROFILE: mean device time of one step's sweep    */
+                        /* kernel(s) over a window of steps, else 0               */
+  int32_t sweep_launches; /* sweep kernels per step                               */
+  int32_t reserved;
+} fomo_stats;
+
+/* ---- context ---------------------------------------------------------- */
+FOMO_API int fomo_version(void);
+FOMO_API int fomo_create(fomo_ctx** out, int device);
+FOMO_API void fomo_destroy(fomo_ctx* ctx);
+FOMO_API const char* fomo_last_error(const fomo_ctx* ctx);
+/* Borrow a caller stream (cudaStream_t); NULL returns to the context's own. */
+FOMO_API int fomo_set_stream(fomo_ctx* ctx, void* stream);
+/* Release the cached device workspace. */
+FOMO_API int fomo_trim(fomo_ctx* ctx);
+
+/* ---- host-side checks shared by the language shims -------------------- */
+/* CFL bound (utils/checks.jl:39-48 staggered, :61-70 centered when
+ * `centered` != 0): writes dt_max and returns FOMO_EARG when dt > dt_max. */
+FOMO_API int fomo_check_numerics(float vmax, float dh, float dt, int32_t fd_order, int32_t centered,
+                        float* dt_max);
+
+/* ---- solvers -------------------------------------------------------------
+ * Outputs are caller-owned, sized (n_rec, nt, n_shots); `snaps` may be NULL.
+ * opts may be NULL (FP32, host pointers, autotuned kernel).
+ */
+
+/* acoustic2d (equations/acoustic2d/acoustic2d.jl:47-192; HABC graph/fused loop
+ * loop_graph.jl:12-76, fused_kernels.jl:166-197).  acq->n_shots must be 1;
+ * acq->n_src sources fire together.  Snapshots hold the interior of p. */
+FOMO_API int fomo_acoustic2d(fomo_ctx* ctx, const fomo_grid2d* g, const float* vp, const float* rho,
+                    const fomo_acq* acq, int32_t snap_interval, float* seis_p, float* seis_vx,
+                    float* seis_vz, float* snaps, const fomo_opts* opts, fomo_stats* stats);
+
+/* acoustic2d_batch (equations/acoustic2d/batch.jl:180-261): n_shots shots of
+ * n_src sources each on one shared model. */
+FOMO_API int fomo_acoustic2d_batch(fomo_ctx* ctx, const fomo_grid2d* g, const float* vp, const float* rho,
+                          const fomo_acq* acq, float* seis_p, float* seis_vx, float* seis_vz,
+                          const fomo_opts* opts, fomo_stats* stats);
+
+/* elastic2d (equations/elastic2d/elastic2d.jl:45-163; loops fused_kernels.jl:200-240,
+ * loop_graph.jl:12-75).  Sources inject into txx and tzz; snapshots hold vz. */
+FOMO_API int fomo_elastic2d(fomo_ctx* ctx, const fomo_grid2d* g, const float* vp, const float* vs,
+                   const float* rho, const fomo_acq* acq, int32_t snap_interval, float* seis_vx,
+                   float* seis_vz, float* snaps, const fomo_opts* opts, fomo_stats* stats);
+
+/* elastic2d_batch (equations/elastic2d/batch.jl:197-261). */
+FOMO_API int fomo_elastic2d_batch(fomo_ctx* ctx, const fomo_grid2d* g, const float* vp, const float* vs,
+                         const float* rho, const fomo_acq* acq, float* seis_vx, float* seis_vz,
+                         const fomo_opts* opts, fomo_stats* stats);
+
+/* scalar2d (equations/scalar2d/scalar2d.jl:104-189).  The wavelet matrix is
+ * already scaled as `source_scale` asks (the shim does :v2dt2 / :dt). */
+FOMO_API int fomo_scalar2d(fomo_ctx* ctx, const fomo_grid2d* g, const float* vp, const fomo_acq* acq,
+                  float* seis_u, const fomo_opts* opts, fomo_stats* stats);
+
+/* ---- diagnostics -------------------------------------------------------- */
+/* Device-side medium preparation, downloaded to `out` (padded, column-major):
+ * kind 0 elastic -> bx,bz,lam,lam2mu,mu_txz; 1 acoustic -> bx,bz,kappa;
+ * 2 scalar -> c2.  Mirrors utils/pad_array.jl and equations/<eq>/medium.jl. */
+FOMO_API int fomo_debug_medium2d(fomo_ctx* ctx, int32_t kind, int32_t nx, int32_t nz, int32_t pad,
+                        float dt, float dh, const float* vp, const float* vs, const float* rho,
+                        float* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FOMO_B200_H */

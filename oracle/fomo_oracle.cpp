@@ -1,0 +1,697 @@
+// fomo_oracle.cpp -- TEST INFRASTRUCTURE ONLY.
+//
+// CPU restatement of Fomo.jl's staggered-grid time stepping (the checker for
+// libfomo_b200, never shipped, never on the product path).  Only tests/,
+// __graft_entry__.smoke() and bench.py's CPU-baseline leg may load it.
+//
+// Templated on the arithmetic type: T=float is the FP32 oracle (same rounding
+// sequence as the CUDA kernels, so GPU==oracle is expected bit-exact), T=double
+// is the FP64 oracle of the same scheme used for error reporting.
+//
+// Parity pinning: the reference ships no golden vectors and Julia is absent
+// here, so absolute seismogram values are pinned by the reference's own test
+// properties (tests/test_oracle_pins.py): the HABC absorption calibration of
+// test/verify_patch.jl:9-11 (1.245e-2 for zone=pad-1, 1.336e-2 for zone=nbc),
+// exact mirror symmetry under causal shielding (verify_patch.jl:59-73),
+// multi-source linearity (:97-104), and the scalar same-scheme CPU transcription
+// (verify_scalar.jl:33-86) and det-HABC CPU reference (verify_det_graph.jl:59-94),
+// which this file restates.
+//
+// Canonical arithmetic (shared with fomo.jl_b200/csrc/stencil.cuh).  The
+// reference writes `acc += c*(a-b)` and `v += b*(dtx*X + dtz*Z)`; CUDA.jl's
+// NVPTX backend contracts these into FMAs.  This restatement fixes one
+// contraction explicitly:
+//   acc = fma(c, a-b, acc)
+//   vx  = fma(bx, fma(dtx, X, dtz*Z), vx)                (elastic velocity)
+//   v   = fma(b*dtx, D, v)                               (acoustic velocity)
+//   p   = fma(kappa, fma(X, dtx, Z*dtz), p)              (acoustic pressure)
+//   ex = X*dtx; ez = Z*dtz; txx = txx + fma(l2m, ex, lam*ez)
+//                           tzz = tzz + fma(lam, ex, l2m*ez)
+//   txz = fma(mu_txz, fma(Xz, dtz, Zx*dtx), txz)
+//   Higdon side term  s = fma(-qxt, fo[n], fma(-qt, fo[p], (-q)*f[n]))
+//   edge   f' = fma(w, f, (1-w)*s);  corner f' = fma(w, f, ((1-w)*0.5)*(sx+sz))
+// Host preparation (padding, buoyancy, Lame, HABC weights) is IEEE without
+// contraction, exactly as the Julia host code computes it (this file must be
+// compiled with -ffp-contract=off).
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+// utils/FD_utils.jl:5-11 (staggered coefficients, orders 2..10)
+const float kFD[6][5] = {
+    {0, 0, 0, 0, 0},
+    {(float)1.0, 0, 0, 0, 0},
+    {(float)1.125, (float)-0.041666667, 0, 0, 0},
+    {(float)1.171875, (float)-0.065104167, (float)0.0046875, 0, 0},
+    {(float)1.1962890625, (float)-0.079752604167, (float)0.0095703125, (float)-0.000697544643, 0},
+    {(float)1.2115478515625, (float)-0.089721679687, (float)0.0138427734375,
+     (float)-0.00176565987723, (float)0.0001186795166},
+};
+// utils/FD_centered.jl:27-41 (centered second derivative)
+const float kD2C0[6] = {0, (float)-2.0, (float)(-5.0 / 2.0), (float)(-49.0 / 18.0), (float)(-205.0 / 72.0),
+                        (float)(-5269.0 / 1800.0)};
+const float kD2[6][5] = {
+    {0, 0, 0, 0, 0},
+    {(float)1.0, 0, 0, 0, 0},
+    {(float)(4.0 / 3.0), (float)(-1.0 / 12.0), 0, 0, 0},
+    {(float)(3.0 / 2.0), (float)(-3.0 / 20.0), (float)(1.0 / 90.0), 0, 0},
+    {(float)(8.0 / 5.0), (float)(-1.0 / 5.0), (float)(8.0 / 315.0), (float)(-1.0 / 560.0), 0},
+    {(float)(5.0 / 3.0), (float)(-5.0 / 21.0), (float)(5.0 / 126.0), (float)(-5.0 / 1008.0),
+     (float)(1.0 / 3150.0)},
+};
+
+inline int order_to_N(int fd_order) {
+  if (fd_order < 2 || fd_order > 10 || (fd_order & 1)) return -1;
+  return fd_order / 2;
+}
+
+inline float fmaT(float a, float b, float c) { return std::fmaf(a, b, c); }
+inline double fmaT(double a, double b, double c) { return std::fma(a, b, c); }
+
+// 1-based (i,j) -> linear index of a column-major (x fastest) padded grid.
+struct G2 {
+  int nx, nz;
+  inline size_t at(int i, int j) const { return (size_t)(i - 1) + (size_t)nx * (size_t)(j - 1); }
+  size_t n() const { return (size_t)nx * (size_t)nz; }
+};
+
+// utils/pad_array.jl:8-22 -- edge replication (x strips first, then z strips
+// over full rows, which equals clamped indexing).
+template <class T>
+std::vector<T> pad_array(const float* d, int nx, int nz, int pad) {
+  G2 g{nx + 2 * pad, nz + 2 * pad};
+  std::vector<T> r(g.n());
+  for (int j = 1; j <= g.nz; ++j) {
+    int jj = std::min(std::max(j - pad, 1), nz);
+    for (int i = 1; i <= g.nx; ++i) {
+      int ii = std::min(std::max(i - pad, 1), nx);
+      r[g.at(i, j)] = (T)d[(size_t)(ii - 1) + (size_t)nx * (jj - 1)];
+    }
+  }
+  return r;
+}
+
+// utils/pad_array.jl:30-67 -- harmonic buoyancy with vacuum rules.
+template <class T>
+inline T harm2(T r1, T r2) {
+  if (r1 == T(0) && r2 == T(0)) return T(0);
+  if (r1 == T(0)) return T(2) / r2;
+  if (r2 == T(0)) return T(2) / r1;
+  return T(2) / (r1 + r2);
+}
+
+template <class T>
+void staggered_buoyancy(const G2& g, const std::vector<T>& rho, std::vector<T>& bx,
+                        std::vector<T>& bz) {
+  bx.assign(g.n(), T(0));
+  bz.assign(g.n(), T(0));
+  for (int j = 1; j <= g.nz; ++j)
+    for (int i = 2; i <= g.nx; ++i) bx[g.at(i, j)] = harm2(rho[g.at(i - 1, j)], rho[g.at(i, j)]);
+  for (int j = 1; j <= g.nz; ++j) bx[g.at(1, j)] = bx[g.at(2, j)];
+  for (int j = 1; j <= g.nz - 1; ++j)
+    for (int i = 1; i <= g.nx; ++i) bz[g.at(i, j)] = harm2(rho[g.at(i, j)], rho[g.at(i, j + 1)]);
+  for (int i = 1; i <= g.nx; ++i) bz[g.at(i, g.nz)] = bz[g.at(i, g.nz - 1)];
+}
+
+// elastic2d/medium.jl:52-74 -- Lame parameters and 4-point harmonic mu at txz.
+template <class T>
+inline T harm4(T m1, T m2, T m3, T m4) {
+  if (m1 == T(0) || m2 == T(0) || m3 == T(0) || m4 == T(0)) return T(0);
+  return T(4) / (T(1) / m1 + T(1) / m2 + T(1) / m3 + T(1) / m4);
+}
+
+template <class T>
+void elastic_params(const G2& g, const std::vector<T>& vp, const std::vector<T>& vs,
+                    const std::vector<T>& rho, std::vector<T>& lam, std::vector<T>& lam2mu,
+                    std::vector<T>& mu_txz) {
+  size_t n = g.n();
+  std::vector<T> mu(n);
+  lam.resize(n);
+  lam2mu.resize(n);
+  for (size_t k = 0; k < n; ++k) {
+    mu[k] = rho[k] * (vs[k] * vs[k]);
+    lam[k] = rho[k] * (vp[k] * vp[k]) - T(2) * mu[k];
+    lam2mu[k] = lam[k] + T(2) * mu[k];
+  }
+  mu_txz.assign(n, T(0));
+  for (int j = 1; j <= g.nz - 1; ++j)
+    for (int i = 2; i <= g.nx; ++i)
+      mu_txz[g.at(i, j)] = harm4(mu[g.at(i - 1, j)], mu[g.at(i, j)], mu[g.at(i - 1, j + 1)],
+                                 mu[g.at(i, j + 1)]);
+  for (int j = 1; j <= g.nz; ++j) mu_txz[g.at(1, j)] = mu_txz[g.at(2, j)];
+  for (int i = 1; i <= g.nx; ++i) mu_txz[g.at(i, g.nz)] = mu_txz[g.at(i, g.nz - 1)];
+}
+
+// boundary/habc/habc.jl:17-44 -- Higdon coefficients (in T) and weight ramps.
+template <class T>
+struct Habc {
+  int nbc;  // = pad - 1, the zone width every loop uses
+  T q, qt, qxt;
+  // weight tables by distance-to-edge for offsets 0 (vx), 0.5 (vz), 0.75 (tau/p)
+  std::vector<T> wtab[3];
+};
+
+template <class T>
+Habc<T> init_habc(int pad, float v_ref, float dt, float dh) {
+  Habc<T> h;
+  h.nbc = pad - 1;
+  T r = (T)v_ref * (T)dt / (T)dh;
+  T b = (T)0.45f, beta = T(1);
+  h.q = (b * (beta + r) - r) / ((beta + r) * (T(1) - b));
+  h.qt = (b * (beta + r) - beta) / ((beta + r) * (T(1) - b));
+  h.qxt = b / (b - T(1));
+  const double offs[3] = {0.0, 0.5, 0.75};
+  for (int k = 0; k < 3; ++k) {
+    h.wtab[k].resize(pad + 2);
+    for (int d = 0; d < pad + 2; ++d) {
+      double w = ((double)d - offs[k]) / (double)(pad - 1);
+      w = std::min(std::max(w, 0.0), 1.0);
+      h.wtab[k][d] = (T)w;
+    }
+  }
+  return h;
+}
+
+template <class T>
+inline T habc_w(const Habc<T>& h, int kind, int dist) {
+  const std::vector<T>& t = h.wtab[kind];
+  return dist < (int)t.size() ? t[dist] : T(1);
+}
+
+// kernels_fused.jl:28-52 -- the frame: 2<=i<=nx-1, 2<=j<=nz-1 and within nbc+1
+// of an edge.  Stored as a list (sides encoded) for the two-pass update.
+struct FramePt {
+  size_t idx;
+  int i, j;
+  int8_t sx, sz;  // -1 left/top neighbour is i+1/j+1 ... encoded: +1 => use +1 neighbour, -1 => -1 neighbour, 0 => none
+  int dist;
+};
+
+std::vector<FramePt> frame_points(const G2& g, int nbc) {
+  std::vector<FramePt> f;
+  for (int j = 2; j <= g.nz - 1; ++j)
+    for (int i = 2; i <= g.nx - 1; ++i) {
+      bool L = i <= nbc + 1, R = i >= g.nx - nbc, T_ = j <= nbc + 1, B = j >= g.nz - nbc;
+      if (!(L || R || T_ || B)) continue;
+      FramePt p;
+      p.idx = g.at(i, j);
+      p.i = i;
+      p.j = j;
+      p.sx = L ? 1 : (R ? -1 : 0);
+      p.sz = T_ ? 1 : (B ? -1 : 0);
+      p.dist = std::min(std::min(i - 1, g.nx - i), std::min(j - 1, g.nz - j));
+      f.push_back(p);
+    }
+  return f;
+}
+
+// kernels_det.jl:22-57 -- Higdon value from read-only pre-correction fields.
+template <class T>
+inline T higdon_side(T q, T qt, T qxt, T f_nb, T fo_p, T fo_nb) {
+  T s = (-q) * f_nb;
+  s = fmaT(-qt, fo_p, s);
+  s = fmaT(-qxt, fo_nb, s);
+  return s;
+}
+
+template <class T>
+inline T habc_value(const G2& g, const Habc<T>& h, const FramePt& p, const T* f, const T* fo,
+                    T w) {
+  T fc = f[p.idx];
+  T one_m_w = T(1) - w;
+  if (p.sx != 0 && p.sz != 0) {
+    size_t nbx = p.sx > 0 ? p.idx + 1 : p.idx - 1;
+    size_t nbz = p.sz > 0 ? p.idx + g.nx : p.idx - g.nx;
+    T sx = higdon_side(h.q, h.qt, h.qxt, f[nbx], fo[p.idx], fo[nbx]);
+    T sz = higdon_side(h.q, h.qt, h.qxt, f[nbz], fo[p.idx], fo[nbz]);
+    return fmaT(w, fc, (one_m_w * T(0.5)) * (sx + sz));
+  } else if (p.sx != 0) {
+    size_t nb = p.sx > 0 ? p.idx + 1 : p.idx - 1;
+    T s = higdon_side(h.q, h.qt, h.qxt, f[nb], fo[p.idx], fo[nb]);
+    return fmaT(w, fc, one_m_w * s);
+  } else {
+    size_t nb = p.sz > 0 ? p.idx + g.nx : p.idx - g.nx;
+    T s = higdon_side(h.q, h.qt, h.qxt, f[nb], fo[p.idx], fo[nb]);
+    return fmaT(w, fc, one_m_w * s);
+  }
+}
+
+// kernels_det.jl:60-132 -- pass 1 into scratch, pass 2 write-back.
+template <class T>
+void habc_det(const G2& g, const Habc<T>& h, const std::vector<FramePt>& fr, int kind, T* f,
+              const T* fo, std::vector<T>& scr) {
+  scr.resize(fr.size());
+  const long n = (long)fr.size();
+#pragma omp parallel for schedule(static)
+  for (long k = 0; k < n; ++k) scr[k] = habc_value(g, h, fr[k], f, fo, habc_w(h, kind, fr[k].dist));
+#pragma omp parallel for schedule(static)
+  for (long k = 0; k < n; ++k) f[fr[k].idx] = scr[k];
+}
+
+template <class T>
+struct Coef {
+  int N;
+  T a[5];
+};
+
+template <class T>
+Coef<T> coef(int fd_order) {
+  Coef<T> c;
+  c.N = order_to_N(fd_order);
+  for (int l = 0; l < 5; ++l) c.a[l] = (T)kFD[c.N][l];
+  return c;
+}
+
+// ---------------------------------------------------------------------------
+// elastic2d: elastic2d/fused_kernels.jl:21-124 + loop order :200-240
+// (batch: elastic2d/batch.jl:278-423, bit-identical per shot by construction)
+// ---------------------------------------------------------------------------
+template <class T>
+struct ElasticState {
+  std::vector<T> vx, vz, txx, tzz, txz, o1, o2, o3;
+};
+
+template <class T>
+void elastic_vel(const G2& g, int M, const Coef<T>& c, T dtx, T dtz, const T* bx, const T* bz,
+                 ElasticState<T>& s) {
+  const size_t nx = g.nx;
+#pragma omp parallel for schedule(static)
+  for (int j = M + 1; j <= g.nz - M; ++j) {
+    for (int i = M + 1; i <= g.nx - M; ++i) {
+      size_t p = g.at(i, j);
+      T dxx = 0, dxzz = 0, dxzx = 0, dzz = 0;
+      for (int l = 1; l <= c.N; ++l) {
+        T a = c.a[l - 1];
+        dxx = fmaT(a, s.txx[p + (l - 1)] - s.txx[p - l], dxx);
+        dxzz = fmaT(a, s.txz[p + (size_t)(l - 1) * nx] - s.txz[p - (size_t)l * nx], dxzz);
+        dxzx = fmaT(a, s.txz[p + l] - s.txz[p - (l - 1)], dxzx);
+        dzz = fmaT(a, s.tzz[p + (size_t)l * nx] - s.tzz[p - (size_t)(l - 1) * nx], dzz);
+      }
+      s.vx[p] = fmaT(bx[p], fmaT(dtx, dxx, dtz * dxzz), s.vx[p]);
+      s.vz[p] = fmaT(bz[p], fmaT(dtx, dxzx, dtz * dzz), s.vz[p]);
+    }
+  }
+}
+
+template <class T>
+void elastic_str(const G2& g, int M, const Coef<T>& c, T dtx, T dtz, const T* lam,
+                 const T* lam2mu, const T* mutxz, ElasticState<T>& s) {
+  const size_t nx = g.nx;
+#pragma omp parallel for schedule(static)
+  for (int j = M + 1; j <= g.nz - M; ++j) {
+    for (int i = M + 1; i <= g.nx - M; ++i) {
+      size_t p = g.at(i, j);
+      T dvxdx = 0, dvzdz = 0, dvxdz = 0, dvzdx = 0;
+      for (int l = 1; l <= c.N; ++l) {
+        T a = c.a[l - 1];
+        dvxdx = fmaT(a, s.vx[p + l] - s.vx[p - (l - 1)], dvxdx);
+        dvzdz = fmaT(a, s.vz[p + (size_t)(l - 1) * nx] - s.vz[p - (size_t)l * nx], dvzdz);
+        dvxdz = fmaT(a, s.vx[p + (size_t)l * nx] - s.vx[p - (size_t)(l - 1) * nx], dvxdz);
+        dvzdx = fmaT(a, s.vz[p + (l - 1)] - s.vz[p - l], dvzdx);
+      }
+      T ex = dvxdx * dtx, ez = dvzdz * dtz;
+      s.txx[p] = s.txx[p] + fmaT(lam2mu[p], ex, lam[p] * ez);
+      s.tzz[p] = s.tzz[p] + fmaT(lam[p], ex, lam2mu[p] * ez);
+      s.txz[p] = fmaT(mutxz[p], fmaT(dvxdz, dtz, dvzdx * dtx), s.txz[p]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// acoustic2d: acoustic2d/fused_kernels.jl:27-114 + loop :166-197
+// ---------------------------------------------------------------------------
+template <class T>
+struct AcousticState {
+  std::vector<T> vx, vz, p, o1, o2, o3;
+};
+
+template <class T>
+void acoustic_vel(const G2& g, int M, const Coef<T>& c, T dtx, T dtz, const T* bx, const T* bz,
+                  AcousticState<T>& s) {
+  const size_t nx = g.nx;
+#pragma omp parallel for schedule(static)
+  for (int j = M + 1; j <= g.nz - M; ++j) {
+    for (int i = M + 1; i <= g.nx - M; ++i) {
+      size_t p = g.at(i, j);
+      T dpdx = 0, dpdz = 0;
+      for (int l = 1; l <= c.N; ++l) {
+        T a = c.a[l - 1];
+        dpdx = fmaT(a, s.p[p + (l - 1)] - s.p[p - l], dpdx);
+        dpdz = fmaT(a, s.p[p + (size_t)l * nx] - s.p[p - (size_t)(l - 1) * nx], dpdz);
+      }
+      s.vx[p] = fmaT(bx[p] * dtx, dpdx, s.vx[p]);
+      s.vz[p] = fmaT(bz[p] * dtz, dpdz, s.vz[p]);
+    }
+  }
+}
+
+template <class T>
+void acoustic_prs(const G2& g, int M, const Coef<T>& c, T dtx, T dtz, const T* kappa,
+                  AcousticState<T>& s) {
+  const size_t nx = g.nx;
+#pragma omp parallel for schedule(static)
+  for (int j = M + 1; j <= g.nz - M; ++j) {
+    for (int i = M + 1; i <= g.nx - M; ++i) {
+      size_t p = g.at(i, j);
+      T dvxdx = 0, dvzdz = 0;
+      for (int l = 1; l <= c.N; ++l) {
+        T a = c.a[l - 1];
+        dvxdx = fmaT(a, s.vx[p + l] - s.vx[p - (l - 1)], dvxdx);
+        dvzdz = fmaT(a, s.vz[p + (size_t)(l - 1) * nx] - s.vz[p - (size_t)l * nx], dvzdz);
+      }
+      s.p[p] = fmaT(kappa[p], fmaT(dvxdx, dtx, dvzdz * dtz), s.p[p]);
+    }
+  }
+}
+
+// Snapshot of the interior (unpadded) part of a padded field.
+template <class T, class O>
+void snap_interior(const G2& g, int pad, const T* f, O* out) {
+  int nxi = g.nx - 2 * pad, nzi = g.nz - 2 * pad;
+  for (int j = 1; j <= nzi; ++j)
+    for (int i = 1; i <= nxi; ++i) out[(size_t)(i - 1) + (size_t)nxi * (j - 1)] = (O)f[g.at(i + pad, j + pad)];
+}
+
+template <class T>
+int run_elastic2d(int nx, int nz, int ns, const float* vp, const float* vs, const float* rho,
+                  float dh, float dt, int nt, int nbc, int fd_order, float v_ref, int n_src,
+                  const int32_t* sx, const int32_t* sz, const float* wavelet, int n_rec,
+                  const int32_t* rx, const int32_t* rz, T* seis_vx, T* seis_vz, int snap_interval,
+                  T* snaps, T* final_fields) {
+  int N = order_to_N(fd_order);
+  if (N < 0) return -2;
+  int M = N, pad = nbc + M;
+  if (pad < 2) return -2;
+  G2 g{nx + 2 * pad, nz + 2 * pad};
+  std::vector<T> vpp = pad_array<T>(vp, nx, nz, pad), vsp = pad_array<T>(vs, nx, nz, pad),
+                 rhop = pad_array<T>(rho, nx, nz, pad);
+  std::vector<T> bx, bz, lam, lam2mu, mutxz;
+  staggered_buoyancy(g, rhop, bx, bz);
+  elastic_params(g, vpp, vsp, rhop, lam, lam2mu, mutxz);
+  Habc<T> h = init_habc<T>(pad, v_ref, dt, dh);
+  std::vector<FramePt> fr = frame_points(g, h.nbc);
+  Coef<T> c = coef<T>(fd_order);
+  T dtx = (T)dt / (T)dh, dtz = dtx;
+  int nsnap = snap_interval > 0 ? nt / snap_interval : 0;
+  size_t ncell = g.n();
+  size_t nint = (size_t)nx * nz;
+  std::vector<T> scr;
+  for (int s = 0; s < ns; ++s) {
+    ElasticState<T> st;
+    for (auto* v : {&st.vx, &st.vz, &st.txx, &st.tzz, &st.txz, &st.o1, &st.o2, &st.o3})
+      v->assign(ncell, T(0));
+    for (int it = 1; it <= nt; ++it) {
+      st.o1 = st.vx;
+      st.o2 = st.vz;
+      elastic_vel(g, M, c, dtx, dtz, bx.data(), bz.data(), st);
+      habc_det(g, h, fr, 0, st.vx.data(), st.o1.data(), scr);
+      habc_det(g, h, fr, 1, st.vz.data(), st.o2.data(), scr);
+      st.o1 = st.txx;
+      st.o2 = st.tzz;
+      st.o3 = st.txz;
+      elastic_str(g, M, c, dtx, dtz, lam.data(), lam2mu.data(), mutxz.data(), st);
+      habc_det(g, h, fr, 2, st.txx.data(), st.o1.data(), scr);
+      habc_det(g, h, fr, 2, st.tzz.data(), st.o2.data(), scr);
+      habc_det(g, h, fr, 2, st.txz.data(), st.o3.data(), scr);
+      for (int q = 0; q < n_src; ++q) {  // batch_acq.jl:58-71, sequential in source order
+        size_t p = g.at(sx[(size_t)s * n_src + q] + pad, sz[(size_t)s * n_src + q] + pad);
+        T w = (T)wavelet[(size_t)q + (size_t)n_src * (it - 1)];
+        st.txx[p] += w;
+        st.tzz[p] += w;
+      }
+      for (int r = 0; r < n_rec; ++r) {  // batch_acq.jl:108-121
+        size_t p = g.at(rx[r] + pad, rz[r] + pad);
+        size_t o = (size_t)r + (size_t)n_rec * ((it - 1) + (size_t)nt * s);
+        seis_vx[o] = st.vx[p];
+        seis_vz[o] = st.vz[p];
+      }
+      if (snaps && snap_interval > 0 && it % snap_interval == 0) {
+        int k = it / snap_interval - 1;
+        snap_interior(g, pad, st.vz.data(), snaps + nint * ((size_t)k + (size_t)nsnap * s));
+      }
+    }
+    if (final_fields) {
+      T* o = final_fields + (size_t)s * 5 * ncell;
+      std::copy(st.vx.begin(), st.vx.end(), o);
+      std::copy(st.vz.begin(), st.vz.end(), o + ncell);
+      std::copy(st.txx.begin(), st.txx.end(), o + 2 * ncell);
+      std::copy(st.tzz.begin(), st.tzz.end(), o + 3 * ncell);
+      std::copy(st.txz.begin(), st.txz.end(), o + 4 * ncell);
+    }
+  }
+  return 0;
+}
+
+template <class T>
+int run_acoustic2d(int nx, int nz, int ns, const float* vp, const float* rho, float dh, float dt,
+                   int nt, int nbc, int fd_order, float v_ref, int n_src, const int32_t* sx,
+                   const int32_t* sz, const float* wavelet, int n_rec, const int32_t* rx,
+                   const int32_t* rz, T* seis_p, T* seis_vx, T* seis_vz, int snap_interval,
+                   T* snaps, T* final_fields, int zone_nbc_override) {
+  int N = order_to_N(fd_order);
+  if (N < 0) return -2;
+  int M = N, pad = nbc + M;
+  if (pad < 2) return -2;
+  G2 g{nx + 2 * pad, nz + 2 * pad};
+  std::vector<T> vpp = pad_array<T>(vp, nx, nz, pad), rhop = pad_array<T>(rho, nx, nz, pad);
+  std::vector<T> bx, bz, kappa(g.n());
+  staggered_buoyancy(g, rhop, bx, bz);
+  for (size_t k = 0; k < g.n(); ++k) kappa[k] = rhop[k] * (vpp[k] * vpp[k]);  // acoustic2d/medium.jl:44
+  Habc<T> h = init_habc<T>(pad, v_ref, dt, dh);
+  // zone_nbc_override > 0 restates the pre-v0.2 zone (= nbc) used by the
+  // calibration in test/verify_patch.jl:9-11; 0 keeps the production zone pad-1.
+  if (zone_nbc_override > 0) h.nbc = zone_nbc_override;
+  std::vector<FramePt> fr = frame_points(g, h.nbc);
+  Coef<T> c = coef<T>(fd_order);
+  T dtx = (T)dt / (T)dh, dtz = dtx;
+  int nsnap = snap_interval > 0 ? nt / snap_interval : 0;
+  size_t ncell = g.n(), nint = (size_t)nx * nz;
+  std::vector<T> scr;
+  for (int s = 0; s < ns; ++s) {
+    AcousticState<T> st;
+    for (auto* v : {&st.vx, &st.vz, &st.p, &st.o1, &st.o2, &st.o3}) v->assign(ncell, T(0));
+    for (int it = 1; it <= nt; ++it) {
+      st.o1 = st.vx;
+      st.o2 = st.vz;
+      acoustic_vel(g, M, c, dtx, dtz, bx.data(), bz.data(), st);
+      habc_det(g, h, fr, 0, st.vx.data(), st.o1.data(), scr);
+      habc_det(g, h, fr, 1, st.vz.data(), st.o2.data(), scr);
+      st.o3 = st.p;
+      acoustic_prs(g, M, c, dtx, dtz, kappa.data(), st);
+      habc_det(g, h, fr, 2, st.p.data(), st.o3.data(), scr);
+      for (int q = 0; q < n_src; ++q) {  // inject_source.jl:4-24
+        size_t p = g.at(sx[(size_t)s * n_src + q] + pad, sz[(size_t)s * n_src + q] + pad);
+        st.p[p] += (T)wavelet[(size_t)q + (size_t)n_src * (it - 1)];
+      }
+      for (int r = 0; r < n_rec; ++r) {  // acoustic2d/fused_kernels.jl:137-149
+        size_t p = g.at(rx[r] + pad, rz[r] + pad);
+        size_t o = (size_t)r + (size_t)n_rec * ((it - 1) + (size_t)nt * s);
+        if (seis_p) seis_p[o] = st.p[p];
+        if (seis_vx) seis_vx[o] = st.vx[p];
+        if (seis_vz) seis_vz[o] = st.vz[p];
+      }
+      if (snaps && snap_interval > 0 && it % snap_interval == 0) {
+        int k = it / snap_interval - 1;
+        snap_interior(g, pad, st.p.data(), snaps + nint * ((size_t)k + (size_t)nsnap * s));
+      }
+    }
+    if (final_fields) {
+      T* o = final_fields + (size_t)s * 3 * ncell;
+      std::copy(st.vx.begin(), st.vx.end(), o);
+      std::copy(st.vz.begin(), st.vz.end(), o + ncell);
+      std::copy(st.p.begin(), st.p.end(), o + 2 * ncell);
+    }
+  }
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// scalar2d: scalar2d/scalar2d.jl:29-84 (leapfrog, carried pad ring, HABC with
+// f_old = u^n); restates verify_scalar.jl:33-86 (cpu_scalar_step!).
+// ---------------------------------------------------------------------------
+template <class T>
+int run_scalar2d(int nx, int nz, const float* vp, float dh, float dt, int nt, int nbc,
+                 int fd_order, float v_ref, int n_src, const int32_t* sx, const int32_t* sz,
+                 const float* wavelet, int n_rec, const int32_t* rx, const int32_t* rz, T* seis_u,
+                 T* final_fields) {
+  int N = order_to_N(fd_order);
+  if (N < 0) return -2;
+  int M = N, pad = nbc + M;
+  if (pad < 2) return -2;
+  G2 g{nx + 2 * pad, nz + 2 * pad};
+  std::vector<T> c2 = pad_array<T>(vp, nx, nz, pad);
+  T r = (T)dt / (T)dh;  // Float32(dt / dh)
+  for (auto& v : c2) {
+    T t = v * r;
+    v = t * t;
+  }
+  Habc<T> h = init_habc<T>(pad, v_ref, dt, dh);
+  std::vector<FramePt> fr = frame_points(g, h.nbc);
+  T c0 = (T)kD2C0[N];
+  T d2[5];
+  for (int l = 0; l < 5; ++l) d2[l] = (T)kD2[N][l];
+  T two_c0 = T(2) * c0;
+  size_t ncell = g.n();
+  const size_t snx = g.nx;
+  std::vector<T> u_old(ncell, T(0)), u_cur(ncell, T(0)), u_nxt(ncell, T(0)), scr;
+  for (int it = 1; it <= nt; ++it) {
+#pragma omp parallel for schedule(static)
+    for (int j = 1; j <= g.nz; ++j) {
+      for (int i = 1; i <= g.nx; ++i) {
+        size_t p = g.at(i, j);
+        T uc = u_cur[p], un = uc;
+        if (i > M && i <= g.nx - M && j > M && j <= g.nz - M) {
+          T lap = two_c0 * uc;
+          for (int l = 1; l <= N; ++l) {
+            T nb = ((u_cur[p + l] + u_cur[p - l]) + u_cur[p + (size_t)l * snx]) + u_cur[p - (size_t)l * snx];
+            lap = fmaT(d2[l - 1], nb, lap);
+          }
+          un = fmaT(c2[p], lap, T(2) * uc - u_old[p]);
+        }
+        u_nxt[p] = un;
+      }
+    }
+    habc_det(g, h, fr, 2, u_nxt.data(), u_cur.data(), scr);
+    for (int q = 0; q < n_src; ++q) {
+      size_t p = g.at(sx[q] + pad, sz[q] + pad);
+      u_nxt[p] += (T)wavelet[(size_t)q + (size_t)n_src * (it - 1)];
+    }
+    for (int rr = 0; rr < n_rec; ++rr) {
+      size_t p = g.at(rx[rr] + pad, rz[rr] + pad);
+      seis_u[(size_t)rr + (size_t)n_rec * (it - 1)] = u_nxt[p];
+    }
+    std::swap(u_old, u_cur);  // u_old <- u^n
+    std::swap(u_cur, u_nxt);  // u_cur <- u^{n+1}
+  }
+  if (final_fields) {
+    std::copy(u_cur.begin(), u_cur.end(), final_fields);
+    std::copy(u_old.begin(), u_old.end(), final_fields + ncell);
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int oracle_version(void) { return 1; }
+
+void oracle_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}
+
+int oracle_max_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+// Host preparation exported for the tests (padded column-major arrays).
+// kind: 0 = elastic (out: bx,bz,lam,lam2mu,mu_txz), 1 = acoustic (out: bx,bz,kappa).
+int oracle_medium2d_f32(int kind, int nx, int nz, const float* vp, const float* vs,
+                        const float* rho, int pad, float* out) {
+  G2 g{nx + 2 * pad, nz + 2 * pad};
+  size_t n = g.n();
+  std::vector<float> vpp = pad_array<float>(vp, nx, nz, pad), rhop = pad_array<float>(rho, nx, nz, pad);
+  std::vector<float> bx, bz;
+  staggered_buoyancy(g, rhop, bx, bz);
+  std::copy(bx.begin(), bx.end(), out);
+  std::copy(bz.begin(), bz.end(), out + n);
+  if (kind == 0) {
+    std::vector<float> vsp = pad_array<float>(vs, nx, nz, pad), lam, l2m, mut;
+    elastic_params(g, vpp, vsp, rhop, lam, l2m, mut);
+    std::copy(lam.begin(), lam.end(), out + 2 * n);
+    std::copy(l2m.begin(), l2m.end(), out + 3 * n);
+    std::copy(mut.begin(), mut.end(), out + 4 * n);
+  } else {
+    for (size_t k = 0; k < n; ++k) out[2 * n + k] = rhop[k] * (vpp[k] * vpp[k]);
+  }
+  return 0;
+}
+
+// Higdon coefficients (q, qt, qxt) and the three weight tables (pad+2 each).
+int oracle_habc_f32(int pad, float v_ref, float dt, float dh, float* qs, float* wtab) {
+  Habc<float> h = init_habc<float>(pad, v_ref, dt, dh);
+  qs[0] = h.q;
+  qs[1] = h.qt;
+  qs[2] = h.qxt;
+  for (int k = 0; k < 3; ++k) std::copy(h.wtab[k].begin(), h.wtab[k].end(), wtab + k * (pad + 2));
+  return h.nbc;
+}
+
+// One two-pass HABC application on a padded field (restates habc_cpu_ref,
+// verify_det_graph.jl:59-94).  kind: 0 vx, 1 vz, 2 tau/p.
+int oracle_habc_apply_f32(int nxp, int nzp, int pad, float v_ref, float dt, float dh, int kind,
+                          float* f, const float* f_old) {
+  G2 g{nxp, nzp};
+  Habc<float> h = init_habc<float>(pad, v_ref, dt, dh);
+  std::vector<FramePt> fr = frame_points(g, h.nbc);
+  std::vector<float> scr;
+  habc_det(g, h, fr, kind, f, f_old, scr);
+  return (int)fr.size();
+}
+
+#define ORACLE_PREC_DISPATCH(prec, call32, call64) \
+  ((prec) == 64 ? (call64) : ((prec) == 32 ? (call32) : -3))
+
+int oracle_elastic2d(int prec, int nx, int nz, int ns, const float* vp, const float* vs,
+                     const float* rho, float dh, float dt, int nt, int nbc, int fd_order,
+                     float v_ref, int n_src, const int32_t* sx, const int32_t* sz,
+                     const float* wavelet, int n_rec, const int32_t* rx, const int32_t* rz,
+                     void* seis_vx, void* seis_vz, int snap_interval, void* snaps,
+                     void* final_fields) {
+  return ORACLE_PREC_DISPATCH(
+      prec,
+      run_elastic2d<float>(nx, nz, ns, vp, vs, rho, dh, dt, nt, nbc, fd_order, v_ref, n_src, sx,
+                           sz, wavelet, n_rec, rx, rz, (float*)seis_vx, (float*)seis_vz,
+                           snap_interval, (float*)snaps, (float*)final_fields),
+      run_elastic2d<double>(nx, nz, ns, vp, vs, rho, dh, dt, nt, nbc, fd_order, v_ref, n_src, sx,
+                            sz, wavelet, n_rec, rx, rz, (double*)seis_vx, (double*)seis_vz,
+                            snap_interval, (double*)snaps, (double*)final_fields));
+}
+
+int oracle_acoustic2d(int prec, int nx, int nz, int ns, const float* vp, const float* rho,
+                      float dh, float dt, int nt, int nbc, int fd_order, float v_ref, int n_src,
+                      const int32_t* sx, const int32_t* sz, const float* wavelet, int n_rec,
+                      const int32_t* rx, const int32_t* rz, void* seis_p, void* seis_vx,
+                      void* seis_vz, int snap_interval, void* snaps, void* final_fields,
+                      int zone_nbc_override) {
+  return ORACLE_PREC_DISPATCH(
+      prec,
+      run_acoustic2d<float>(nx, nz, ns, vp, rho, dh, dt, nt, nbc, fd_order, v_ref, n_src, sx, sz,
+                            wavelet, n_rec, rx, rz, (float*)seis_p, (float*)seis_vx,
+                            (float*)seis_vz, snap_interval, (float*)snaps, (float*)final_fields,
+                            zone_nbc_override),
+      run_acoustic2d<double>(nx, nz, ns, vp, rho, dh, dt, nt, nbc, fd_order, v_ref, n_src, sx, sz,
+                             wavelet, n_rec, rx, rz, (double*)seis_p, (double*)seis_vx,
+                             (double*)seis_vz, snap_interval, (double*)snaps,
+                             (double*)final_fields, zone_nbc_override));
+}
+
+int oracle_scalar2d(int prec, int nx, int nz, const float* vp, float dh, float dt, int nt,
+                    int nbc, int fd_order, float v_ref, int n_src, const int32_t* sx,
+                    const int32_t* sz, const float* wavelet, int n_rec, const int32_t* rx,
+                    const int32_t* rz, void* seis_u, void* final_fields) {
+  return ORACLE_PREC_DISPATCH(
+      prec,
+      run_scalar2d<float>(nx, nz, vp, dh, dt, nt, nbc, fd_order, v_ref, n_src, sx, sz, wavelet,
+                          n_rec, rx, rz, (float*)seis_u, (float*)final_fields),
+      run_scalar2d<double>(nx, nz, vp, dh, dt, nt, nbc, fd_order, v_ref, n_src, sx, sz, wavelet,
+                           n_rec, rx, rz, (double*)seis_u, (double*)final_fields));
+}
+
+}  // extern "C"

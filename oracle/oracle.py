@@ -1,0 +1,221 @@
+"""ctypes front end of the CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+The oracle (``fomo_oracle.cpp``) restates Fomo.jl's time stepping on the CPU in
+FP32 and FP64.  Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline
+leg of ``bench.py`` may import this module; the product library never does.
+
+Array conventions mirror the Julia reference: grids are ``(nx, nz)`` with x the
+fastest (Fortran order), indices are 1-based and unpadded, source index
+matrices are ``(n_src, n_shots)``, the wavelet matrix is ``(n_src, nt)`` and
+seismograms are ``(n_rec, nt[, n_shots])``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+_LIB_PATH = _HERE / "lib" / "libfomo_oracle.so"
+_lib = None
+
+_f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="F_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="F_CONTIGUOUS")
+
+
+def build(force: bool = False) -> Path:
+    """Compile the oracle with its Makefile (no-op when up to date)."""
+    if force or not _LIB_PATH.exists() or (
+        _LIB_PATH.stat().st_mtime < (_HERE / "fomo_oracle.cpp").stat().st_mtime
+    ):
+        subprocess.run(["make", "-C", str(_HERE)], check=True, capture_output=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(str(_LIB_PATH))
+        vp = C.c_void_p
+        L.oracle_elastic2d.restype = C.c_int
+        L.oracle_elastic2d.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _f32p, _f32p, _f32p,
+                                       C.c_float, C.c_float, C.c_int, C.c_int, C.c_int, C.c_float,
+                                       C.c_int, _i32p, _i32p, _f32p, C.c_int, _i32p, _i32p,
+                                       vp, vp, C.c_int, vp, vp]
+        L.oracle_acoustic2d.restype = C.c_int
+        L.oracle_acoustic2d.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _f32p, _f32p,
+                                        C.c_float, C.c_float, C.c_int, C.c_int, C.c_int, C.c_float,
+                                        C.c_int, _i32p, _i32p, _f32p, C.c_int, _i32p, _i32p,
+                                        vp, vp, vp, C.c_int, vp, vp, C.c_int]
+        L.oracle_scalar2d.restype = C.c_int
+        L.oracle_scalar2d.argtypes = [C.c_int, C.c_int, C.c_int, _f32p, C.c_float, C.c_float,
+                                      C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, _i32p, _i32p,
+                                      _f32p, C.c_int, _i32p, _i32p, vp, vp]
+        L.oracle_medium2d_f32.restype = C.c_int
+        L.oracle_medium2d_f32.argtypes = [C.c_int, C.c_int, C.c_int, _f32p, _f32p, _f32p, C.c_int, vp]
+        L.oracle_habc_f32.restype = C.c_int
+        L.oracle_habc_f32.argtypes = [C.c_int, C.c_float, C.c_float, C.c_float, vp, vp]
+        L.oracle_habc_apply_f32.restype = C.c_int
+        L.oracle_habc_apply_f32.argtypes = [C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
+                                            C.c_float, C.c_int, vp, vp]
+        L.oracle_set_threads.argtypes = [C.c_int]
+        L.oracle_max_threads.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def set_threads(n: int) -> None:
+    lib().oracle_set_threads(int(n))
+
+
+def max_threads() -> int:
+    return int(lib().oracle_max_threads())
+
+
+def _f32(a):
+    return np.asfortranarray(np.asarray(a, dtype=np.float32))
+
+
+def _i32(a):
+    return np.asfortranarray(np.asarray(a, dtype=np.int32))
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _dt(prec):
+    return {32: np.float32, 64: np.float64}[prec]
+
+
+def default_v_ref(vp) -> float:
+    vp = np.asarray(vp, dtype=np.float32)
+    return float(vp[vp > 0].min())
+
+
+def _src_matrix(sx, ns):
+    a = _i32(sx)
+    if a.ndim == 1:
+        a = a.reshape(-1, 1, order="F") if ns == 1 else a.reshape(1, -1, order="F")
+    return np.asfortranarray(a)
+
+
+def elastic2d(vp, vs, rho, dh, dt, nt, *, sx, sz, rx, rz, wavelet, nbc=50, fd_order=8,
+              v_ref=None, snap_interval=0, prec=32, n_shots=1, final=False):
+    """Elastic velocity-stress run.  ``sx``/``sz``: (n_src, n_shots).  ``wavelet``: (n_src, nt)."""
+    vp, vs, rho = _f32(vp), _f32(vs), _f32(rho)
+    nx, nz = vp.shape
+    sxm, szm = _src_matrix(sx, n_shots), _src_matrix(sz, n_shots)
+    n_src, ns = sxm.shape
+    w = _f32(wavelet).reshape(n_src, nt, order="F")
+    rx, rz = _i32(rx), _i32(rz)
+    nrec = rx.size
+    T = _dt(prec)
+    svx = np.zeros((nrec, nt, ns), dtype=T, order="F")
+    svz = np.zeros_like(svx)
+    nsnap = nt // snap_interval if snap_interval > 0 else 0
+    snaps = np.zeros((nx, nz, nsnap, ns), dtype=T, order="F") if nsnap else None
+    M = fd_order // 2
+    nxp, nzp = nx + 2 * (nbc + M), nz + 2 * (nbc + M)
+    fin = np.zeros((nxp, nzp, 5, ns), dtype=T, order="F") if final else None
+    vr = default_v_ref(vp) if v_ref is None else float(v_ref)
+    rc = lib().oracle_elastic2d(prec, nx, nz, ns, vp, vs, rho, dh, dt, nt, nbc, fd_order, vr,
+                                n_src, sxm, szm, w, nrec, rx, rz, _ptr(svx), _ptr(svz),
+                                snap_interval, _ptr(snaps), _ptr(fin))
+    if rc != 0:
+        raise RuntimeError(f"oracle_elastic2d failed: {rc}")
+    return dict(seis_vx=svx, seis_vz=svz, snaps=snaps, final=fin)
+
+
+def acoustic2d(vp, rho, dh, dt, nt, *, sx, sz, rx, rz, wavelet, nbc=50, fd_order=8, v_ref=None,
+               snap_interval=0, prec=32, n_shots=1, final=False, zone_nbc=0):
+    vp, rho = _f32(vp), _f32(rho)
+    nx, nz = vp.shape
+    sxm, szm = _src_matrix(sx, n_shots), _src_matrix(sz, n_shots)
+    n_src, ns = sxm.shape
+    w = _f32(wavelet).reshape(n_src, nt, order="F")
+    rx, rz = _i32(rx), _i32(rz)
+    nrec = rx.size
+    T = _dt(prec)
+    sp = np.zeros((nrec, nt, ns), dtype=T, order="F")
+    svx, svz = np.zeros_like(sp), np.zeros_like(sp)
+    nsnap = nt // snap_interval if snap_interval > 0 else 0
+    snaps = np.zeros((nx, nz, nsnap, ns), dtype=T, order="F") if nsnap else None
+    M = fd_order // 2
+    nxp, nzp = nx + 2 * (nbc + M), nz + 2 * (nbc + M)
+    fin = np.zeros((nxp, nzp, 3, ns), dtype=T, order="F") if final else None
+    vr = default_v_ref(vp) if v_ref is None else float(v_ref)
+    rc = lib().oracle_acoustic2d(prec, nx, nz, ns, vp, rho, dh, dt, nt, nbc, fd_order, vr, n_src,
+                                 sxm, szm, w, nrec, rx, rz, _ptr(sp), _ptr(svx), _ptr(svz),
+                                 snap_interval, _ptr(snaps), _ptr(fin), int(zone_nbc))
+    if rc != 0:
+        raise RuntimeError(f"oracle_acoustic2d failed: {rc}")
+    return dict(seis_p=sp, seis_vx=svx, seis_vz=svz, snaps=snaps, final=fin)
+
+
+def scalar2d(vp, dh, dt, nt, *, sx, sz, rx, rz, wavelet, nbc=50, fd_order=8, v_ref=None,
+             prec=32, final=False):
+    """``wavelet``: (n_src, nt), already scaled as the caller's source_scale asks."""
+    vp = _f32(vp)
+    nx, nz = vp.shape
+    sx, sz = _i32(sx).ravel(order="F"), _i32(sz).ravel(order="F")
+    n_src = sx.size
+    w = _f32(wavelet).reshape(n_src, nt, order="F")
+    rx, rz = _i32(rx), _i32(rz)
+    nrec = rx.size
+    T = _dt(prec)
+    su = np.zeros((nrec, nt), dtype=T, order="F")
+    M = fd_order // 2
+    nxp, nzp = nx + 2 * (nbc + M), nz + 2 * (nbc + M)
+    fin = np.zeros((nxp, nzp, 2), dtype=T, order="F") if final else None
+    vr = default_v_ref(vp) if v_ref is None else float(v_ref)
+    rc = lib().oracle_scalar2d(prec, nx, nz, vp, dh, dt, nt, nbc, fd_order, vr, n_src,
+                               np.asfortranarray(sx), np.asfortranarray(sz), w, nrec, rx, rz,
+                               _ptr(su), _ptr(fin))
+    if rc != 0:
+        raise RuntimeError(f"oracle_scalar2d failed: {rc}")
+    return dict(seis_u=su, final=fin)
+
+
+def medium2d(kind, vp, vs, rho, pad):
+    """Padded host preparation.  kind 'elastic' -> (bx,bz,lam,lam2mu,mu_txz); 'acoustic' -> (bx,bz,kappa)."""
+    vp, rho = _f32(vp), _f32(rho)
+    vs = _f32(vs) if vs is not None else vp
+    nx, nz = vp.shape
+    k = 0 if kind == "elastic" else 1
+    nf = 5 if k == 0 else 3
+    out = np.zeros((nx + 2 * pad, nz + 2 * pad, nf), dtype=np.float32, order="F")
+    lib().oracle_medium2d_f32(k, nx, nz, vp, vs, rho, pad, _ptr(out))
+    return out
+
+
+def habc_coeffs(pad, v_ref, dt, dh):
+    qs = np.zeros(3, dtype=np.float32)
+    wt = np.zeros((pad + 2, 3), dtype=np.float32, order="F")
+    nbc = lib().oracle_habc_f32(pad, v_ref, dt, dh, _ptr(qs), _ptr(wt))
+    return nbc, qs, wt
+
+
+def habc_apply(f, f_old, pad, v_ref, dt, dh, kind):
+    """One deterministic two-pass Higdon application (returns the corrected copy)."""
+    f = np.array(f, dtype=np.float32, order="F", copy=True)
+    fo = _f32(f_old)
+    nxp, nzp = f.shape
+    lib().oracle_habc_apply_f32(nxp, nzp, pad, v_ref, dt, dh, kind, _ptr(f), _ptr(fo))
+    return f
+
+
+def ricker(f0, dt, nt):
+    """Ricker wavelet (utils/ricker_wavelet.jl:6-12), evaluated in float64 and rounded to float32."""
+    t = np.arange(nt, dtype=np.float64) * float(np.float32(dt))
+    tau = t - 1.5 / float(np.float32(f0))
+    a = (np.pi * float(np.float32(f0)) * tau) ** 2
+    return ((1.0 - 2.0 * a) * np.exp(-a)).astype(np.float32)
+
+
+if __name__ == "__main__":  # pragma: no cover
+    print(build(), max_threads(), os.cpu_count())

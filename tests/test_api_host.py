@@ -1,0 +1,97 @@
+"""Host-side behaviour of the Fomo API mirror: validation before any launch (no GPU)."""
+import warnings
+
+import numpy as np
+import pytest
+
+
+def _acoustic_inputs(nx=40, nz=30):
+    vp = np.full((nx, nz), 3000.0, np.float32)
+    rho = np.full((nx, nz), 2200.0, np.float32)
+    return vp, rho
+
+
+def test_geometry_errors(fomo):
+    vp, rho = _acoustic_inputs()
+    kw = dict(rx=[5, 10], rz=[3, 3])
+    with pytest.raises(fomo.ArgumentError):
+        fomo.acoustic2d(vp, rho, 10.0, 1e-3, 50, 15.0, sx=[45], sz=[3], **kw)
+    with pytest.raises(fomo.ArgumentError):
+        fomo.acoustic2d(vp, rho, 10.0, 1e-3, 50, 15.0, sx=[5], sz=[0], **kw)
+    with pytest.raises(fomo.ArgumentError):
+        fomo.elastic2d(vp, vp / 1.7, rho, 10.0, 1e-3, 50, 15.0, sx=[5], sz=[3], rx=[41], rz=[3])
+    with pytest.raises(fomo.ArgumentError):
+        fomo.elastic2d_batch(vp, vp / 1.7, rho, 10.0, 1e-3, 50, 15.0, sx=[5, 50], sz=[3, 3],
+                             rx=[4], rz=[3])
+
+
+def test_cfl_error(fomo):
+    vp, rho = _acoustic_inputs()
+    with pytest.raises(fomo.ArgumentError):  # verify_patch.jl:106-110
+        fomo.acoustic2d(vp, rho, 10.0, 9e-3, 50, 15.0, sx=[5], sz=[3], rx=[4], rz=[3])
+    with pytest.raises(fomo.ArgumentError):
+        fomo.scalar2d(vp, 10.0, 9e-3, 50, 15.0, sx=[5], sz=[3], rx=[4], rz=[3])
+
+
+def test_wavelet_length_and_keywords(fomo):
+    vp, rho = _acoustic_inputs()
+    kw = dict(sx=[5], sz=[3], rx=[4], rz=[3])
+    with pytest.raises(fomo.ArgumentError):
+        fomo.acoustic2d(vp, rho, 10.0, 1e-3, 50, 15.0, wavelet=np.zeros(49), **kw)
+    with pytest.raises(fomo.ArgumentError):
+        fomo.acoustic2d(vp, rho, 10.0, 1e-3, 50, 15.0, boundary="pml", **kw)
+    with pytest.raises(NotImplementedError):
+        fomo.acoustic2d(vp, rho, 10.0, 1e-3, 50, 15.0, boundary=":sponge", **kw)
+    with pytest.raises(fomo.ArgumentError):
+        fomo.scalar2d(vp, 10.0, 1e-3, 50, 15.0, source_scale=":foo", **kw)
+    with pytest.raises(fomo.ArgumentError):
+        fomo.acoustic2d_batch(vp, rho, 10.0, 1e-3, 50, 15.0, sx=[[5, 6]], sz=[[3]], rx=[4], rz=[3])
+
+
+def test_dispersion_warning(fomo):
+    from fomo_b200.api import _check_numerics
+
+    with warnings.catch_warnings(record=True) as w:
+        warnings.simplefilter("always")
+        _check_numerics(3000.0, 500.0, 10.0, 1e-3, 30.0, 8)
+    assert any("dispersion" in str(x.message) for x in w)
+
+
+def test_ricker_matches_oracle(fomo, oracle):
+    assert np.array_equal(fomo.ricker_wavelet(15.0, 1e-3, 700), oracle.ricker(15.0, 1e-3, 700))
+    w = fomo.ricker_wavelet(10.0, 1e-3, 1000)
+    assert abs(float(w.max()) - 1.0) < 1e-6 and np.argmax(w) == 150  # peak at 1.5/f0
+
+
+def test_scalar_source_scaling(fomo):
+    from fomo_b200.api import scalar_wavelet_matrix
+
+    vp = np.full((10, 8), 2000.0, np.float32)
+    vp[3, 2] = 2500.0
+    w = np.linspace(-1, 1, 7).astype(np.float32)
+    m = scalar_wavelet_matrix(w, vp, 1e-3, [4, 1], [3, 1], "v2dt2")
+    s0 = np.float32(np.float32(2500.0) * np.float32(2500.0) * (np.float32(1e-3) * np.float32(1e-3)))
+    assert np.array_equal(m[0], (w * s0).astype(np.float32))
+    assert np.array_equal(scalar_wavelet_matrix(w, vp, 1e-3, [4], [3], "none")[0], w)
+    assert np.array_equal(scalar_wavelet_matrix(w, vp, 1e-3, [4], [3], "dt")[0],
+                          (w * np.float32(1e-3)).astype(np.float32))
+
+
+def test_fd_coefficients(fomo):
+    a = fomo.get_fd_coefficients(8)
+    assert a.dtype == np.float32 and a.size == 4
+    assert np.float32(a[0]) == np.float32(1.1962890625)
+    c0, d2 = fomo.get_centered_d2(4)
+    assert c0 == np.float32(-2.5) and d2[0] == np.float32(4 / 3)
+    with pytest.raises(ValueError):
+        fomo.get_fd_coefficients(12)
+
+
+def test_synthetic_layered_config(fomo):
+    from fomo_b200.synthetic import elastic_batch_config
+
+    c = elastic_batch_config()
+    assert c["vp"].shape == (1000, 500) and c["sx"].size == 32 and c["rx"].size == 500
+    assert 1500 <= c["vp"].min() and c["vp"].max() <= 4500
+    assert np.allclose(c["vs"], c["vp"] / 1.73, rtol=1e-6)
+    assert len(np.unique(c["vp"][0])) == 12
