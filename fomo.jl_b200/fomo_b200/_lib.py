@@ -30,6 +30,7 @@ EXPORTS = (
     "fomo_version", "fomo_create", "fomo_destroy", "fomo_last_error", "fomo_set_stream",
     "fomo_trim", "fomo_check_numerics", "fomo_acoustic2d", "fomo_acoustic2d_batch",
     "fomo_elastic2d", "fomo_elastic2d_batch", "fomo_scalar2d", "fomo_debug_medium2d",
+    "fomo_scalar2d_noalloc",
 )
 
 
@@ -96,6 +97,8 @@ def lib() -> C.CDLL:
             L.fomo_elastic2d_batch.argtypes = [vp, g, vp, vp, vp, a, vp, vp, o, s]
             L.fomo_scalar2d.argtypes = [vp, g, vp, a, vp, o, s]
             L.fomo_debug_medium2d.argtypes = [vp, i32, i32, i32, i32, f32, f32, vp, vp, vp, vp]
+            L.fomo_scalar2d_noalloc.argtypes = [g, vp, a, vp, vp, C.c_char_p, i32]
+            L.fomo_scalar2d_noalloc.restype = C.c_int
             for name in ("fomo_acoustic2d", "fomo_acoustic2d_batch", "fomo_elastic2d",
                          "fomo_elastic2d_batch", "fomo_scalar2d", "fomo_debug_medium2d",
                          "fomo_set_stream", "fomo_trim"):

@@ -160,6 +160,24 @@ FOMO_API int fomo_elastic2d_batch(fomo_ctx* ctx, const fomo_grid2d* g, const flo
 FOMO_API int fomo_scalar2d(fomo_ctx* ctx, const fomo_grid2d* g, const float* vp, const fomo_acq* acq,
                   float* seis_u, const fomo_opts* opts, fomo_stats* stats);
 
+/* ---- allocation-free entry -------------------------------------------------
+ * No counterpart in the reference.  scalar2d for callers that cannot allocate
+ * device memory (a plugin inside a framework whose allocator owns all device
+ * memory, a fixed-budget service): every working buffer lives in one static
+ * 32 MiB device array that each GPU loading this library holds until exit, so
+ * this call makes no cudaMalloc/cudaFree.  Every array argument (vp, acq's
+ * sx/sz/wavelet/rx/rz, seis_u) is a DEVICE pointer; g->v_ref must be > 0;
+ * acq->n_shots must be 1; the wavelet is pre-scaled as for fomo_scalar2d.
+ * Runs on the calling thread's current device, on `stream` (NULL = default),
+ * and returns after the stream has finished the run.  Problems whose working
+ * set exceeds the array return FOMO_EARG.  All calls share the array (it keeps
+ * the previous call's contents; the wavefields are cleared at each start), so
+ * calls that overlap on the GPU race.  The first call on a device looks up the
+ * array's address and should come before any stream capture.  `err` (may be
+ * NULL) receives a message of at most err_len bytes. */
+FOMO_API int fomo_scalar2d_noalloc(const fomo_grid2d* g, const float* vp, const fomo_acq* acq,
+                                   float* seis_u, void* stream, char* err, int32_t err_len);
+
 /* ---- diagnostics -------------------------------------------------------- */
 /* Device-side medium preparation, downloaded to `out` (padded, column-major):
  * kind 0 elastic -> bx,bz,lam,lam2mu,mu_txz; 1 acoustic -> bx,bz,kappa;
