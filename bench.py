@@ -238,6 +238,16 @@ def ours(args, cfg):
     achieved = alg_step / (sweep * 1e-3) / 1e9 if sweep > 0 else None
     finite = bool(torch.isfinite(d_svz).all().item())
 
+    if os.environ.get("FOMO_BENCH_NO_E2E"):
+        line = {"metric": METRIC, "value": value, "unit": "shots/s", "ms_per_step": ms,
+                "gcell_updates_per_s": gcell, "sweep_ms_per_step": sweep,
+                "roofline_frac": (achieved / peak) if achieved else None, "n_shots": int(ns),
+                "nt": nt, "kernel_family": st.kernel, "clocks": clocks,
+                "sweep_config": st.sweep_config}
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        return
+
     # ---- e2e through the public API: pinned host inputs, D2H of the seismograms
     def pinned(a):
         t = torch.empty(a.shape[::-1], dtype=torch.float32, pin_memory=True)
@@ -276,7 +286,8 @@ def ours(args, cfg):
         "config": {"workload": WORKLOAD, "n_shots_per_gpu": int(ns), "global_shots": int(ns * world),
                    "padded_grid": [1170, 670], "nt": nt, "parallelism": f"shots sharded x{world}",
                    "l2": "inputs larger than L2 (1.0 GB wavefield state per GPU)",
-                   "kernel_family": {1: "two-phase", 2: "single-sweep"}.get(st.kernel, str(st.kernel))},
+                   "kernel_family": {1: "two-phase", 2: "single-sweep"}.get(st.kernel, str(st.kernel)),
+                   "sweep_config": st.sweep_config},
         "gcell_updates_per_s": gcell,
         "e2e": {"value": ns * world / (e2e_ms * 1e-3), "unit": "shots/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
@@ -309,10 +320,20 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    # reduced cases for profiling captures (same model, fewer shots / time steps)
+    ap.add_argument("--shots", type=int, default=32)
+    ap.add_argument("--nt", type=int, default=3000)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     from fomo_b200.synthetic import elastic_batch_config
 
-    cfg = elastic_batch_config()
+    cfg = elastic_batch_config(n_shots=args.shots)
+    cfg["nt"] = args.nt
+    if args.no_cpu:
+        os.environ["FOMO_BENCH_NO_CPU"] = "1"
+    if args.no_e2e:
+        os.environ["FOMO_BENCH_NO_E2E"] = "1"
     if args.impl == "reference":
         reference_arm(args, cfg)
     else:

@@ -82,9 +82,10 @@ struct HabcDev {
 // Padded 2D geometry (0-based x in [0,nx), z in [0,nz)).
 struct Geo2 {
   int nx, nz;      // padded
+  int ld;          // row pitch in elements (>= nx)
   int M;           // fd_order / 2
   int nbc;         // HABC zone = pad - 1
-  long long plane; // nx * nz
+  long long plane; // ld * nz
 };
 
 __device__ __forceinline__ bool interior2(const Geo2& g, int x, int z) {
@@ -151,7 +152,7 @@ inline int order_to_N(int fd_order) {
 inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
 
 // Device medium preparation (medium.cu).
-cudaError_t launch_medium2d(cudaStream_t st, int kind, int nx, int nz, int pad, float dtdh,
+cudaError_t launch_medium2d(cudaStream_t st, int kind, int nx, int nz, int pad, int ld, float dtdh,
                             const float* vp, const float* vs, const float* rho, float* out0,
                             float* out1, float* out2, float* out3, float* out4);
 

@@ -43,7 +43,7 @@ __device__ __forceinline__ float mu_at(const Raw2& rho, const Raw2& vs, int x, i
 // kind 0 elastic: out0..4 = bx, bz, lam, lam2mu, mu_txz
 // kind 1 acoustic: out0..2 = bx, bz, kappa
 // kind 2 scalar: out0 = c2 = (vp * dt/dh)^2
-__global__ void k_medium2d(int kind, int nx, int nz, int pad, float dtdh, Raw2 vp, Raw2 vs,
+__global__ void k_medium2d(int kind, int nx, int nz, int pad, int ld, float dtdh, Raw2 vp, Raw2 vs,
                            Raw2 rho, float* __restrict__ o0, float* __restrict__ o1,
                            float* __restrict__ o2, float* __restrict__ o3,
                            float* __restrict__ o4) {
@@ -51,7 +51,7 @@ __global__ void k_medium2d(int kind, int nx, int nz, int pad, float dtdh, Raw2 v
   int x = blockIdx.x * blockDim.x + threadIdx.x;
   int z = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= nxp || z >= nzp) return;
-  long long p = (long long)z * nxp + x;
+  long long p = (long long)z * ld + x;
   if (kind == 2) {
     float t = __fmul_rn(vp.at(x, z), dtdh);
     o0[p] = __fmul_rn(t, t);
@@ -81,13 +81,13 @@ __global__ void k_medium2d(int kind, int nx, int nz, int pad, float dtdh, Raw2 v
 
 }  // namespace
 
-cudaError_t launch_medium2d(cudaStream_t st, int kind, int nx, int nz, int pad, float dtdh,
+cudaError_t launch_medium2d(cudaStream_t st, int kind, int nx, int nz, int pad, int ld, float dtdh,
                             const float* vp, const float* vs, const float* rho, float* out0,
                             float* out1, float* out2, float* out3, float* out4) {
   int nxp = nx + 2 * pad, nzp = nz + 2 * pad;
   dim3 b(32, 8), gr(cdiv(nxp, 32), cdiv(nzp, 8));
   Raw2 a{vp, nx, nz, pad}, s{vs ? vs : vp, nx, nz, pad}, r{rho ? rho : vp, nx, nz, pad};
-  k_medium2d<<<gr, b, 0, st>>>(kind, nx, nz, pad, dtdh, a, s, r, out0, out1, out2, out3, out4);
+  k_medium2d<<<gr, b, 0, st>>>(kind, nx, nz, pad, ld, dtdh, a, s, r, out0, out1, out2, out3, out4);
   return cudaGetLastError();
 }
 

@@ -187,7 +187,7 @@ extern "C" int fomo_scalar2d_noalloc(const fomo_grid2d* g, const float* vp, cons
   const float r = (g->v_ref * g->dt) / g->dh;
   const float b = 0.45f, beta = 1.0f, br = beta + r, den = br * (1.0f - b);
   HabcDev h{(b * br - r) / den, (b * br - beta) / den, b / (b - 1.0f), pad - 1, wstride, wtab};
-  Geo2 geo{nxp, nzp, N, pad - 1, plane};
+  Geo2 geo{nxp, nzp, nxp, N, pad - 1, plane};
   D2Coef dc;
   dc.two_c0 = 2.0f * kD2C0[N];
   for (int l = 0; l < 5; ++l) dc.d[l] = kD2[N][l];
@@ -202,7 +202,7 @@ extern "C" int fomo_scalar2d_noalloc(const fomo_grid2d* g, const float* vp, cons
     e = cudaGetLastError();
   }
   if (e == cudaSuccess)
-    e = launch_medium2d(st, 2, g->nx, g->nz, pad, g->dt / g->dh, vp, nullptr, nullptr, c2, nullptr,
+    e = launch_medium2d(st, 2, g->nx, g->nz, pad, nxp, g->dt / g->dh, vp, nullptr, nullptr, c2, nullptr,
                         nullptr, nullptr, nullptr);
   int hflag = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, st);

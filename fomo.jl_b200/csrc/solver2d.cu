@@ -3,8 +3,13 @@
 // medium preparation, the time loop and the result download.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
 
 #include "solver2d_kernels.cuh"
 #include "sweep2d.cuh"
@@ -17,6 +22,7 @@ enum Phys { kAcoustic = 0, kElastic = 1, kScalar = 2 };
 struct Plan2 {
   Phys phys;
   int nx, nz, nt, nbc, fd_order, N, M, pad, nxp, nzp;
+  int ld;  // row pitch: nxp rounded up to 32 floats (128-byte rows, TMA-legal strides)
   long long plane;
   float dh, dt, v_ref;
   int ns, n_src, n_rec;
@@ -74,7 +80,8 @@ int make_plan(fomo_ctx* ctx, Phys phys, const fomo_grid2d* g, const fomo_acq* ac
   if (P.pad < 2) return fail(ctx, FOMO_EARG, "nbc + fd_order/2 must be >= 2");
   P.nxp = P.nx + 2 * P.pad;
   P.nzp = P.nz + 2 * P.pad;
-  P.plane = (long long)P.nxp * P.nzp;
+  P.ld = (P.nxp + 31) & ~31;
+  P.plane = (long long)P.ld * P.nzp;
   P.ns = acq->n_shots;
   P.n_src = acq->n_src;
   P.n_rec = acq->n_rec;
@@ -101,6 +108,109 @@ float min_positive(const std::vector<float>& v) {
   for (float x : v)
     if (x > 0.0f && x < m) m = x;
   return m;
+}
+
+// Autotuner of the single-sweep kernel: times each (variant, strip width,
+// z-segments) candidate on the problem itself and keeps the fastest; the
+// choice is cached per (N, padded grid, shots) for the process.
+struct TuneKey {
+  int N, nx, nz, ns;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(N, nx, nz, ns) < std::tie(o.N, o.nx, o.nz, o.ns);
+  }
+};
+struct TuneVal {
+  int variant, TX, per_sm;
+  float frame_weight;
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneVal> g_tune;
+
+template <class FieldFn>
+int tune_sweep(fomo_ctx* ctx, cudaStream_t st, SweepPlan& sp, int N, const Geo2& g, int ns,
+               float* const sets[2][3], const Coef& c, float dtx, float dtz, const HabcDev& h,
+               const ElMat& m, FieldFn field, long long* d_bounds) {
+  const TuneKey key{N, g.nx, g.nz, ns};
+  // FOMO_SWEEP_CONFIG="variant,TX,ctas_per_sm" pins the configuration (tests, sweeps)
+  if (const char* env = std::getenv("FOMO_SWEEP_CONFIG")) {
+    int v = 0, tx = 0, per_sm = 0;
+    float fw = 1.0f;
+    const int nr = std::sscanf(env, "%d,%d,%d,%f", &v, &tx, &per_sm, &fw);
+    if (nr >= 3 && v >= 0 && v < sweep_num_variants() && per_sm >= 1) {
+      FOMO_CU(ctx, make_sweep_plan(sp, N, v, tx, per_sm, g, ns, sets, fw, d_bounds, st));
+      return FOMO_OK;
+    }
+    return fail(ctx, FOMO_EARG, "bad FOMO_SWEEP_CONFIG (want variant,TX,ctas_per_sm[,frame_weight])");
+  }
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) {
+      FOMO_CU(ctx, make_sweep_plan(sp, N, it->second.variant, it->second.TX, it->second.per_sm, g,
+                                   ns, sets, it->second.frame_weight, d_bounds, st));
+      return FOMO_OK;
+    }
+  }
+  ElFields a{field(0, 0), field(0, 1), field(0, 2), field(0, 3), field(0, 4)};
+  ElOut o{field(1, 0), field(1, 1), field(1, 2), field(1, 3), field(1, 4)};
+  cudaEvent_t e0, e1;
+  FOMO_CU(ctx, cudaEventCreate(&e0));
+  FOMO_CU(ctx, cudaEventCreate(&e1));
+  float best = 1e30f;
+  TuneVal bv{-1, 0, 0, 1.0f};
+  auto time_plan = [&](const SweepPlan& cand, float& ms) -> int {
+    FOMO_CU(ctx, launch_sweep_elastic(st, cand, 0, c, dtx, dtz, h, a, m, o, ctx->d_flag));
+    FOMO_CU(ctx, cudaEventRecord(e0, st));
+    for (int r = 0; r < 3; ++r)
+      FOMO_CU(ctx, launch_sweep_elastic(st, cand, 0, c, dtx, dtz, h, a, m, o, ctx->d_flag));
+    FOMO_CU(ctx, cudaEventRecord(e1, st));
+    FOMO_CU(ctx, cudaEventSynchronize(e1));
+    FOMO_CU(ctx, cudaEventElapsedTime(&ms, e0, e1));
+    return FOMO_OK;
+  };
+  for (int v = 0; v < sweep_num_variants(); ++v) {
+    int txs[4];
+    int ntx = sweep_tx_candidates(v, N, txs, 4);
+    for (int k = 0; k < ntx; ++k) {
+      SweepPlan cand;
+      if (make_sweep_plan(cand, N, v, txs[k], 64, g, ns, sets, 1.0f, d_bounds, st) != cudaSuccess)
+        continue;
+      const int full = cand.per_sm;  // all resident CTAs; also try one fewer
+      for (int per_sm = full; per_sm >= 1 && per_sm >= full - 1; --per_sm) {
+        if (make_sweep_plan(cand, N, v, txs[k], per_sm, g, ns, sets, 1.0f, d_bounds, st) !=
+            cudaSuccess)
+          continue;
+        float ms = 0.0f;
+        if (int rc = time_plan(cand, ms)) return rc;
+        if (ms < best) {
+          best = ms;
+          bv = TuneVal{v, txs[k], per_sm, 1.0f};
+        }
+      }
+    }
+  }
+  // then the cost weight of frame cells for the row-range split
+  if (bv.variant >= 0)
+    for (float fw : {0.0f, 0.5f, 2.0f, 3.0f}) {
+      SweepPlan cand;
+      if (make_sweep_plan(cand, N, bv.variant, bv.TX, bv.per_sm, g, ns, sets, fw, d_bounds, st) !=
+          cudaSuccess)
+        continue;
+      float ms = 0.0f;
+      if (int rc = time_plan(cand, ms)) return rc;
+      if (ms < best) {
+        best = ms;
+        bv.frame_weight = fw;
+      }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (bv.variant < 0) return fail(ctx, FOMO_ECUDA, "no single-sweep configuration fits");
+  FOMO_CU(ctx, make_sweep_plan(sp, N, bv.variant, bv.TX, bv.per_sm, g, ns, sets, bv.frame_weight,
+                               d_bounds, st));
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[key] = bv;
+  return FOMO_OK;
 }
 
 struct Outs {
@@ -132,8 +242,8 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
     return rc;
   std::vector<int32_t> src_lin(nsrc_all), rec_lin(P.n_rec);
   for (long long k = 0; k < nsrc_all; ++k)
-    src_lin[k] = (hsx[k] - 1 + P.pad) + P.nxp * (hsz[k] - 1 + P.pad);
-  for (int r = 0; r < P.n_rec; ++r) rec_lin[r] = (hrx[r] - 1 + P.pad) + P.nxp * (hrz[r] - 1 + P.pad);
+    src_lin[k] = (hsx[k] - 1 + P.pad) + P.ld * (hsz[k] - 1 + P.pad);
+  for (int r = 0; r < P.n_rec; ++r) rec_lin[r] = (hrx[r] - 1 + P.pad) + P.ld * (hrz[r] - 1 + P.pad);
 
   // ---- v_ref default: minimum(vp > 0) (acoustic2d.jl:55) ----
   if (!(P.v_ref > 0.0f)) {
@@ -159,6 +269,7 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
   size_t o_wav = P.dev ? 0 : ar.take<float>(std::max<long long>((long long)P.n_src * P.nt, 1));
   size_t o_seis = P.dev ? 0 : ar.take<float>(std::max<long long>(outs.nseis * seis_n, 1));
   size_t o_snap = (!P.dev && outs.snaps && P.nsnap) ? ar.take<float>(P.nsnap * nint) : 0;
+  size_t o_bounds = ar.take<long long>(kMaxGrid + 1);
   if ((rc = ensure_workspace(ctx, ar.off))) return rc;
 
   const float* d_vp = vp;
@@ -207,7 +318,7 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
   // ---- medium (device) ----
   float dtdh = P.dt / P.dh;  // Float32(dt / dh)
   FOMO_CU(ctx, launch_medium2d(st, P.phys == kElastic ? 0 : (P.phys == kAcoustic ? 1 : 2), P.nx,
-                               P.nz, P.pad, dtdh, d_vp, d_vs, d_rho, d_mat, d_mat + P.plane,
+                               P.nz, P.pad, P.ld, dtdh, d_vp, d_vs, d_rho, d_mat, d_mat + P.plane,
                                d_mat + 2 * P.plane, d_mat + 3 * P.plane, d_mat + 4 * P.plane));
   // ---- zero state (reset!, batch.jl:30-35) ----
   FOMO_CU(ctx, cudaMemsetAsync(d_state, 0, sizeof(float) * nsets * nfield * P.ns * P.plane, st));
@@ -215,7 +326,7 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
     for (int k = 0; k < outs.nseis; ++k)
       if (d_seis[k]) FOMO_CU(ctx, cudaMemsetAsync(d_seis[k], 0, sizeof(float) * seis_n, st));
 
-  Geo2 g{P.nxp, P.nzp, P.M, hh.nbc, P.plane};
+  Geo2 g{P.nxp, P.nzp, P.ld, P.M, hh.nbc, P.plane};
   Coef c;
   for (int l = 0; l < 5; ++l) c.a[l] = kFD[P.N][l];
   HabcDev h{hh.q, hh.qt, hh.qxt, hh.nbc, hh.wstride, d_w};
@@ -226,6 +337,18 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
   if (kernel == FOMO_KERNEL_AUTO) kernel = pick_kernel_2d((int)P.phys, P.N, P.nxp, P.nzp, P.ns);
   if (kernel == FOMO_KERNEL_SINGLE_SWEEP && !sweep2d_supported((int)P.phys, P.N))
     kernel = FOMO_KERNEL_TWO_PHASE;
+  ElMat emat{d_mat, d_mat + P.plane, d_mat + 2 * P.plane, d_mat + 3 * P.plane, d_mat + 4 * P.plane};
+  SweepPlan sp;
+  if (kernel == FOMO_KERNEL_SINGLE_SWEEP) {
+    float* sets[2][3] = {{field(0, 2), field(0, 3), field(0, 4)}, {field(1, 2), field(1, 3), field(1, 4)}};
+    rc = tune_sweep(ctx, st, sp, P.N, g, P.ns, sets, c, dtx, dtz, h, emat,
+                    [&](int set, int f) { return field(set, f); },
+                    ws_ptr<long long>(ctx, o_bounds));
+    if (rc) return rc;
+    // the tuning launches ran on the zero state; restore it
+    FOMO_CU(ctx, cudaMemsetAsync(d_state, 0, sizeof(float) * nsets * nfield * P.ns * P.plane, st));
+  }
+  FOMO_CU(ctx, cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), st));
 
   dim3 blk(32, 8), grd(cdiv(P.nxp, 32), cdiv(P.nzp, 8), P.ns);
   int launches = 0;
@@ -246,10 +369,10 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
     FOMO_CU(ctx, prof_mark(it, 0));
     if (P.phys == kElastic) {
       ElFields a{field(A, 0), field(A, 1), field(A, 2), field(A, 3), field(A, 4)};
-      ElMat m{d_mat, d_mat + P.plane, d_mat + 2 * P.plane, d_mat + 3 * P.plane, d_mat + 4 * P.plane};
+      const ElMat& m = emat;
       if (kernel == FOMO_KERNEL_SINGLE_SWEEP) {
         ElOut o{field(B, 0), field(B, 1), field(B, 2), field(B, 3), field(B, 4)};
-        FOMO_CU(ctx, launch_sweep_elastic(st, P.N, g, c, dtx, dtz, h, a, m, o, P.ns));
+        FOMO_CU(ctx, launch_sweep_elastic(st, sp, A, c, dtx, dtz, h, a, m, o, ctx->d_flag));
         launches += 1;
         sweeps_per_step = 1;
       } else {
@@ -312,9 +435,9 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
     // snapshot of the interior (fused_kernels.jl:192-195): p (acoustic), vz (elastic)
     if (d_snap && P.snap_interval > 0 && it % P.snap_interval == 0) {
       int k = it / P.snap_interval - 1;
-      const float* src = (P.phys == kAcoustic ? field(B, 2) : field(B, 1)) + P.pad + (long long)P.pad * P.nxp;
+      const float* src = (P.phys == kAcoustic ? field(B, 2) : field(B, 1)) + P.pad + (long long)P.pad * P.ld;
       FOMO_CU(ctx, cudaMemcpy2DAsync(d_snap + (long long)k * nint, sizeof(float) * P.nx, src,
-                                     sizeof(float) * P.nxp, sizeof(float) * P.nx, P.nz,
+                                     sizeof(float) * P.ld, sizeof(float) * P.nx, P.nz,
                                      cudaMemcpyDeviceToDevice, st));
     }
     if (P.phys == kScalar) {
@@ -339,19 +462,23 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
                                    cudaMemcpyDeviceToHost, st));
   }
   if (opts && opts->final_state) {
-    // (nxp, nzp, nfield, ns) host layout; scalar returns (u^n, u^{n-1})
+    // (nxp, nzp, nfield, ns) unpitched host layout; scalar returns (u^n, u^{n-1})
+    const long long hp = (long long)P.nxp * P.nzp;
     for (int s = 0; s < P.ns; ++s)
-      for (int f = 0; f < nfield; ++f) {
-        int set = P.phys == kScalar ? (f == 0 ? B : A) : A;
-        const float* src = P.phys == kScalar ? field(set, 0) : field(A, f) + (long long)s * P.plane;
-        FOMO_CU(ctx, cudaMemcpyAsync(opts->final_state + ((long long)s * nfield + f) * P.plane, src,
-                                     sizeof(float) * P.plane, cudaMemcpyDeviceToHost, st));
+      for (int f = 0; f < (P.phys == kScalar ? 2 : nfield); ++f) {
+        const float* src = P.phys == kScalar ? field(f == 0 ? B : A, 0)
+                                             : field(A, f) + (long long)s * P.plane;
+        FOMO_CU(ctx, cudaMemcpy2DAsync(opts->final_state + ((long long)s * nfield + f) * hp,
+                                       sizeof(float) * P.nxp, src, sizeof(float) * P.ld,
+                                       sizeof(float) * P.nxp, P.nzp, cudaMemcpyDeviceToHost, st));
       }
-    if (P.phys == kScalar)
-      FOMO_CU(ctx, cudaMemcpyAsync(opts->final_state + P.plane, field(A, 0),
-                                   sizeof(float) * P.plane, cudaMemcpyDeviceToHost, st));
   }
   FOMO_CU(ctx, cudaStreamSynchronize(st));
+  if (kernel == FOMO_KERNEL_SINGLE_SWEEP) {
+    int hflag = 0;
+    FOMO_CU(ctx, cudaMemcpy(&hflag, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost));
+    if (hflag) return fail(ctx, FOMO_ECUDA, "single-sweep kernel: a bounded TMA wait timed out");
+  }
   float ms = 0.0f;
   FOMO_CU(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
   double sweep_ms = 0.0;
@@ -374,6 +501,9 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
     stats->status = FOMO_OK;
     stats->sweep_ms = sweep_ms;
     stats->sweep_launches = sweeps_per_step;
+    stats->sweep_config = kernel == FOMO_KERNEL_SINGLE_SWEEP
+                              ? sp.variant * 1000000 + sp.gm.TX * 1000 + sp.per_sm
+                              : 0;
   }
   return FOMO_OK;
 }
@@ -455,7 +585,7 @@ int fomo_debug_medium2d(fomo_ctx* ctx, int32_t kind, int32_t nx, int32_t nz, int
   if (vs) FOMO_CU(ctx, cudaMemcpyAsync(m + nint, vs, sizeof(float) * nint, cudaMemcpyHostToDevice, st));
   if (rho)
     FOMO_CU(ctx, cudaMemcpyAsync(m + 2 * nint, rho, sizeof(float) * nint, cudaMemcpyHostToDevice, st));
-  FOMO_CU(ctx, launch_medium2d(st, kind, nx, nz, pad, dt / dh, m, vs ? m + nint : nullptr,
+  FOMO_CU(ctx, launch_medium2d(st, kind, nx, nz, pad, nx + 2 * pad, dt / dh, m, vs ? m + nint : nullptr,
                                rho ? m + 2 * nint : nullptr, o, o + plane, o + 2 * plane,
                                o + 3 * plane, o + 4 * plane));
   FOMO_CU(ctx, cudaMemcpyAsync(out, o, sizeof(float) * nf * plane, cudaMemcpyDeviceToHost, st));

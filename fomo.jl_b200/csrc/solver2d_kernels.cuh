@@ -42,10 +42,10 @@ template <int N>
 __device__ __forceinline__ void el_vel_at(const Geo2& g, const Coef& c, float dtx, float dtz,
                                           const ElFields& a, const ElMat& m, int x, int z,
                                           float& ux, float& uz) {
-  long long p = (long long)z * g.nx + x;
+  long long p = (long long)z * g.ld + x;
   float vx = __ldg(a.vx + p), vz = __ldg(a.vz + p);
   if (interior2(g, x, z)) {
-    const long long sz = g.nx;
+    const long long sz = g.ld;
     float dxx = dm<N>(a.txx, p, 1, c);
     float dxzz = dm<N>(a.txz, p, sz, c);
     float dxzx = dp<N>(a.txz, p, 1, c);
@@ -68,13 +68,13 @@ __global__ void __launch_bounds__(256) k_el_vel(Geo2 g, Coef c, float dtx, float
   a.vx += so; a.vz += so; a.txx += so; a.tzz += so; a.txz += so;
   float ux, uz;
   el_vel_at<N>(g, c, dtx, dtz, a, m, x, z, ux, uz);
-  long long p = (long long)z * g.nx + x;
+  long long p = (long long)z * g.ld + x;
   int sx, sz, dist;
   if (frame2(g, x, z, sx, sz, dist)) {
     float wx = habc_weight(h, 0, dist), wz = habc_weight(h, 1, dist);
     float fox = __ldg(a.vx + p), foz = __ldg(a.vz + p);
     if (sx != 0 && sz != 0) {
-      long long px = p + sx, pz = p + (long long)sz * g.nx;
+      long long px = p + sx, pz = p + (long long)sz * g.ld;
       float ax, az, bx, bz;
       el_vel_at<N>(g, c, dtx, dtz, a, m, x + sx, z, ax, az);
       el_vel_at<N>(g, c, dtx, dtz, a, m, x, z + sz, bx, bz);
@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(256) k_el_vel(Geo2 g, Coef c, float dtx, float
                          higdon_side(h, bz, foz, __ldg(a.vz + pz)));
     } else {
       int nxp = x + sx, nzp = z + sz;
-      long long pn = (long long)nzp * g.nx + nxp;
+      long long pn = (long long)nzp * g.ld + nxp;
       float nx_, nz_;
       el_vel_at<N>(g, c, dtx, dtz, a, m, nxp, nzp, nx_, nz_);
       ux = higdon_edge(wx, ux, higdon_side(h, nx_, fox, __ldg(a.vx + pn)));
@@ -100,12 +100,12 @@ __device__ __forceinline__ void el_str_at(const Geo2& g, const Coef& c, float dt
                                           const float* __restrict__ vx, const float* __restrict__ vz,
                                           const ElFields& a, const ElMat& m, int x, int z,
                                           float& sxx, float& szz, float& sxz) {
-  long long p = (long long)z * g.nx + x;
+  long long p = (long long)z * g.ld + x;
   sxx = __ldg(a.txx + p);
   szz = __ldg(a.tzz + p);
   sxz = __ldg(a.txz + p);
   if (interior2(g, x, z)) {
-    const long long sz = g.nx;
+    const long long sz = g.ld;
     float dvxdx = dp<N>(vx, p, 1, c);
     float dvzdz = dm<N>(vz, p, sz, c);
     float dvxdz = dp<N>(vx, p, sz, c);
@@ -133,13 +133,13 @@ __global__ void __launch_bounds__(256) k_el_str(Geo2 g, Coef c, float dtx, float
   const float* vz = vz1 + so;
   float sxx, szz, sxz;
   el_str_at<N>(g, c, dtx, dtz, vx, vz, a, m, x, z, sxx, szz, sxz);
-  long long p = (long long)z * g.nx + x;
+  long long p = (long long)z * g.ld + x;
   int sx, sz, dist;
   if (frame2(g, x, z, sx, sz, dist)) {
     float w = habc_weight(h, 2, dist);
     float o1 = __ldg(a.txx + p), o2 = __ldg(a.tzz + p), o3 = __ldg(a.txz + p);
     if (sx != 0 && sz != 0) {
-      long long px = p + sx, pz = p + (long long)sz * g.nx;
+      long long px = p + sx, pz = p + (long long)sz * g.ld;
       float a1, a2, a3, b1, b2, b3;
       el_str_at<N>(g, c, dtx, dtz, vx, vz, a, m, x + sx, z, a1, a2, a3);
       el_str_at<N>(g, c, dtx, dtz, vx, vz, a, m, x, z + sz, b1, b2, b3);
@@ -151,7 +151,7 @@ __global__ void __launch_bounds__(256) k_el_str(Geo2 g, Coef c, float dtx, float
                           higdon_side(h, b3, o3, __ldg(a.txz + pz)));
     } else {
       int xn = x + sx, zn = z + sz;
-      long long pn = (long long)zn * g.nx + xn;
+      long long pn = (long long)zn * g.ld + xn;
       float n1, n2, n3;
       el_str_at<N>(g, c, dtx, dtz, vx, vz, a, m, xn, zn, n1, n2, n3);
       sxx = higdon_edge(w, sxx, higdon_side(h, n1, o1, __ldg(a.txx + pn)));
@@ -174,11 +174,11 @@ __device__ __forceinline__ void ac_vel_at(const Geo2& g, const Coef& c, float dt
                                           const float* __restrict__ vz0, const float* __restrict__ bx,
                                           const float* __restrict__ bz, int x, int z, float& ux,
                                           float& uz) {
-  long long p = (long long)z * g.nx + x;
+  long long p = (long long)z * g.ld + x;
   float vx = __ldg(vx0 + p), vz = __ldg(vz0 + p);
   if (interior2(g, x, z)) {
     float dpdx = dm<N>(pr, p, 1, c);
-    float dpdz = dp<N>(pr, p, g.nx, c);
+    float dpdz = dp<N>(pr, p, g.ld, c);
     vx = __fmaf_rn(__fmul_rn(__ldg(bx + p), dtx), dpdx, vx);
     vz = __fmaf_rn(__fmul_rn(__ldg(bz + p), dtz), dpdz, vz);
   }
@@ -201,13 +201,13 @@ __global__ void __launch_bounds__(256) k_ac_vel(Geo2 g, Coef c, float dtx, float
   p0 += so; vx0 += so; vz0 += so;
   float ux, uz;
   ac_vel_at<N>(g, c, dtx, dtz, p0, vx0, vz0, bx, bz, x, z, ux, uz);
-  long long p = (long long)z * g.nx + x;
+  long long p = (long long)z * g.ld + x;
   int sx, sz, dist;
   if (frame2(g, x, z, sx, sz, dist)) {
     float wx = habc_weight(h, 0, dist), wz = habc_weight(h, 1, dist);
     float fox = __ldg(vx0 + p), foz = __ldg(vz0 + p);
     if (sx != 0 && sz != 0) {
-      long long px = p + sx, pz = p + (long long)sz * g.nx;
+      long long px = p + sx, pz = p + (long long)sz * g.ld;
       float ax, az, bxv, bzv;
       ac_vel_at<N>(g, c, dtx, dtz, p0, vx0, vz0, bx, bz, x + sx, z, ax, az);
       ac_vel_at<N>(g, c, dtx, dtz, p0, vx0, vz0, bx, bz, x, z + sz, bxv, bzv);
@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(256) k_ac_vel(Geo2 g, Coef c, float dtx, float
                          higdon_side(h, bzv, foz, __ldg(vz0 + pz)));
     } else {
       int xn = x + sx, zn = z + sz;
-      long long pn = (long long)zn * g.nx + xn;
+      long long pn = (long long)zn * g.ld + xn;
       float nx_, nz_;
       ac_vel_at<N>(g, c, dtx, dtz, p0, vx0, vz0, bx, bz, xn, zn, nx_, nz_);
       ux = higdon_edge(wx, ux, higdon_side(h, nx_, fox, __ldg(vx0 + pn)));
@@ -233,11 +233,11 @@ __device__ __forceinline__ float ac_prs_at(const Geo2& g, const Coef& c, float d
                                            const float* __restrict__ vx, const float* __restrict__ vz,
                                            const float* __restrict__ p0,
                                            const float* __restrict__ kappa, int x, int z) {
-  long long p = (long long)z * g.nx + x;
+  long long p = (long long)z * g.ld + x;
   float v = __ldg(p0 + p);
   if (interior2(g, x, z)) {
     float dvxdx = dp<N>(vx, p, 1, c);
-    float dvzdz = dm<N>(vz, p, g.nx, c);
+    float dvzdz = dm<N>(vz, p, g.ld, c);
     v = __fmaf_rn(__ldg(kappa + p), __fmaf_rn(dvxdx, dtx, __fmul_rn(dvzdz, dtz)), v);
   }
   return v;
@@ -258,20 +258,20 @@ __global__ void __launch_bounds__(256) k_ac_prs(Geo2 g, Coef c, float dtx, float
   const float* vx = vx1 + so;
   const float* vz = vz1 + so;
   float u = ac_prs_at<N>(g, c, dtx, dtz, vx, vz, p0, kappa, x, z);
-  long long p = (long long)z * g.nx + x;
+  long long p = (long long)z * g.ld + x;
   int sx, sz, dist;
   if (frame2(g, x, z, sx, sz, dist)) {
     float w = habc_weight(h, 2, dist);
     float fo = __ldg(p0 + p);
     if (sx != 0 && sz != 0) {
-      long long px = p + sx, pz = p + (long long)sz * g.nx;
+      long long px = p + sx, pz = p + (long long)sz * g.ld;
       float a = ac_prs_at<N>(g, c, dtx, dtz, vx, vz, p0, kappa, x + sx, z);
       float b = ac_prs_at<N>(g, c, dtx, dtz, vx, vz, p0, kappa, x, z + sz);
       u = higdon_corner(w, u, higdon_side(h, a, fo, __ldg(p0 + px)),
                         higdon_side(h, b, fo, __ldg(p0 + pz)));
     } else {
       int xn = x + sx, zn = z + sz;
-      long long pn = (long long)zn * g.nx + xn;
+      long long pn = (long long)zn * g.ld + xn;
       float a = ac_prs_at<N>(g, c, dtx, dtz, vx, vz, p0, kappa, xn, zn);
       u = higdon_edge(w, u, higdon_side(h, a, fo, __ldg(p0 + pn)));
     }
@@ -292,11 +292,11 @@ template <int N>
 __device__ __forceinline__ float sc_at(const Geo2& g, const D2Coef& c, const float* __restrict__ u1,
                                        const float* __restrict__ u0, const float* __restrict__ c2,
                                        int x, int z) {
-  long long p = (long long)z * g.nx + x;
+  long long p = (long long)z * g.ld + x;
   float uc = __ldg(u1 + p);
   if (!interior2(g, x, z)) return uc;
   float lap = __fmul_rn(c.two_c0, uc);
-  const long long s = g.nx;
+  const long long s = g.ld;
 #pragma unroll
   for (int l = 1; l <= N; ++l) {
     float nb = __fadd_rn(__fadd_rn(__fadd_rn(__ldg(u1 + p + l), __ldg(u1 + p - l)),
@@ -317,20 +317,20 @@ __global__ void __launch_bounds__(256) k_sc_step(Geo2 g, D2Coef c, HabcDev h,
   int z = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= g.nx || z >= g.nz) return;
   float u = sc_at<N>(g, c, u1, u0, c2, x, z);
-  long long p = (long long)z * g.nx + x;
+  long long p = (long long)z * g.ld + x;
   int sx, sz, dist;
   if (frame2(g, x, z, sx, sz, dist)) {
     float w = habc_weight(h, 2, dist);
     float fo = __ldg(u1 + p);
     if (sx != 0 && sz != 0) {
-      long long px = p + sx, pz = p + (long long)sz * g.nx;
+      long long px = p + sx, pz = p + (long long)sz * g.ld;
       float a = sc_at<N>(g, c, u1, u0, c2, x + sx, z);
       float b = sc_at<N>(g, c, u1, u0, c2, x, z + sz);
       u = higdon_corner(w, u, higdon_side(h, a, fo, __ldg(u1 + px)),
                         higdon_side(h, b, fo, __ldg(u1 + pz)));
     } else {
       int xn = x + sx, zn = z + sz;
-      long long pn = (long long)zn * g.nx + xn;
+      long long pn = (long long)zn * g.ld + xn;
       float a = sc_at<N>(g, c, u1, u0, c2, xn, zn);
       u = higdon_edge(w, u, higdon_side(h, a, fo, __ldg(u1 + pn)));
     }

@@ -55,7 +55,7 @@ class Stats(C.Structure):
     _fields_ = [("kernel_time_s", C.c_double), ("cell_updates", C.c_double),
                 ("alg_bytes", C.c_double), ("n_shots", C.c_int32), ("gpu_launches", C.c_int32),
                 ("kernel", C.c_int32), ("status", C.c_int32), ("sweep_ms", C.c_double),
-                ("sweep_launches", C.c_int32), ("reserved", C.c_int32)]
+                ("sweep_launches", C.c_int32), ("sweep_config", C.c_int32)]
 
 
 class FomoError(RuntimeError):

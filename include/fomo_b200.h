@@ -107,7 +107,7 @@ typedef struct fomo_stats {
   double sweep_ms;      /* FOMO_F_PROFILE: mean device time of one step's sweep    */
                         /* kernel(s) over a window of steps, else 0               */
   int32_t sweep_launches; /* sweep kernels per step                               */
-  int32_t reserved;
+  int32_t sweep_config;   /* single-sweep: variant*1000000 + strip*1000 + z-segments */
 } fomo_stats;
 
 /* ---- context ---------------------------------------------------------- */

@@ -15,8 +15,17 @@ pytestmark = pytest.mark.gpu
 KERNELS = [1, 2]  # two-phase, single-sweep
 
 
-def _kernel_ok(fomo, kernel):
-    return True
+SWEEP_CONFIGS = ["0,112,3", "1,144,1", "2,80,2", "2,20,4", "3,112,2", "0,64,1"]  # variant,TX,CTAs per SM
+
+
+@pytest.fixture
+def sweep_config(monkeypatch):
+    def pin(cfg):
+        if cfg:
+            monkeypatch.setenv("FOMO_SWEEP_CONFIG", cfg)
+        else:
+            monkeypatch.delenv("FOMO_SWEEP_CONFIG", raising=False)
+    return pin
 
 
 def _vacuum_top(vp, *others):
@@ -104,6 +113,34 @@ def test_elastic2d_bitwise_vs_oracle(fomo, oracle, fd_order, kernel):
                            rz=rz, wavelet=np.repeat(w.reshape(1, -1), 2, axis=0), nbc=nbc,
                            fd_order=fd_order, prec=64)
     assert rel_l2(r.seis_vz, o64["seis_vz"][:, :, 0]) < 1e-5
+
+
+@pytest.mark.parametrize("cfg", SWEEP_CONFIGS)
+@pytest.mark.parametrize("fd_order", [2, 6, 10])
+def test_elastic_single_sweep_configs_bitwise(fomo, oracle, sweep_config, cfg, fd_order):
+    """Every strip width / z-segmentation of the single-sweep kernel, including
+    segment boundaries inside the HABC bands, equals the oracle bit for bit."""
+    from fomo_b200.synthetic import layered_elastic
+
+    sweep_config(cfg)
+    vp, vs, rho = layered_elastic(150, 131, n_layers=6, seed=12)
+    vp, vs, rho = _vacuum_top(vp, vs, rho)
+    nt, nbc = 140, 9
+    rx = np.arange(1, 151, 7)
+    rz = np.full(rx.size, 3)
+    M = fd_order // 2
+    fin = np.zeros((150 + 2 * (nbc + M), 131 + 2 * (nbc + M), 5, 2), np.float32, order="F")
+    sx = np.array([[20], [131]])
+    sz = np.array([[4], [120]])
+    r = fomo.elastic2d_batch(vp, vs, rho, 5.0, 5e-4, nt, 20.0, sx=sx, sz=sz, rx=rx, rz=rz,
+                             nbc=nbc, fd_order=fd_order, kernel=2, final_state=fin)
+    w = fomo.ricker_wavelet(20.0, 5e-4, nt)
+    o = oracle.elastic2d(vp, vs, rho, 5.0, 5e-4, nt, sx=sx.T, sz=sz.T, rx=rx, rz=rz,
+                         wavelet=w.reshape(1, -1), nbc=nbc, fd_order=fd_order, n_shots=2,
+                         final=True)
+    assert np.array_equal(r.seis_vx, o["seis_vx"])
+    assert np.array_equal(r.seis_vz, o["seis_vz"])
+    assert np.array_equal(fin, o["final"])
 
 
 @pytest.mark.parametrize("kernel", KERNELS)
