@@ -35,6 +35,16 @@ WORKLOAD = ("elastic2d_batch fp32: 32 shots, 1000x500 grid (padded 1170x670), dh
             "nt 3000, fd_order 10, nbc 80, 12 seeded layers, 500 receivers, 20 Hz Ricker")
 
 
+def _traffic():
+    """DRAM bytes per launch of the sweep kernel from the committed ncu summary."""
+    p = ROOT / "profiles" / "traffic.txt"
+    if p.exists():
+        for line in p.read_text().splitlines():
+            if line.startswith("dram_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    return None
+
+
 def _peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -292,7 +302,8 @@ def ours(args, cfg):
         "e2e": {"value": ns * world / (e2e_ms * 1e-3), "unit": "shots/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "traffic": None,
+                     "frac": (achieved / peak) if achieved else None,
+                     "traffic": _traffic() if st.kernel == 2 else None,
                      "peak_kind": peak_kind,
                      "kernel": f"time-step sweep ({st.sweep_launches} kernel(s)/step)",
                      "alg_bytes_per_launch": alg_step / max(st.sweep_launches, 1),
