@@ -578,6 +578,403 @@ int run_scalar2d(int nx, int nz, const float* vp, float dh, float dt, int nt, in
   return 0;
 }
 
+
+// ===========================================================================
+// 3D: pad_array_3d.jl:8-89, elastic3d/medium.jl:31-123, acoustic3d/medium.jl:33-63,
+// habc_3d.jl:23-55, kernels_3d.jl:172-244 (Higdon averaged over the active
+// directions, evaluated two-pass from read-only inputs), update kernels of
+// elastic3d/update_*.jl and acoustic3d/update_*.jl, loops elastic3d.jl:122-162
+// and acoustic3d.jl:134-185.
+// ===========================================================================
+struct G3 {
+  int nx, ny, nz;
+  inline size_t at(int i, int j, int k) const {
+    return (size_t)(i - 1) + (size_t)nx * ((size_t)(j - 1) + (size_t)ny * (size_t)(k - 1));
+  }
+  size_t n() const { return (size_t)nx * ny * nz; }
+};
+
+template <class T>
+std::vector<T> pad_array3(const float* d, int nx, int ny, int nz, int pad) {
+  G3 g{nx + 2 * pad, ny + 2 * pad, nz + 2 * pad};
+  std::vector<T> r(g.n());
+  for (int k = 1; k <= g.nz; ++k) {
+    int kk = std::min(std::max(k - pad, 1), nz);
+    for (int j = 1; j <= g.ny; ++j) {
+      int jj = std::min(std::max(j - pad, 1), ny);
+      for (int i = 1; i <= g.nx; ++i) {
+        int ii = std::min(std::max(i - pad, 1), nx);
+        r[g.at(i, j, k)] = (T)d[(size_t)(ii - 1) + (size_t)nx * ((jj - 1) + (size_t)ny * (kk - 1))];
+      }
+    }
+  }
+  return r;
+}
+
+// pad_array_3d.jl:37-89: bx (i-1,i; row 1 copies 2), by (j-1,j; copies 2), bz (k,k+1; last copies)
+template <class T>
+void buoyancy3(const G3& g, const std::vector<T>& rho, std::vector<T>& bx, std::vector<T>& by,
+               std::vector<T>& bz) {
+  bx.assign(g.n(), T(0));
+  by.assign(g.n(), T(0));
+  bz.assign(g.n(), T(0));
+  for (int k = 1; k <= g.nz; ++k)
+    for (int j = 1; j <= g.ny; ++j) {
+      for (int i = 2; i <= g.nx; ++i) bx[g.at(i, j, k)] = harm2(rho[g.at(i - 1, j, k)], rho[g.at(i, j, k)]);
+      bx[g.at(1, j, k)] = bx[g.at(2, j, k)];
+    }
+  for (int k = 1; k <= g.nz; ++k) {
+    for (int j = 2; j <= g.ny; ++j)
+      for (int i = 1; i <= g.nx; ++i) by[g.at(i, j, k)] = harm2(rho[g.at(i, j - 1, k)], rho[g.at(i, j, k)]);
+    for (int i = 1; i <= g.nx; ++i) by[g.at(i, 1, k)] = by[g.at(i, 2, k)];
+  }
+  for (int k = 1; k <= g.nz - 1; ++k)
+    for (int j = 1; j <= g.ny; ++j)
+      for (int i = 1; i <= g.nx; ++i) bz[g.at(i, j, k)] = harm2(rho[g.at(i, j, k)], rho[g.at(i, j, k + 1)]);
+  for (int j = 1; j <= g.ny; ++j)
+    for (int i = 1; i <= g.nx; ++i) bz[g.at(i, j, g.nz)] = bz[g.at(i, j, g.nz - 1)];
+}
+
+// elastic3d/medium.jl:73-123
+template <class T>
+void elastic_params3(const G3& g, const std::vector<T>& vp, const std::vector<T>& vs,
+                     const std::vector<T>& rho, std::vector<T>& lam, std::vector<T>& l2m,
+                     std::vector<T>& mxy, std::vector<T>& mxz, std::vector<T>& myz) {
+  size_t n = g.n();
+  std::vector<T> mu(n);
+  lam.resize(n);
+  l2m.resize(n);
+  for (size_t q = 0; q < n; ++q) {
+    mu[q] = rho[q] * (vs[q] * vs[q]);
+    lam[q] = rho[q] * (vp[q] * vp[q]) - T(2) * mu[q];
+    l2m[q] = lam[q] + T(2) * mu[q];
+  }
+  mxy.assign(n, T(0));
+  mxz.assign(n, T(0));
+  myz.assign(n, T(0));
+  for (int k = 1; k <= g.nz; ++k)
+    for (int j = 2; j <= g.ny; ++j)
+      for (int i = 2; i <= g.nx; ++i)
+        mxy[g.at(i, j, k)] = harm4(mu[g.at(i - 1, j - 1, k)], mu[g.at(i, j - 1, k)], mu[g.at(i - 1, j, k)],
+                                   mu[g.at(i, j, k)]);
+  for (int k = 1; k <= g.nz; ++k)
+    for (int j = 1; j <= g.ny; ++j) mxy[g.at(1, j, k)] = mxy[g.at(2, j, k)];
+  for (int k = 1; k <= g.nz; ++k)
+    for (int i = 1; i <= g.nx; ++i) mxy[g.at(i, 1, k)] = mxy[g.at(i, 2, k)];
+  for (int k = 1; k <= g.nz - 1; ++k)
+    for (int j = 1; j <= g.ny; ++j)
+      for (int i = 2; i <= g.nx; ++i)
+        mxz[g.at(i, j, k)] = harm4(mu[g.at(i - 1, j, k)], mu[g.at(i, j, k)], mu[g.at(i - 1, j, k + 1)],
+                                   mu[g.at(i, j, k + 1)]);
+  for (int k = 1; k <= g.nz; ++k)
+    for (int j = 1; j <= g.ny; ++j) mxz[g.at(1, j, k)] = mxz[g.at(2, j, k)];
+  for (int j = 1; j <= g.ny; ++j)
+    for (int i = 1; i <= g.nx; ++i) mxz[g.at(i, j, g.nz)] = mxz[g.at(i, j, g.nz - 1)];
+  for (int k = 1; k <= g.nz - 1; ++k)
+    for (int j = 2; j <= g.ny; ++j)
+      for (int i = 1; i <= g.nx; ++i)
+        myz[g.at(i, j, k)] = harm4(mu[g.at(i, j - 1, k)], mu[g.at(i, j, k)], mu[g.at(i, j - 1, k + 1)],
+                                   mu[g.at(i, j, k + 1)]);
+  for (int k = 1; k <= g.nz; ++k)
+    for (int i = 1; i <= g.nx; ++i) myz[g.at(i, 1, k)] = myz[g.at(i, 2, k)];
+  for (int j = 1; j <= g.ny; ++j)
+    for (int i = 1; i <= g.nx; ++i) myz[g.at(i, j, g.nz)] = myz[g.at(i, j, g.nz - 1)];
+}
+
+// habc_3d.jl:23-55: same q, qt, qxt as 2D; four ramps (offsets 0, .25, .5, .75)
+template <class T>
+struct Habc3 {
+  int nbc;
+  T q, qt, qxt;
+  std::vector<T> wtab[4];
+};
+
+template <class T>
+Habc3<T> init_habc3(int pad, float v_ref, float dt, float dh) {
+  Habc<T> h2 = init_habc<T>(pad, v_ref, dt, dh);
+  Habc3<T> h;
+  h.nbc = h2.nbc;
+  h.q = h2.q;
+  h.qt = h2.qt;
+  h.qxt = h2.qxt;
+  const double offs[4] = {0.0, 0.25, 0.5, 0.75};
+  for (int k = 0; k < 4; ++k) {
+    h.wtab[k].resize(pad + 2);
+    for (int d = 0; d < pad + 2; ++d) {
+      double w = ((double)d - offs[k]) / (double)(pad - 1);
+      h.wtab[k][d] = (T)std::min(std::max(w, 0.0), 1.0);
+    }
+  }
+  return h;
+}
+
+struct FramePt3 {
+  size_t idx;
+  int8_t sx, sy, sz;
+  int dist;
+};
+
+std::vector<FramePt3> frame_points3(const G3& g, int nbc) {
+  std::vector<FramePt3> f;
+  for (int k = 2; k <= g.nz - 1; ++k)
+    for (int j = 2; j <= g.ny - 1; ++j)
+      for (int i = 2; i <= g.nx - 1; ++i) {
+        int8_t sx = i <= nbc + 1 ? 1 : (i >= g.nx - nbc ? -1 : 0);
+        int8_t sy = j <= nbc + 1 ? 1 : (j >= g.ny - nbc ? -1 : 0);
+        int8_t sz = k <= nbc + 1 ? 1 : (k >= g.nz - nbc ? -1 : 0);
+        if (!sx && !sy && !sz) continue;
+        int d = std::min(std::min(std::min(i - 1, g.nx - i), std::min(j - 1, g.ny - j)),
+                         std::min(k - 1, g.nz - k));
+        f.push_back(FramePt3{g.at(i, j, k), sx, sy, sz, d});
+      }
+  return f;
+}
+
+template <class T>
+void habc3_det(const G3& g, const Habc3<T>& h, const std::vector<FramePt3>& fr, int kind, T* f,
+               const T* fo, std::vector<T>& scr) {
+  scr.resize(fr.size());
+  const long n = (long)fr.size();
+  const size_t sxs = 1, sys = (size_t)g.nx, szs = (size_t)g.nx * g.ny;
+#pragma omp parallel for schedule(static)
+  for (long q = 0; q < n; ++q) {
+    const FramePt3& p = fr[q];
+    T sum = 0;
+    int nd = 0;
+    if (p.sx) {
+      size_t nb = p.sx > 0 ? p.idx + sxs : p.idx - sxs;
+      sum = sum + higdon_side(h.q, h.qt, h.qxt, f[nb], fo[p.idx], fo[nb]);
+      ++nd;
+    }
+    if (p.sy) {
+      size_t nb = p.sy > 0 ? p.idx + sys : p.idx - sys;
+      sum = sum + higdon_side(h.q, h.qt, h.qxt, f[nb], fo[p.idx], fo[nb]);
+      ++nd;
+    }
+    if (p.sz) {
+      size_t nb = p.sz > 0 ? p.idx + szs : p.idx - szs;
+      sum = sum + higdon_side(h.q, h.qt, h.qxt, f[nb], fo[p.idx], fo[nb]);
+      ++nd;
+    }
+    const std::vector<T>& t = h.wtab[kind];
+    T w = p.dist < (int)t.size() ? t[p.dist] : T(1);
+    scr[q] = fmaT(w, f[p.idx], ((T(1) - w) * sum) / (T)nd);
+  }
+#pragma omp parallel for schedule(static)
+  for (long q = 0; q < n; ++q) f[fr[q].idx] = scr[q];
+}
+
+template <class T>
+int run_acoustic3d(int nx, int ny, int nz, const float* vp, const float* rho, float dh, float dt,
+                   int nt, int nbc, int fd_order, float v_ref, int n_src, const int32_t* sx,
+                   const int32_t* sy, const int32_t* sz, const float* wavelet, int n_rec,
+                   const int32_t* rx, const int32_t* ry, const int32_t* rz, T* svx, T* svy, T* svz,
+                   int snap_interval, int snap_plane, int snap_index, T* snaps, T* final_fields) {
+  int N = order_to_N(fd_order);
+  if (N < 0) return -2;
+  int M = N, pad = nbc + M;
+  if (pad < 2) return -2;
+  G3 g{nx + 2 * pad, ny + 2 * pad, nz + 2 * pad};
+  std::vector<T> vpp = pad_array3<T>(vp, nx, ny, nz, pad), rhop = pad_array3<T>(rho, nx, ny, nz, pad);
+  std::vector<T> bx, by, bz, kap(g.n());
+  buoyancy3(g, rhop, bx, by, bz);
+  for (size_t q = 0; q < g.n(); ++q) kap[q] = rhop[q] * (vpp[q] * vpp[q]);
+  Habc3<T> h = init_habc3<T>(pad, v_ref, dt, dh);
+  std::vector<FramePt3> fr = frame_points3(g, h.nbc);
+  Coef<T> c = coef<T>(fd_order);
+  const T dtdh = (T)dt / (T)dh;
+  const size_t n = g.n(), sy_ = (size_t)g.nx, sz_ = (size_t)g.nx * g.ny;
+  std::vector<T> vx(n, T(0)), vy(n, T(0)), vz(n, T(0)), p(n, T(0)), o1, o2, o3, scr;
+  for (int it = 1; it <= nt; ++it) {
+    o1 = vx;
+    o2 = vy;
+    o3 = vz;
+#pragma omp parallel for schedule(static)
+    for (int k = M + 1; k <= g.nz - M; ++k)
+      for (int j = M + 1; j <= g.ny - M; ++j)
+        for (int i = M + 1; i <= g.nx - M; ++i) {
+          size_t q = g.at(i, j, k);
+          T dx = 0, dy = 0, dz = 0;
+          for (int l = 1; l <= N; ++l) {
+            T a = c.a[l - 1];
+            dx = fmaT(a, p[q + (l - 1)] - p[q - l], dx);
+            dy = fmaT(a, p[q + (l - 1) * sy_] - p[q - l * sy_], dy);
+            dz = fmaT(a, p[q + l * sz_] - p[q - (l - 1) * sz_], dz);
+          }
+          vx[q] = fmaT(bx[q] * dtdh, dx, vx[q]);
+          vy[q] = fmaT(by[q] * dtdh, dy, vy[q]);
+          vz[q] = fmaT(bz[q] * dtdh, dz, vz[q]);
+        }
+    habc3_det(g, h, fr, 0, vx.data(), o1.data(), scr);
+    habc3_det(g, h, fr, 1, vy.data(), o2.data(), scr);
+    habc3_det(g, h, fr, 2, vz.data(), o3.data(), scr);
+    o1 = p;
+#pragma omp parallel for schedule(static)
+    for (int k = M + 1; k <= g.nz - M; ++k)
+      for (int j = M + 1; j <= g.ny - M; ++j)
+        for (int i = M + 1; i <= g.nx - M; ++i) {
+          size_t q = g.at(i, j, k);
+          T dx = 0, dy = 0, dz = 0;
+          for (int l = 1; l <= N; ++l) {
+            T a = c.a[l - 1];
+            dx = fmaT(a, vx[q + l] - vx[q - (l - 1)], dx);
+            dy = fmaT(a, vy[q + l * sy_] - vy[q - (l - 1) * sy_], dy);
+            dz = fmaT(a, vz[q + (l - 1) * sz_] - vz[q - l * sz_], dz);
+          }
+          p[q] = fmaT(kap[q] * dtdh, (dx + dy) + dz, p[q]);
+        }
+    habc3_det(g, h, fr, 3, p.data(), o1.data(), scr);
+    for (int s = 0; s < n_src; ++s)
+      p[g.at(sx[s] + pad, sy[s] + pad, sz[s] + pad)] += (T)wavelet[(size_t)s + (size_t)n_src * (it - 1)];
+    for (int r = 0; r < n_rec; ++r) {
+      size_t q = g.at(rx[r] + pad, ry[r] + pad, rz[r] + pad), o = (size_t)r + (size_t)n_rec * (it - 1);
+      svx[o] = vx[q];
+      svy[o] = vy[q];
+      svz[o] = vz[q];
+    }
+    if (snaps && snap_interval > 0 && it % snap_interval == 0) {
+      T* out = snaps + (size_t)(it / snap_interval - 1) * (snap_plane == 1 ? (size_t)nx * ny
+                                                          : snap_plane == 2 ? (size_t)ny * nz
+                                                                            : (size_t)nx * nz);
+      int si = snap_index + pad;
+      if (snap_plane == 0)
+        for (int k = 1; k <= nz; ++k)
+          for (int i = 1; i <= nx; ++i) out[(i - 1) + (size_t)nx * (k - 1)] = p[g.at(i + pad, si, k + pad)];
+      else if (snap_plane == 1)
+        for (int j = 1; j <= ny; ++j)
+          for (int i = 1; i <= nx; ++i) out[(i - 1) + (size_t)nx * (j - 1)] = p[g.at(i + pad, j + pad, si)];
+      else
+        for (int k = 1; k <= nz; ++k)
+          for (int j = 1; j <= ny; ++j) out[(j - 1) + (size_t)ny * (k - 1)] = p[g.at(si, j + pad, k + pad)];
+    }
+  }
+  if (final_fields) {
+    std::copy(vx.begin(), vx.end(), final_fields);
+    std::copy(vy.begin(), vy.end(), final_fields + n);
+    std::copy(vz.begin(), vz.end(), final_fields + 2 * n);
+    std::copy(p.begin(), p.end(), final_fields + 3 * n);
+  }
+  return 0;
+}
+
+template <class T>
+int run_elastic3d(int nx, int ny, int nz, const float* vp, const float* vs, const float* rho,
+                  float dh, float dt, int nt, int nbc, int fd_order, float v_ref, int n_src,
+                  const int32_t* sx, const int32_t* sy, const int32_t* sz, const float* wavelet,
+                  int n_rec, const int32_t* rx, const int32_t* ry, const int32_t* rz, T* svx,
+                  T* svy, T* svz, int snap_interval, int snap_plane, int snap_index, T* snaps,
+                  T* final_fields) {
+  int N = order_to_N(fd_order);
+  if (N < 0) return -2;
+  int M = N, pad = nbc + M;
+  if (pad < 2) return -2;
+  G3 g{nx + 2 * pad, ny + 2 * pad, nz + 2 * pad};
+  std::vector<T> vpp = pad_array3<T>(vp, nx, ny, nz, pad), vsp = pad_array3<T>(vs, nx, ny, nz, pad),
+                 rhop = pad_array3<T>(rho, nx, ny, nz, pad);
+  std::vector<T> bx, by, bz, lam, l2m, mxy, mxz, myz;
+  buoyancy3(g, rhop, bx, by, bz);
+  elastic_params3(g, vpp, vsp, rhop, lam, l2m, mxy, mxz, myz);
+  Habc3<T> h = init_habc3<T>(pad, v_ref, dt, dh);
+  std::vector<FramePt3> fr = frame_points3(g, h.nbc);
+  Coef<T> c = coef<T>(fd_order);
+  const T dtdh = (T)dt / (T)dh;
+  const size_t n = g.n(), Y = (size_t)g.nx, Z = (size_t)g.nx * g.ny;
+  std::vector<T> F[9], O[9], scr;  // vx vy vz txx tyy tzz txy txz tyz
+  for (auto& v : F) v.assign(n, T(0));
+  for (int it = 1; it <= nt; ++it) {
+    for (int f = 0; f < 3; ++f) O[f] = F[f];
+    T *vx = F[0].data(), *vy = F[1].data(), *vz = F[2].data();
+    const T *txx = F[3].data(), *tyy = F[4].data(), *tzz = F[5].data(), *txy = F[6].data(),
+            *txz = F[7].data(), *tyz = F[8].data();
+#pragma omp parallel for schedule(static)
+    for (int k = M + 1; k <= g.nz - M; ++k)
+      for (int j = M + 1; j <= g.ny - M; ++j)
+        for (int i = M + 1; i <= g.nx - M; ++i) {
+          size_t q = g.at(i, j, k);
+          T a1 = 0, a2 = 0, a3 = 0, b1 = 0, b2 = 0, b3 = 0, c1 = 0, c2 = 0, c3 = 0;
+          for (int l = 1; l <= N; ++l) {  // elastic3d/update_velocity.jl:211-237
+            T a = c.a[l - 1];
+            a1 = fmaT(a, txx[q + (l - 1)] - txx[q - l], a1);          // dtxxdx
+            a2 = fmaT(a, txy[q + l * Y] - txy[q - (l - 1) * Y], a2);  // dtxydy
+            a3 = fmaT(a, txz[q + (l - 1) * Z] - txz[q - l * Z], a3);  // dtxzdz
+            b1 = fmaT(a, txy[q + l] - txy[q - (l - 1)], b1);          // dtxydx
+            b2 = fmaT(a, tyy[q + (l - 1) * Y] - tyy[q - l * Y], b2);  // dtyydy
+            b3 = fmaT(a, tyz[q + (l - 1) * Z] - tyz[q - l * Z], b3);  // dtyzdz
+            c1 = fmaT(a, txz[q + l] - txz[q - (l - 1)], c1);          // dtxzdx
+            c2 = fmaT(a, tyz[q + l * Y] - tyz[q - (l - 1) * Y], c2);  // dtyzdy
+            c3 = fmaT(a, tzz[q + l * Z] - tzz[q - (l - 1) * Z], c3);  // dtzzdz
+          }
+          vx[q] = fmaT(bx[q] * dtdh, (a1 + a2) + a3, vx[q]);
+          vy[q] = fmaT(by[q] * dtdh, (b1 + b2) + b3, vy[q]);
+          vz[q] = fmaT(bz[q] * dtdh, (c1 + c2) + c3, vz[q]);
+        }
+    habc3_det(g, h, fr, 0, vx, O[0].data(), scr);
+    habc3_det(g, h, fr, 1, vy, O[1].data(), scr);
+    habc3_det(g, h, fr, 2, vz, O[2].data(), scr);
+    for (int f = 3; f < 9; ++f) O[f] = F[f];
+    T *sxx = F[3].data(), *syy = F[4].data(), *szz = F[5].data(), *sxy = F[6].data(),
+      *sxz = F[7].data(), *syz = F[8].data();
+#pragma omp parallel for schedule(static)
+    for (int k = M + 1; k <= g.nz - M; ++k)
+      for (int j = M + 1; j <= g.ny - M; ++j)
+        for (int i = M + 1; i <= g.nx - M; ++i) {
+          size_t q = g.at(i, j, k);
+          T dxx = 0, dyy = 0, dzz = 0, dxy = 0, dyx = 0, dxz = 0, dzx = 0, dyz = 0, dzy = 0;
+          for (int l = 1; l <= N; ++l) {  // elastic3d/update_stress.jl:316-339
+            T a = c.a[l - 1];
+            dxx = fmaT(a, vx[q + l] - vx[q - (l - 1)], dxx);
+            dyy = fmaT(a, vy[q + l * Y] - vy[q - (l - 1) * Y], dyy);
+            dzz = fmaT(a, vz[q + (l - 1) * Z] - vz[q - l * Z], dzz);
+            dxy = fmaT(a, vx[q + (l - 1) * Y] - vx[q - l * Y], dxy);
+            dyx = fmaT(a, vy[q + (l - 1)] - vy[q - l], dyx);
+            dxz = fmaT(a, vx[q + l * Z] - vx[q - (l - 1) * Z], dxz);
+            dzx = fmaT(a, vz[q + (l - 1)] - vz[q - l], dzx);
+            dyz = fmaT(a, vy[q + l * Z] - vy[q - (l - 1) * Z], dyz);
+            dzy = fmaT(a, vz[q + (l - 1) * Y] - vz[q - l * Y], dzy);
+          }
+          const T lm = lam[q], l2 = l2m[q];
+          sxx[q] = fmaT(fmaT(lm, dzz, fmaT(lm, dyy, l2 * dxx)), dtdh, sxx[q]);
+          syy[q] = fmaT(fmaT(lm, dzz, fmaT(l2, dyy, lm * dxx)), dtdh, syy[q]);
+          szz[q] = fmaT(fmaT(l2, dzz, fmaT(lm, dyy, lm * dxx)), dtdh, szz[q]);
+          sxy[q] = fmaT(mxy[q] * (dxy + dyx), dtdh, sxy[q]);
+          sxz[q] = fmaT(mxz[q] * (dxz + dzx), dtdh, sxz[q]);
+          syz[q] = fmaT(myz[q] * (dyz + dzy), dtdh, syz[q]);
+        }
+    for (int f = 3; f < 9; ++f) habc3_det(g, h, fr, 3, F[f].data(), O[f].data(), scr);
+    for (int s = 0; s < n_src; ++s) {
+      size_t q = g.at(sx[s] + pad, sy[s] + pad, sz[s] + pad);
+      T w = (T)wavelet[(size_t)s + (size_t)n_src * (it - 1)];
+      sxx[q] += w;
+      syy[q] += w;
+      szz[q] += w;
+    }
+    for (int r = 0; r < n_rec; ++r) {
+      size_t q = g.at(rx[r] + pad, ry[r] + pad, rz[r] + pad), o = (size_t)r + (size_t)n_rec * (it - 1);
+      svx[o] = vx[q];
+      svy[o] = vy[q];
+      svz[o] = vz[q];
+    }
+    if (snaps && snap_interval > 0 && it % snap_interval == 0) {
+      T* out = snaps + (size_t)(it / snap_interval - 1) * (snap_plane == 1 ? (size_t)nx * ny
+                                                          : snap_plane == 2 ? (size_t)ny * nz
+                                                                            : (size_t)nx * nz);
+      int si = snap_index + pad;
+      if (snap_plane == 0)
+        for (int k = 1; k <= nz; ++k)
+          for (int i = 1; i <= nx; ++i) out[(i - 1) + (size_t)nx * (k - 1)] = vz[g.at(i + pad, si, k + pad)];
+      else if (snap_plane == 1)
+        for (int j = 1; j <= ny; ++j)
+          for (int i = 1; i <= nx; ++i) out[(i - 1) + (size_t)nx * (j - 1)] = vz[g.at(i + pad, j + pad, si)];
+      else
+        for (int k = 1; k <= nz; ++k)
+          for (int j = 1; j <= ny; ++j) out[(j - 1) + (size_t)ny * (k - 1)] = vz[g.at(si, j + pad, k + pad)];
+    }
+  }
+  if (final_fields)
+    for (int f = 0; f < 9; ++f) std::copy(F[f].begin(), F[f].end(), final_fields + f * n);
+  return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -692,6 +1089,44 @@ int oracle_scalar2d(int prec, int nx, int nz, const float* vp, float dh, float d
                           n_rec, rx, rz, (float*)seis_u, (float*)final_fields),
       run_scalar2d<double>(nx, nz, vp, dh, dt, nt, nbc, fd_order, v_ref, n_src, sx, sz, wavelet,
                            n_rec, rx, rz, (double*)seis_u, (double*)final_fields));
+}
+
+
+int oracle_acoustic3d(int prec, int nx, int ny, int nz, const float* vp, const float* rho, float dh,
+                      float dt, int nt, int nbc, int fd_order, float v_ref, int n_src,
+                      const int32_t* sx, const int32_t* sy, const int32_t* sz, const float* wavelet,
+                      int n_rec, const int32_t* rx, const int32_t* ry, const int32_t* rz, void* svx,
+                      void* svy, void* svz, int snap_interval, int snap_plane, int snap_index,
+                      void* snaps, void* final_fields) {
+  return ORACLE_PREC_DISPATCH(
+      prec,
+      run_acoustic3d<float>(nx, ny, nz, vp, rho, dh, dt, nt, nbc, fd_order, v_ref, n_src, sx, sy,
+                            sz, wavelet, n_rec, rx, ry, rz, (float*)svx, (float*)svy, (float*)svz,
+                            snap_interval, snap_plane, snap_index, (float*)snaps,
+                            (float*)final_fields),
+      run_acoustic3d<double>(nx, ny, nz, vp, rho, dh, dt, nt, nbc, fd_order, v_ref, n_src, sx, sy,
+                             sz, wavelet, n_rec, rx, ry, rz, (double*)svx, (double*)svy,
+                             (double*)svz, snap_interval, snap_plane, snap_index, (double*)snaps,
+                             (double*)final_fields));
+}
+
+int oracle_elastic3d(int prec, int nx, int ny, int nz, const float* vp, const float* vs,
+                     const float* rho, float dh, float dt, int nt, int nbc, int fd_order,
+                     float v_ref, int n_src, const int32_t* sx, const int32_t* sy,
+                     const int32_t* sz, const float* wavelet, int n_rec, const int32_t* rx,
+                     const int32_t* ry, const int32_t* rz, void* svx, void* svy, void* svz,
+                     int snap_interval, int snap_plane, int snap_index, void* snaps,
+                     void* final_fields) {
+  return ORACLE_PREC_DISPATCH(
+      prec,
+      run_elastic3d<float>(nx, ny, nz, vp, vs, rho, dh, dt, nt, nbc, fd_order, v_ref, n_src, sx,
+                           sy, sz, wavelet, n_rec, rx, ry, rz, (float*)svx, (float*)svy,
+                           (float*)svz, snap_interval, snap_plane, snap_index, (float*)snaps,
+                           (float*)final_fields),
+      run_elastic3d<double>(nx, ny, nz, vp, vs, rho, dh, dt, nt, nbc, fd_order, v_ref, n_src, sx,
+                            sy, sz, wavelet, n_rec, rx, ry, rz, (double*)svx, (double*)svy,
+                            (double*)svz, snap_interval, snap_plane, snap_index, (double*)snaps,
+                            (double*)final_fields));
 }
 
 }  // extern "C"

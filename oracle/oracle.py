@@ -62,6 +62,17 @@ def lib():
         L.oracle_habc_apply_f32.restype = C.c_int
         L.oracle_habc_apply_f32.argtypes = [C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
                                             C.c_float, C.c_int, vp, vp]
+        a3 = [C.c_int, C.c_int, C.c_int, C.c_int]
+        L.oracle_acoustic3d.restype = C.c_int
+        L.oracle_acoustic3d.argtypes = a3 + [_f32p, _f32p, C.c_float, C.c_float, C.c_int, C.c_int,
+                                             C.c_int, C.c_float, C.c_int, _i32p, _i32p, _i32p,
+                                             _f32p, C.c_int, _i32p, _i32p, _i32p, vp, vp, vp,
+                                             C.c_int, C.c_int, C.c_int, vp, vp]
+        L.oracle_elastic3d.restype = C.c_int
+        L.oracle_elastic3d.argtypes = a3 + [_f32p, _f32p, _f32p, C.c_float, C.c_float, C.c_int,
+                                            C.c_int, C.c_int, C.c_float, C.c_int, _i32p, _i32p,
+                                            _i32p, _f32p, C.c_int, _i32p, _i32p, _i32p, vp, vp, vp,
+                                            C.c_int, C.c_int, C.c_int, vp, vp]
         L.oracle_set_threads.argtypes = [C.c_int]
         L.oracle_max_threads.restype = C.c_int
         _lib = L
@@ -179,6 +190,55 @@ def scalar2d(vp, dh, dt, nt, *, sx, sz, rx, rz, wavelet, nbc=50, fd_order=8, v_r
     if rc != 0:
         raise RuntimeError(f"oracle_scalar2d failed: {rc}")
     return dict(seis_u=su, final=fin)
+
+
+_PLANES = {"xz": 0, "xy": 1, "yz": 2}
+
+
+def _run3d(kind, vp, vs, rho, dh, dt, nt, sx, sy, sz, rx, ry, rz, wavelet, nbc, fd_order, v_ref,
+           snap_interval, snap_plane, snap_index, prec, final):
+    vp, rho = _f32(vp), _f32(rho)
+    nx, ny, nz = vp.shape
+    sx, sy, sz = (_i32(a).ravel(order="F") for a in (sx, sy, sz))
+    rx, ry, rz = (_i32(a).ravel(order="F") for a in (rx, ry, rz))
+    n_src, nrec = sx.size, rx.size
+    w = _f32(wavelet).reshape(n_src, nt, order="F")
+    T = _dt(prec)
+    seis = [np.zeros((nrec, nt), dtype=T, order="F") for _ in range(3)]
+    plane = _PLANES[str(snap_plane).lstrip(":")]
+    si = snap_index if snap_index > 0 else ny // 2
+    shp = {0: (nx, nz), 1: (nx, ny), 2: (ny, nz)}[plane]
+    nsnap = nt // snap_interval if snap_interval > 0 else 0
+    snaps = np.zeros(shp + (nsnap,), dtype=T, order="F") if nsnap else None
+    M = fd_order // 2
+    pad = nbc + M
+    nf = 9 if kind == "elastic" else 4
+    fin = (np.zeros((nx + 2 * pad, ny + 2 * pad, nz + 2 * pad, nf), dtype=T, order="F")
+           if final else None)
+    vr = default_v_ref(vp) if v_ref is None else float(v_ref)
+    common = (dh, dt, nt, nbc, fd_order, vr, n_src, np.asfortranarray(sx), np.asfortranarray(sy),
+              np.asfortranarray(sz), w, nrec, np.asfortranarray(rx), np.asfortranarray(ry),
+              np.asfortranarray(rz), _ptr(seis[0]), _ptr(seis[1]), _ptr(seis[2]), snap_interval,
+              plane, si, _ptr(snaps), _ptr(fin))
+    if kind == "elastic":
+        rc = lib().oracle_elastic3d(prec, nx, ny, nz, vp, _f32(vs), rho, *common)
+    else:
+        rc = lib().oracle_acoustic3d(prec, nx, ny, nz, vp, rho, *common)
+    if rc != 0:
+        raise RuntimeError(f"oracle_{kind}3d failed: {rc}")
+    return dict(seis_vx=seis[0], seis_vy=seis[1], seis_vz=seis[2], snaps=snaps, final=fin)
+
+
+def acoustic3d(vp, rho, dh, dt, nt, *, sx, sy, sz, rx, ry, rz, wavelet, nbc=50, fd_order=8,
+               v_ref=None, snap_interval=0, snap_plane="xz", snap_index=0, prec=32, final=False):
+    return _run3d("acoustic", vp, None, rho, dh, dt, nt, sx, sy, sz, rx, ry, rz, wavelet, nbc,
+                  fd_order, v_ref, snap_interval, snap_plane, snap_index, prec, final)
+
+
+def elastic3d(vp, vs, rho, dh, dt, nt, *, sx, sy, sz, rx, ry, rz, wavelet, nbc=50, fd_order=8,
+              v_ref=None, snap_interval=0, snap_plane="xz", snap_index=0, prec=32, final=False):
+    return _run3d("elastic", vp, vs, rho, dh, dt, nt, sx, sy, sz, rx, ry, rz, wavelet, nbc,
+                  fd_order, v_ref, snap_interval, snap_plane, snap_index, prec, final)
 
 
 def medium2d(kind, vp, vs, rho, pad):
