@@ -18,7 +18,8 @@ from . import _lib as L
 
 __all__ = [
     "ArgumentError", "acoustic2d", "acoustic2d_batch", "elastic2d", "elastic2d_batch",
-    "scalar2d", "ricker_wavelet", "get_fd_coefficients", "get_centered_d2",
+    "scalar2d", "acoustic3d", "elastic3d", "ricker_wavelet", "get_fd_coefficients",
+    "get_centered_d2",
 ]
 
 
@@ -400,6 +401,90 @@ def scalar2d(vp, dh, dt, nt, f0, *, sx, sz, rx, rz, nbc: int = 50, fd_order: int
     ctx.check(L.lib().fomo_scalar2d(ctx.handle, C.byref(g), _ptr(vp), C.byref(acq), _ptr(seis),
                                     C.byref(o), C.byref(st)))
     return Scalar2DResult(seis, Stats(st.kernel_time_s))
+
+
+# ---------------------------------------------------------------------------
+# 3D solvers: return (seis_vx, seis_vy, seis_vz, snaps) as the reference does
+# ---------------------------------------------------------------------------
+_PLANES = {"xz": 0, "xy": 1, "yz": 2}
+
+
+def _run3d(elastic, vp, vs, rho, dh, dt, nt, f0, sx, sy, sz, rx, ry, rz, nbc, fd_order,
+           snap_interval, snap_plane, snap_index, v_ref, wavelet, device, final_state):
+    vp, rho = _f32F(vp), _f32F(rho)
+    vs = _f32F(vs) if elastic else None
+    if vp.ndim != 3:
+        raise ArgumentError("3D models are (nx, ny, nz) arrays")
+    nx, ny, nz = vp.shape
+    plane = _PLANES.get(str(snap_plane).lstrip(":"))
+    if plane is None:
+        raise ArgumentError(f"snap_plane must be :xz, :xy or :yz, got {snap_plane}")
+    if fd_order not in _FD:
+        raise ValueError(f"Unsupported FD order: {fd_order}")
+    sxv, syv, szv = (_i32F(a).ravel() for a in (sx, sy, sz))
+    rxv, ryv, rzv = (_i32F(a).ravel() for a in (rx, ry, rz))
+    if not (sxv.size == syv.size == szv.size) or not (rxv.size == ryv.size == rzv.size):
+        raise ArgumentError("coordinate vectors differ in length")
+    for name, v, n in (("sx", sxv, nx), ("sy", syv, ny), ("sz", szv, nz), ("rx", rxv, nx),
+                       ("ry", ryv, ny), ("rz", rzv, nz)):
+        if not np.all((1 <= v) & (v <= n)):
+            raise ArgumentError(f"{name} out of range 1..{n}")
+    if snap_index == 0:
+        snap_index = ny // 2  # acoustic3d.jl:50-52 (ny÷2 for every plane)
+    dh, dt, f0 = np.float32(dh), np.float32(dt), np.float32(f0)
+    v_ref = _min_pos(vp) if v_ref is None else np.float32(v_ref)
+    w = _wavelet_row(wavelet, f0, dt, nt)
+    # every source fires the one Ricker row (acoustic3d.jl:64-66)
+    wm = np.asfortranarray(np.repeat(w[None, :], sxv.size, axis=0))
+    seis = [np.zeros((rxv.size, nt), dtype=np.float32, order="F") for _ in range(3)]
+    nsnap = nt // snap_interval if snap_interval > 0 else 0
+    shape = {0: (nx, nz), 1: (nx, ny), 2: (ny, nz)}[plane]
+    snaps = np.zeros(shape + (nsnap,), dtype=np.float32, order="F") if nsnap else None
+    st = L.Stats()
+    ctx = L.context(device)
+    g = L.Grid3D(nx, ny, nz, float(dh), float(dt), int(nt), int(nbc), int(fd_order), float(v_ref))
+    acq = L.Acq3D(sxv.size, _ptr(sxv), _ptr(syv), _ptr(szv), _ptr(wm), rxv.size, _ptr(rxv),
+                  _ptr(ryv), _ptr(rzv))
+    o = _opts(0, final_state)
+    if elastic:
+        rc = L.lib().fomo_elastic3d(ctx.handle, C.byref(g), _ptr(vp), _ptr(vs), _ptr(rho),
+                                    C.byref(acq), int(snap_interval), plane, int(snap_index),
+                                    _ptr(seis[0]), _ptr(seis[1]), _ptr(seis[2]), _ptr(snaps),
+                                    C.byref(o), C.byref(st))
+    else:
+        rc = L.lib().fomo_acoustic3d(ctx.handle, C.byref(g), _ptr(vp), _ptr(rho), C.byref(acq),
+                                     int(snap_interval), plane, int(snap_index), _ptr(seis[0]),
+                                     _ptr(seis[1]), _ptr(seis[2]), _ptr(snaps), C.byref(o),
+                                     C.byref(st))
+    ctx.check(rc)
+    return seis[0], seis[1], seis[2], _snap_list(snaps)
+
+
+def acoustic3d(vp, rho, dh, dt, nt, f0, *, sx, sy, sz, rx, ry, rz, nbc: int = 50,
+               fd_order: int = 8, snap_interval: int = 0, snap_plane="xz", snap_index: int = 0,
+               v_ref=None, wavelet=None, device: int = 0,
+               final_state: Optional[np.ndarray] = None):
+    """3D acoustic simulation (equations/acoustic3d/acoustic3d.jl:37-188).
+
+    Returns ``(seis_vx, seis_vy, seis_vz, snaps)``; snapshots hold p on the
+    chosen plane.  The HABC is the reference's 3D Higdon formula evaluated in
+    two passes (deterministic; the reference updates in place).
+    """
+    return _run3d(False, vp, None, rho, dh, dt, nt, f0, sx, sy, sz, rx, ry, rz, nbc, fd_order,
+                  snap_interval, snap_plane, snap_index, v_ref, wavelet, device, final_state)
+
+
+def elastic3d(vp, vs, rho, dh, dt, nt, f0, *, sx, sy, sz, rx, ry, rz, nbc: int = 50,
+              fd_order: int = 8, snap_interval: int = 0, snap_plane="xz", snap_index: int = 0,
+              v_ref=None, wavelet=None, device: int = 0,
+              final_state: Optional[np.ndarray] = None):
+    """3D elastic simulation (equations/elastic3d/elastic3d.jl:37-165).
+
+    Returns ``(seis_vx, seis_vy, seis_vz, snaps)``; sources inject into txx,
+    tyy and tzz; snapshots hold vz.
+    """
+    return _run3d(True, vp, vs, rho, dh, dt, nt, f0, sx, sy, sz, rx, ry, rz, nbc, fd_order,
+                  snap_interval, snap_plane, snap_index, v_ref, wavelet, device, final_state)
 
 
 def debug_medium2d(kind: str, vp, vs, rho, pad: int, dt=1.0, dh=1.0, device: int = 0):

@@ -96,3 +96,38 @@ def grf2d(nx: int, nz: int, dh: float, mean: float, std: float, corr: float, see
     f = np.real(np.fft.ifft2(np.fft.fft2(w) * np.sqrt(spec)))
     f = (f - f.mean()) / (f.std() + 1e-30)
     return np.asfortranarray(np.clip(mean + std * f, vmin, vmax).astype(np.float32))
+
+
+def grf3d(nx: int, ny: int, nz: int, dh: float, mean: float, std: float, corr: float, seed: int,
+          vmin: float, vmax: float) -> np.ndarray:
+    """3D Gaussian random field (the 2D recipe of grf2d over three axes)."""
+    rng = np.random.default_rng(seed)
+    w = rng.standard_normal((nx, ny, nz)).astype(np.float32)
+    k2 = None
+    for ax, n in enumerate((nx, ny, nz)):
+        k = (np.fft.fftfreq(n, d=dh) * 2 * np.pi).astype(np.float32)
+        shape = [1, 1, 1]
+        shape[ax] = n
+        k = k.reshape(shape) ** 2
+        k2 = k if k2 is None else k2 + k
+    spec = np.sqrt(np.exp(-k2 * np.float32(corr * corr / 4.0)))
+    f = np.real(np.fft.ifftn(np.fft.fftn(w) * spec)).astype(np.float32)
+    f = (f - f.mean()) / (f.std() + 1e-30)
+    return np.asfortranarray(np.clip(mean + std * f, vmin, vmax).astype(np.float32))
+
+
+def elastic3d_config(nx=400, ny=400, nz=300, seed=4, vmax=5000.0):
+    """Single-shot elastic 3D workload: 400x400x300, dh 10 m, dt 0.8 ms,
+    nt 2500, order 8, nbc 40; vp a 3D Gaussian random field (mean 3200, std
+    500, correlation 250 m) clipped to 1500..vmax so dt meets the 3D CFL bound,
+    vs = vp/1.8, Gardner rho, vacuum top plane; 12 Hz source at the centre at
+    z=10; 200x200 receiver grid (every 2nd x and y) at z=10."""
+    vp = grf3d(nx, ny, nz, 10.0, 3200.0, 500.0, 250.0, seed, 1500.0, vmax)
+    vs = np.asfortranarray((vp / np.float32(1.8)).astype(np.float32))
+    rho = np.asfortranarray(gardner_rho(vp))
+    for a in (vp, vs, rho):
+        a[:, :, 0] = 0.0
+    gx, gy = np.meshgrid(np.arange(1, nx + 1, 2), np.arange(1, ny + 1, 2), indexing="ij")
+    rx, ry = gx.ravel(order="F"), gy.ravel(order="F")
+    return dict(vp=vp, vs=vs, rho=rho, dh=10.0, dt=8e-4, nt=2500, f0=12.0, fd_order=8, nbc=40,
+                sx=[nx // 2], sy=[ny // 2], sz=[10], rx=rx, ry=ry, rz=np.full(rx.size, 10))

@@ -160,6 +160,45 @@ FOMO_API int fomo_elastic2d_batch(fomo_ctx* ctx, const fomo_grid2d* g, const flo
 FOMO_API int fomo_scalar2d(fomo_ctx* ctx, const fomo_grid2d* g, const float* vp, const fomo_acq* acq,
                   float* seis_u, const fomo_opts* opts, fomo_stats* stats);
 
+/* ---- 3D solvers ------------------------------------------------------------ */
+typedef struct fomo_grid3d {
+  int32_t nx, ny, nz; /* interior grid                                          */
+  float dh, dt;
+  int32_t nt, nbc, fd_order;
+  float v_ref;        /* <= 0 selects min(vp > 0)                               */
+} fomo_grid3d;
+
+typedef struct fomo_acq3d {
+  int32_t n_src;        /* sources (fire together)                              */
+  const int32_t* sx;    /* (n_src), 1-based interior indices                    */
+  const int32_t* sy;
+  const int32_t* sz;
+  const float* wavelet; /* (n_src, nt), injected raw                            */
+  int32_t n_rec;
+  const int32_t* rx;    /* (n_rec), 1-based interior indices                    */
+  const int32_t* ry;
+  const int32_t* rz;
+} fomo_acq3d;
+
+/* acoustic3d (equations/acoustic3d/acoustic3d.jl:37-188) and elastic3d
+ * (equations/elastic3d/elastic3d.jl:37-165).  Seismograms (n_rec, nt) of vx,
+ * vy, vz.  Snapshots every snap_interval steps of p (acoustic) or vz (elastic)
+ * on the plane snap_plane (0 :xz at y = snap_index, 1 :xy at z, 2 :yz at x;
+ * snap_index 1-based, 0 selects ny/2 as the reference does), laid out
+ * (nx, nz) / (nx, ny) / (ny, nz) per snapshot, nt / snap_interval of them.
+ * The HABC is the reference's 3D Higdon formula (boundary/habc/kernels_3d.jl)
+ * evaluated two-pass, so results are deterministic.  FP32 only.
+ * opts->final_state receives (nxp, nyp, nzp, nfield) padded fields:
+ * acoustic vx,vy,vz,p; elastic vx,vy,vz,txx,tyy,tzz,txy,txz,tyz. */
+FOMO_API int fomo_acoustic3d(fomo_ctx* ctx, const fomo_grid3d* g, const float* vp, const float* rho,
+                             const fomo_acq3d* acq, int32_t snap_interval, int32_t snap_plane,
+                             int32_t snap_index, float* seis_vx, float* seis_vy, float* seis_vz,
+                             float* snaps, const fomo_opts* opts, fomo_stats* stats);
+FOMO_API int fomo_elastic3d(fomo_ctx* ctx, const fomo_grid3d* g, const float* vp, const float* vs,
+                            const float* rho, const fomo_acq3d* acq, int32_t snap_interval,
+                            int32_t snap_plane, int32_t snap_index, float* seis_vx, float* seis_vy,
+                            float* seis_vz, float* snaps, const fomo_opts* opts, fomo_stats* stats);
+
 /* ---- allocation-free entry -------------------------------------------------
  * No counterpart in the reference.  scalar2d for callers that cannot allocate
  * device memory (a plugin inside a framework whose allocator owns all device
