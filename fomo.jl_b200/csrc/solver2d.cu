@@ -128,7 +128,7 @@ std::map<TuneKey, TuneVal> g_tune;
 
 template <class FieldFn>
 int tune_sweep(fomo_ctx* ctx, cudaStream_t st, SweepPlan& sp, int N, const Geo2& g, int ns,
-               float* const sets[2][3], const Coef& c, float dtx, float dtz, const HabcDev& h,
+               float* const sets[2][5], const Coef& c, float dtx, float dtz, const HabcDev& h,
                const ElMat& m, FieldFn field, long long* d_bounds) {
   const TuneKey key{N, g.nx, g.nz, ns};
   // FOMO_SWEEP_CONFIG="variant,TX,ctas_per_sm" pins the configuration (tests, sweeps)
@@ -170,7 +170,7 @@ int tune_sweep(fomo_ctx* ctx, cudaStream_t st, SweepPlan& sp, int N, const Geo2&
   };
   for (int v = 0; v < sweep_num_variants(); ++v) {
     int txs[4];
-    int ntx = sweep_tx_candidates(v, N, txs, 4);
+    int ntx = sweep_tx_candidates(v, N, g.nx, txs, 4);
     for (int k = 0; k < ntx; ++k) {
       SweepPlan cand;
       if (make_sweep_plan(cand, N, v, txs[k], 64, g, ns, sets, 1.0f, d_bounds, st) != cudaSuccess)
@@ -340,7 +340,8 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
   ElMat emat{d_mat, d_mat + P.plane, d_mat + 2 * P.plane, d_mat + 3 * P.plane, d_mat + 4 * P.plane};
   SweepPlan sp;
   if (kernel == FOMO_KERNEL_SINGLE_SWEEP) {
-    float* sets[2][3] = {{field(0, 2), field(0, 3), field(0, 4)}, {field(1, 2), field(1, 3), field(1, 4)}};
+    float* sets[2][5] = {{field(0, 2), field(0, 3), field(0, 4), field(0, 0), field(0, 1)},
+                         {field(1, 2), field(1, 3), field(1, 4), field(1, 0), field(1, 1)}};
     rc = tune_sweep(ctx, st, sp, P.N, g, P.ns, sets, c, dtx, dtz, h, emat,
                     [&](int set, int f) { return field(set, f); },
                     ws_ptr<long long>(ctx, o_bounds));

@@ -422,6 +422,412 @@ __global__ void __launch_bounds__(NT) k_el_sweep(const __grid_constant__ CUtenso
       mbar_wait_bounded(&bars[g % NSLOT], (uint32_t)((g / NSLOT) & 1), err);
 }
 
+// ===========================================================================
+// Pair-blocked single sweep (the "x2" variants).
+//
+// 256 threads = two row halves of 128; a thread owns two adjacent columns and
+// every iteration advances two rows, half hh taking row +hh of each stage.
+// Iteration i of a segment (v' rows zv = zv0 + 2i, zv + 1):
+//   stage A:  v'(zv+hh)      from the tau ring (stress of time n)
+//             s'(zv-3-M+hh)  from the v'' ring
+//   stage B:  v''(zv-1+hh)   = HABC(v')  -> v'' ring, B.v
+//             s''(zv-4-M+hh) = HABC(s')  -> B.stress
+// The stress of time n (3 fields) and A.v (2 fields) arrive by TMA in boxes
+// of 2 rows x 256 columns into shared rings; the materials come from L2 (they
+// are shared by every shot).  Each cell is computed with the canonical
+// arithmetic of the two-phase kernels, so results are bit-identical to them.
+//
+// Columns (relative to the strip's first output column X0):
+//   s''  [0, TX)                 outputs
+//   s'   [-2, TX+2)              HABC of s'' needs s' at +-1
+//   v''  [-2-M, TX+2+M)          stress derivatives need v'' at +-M
+//   v'   [-HV, TX+HV), HV>=M+3   HABC of v'' needs v' at +-1
+//   tau  [-HV-TN, -HV-TN+256)    v' derivatives need tau at +-M
+// ===========================================================================
+constexpr int kX2Threads = 256;
+constexpr int kX2W = 256;  // ring row pitch = TMA box width (floats)
+__host__ __device__ constexpr int x2_hv(int N) { return (N + 3 + 3) & ~3; }
+__host__ __device__ constexpr int x2_tn(int N) { return (N + 3) & ~3; }
+__host__ __device__ constexpr int x2_txmax(int N) {
+  return (kX2W - x2_tn(N) - N - 2 * x2_hv(N)) & ~3;
+}
+
+template <int N, int P>
+struct X2Shape {
+  static constexpr int TN = x2_tn(N), HV = x2_hv(N);
+  // tau pairs live at iteration i: i-3 .. i+N (s'' old rows .. v' window), + P prefetched
+  static constexpr int NPT = N + 4 + P;
+  static constexpr int NPV = 2 + P;   // A.v pairs i-1, i, + P prefetched
+  static constexpr int NPVV = N + 2;  // v'' rows zv-3-2N .. zv
+  static constexpr int LRT = 2 * NPT, LRV = 2 * NPV, LRVV = 2 * NPVV;
+  static constexpr int O_TAU = 0;                            // [3][LRT][W]
+  static constexpr int O_VO = O_TAU + 3 * LRT * kX2W;        // [2][LRV][W]
+  static constexpr int O_VP = O_VO + 2 * LRV * kX2W;         // [2][4][W]
+  static constexpr int O_VV = O_VP + 2 * 4 * kX2W;           // [2][LRVV][W]
+  static constexpr int O_SP = O_VV + 2 * LRVV * kX2W;        // [3][4][W]
+  static constexpr int O_WT = O_SP + 3 * 4 * kX2W;           // [3][wstride]
+};
+
+__device__ __forceinline__ int pmod(int x, int n) {
+  const int r = x % n;
+  return r < 0 ? r + n : r;
+}
+
+// x-derivative windows: xv[j] holds column c - 2E + j of a ring row, j < 4E+2
+template <int N>
+__device__ __forceinline__ void load_xwin(const float* row, int c, float* xv) {
+  constexpr int E = (N + 1) / 2;
+#pragma unroll
+  for (int j = 0; j <= 2 * E; ++j) {
+    const float2 v = *reinterpret_cast<const float2*>(row + c - 2 * E + 2 * j);
+    xv[2 * j] = v.x;
+    xv[2 * j + 1] = v.y;
+  }
+}
+// backward-staggered x derivative at cell c+e:  sum a_l (f[c+e+l-1] - f[c+e-l])
+template <int N>
+__device__ __forceinline__ float xdm(const float* xv, int e, const Coef& c) {
+  constexpr int E = (N + 1) / 2;
+  float acc = 0.0f;
+#pragma unroll
+  for (int l = 1; l <= N; ++l)
+    acc = __fmaf_rn(c.a[l - 1], __fsub_rn(xv[2 * E + e + l - 1], xv[2 * E + e - l]), acc);
+  return acc;
+}
+// forward-staggered x derivative at cell c+e:  sum a_l (f[c+e+l] - f[c+e-l+1])
+template <int N>
+__device__ __forceinline__ float xdp(const float* xv, int e, const Coef& c) {
+  constexpr int E = (N + 1) / 2;
+  float acc = 0.0f;
+#pragma unroll
+  for (int l = 1; l <= N; ++l)
+    acc = __fmaf_rn(c.a[l - 1], __fsub_rn(xv[2 * E + e + l], xv[2 * E + e - l + 1]), acc);
+  return acc;
+}
+
+template <int N, int P>
+__global__ void __launch_bounds__(kX2Threads, 1)
+    k_el_sweep_x2(const __grid_constant__ CUtensorMap tm_xx, const __grid_constant__ CUtensorMap tm_zz,
+                  const __grid_constant__ CUtensorMap tm_xz, const __grid_constant__ CUtensorMap tm_vx,
+                  const __grid_constant__ CUtensorMap tm_vz, SweepGeom gm, Coef c, float dtx,
+                  float dtz, HabcDev h, ElMat m, ElOut o, const long long* __restrict__ bounds,
+                  int* __restrict__ err) {
+  using S = X2Shape<N, P>;
+  constexpr int W = kX2W, M = N, TN = S::TN, HV = S::HV;
+  constexpr int NPT = S::NPT, NPV = S::NPV, LRT = S::LRT, LRV = S::LRV, LRVV = S::LRVV;
+  extern __shared__ __align__(128) float sm[];
+  float* s_tau = sm + S::O_TAU;
+  float* s_vo = sm + S::O_VO;
+  float* s_vp = sm + S::O_VP;
+  float* s_vv = sm + S::O_VV;
+  float* s_sp = sm + S::O_SP;
+  float* s_wt = sm + S::O_WT;
+  const int nwt = (3 * h.wstride + 31) & ~31;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sm + S::O_WT + nwt);  // [NPT]
+
+  const int tid = threadIdx.x, hh = tid >> 7, sc = 2 * (tid & 127);
+  const int TX = gm.TX, WV = TX + 2 * HV;
+  const Geo2 g2{gm.nx, gm.nz, gm.ld, M, gm.nbc, gm.plane};
+
+  for (int k = tid; k < S::O_WT; k += kX2Threads) sm[k] = 0.0f;
+  for (int k = tid; k < 3 * h.wstride; k += kX2Threads) s_wt[k] = __ldg(h.wtab + k);
+  if (tid == 0) {
+    for (int k = 0; k < NPT; ++k) mbar_init(&bars[k], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  auto wsm = [&](int kind, int dist) {
+    return dist < h.wstride ? s_wt[kind * h.wstride + dist] : 1.0f;
+  };
+  auto interior = [&](int x, int z) { return x >= M && x < gm.nx - M && z >= M && z < gm.nz - M; };
+
+  const long long r_lo = bounds[blockIdx.x];
+  const long long r_hi = bounds[blockIdx.x + 1];
+  int gt = 0, gv = 0;  // tau / A.v pairs this CTA has consumed (ring slot bases)
+  bool live = true;
+  for (long long r = r_lo; r < r_hi;) {
+    const long long item = r / gm.nz;
+    const int za = (int)(r - item * gm.nz);
+    const int zb = (int)min((long long)gm.nz, za + (r_hi - r));
+    r += zb - za;
+    const int strip = (int)(item % gm.nstrip);
+    const int shot = (int)(item / gm.nstrip);
+    const long long so = (long long)shot * gm.plane;
+    const int X0 = strip * TX, XV = X0 - HV, XT = XV - TN;
+    const int zv0 = za - 2 - M;  // first v' row: v'' from za-1-M feeds s' from za-1
+    // iterations until s''(zb-1) (row zv0+2i-3-M at hh=1)
+    const int I = (zb - za + 4 + 2 * M + 1) / 2 + 1;
+    const int KT = I + M;  // tau pairs 0 .. I-1+M (pair k: rows zv0-M+2k, +1)
+    const int tbase = (2 * gt) % LRT, vbase = (2 * gv) % LRV;
+    auto issue = [&](int k) {  // tau pair k, plus A.v pair k-M (rows zv0+2(k-M), +1)
+      const int slot = (gt + k) % NPT;
+      uint64_t* bar = &bars[slot];
+      const bool wv = k >= M;
+      mbar_expect_tx(bar, (uint32_t)((wv ? 5 : 3) * 2 * W * 4));
+      const int zt = zv0 - M + 2 * k;
+      tma_load_3d(s_tau + (0 * LRT + 2 * slot) * W, &tm_xx, XT, zt, shot, bar);
+      tma_load_3d(s_tau + (1 * LRT + 2 * slot) * W, &tm_zz, XT, zt, shot, bar);
+      tma_load_3d(s_tau + (2 * LRT + 2 * slot) * W, &tm_xz, XT, zt, shot, bar);
+      if (wv) {
+        const int vs = (gv + k - M) % NPV;
+        const int zw = zv0 + 2 * (k - M);
+        tma_load_3d(s_vo + (0 * LRV + 2 * vs) * W, &tm_vx, XV, zw, shot, bar);
+        tma_load_3d(s_vo + (1 * LRV + 2 * vs) * W, &tm_vz, XV, zw, shot, bar);
+      }
+    };
+    __syncthreads();  // the previous segment's readers are done with every ring
+    if (tid == 0 && live) {
+      fence_proxy_async();
+      for (int k = 0; k <= M + P && k < KT; ++k) issue(k);
+    }
+    const int xc = XV + sc;  // global column of the thread's first cell
+    for (int i = 0; i < I; ++i) {
+      const int zv = zv0 + 2 * i;
+      if (live)
+        for (int k = (i == 0 ? 0 : i + M); k <= i + M; ++k) {
+          const int gk = gt + k;
+          live = mbar_wait_bounded(&bars[gk % NPT], (uint32_t)((gk / NPT) & 1), err) && live;
+        }
+
+      // ================= stage A =================
+      // ---- v' at row zr ----
+      if (sc < WV) {
+        const int zr = zv + hh;
+        const int tb = pmod(tbase + 2 * i + hh + M, LRT);  // tau ring row of zr
+        const int ct = sc + TN;                             // tau column of the first cell
+        const float* txx = s_tau;
+        const float* tzz = s_tau + LRT * W;
+        const float* txz = s_tau + 2 * LRT * W;
+        float xw[4 * ((N + 1) / 2) + 2];
+        float dxx[2], dxzx[2], dxzz[2], dzz[2];
+        load_xwin<N>(txx + tb * W, ct, xw);
+        dxx[0] = xdm<N>(xw, 0, c);
+        dxx[1] = xdm<N>(xw, 1, c);
+        load_xwin<N>(txz + tb * W, ct, xw);
+        dxzx[0] = xdp<N>(xw, 0, c);
+        dxzx[1] = xdp<N>(xw, 1, c);
+        dxzz[0] = dxzz[1] = dzz[0] = dzz[1] = 0.0f;
+#pragma unroll
+        for (int l = 1; l <= N; ++l) {
+          const float a = c.a[l - 1];
+          const float2 p0 = *reinterpret_cast<const float2*>(txz + wrap(tb, l - 1, LRT) * W + ct);
+          const float2 p1 = *reinterpret_cast<const float2*>(txz + wrap(tb, -l, LRT) * W + ct);
+          dxzz[0] = __fmaf_rn(a, __fsub_rn(p0.x, p1.x), dxzz[0]);
+          dxzz[1] = __fmaf_rn(a, __fsub_rn(p0.y, p1.y), dxzz[1]);
+          const float2 q0 = *reinterpret_cast<const float2*>(tzz + wrap(tb, l, LRT) * W + ct);
+          const float2 q1 = *reinterpret_cast<const float2*>(tzz + wrap(tb, 1 - l, LRT) * W + ct);
+          dzz[0] = __fmaf_rn(a, __fsub_rn(q0.x, q1.x), dzz[0]);
+          dzz[1] = __fmaf_rn(a, __fsub_rn(q0.y, q1.y), dzz[1]);
+        }
+        const int vr = pmod(vbase + 2 * i + hh, LRV);  // A.v ring row of zr
+        const float2 ox = *reinterpret_cast<const float2*>(s_vo + vr * W + sc);
+        const float2 oz = *reinterpret_cast<const float2*>(s_vo + (LRV + vr) * W + sc);
+        float ux[2] = {ox.x, ox.y}, uz[2] = {oz.x, oz.y};
+        float bx[2] = {0.0f, 0.0f}, bz[2] = {0.0f, 0.0f};
+        if (zr >= 0 && zr < gm.nz) {
+          const long long pm = (long long)zr * gm.ld + xc;
+          if (xc >= 0 && xc + 1 < gm.nx) {
+            const float2 b0 = __ldg(reinterpret_cast<const float2*>(m.bx + pm));
+            const float2 b1 = __ldg(reinterpret_cast<const float2*>(m.bz + pm));
+            bx[0] = b0.x; bx[1] = b0.y; bz[0] = b1.x; bz[1] = b1.y;
+          } else {
+#pragma unroll
+            for (int e = 0; e < 2; ++e)
+              if (xc + e >= 0 && xc + e < gm.nx) {
+                bx[e] = __ldg(m.bx + pm + e);
+                bz[e] = __ldg(m.bz + pm + e);
+              }
+          }
+        }
+#pragma unroll
+        for (int e = 0; e < 2; ++e)
+          if (interior(xc + e, zr)) {
+            ux[e] = __fmaf_rn(bx[e], __fmaf_rn(dtx, dxx[e], __fmul_rn(dtz, dxzz[e])), ux[e]);
+            uz[e] = __fmaf_rn(bz[e], __fmaf_rn(dtx, dxzx[e], __fmul_rn(dtz, dzz[e])), uz[e]);
+          }
+        const int pr = (2 * i + hh) & 3;  // v' ring row of zr
+        *reinterpret_cast<float2*>(s_vp + pr * W + sc) = make_float2(ux[0], ux[1]);
+        *reinterpret_cast<float2*>(s_vp + (4 + pr) * W + sc) = make_float2(uz[0], uz[1]);
+      }
+      // ---- s' at row q ----
+      if (sc >= HV - 2 && sc < HV + TX + 2) {
+        const int q = zv - 3 - M + hh;
+        const int vb = pmod(2 * i - 2 - M + hh, LRVV);  // v'' ring row of q
+        const float* vvx = s_vv;
+        const float* vvz = s_vv + LRVV * W;
+        float xw[4 * ((N + 1) / 2) + 2];
+        float dvxdx[2], dvzdx[2], dvxdz[2], dvzdz[2];
+        load_xwin<N>(vvx + vb * W, sc, xw);
+        dvxdx[0] = xdp<N>(xw, 0, c);
+        dvxdx[1] = xdp<N>(xw, 1, c);
+        load_xwin<N>(vvz + vb * W, sc, xw);
+        dvzdx[0] = xdm<N>(xw, 0, c);
+        dvzdx[1] = xdm<N>(xw, 1, c);
+        dvxdz[0] = dvxdz[1] = dvzdz[0] = dvzdz[1] = 0.0f;
+#pragma unroll
+        for (int l = 1; l <= N; ++l) {
+          const float a = c.a[l - 1];
+          const float2 p0 = *reinterpret_cast<const float2*>(vvx + wrap(vb, l, LRVV) * W + sc);
+          const float2 p1 = *reinterpret_cast<const float2*>(vvx + wrap(vb, 1 - l, LRVV) * W + sc);
+          dvxdz[0] = __fmaf_rn(a, __fsub_rn(p0.x, p1.x), dvxdz[0]);
+          dvxdz[1] = __fmaf_rn(a, __fsub_rn(p0.y, p1.y), dvxdz[1]);
+          const float2 q0 = *reinterpret_cast<const float2*>(vvz + wrap(vb, l - 1, LRVV) * W + sc);
+          const float2 q1 = *reinterpret_cast<const float2*>(vvz + wrap(vb, -l, LRVV) * W + sc);
+          dvzdz[0] = __fmaf_rn(a, __fsub_rn(q0.x, q1.x), dvzdz[0]);
+          dvzdz[1] = __fmaf_rn(a, __fsub_rn(q0.y, q1.y), dvzdz[1]);
+        }
+        const int tq = pmod(tbase + 2 * i - 3 + hh, LRT);  // tau ring row of q
+        const float2 oxx = *reinterpret_cast<const float2*>(s_tau + tq * W + sc + TN);
+        const float2 ozz = *reinterpret_cast<const float2*>(s_tau + (LRT + tq) * W + sc + TN);
+        const float2 oxz = *reinterpret_cast<const float2*>(s_tau + (2 * LRT + tq) * W + sc + TN);
+        float sxx[2] = {oxx.x, oxx.y}, szz[2] = {ozz.x, ozz.y}, sxz[2] = {oxz.x, oxz.y};
+        float lam[2] = {0.0f, 0.0f}, l2m[2] = {0.0f, 0.0f}, mut[2] = {0.0f, 0.0f};
+        if (q >= 0 && q < gm.nz) {
+          const long long pm = (long long)q * gm.ld + xc;
+          if (xc >= 0 && xc + 1 < gm.nx) {
+            const float2 a0 = __ldg(reinterpret_cast<const float2*>(m.lam + pm));
+            const float2 a1 = __ldg(reinterpret_cast<const float2*>(m.l2m + pm));
+            const float2 a2 = __ldg(reinterpret_cast<const float2*>(m.mut + pm));
+            lam[0] = a0.x; lam[1] = a0.y; l2m[0] = a1.x; l2m[1] = a1.y; mut[0] = a2.x; mut[1] = a2.y;
+          } else {
+#pragma unroll
+            for (int e = 0; e < 2; ++e)
+              if (xc + e >= 0 && xc + e < gm.nx) {
+                lam[e] = __ldg(m.lam + pm + e);
+                l2m[e] = __ldg(m.l2m + pm + e);
+                mut[e] = __ldg(m.mut + pm + e);
+              }
+          }
+        }
+#pragma unroll
+        for (int e = 0; e < 2; ++e)
+          if (interior(xc + e, q)) {
+            const float ex = __fmul_rn(dvxdx[e], dtx), ez = __fmul_rn(dvzdz[e], dtz);
+            sxx[e] = __fadd_rn(sxx[e], __fmaf_rn(l2m[e], ex, __fmul_rn(lam[e], ez)));
+            szz[e] = __fadd_rn(szz[e], __fmaf_rn(lam[e], ex, __fmul_rn(l2m[e], ez)));
+            sxz[e] = __fmaf_rn(mut[e], __fmaf_rn(dvxdz[e], dtz, __fmul_rn(dvzdx[e], dtx)), sxz[e]);
+          }
+        const int sr = (2 * i + hh) & 3;  // s' ring row of q
+        *reinterpret_cast<float2*>(s_sp + sr * W + sc) = make_float2(sxx[0], sxx[1]);
+        *reinterpret_cast<float2*>(s_sp + (4 + sr) * W + sc) = make_float2(szz[0], szz[1]);
+        *reinterpret_cast<float2*>(s_sp + (8 + sr) * W + sc) = make_float2(sxz[0], sxz[1]);
+      }
+      __syncthreads();
+
+      // ================= stage B =================
+      // ---- v'' at row qv: Higdon on frame cells; -> v'' ring, B.v ----
+      if (sc < WV) {
+        const int qv = zv - 1 + hh;
+        const int pr = (2 * i - 1 + hh) & 3;           // v' ring row of qv
+        const int orow = pmod(vbase + 2 * i - 1 + hh, LRV);  // A.v ring row of qv
+        float v[2][2];  // [field][cell]
+        {
+          const float2 fx = *reinterpret_cast<const float2*>(s_vp + pr * W + sc);
+          const float2 fz = *reinterpret_cast<const float2*>(s_vp + (4 + pr) * W + sc);
+          v[0][0] = fx.x; v[0][1] = fx.y; v[1][0] = fz.x; v[1][1] = fz.y;
+        }
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          int sx, sz, dist;
+          if (!frame2(g2, xc + e, qv, sx, sz, dist)) continue;
+          const int col = sc + e;
+          const int coln = min(max(col + sx, 0), W - 1);
+          const int prn = (2 * i - 1 + hh + sz) & 3;
+          const int orn = pmod(vbase + 2 * i - 1 + hh + sz, LRV);
+#pragma unroll
+          for (int f = 0; f < 2; ++f) {
+            const float* fp = s_vp + f * 4 * W;
+            const float* fo = s_vo + f * LRV * W;
+            const float w = wsm(f, dist);
+            const float fop = fo[orow * W + col];
+            if (sx != 0 && sz != 0)
+              v[f][e] = higdon_corner(w, v[f][e],
+                                      higdon_side(h, fp[pr * W + coln], fop, fo[orow * W + coln]),
+                                      higdon_side(h, fp[prn * W + col], fop, fo[orn * W + col]));
+            else if (sx != 0)
+              v[f][e] = higdon_edge(w, v[f][e],
+                                    higdon_side(h, fp[pr * W + coln], fop, fo[orow * W + coln]));
+            else
+              v[f][e] = higdon_edge(w, v[f][e],
+                                    higdon_side(h, fp[prn * W + col], fop, fo[orn * W + col]));
+          }
+        }
+        const int vw = (2 * i + hh) % LRVV;  // v'' ring row of qv
+        *reinterpret_cast<float2*>(s_vv + vw * W + sc) = make_float2(v[0][0], v[0][1]);
+        *reinterpret_cast<float2*>(s_vv + (LRVV + vw) * W + sc) = make_float2(v[1][0], v[1][1]);
+        if (qv >= za && qv < zb && sc >= HV && sc < HV + TX && xc < gm.nx) {
+          const long long p = so + (long long)qv * gm.ld + xc;
+          if (xc + 1 < gm.nx) {
+            *reinterpret_cast<float2*>(o.vx + p) = make_float2(v[0][0], v[0][1]);
+            *reinterpret_cast<float2*>(o.vz + p) = make_float2(v[1][0], v[1][1]);
+          } else {
+            o.vx[p] = v[0][0];
+            o.vz[p] = v[1][0];
+          }
+        }
+      }
+      // ---- s'' at row qs: Higdon on frame cells -> B.stress ----
+      {
+        const int qs = zv - 4 - M + hh;
+        if (qs >= za && qs < zb && sc >= HV && sc < HV + TX && xc < gm.nx) {
+          const int sr = (2 * i - 1 + hh) & 3;  // s' ring row of qs
+          float v[3][2];
+#pragma unroll
+          for (int f = 0; f < 3; ++f) {
+            const float2 t2 = *reinterpret_cast<const float2*>(s_sp + (4 * f + sr) * W + sc);
+            v[f][0] = t2.x;
+            v[f][1] = t2.y;
+          }
+          const int trow = pmod(tbase + 2 * i - 4 + hh, LRT);  // tau ring row of qs
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            int sx, sz, dist;
+            if (!frame2(g2, xc + e, qs, sx, sz, dist)) continue;
+            const int col = sc + e;
+            const int coln = min(max(col + sx, 0), W - 1);
+            const int srn = (2 * i - 1 + hh + sz) & 3;
+            const int trn = pmod(tbase + 2 * i - 4 + hh + sz, LRT);
+            const float w = wsm(2, dist);
+#pragma unroll
+            for (int f = 0; f < 3; ++f) {
+              const float* fp = s_sp + 4 * f * W;
+              const float* fo = s_tau + f * LRT * W + TN;
+              const float fop = fo[trow * W + col];
+              if (sx != 0 && sz != 0)
+                v[f][e] = higdon_corner(w, v[f][e],
+                                        higdon_side(h, fp[sr * W + coln], fop, fo[trow * W + coln]),
+                                        higdon_side(h, fp[srn * W + col], fop, fo[trn * W + col]));
+              else if (sx != 0)
+                v[f][e] = higdon_edge(w, v[f][e],
+                                      higdon_side(h, fp[sr * W + coln], fop, fo[trow * W + coln]));
+              else
+                v[f][e] = higdon_edge(w, v[f][e],
+                                      higdon_side(h, fp[srn * W + col], fop, fo[trn * W + col]));
+            }
+          }
+          const long long p = so + (long long)qs * gm.ld + xc;
+          float* out[3] = {o.txx, o.tzz, o.txz};
+#pragma unroll
+          for (int f = 0; f < 3; ++f) {
+            if (xc + 1 < gm.nx)
+              *reinterpret_cast<float2*>(out[f] + p) = make_float2(v[f][0], v[f][1]);
+            else
+              out[f][p] = v[f][0];
+          }
+        }
+      }
+      __syncthreads();
+      // tau pair i-3 and A.v pair i-1 are dead: refill their slots
+      if (tid == 0 && live && i + M + 1 + P < KT) {
+        fence_proxy_async();
+        issue(i + M + 1 + P);
+      }
+    }
+    gt += KT;
+    gv += I;
+  }
+}
+
 // ---- host side --------------------------------------------------------------
 PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 std::once_flag g_encode_once;
@@ -450,6 +856,16 @@ size_t smem_bytes(int W, int wstride) {
 }
 
 constexpr int kMaxDynSmem = 227 * 1024;
+
+template <int N, int P>
+size_t x2_smem_bytes(int wstride) {
+  using S = X2Shape<N, P>;
+  return (size_t)(S::O_WT + ((3 * wstride + 31) & ~31)) * 4 + sizeof(uint64_t) * S::NPT;
+}
+// pair-blocked variants: prefetch depth in row pairs
+constexpr int kX2P[] = {1, 2, 3};
+constexpr int kNumX2 = sizeof(kX2P) / sizeof(kX2P[0]);
+#define FOMO_X2_VARIANTS(X, NN) X(0, NN, 1) X(1, NN, 2) X(2, NN, 3)
 
 struct Variant {
   int NT, R, P;
@@ -491,6 +907,47 @@ cudaError_t launch_n(cudaStream_t st, const SweepPlan& sp, int set, const Coef& 
   return cudaErrorInvalidValue;
 }
 
+template <int N, int P>
+cudaError_t launch_x2(cudaStream_t st, const SweepPlan& sp, int set, const Coef& c, float dtx,
+                      float dtz, const HabcDev& h, const ElMat& m, const ElOut& o, int* err) {
+  auto kern = k_el_sweep_x2<N, P>;
+  static std::atomic<int> attr_set{0};
+  if (!attr_set.load(std::memory_order_acquire)) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kMaxDynSmem);
+    if (e != cudaSuccess) return e;
+    attr_set.store(1, std::memory_order_release);
+  }
+  if (sp.smem > (size_t)kMaxDynSmem) return cudaErrorInvalidValue;
+  kern<<<(unsigned)sp.grid, kX2Threads, sp.smem, st>>>(sp.tm[set][0], sp.tm[set][1], sp.tm[set][2],
+                                                        sp.tm[set][3], sp.tm[set][4], sp.gm, c, dtx,
+                                                        dtz, h, m, o, sp.d_bounds, err);
+  return cudaGetLastError();
+}
+
+template <int N>
+cudaError_t launch_x2_n(cudaStream_t st, const SweepPlan& sp, int set, const Coef& c, float dtx,
+                        float dtz, const HabcDev& h, const ElMat& m, const ElOut& o, int* err) {
+#define FOMO_LAUNCH_X2(V, NN, PP) \
+  case V: return launch_x2<NN, PP>(st, sp, set, c, dtx, dtz, h, m, o, err);
+  switch (sp.variant - kNumVariants) { FOMO_X2_VARIANTS(FOMO_LAUNCH_X2, N) }
+#undef FOMO_LAUNCH_X2
+  return cudaErrorInvalidValue;
+}
+
+size_t x2_smem_for(int N, int v2, int wstride) {
+#define FOMO_SMEM_X2(V, NN, PP) \
+  case V: return x2_smem_bytes<NN, PP>(wstride);
+#define FOMO_SMEM_X2N(NN)                                  \
+  case NN:                                                 \
+    switch (v2) { FOMO_X2_VARIANTS(FOMO_SMEM_X2, NN) }     \
+    break;
+  switch (N) { FOMO_SMEM_X2N(1) FOMO_SMEM_X2N(2) FOMO_SMEM_X2N(3) FOMO_SMEM_X2N(4) FOMO_SMEM_X2N(5) }
+#undef FOMO_SMEM_X2N
+#undef FOMO_SMEM_X2
+  return 0;
+}
+
 size_t smem_for(int N, int variant, int W, int wstride) {
 #define FOMO_SMEM_V(V, NN, NT, R, P) \
   case V: return smem_bytes<NN, NT, R, P>(W, wstride);
@@ -516,23 +973,35 @@ int pick_kernel_2d(int phys, int N, int nxp, int nzp, int ns) {
 
 bool sweep2d_supported(int phys, int N) { return phys == 1 && N >= 1 && N <= 5 && encoder(); }
 
-int sweep_num_variants() { return kNumVariants; }
+int sweep_num_variants() { return kNumVariants + kNumX2; }
 
 // Builds the work decomposition and the six tensor maps (3 stress fields x 2
 // ping-pong sets).  variant selects (threads, rows per chunk, prefetch depth);
 // TX is the strip width (multiple of 4).
 cudaError_t make_sweep_plan(SweepPlan& sp, int N, int variant, int TX, int per_sm, const Geo2& g,
-                            int ns, float* const stress_sets[2][3], float frame_weight,
+                            int ns, float* const sets[2][5], float frame_weight,
                             long long* d_bounds, cudaStream_t st) {
   auto enc = encoder();
   if (!enc) return cudaErrorNotSupported;
-  if (variant < 0 || variant >= kNumVariants || per_sm < 1) return cudaErrorInvalidValue;
-  const int NT = kVariants[variant].NT, R = kVariants[variant].R;
-  const int M = N, HS = halo_x(M);
-  if (TX < 8 || TX + 2 * M + 4 > NT || (TX & 3)) return cudaErrorInvalidValue;
-  const int walign = 32 / R;  // R rows of W floats = a multiple of 128 bytes (TMA destination)
-  int W = (TX + 2 * HS + walign - 1) / walign * walign;
-  if (W > 256) return cudaErrorInvalidValue;
+  if (variant < 0 || variant >= kNumVariants + kNumX2 || per_sm < 1) return cudaErrorInvalidValue;
+  const bool x2 = variant >= kNumVariants;
+  int W = 0, R = 2;
+  if (x2) {
+    if (TX < 8 || TX > x2_txmax(N) || (TX & 3)) return cudaErrorInvalidValue;
+    W = kX2W;
+    sp.family = 1;
+    sp.P = kX2P[variant - kNumVariants];
+  } else {
+    const int NT = kVariants[variant].NT;
+    R = kVariants[variant].R;
+    const int M = N, HS = halo_x(M);
+    if (TX < 8 || TX + 2 * M + 4 > NT || (TX & 3)) return cudaErrorInvalidValue;
+    const int walign = 32 / R;  // R rows of W floats = a multiple of 128 bytes (TMA destination)
+    W = (TX + 2 * HS + walign - 1) / walign * walign;
+    if (W > 256) return cudaErrorInvalidValue;
+    sp.family = 0;
+    sp.P = 0;
+  }
   sp.variant = variant;
   sp.N = N;
   sp.gm.nx = g.nx;
@@ -544,7 +1013,8 @@ cudaError_t make_sweep_plan(SweepPlan& sp, int N, int variant, int TX, int per_s
   sp.gm.W = W;
   sp.gm.nstrip = (g.nx + TX - 1) / TX;
   sp.gm.ns = ns;
-  sp.smem = smem_for(N, variant, W, g.nbc + 3);
+  sp.smem = x2 ? x2_smem_for(N, variant - kNumVariants, g.nbc + 3)
+             : smem_for(N, variant, W, g.nbc + 3);
   const int bps = sweep_blocks_per_sm(sp);
   if (bps < 1) return cudaErrorInvalidConfiguration;
   int dev = 0, nsm = 148;
@@ -590,12 +1060,12 @@ cudaError_t make_sweep_plan(SweepPlan& sp, int N, int variant, int TX, int per_s
     sp.d_bounds = d_bounds;
   }
   for (int s = 0; s < 2; ++s)
-    for (int f = 0; f < 3; ++f) {
+    for (int f = 0; f < (x2 ? 5 : 3); ++f) {
       cuuint64_t dims[3] = {(cuuint64_t)g.nx, (cuuint64_t)g.nz, (cuuint64_t)ns};
       cuuint64_t strides[2] = {(cuuint64_t)g.ld * 4, (cuuint64_t)g.plane * 4};
       cuuint32_t box[3] = {(cuuint32_t)W, (cuuint32_t)R, 1};
       cuuint32_t es[3] = {1, 1, 1};
-      CUresult r = enc(&sp.tm[s][f], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, stress_sets[s][f], dims,
+      CUresult r = enc(&sp.tm[s][f], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, sets[s][f], dims,
                        strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
       if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
@@ -603,9 +1073,18 @@ cudaError_t make_sweep_plan(SweepPlan& sp, int N, int variant, int TX, int per_s
   return cudaSuccess;
 }
 
-int sweep_tx_candidates(int variant, int N, int* out, int max_out) {
-  // the widest strip whose v' columns (TX + 2M + 4) fill the CTA's threads
+int sweep_tx_candidates(int variant, int N, int nx, int* out, int max_out) {
   int n = 0;
+  if (variant >= kNumVariants) {
+    // the widest strip, and the narrowest strip with the same strip count
+    const int tmax = x2_txmax(N);
+    if (tmax >= 8 && n < max_out) out[n++] = tmax;
+    const int ns = (nx + tmax - 1) / tmax;
+    const int tbal = (((nx + ns - 1) / ns) + 3) & ~3;
+    if (tbal >= 8 && tbal < tmax && n < max_out) out[n++] = tbal;
+    return n;
+  }
+  // the widest strip whose v' columns (TX + 2M + 4) fill the CTA's threads
   const int tmax = (kVariants[variant].NT - 2 * N - 4) & ~3;
   if (tmax >= 8 && n < max_out) out[n++] = tmax;
   return n;
@@ -624,7 +1103,32 @@ int occ_v(const SweepPlan& sp) {
   return nb;
 }
 
+template <int N, int P>
+int occ_x2(const SweepPlan& sp) {
+  int nb = 0;
+  cudaFuncSetAttribute(k_el_sweep_x2<N, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       kMaxDynSmem);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_el_sweep_x2<N, P>, kX2Threads,
+                                                    sp.smem) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return nb;
+}
+
 int sweep_blocks_per_sm(const SweepPlan& sp) {
+  if (sp.family == 1) {
+#define FOMO_OCC_X2(V, NN, PP) \
+  case V: return occ_x2<NN, PP>(sp);
+#define FOMO_OCC_X2N(NN)                                                     \
+  case NN:                                                                   \
+    switch (sp.variant - kNumVariants) { FOMO_X2_VARIANTS(FOMO_OCC_X2, NN) } \
+    break;
+    switch (sp.N) { FOMO_OCC_X2N(1) FOMO_OCC_X2N(2) FOMO_OCC_X2N(3) FOMO_OCC_X2N(4) FOMO_OCC_X2N(5) }
+#undef FOMO_OCC_X2N
+#undef FOMO_OCC_X2
+    return 0;
+  }
 #define FOMO_OCC_V(V, NN, NT, R, P) \
   case V: return occ_v<NN, NT, R, P>(sp);
 #define FOMO_OCC_N(NN)                                     \
@@ -640,6 +1144,16 @@ int sweep_blocks_per_sm(const SweepPlan& sp) {
 cudaError_t launch_sweep_elastic(cudaStream_t st, const SweepPlan& sp, int set, const Coef& c,
                                  float dtx, float dtz, const HabcDev& h, const ElFields& a,
                                  const ElMat& m, const ElOut& o, int* err) {
+  if (sp.family == 1) {
+    switch (sp.N) {
+      case 1: return launch_x2_n<1>(st, sp, set, c, dtx, dtz, h, m, o, err);
+      case 2: return launch_x2_n<2>(st, sp, set, c, dtx, dtz, h, m, o, err);
+      case 3: return launch_x2_n<3>(st, sp, set, c, dtx, dtz, h, m, o, err);
+      case 4: return launch_x2_n<4>(st, sp, set, c, dtx, dtz, h, m, o, err);
+      case 5: return launch_x2_n<5>(st, sp, set, c, dtx, dtz, h, m, o, err);
+    }
+    return cudaErrorInvalidValue;
+  }
   switch (sp.N) {
     case 1: return launch_n<1>(st, sp, set, c, dtx, dtz, h, a, m, o, err);
     case 2: return launch_n<2>(st, sp, set, c, dtx, dtz, h, a, m, o, err);

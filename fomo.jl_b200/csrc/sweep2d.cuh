@@ -21,26 +21,30 @@ constexpr int kMaxGrid = 4096;
 
 struct SweepPlan {
   int N = 0, variant = 0;
+  int family = 0;            // 0: column-per-thread kernel, 1: pair-blocked kernel
+  int P = 0;                 // pair-blocked: prefetch depth (row pairs)
   int per_sm = 1, grid = 1;  // persistent CTAs per SM, grid size
   float frame_weight = 1.0f; // extra cost of a frame cell in the row-range split
   const long long* d_bounds = nullptr;  // [grid + 1] row ranges (device)
   size_t smem = 0;
   SweepGeom gm{};
-  CUtensorMap tm[2][3];  // [ping-pong set][txx, tzz, txz]
+  CUtensorMap tm[2][5];  // [ping-pong set][txx, tzz, txz, vx, vz]
 };
 
 // Kernel family for a problem (FOMO_KERNEL_TWO_PHASE / _SINGLE_SWEEP).
 int pick_kernel_2d(int phys, int N, int nxp, int nzp, int ns);
 bool sweep2d_supported(int phys, int N);
 int sweep_num_variants();
-// Candidate strip widths for a variant (multiples of 4 that fit its threads).
-int sweep_tx_candidates(int variant, int N, int* out, int max_out);
+// Candidate strip widths for a variant (multiples of 4 that fit its threads)
+// on a padded grid nx columns wide.
+int sweep_tx_candidates(int variant, int N, int nx, int* out, int max_out);
 // per_sm: persistent CTAs per SM (capped by occupancy); each CTA owns a
 // contiguous share of the flattened (strip, shot, row) space of equal
 // estimated cost (frame cells weigh 1 + frame_weight); the row-range table is
 // written to d_bounds (kMaxGrid + 1 entries) on stream st.
+// sets: per ping-pong set the fields txx, tzz, txz, vx, vz.
 cudaError_t make_sweep_plan(SweepPlan& sp, int N, int variant, int TX, int per_sm, const Geo2& g,
-                            int ns, float* const stress_sets[2][3], float frame_weight,
+                            int ns, float* const sets[2][5], float frame_weight,
                             long long* d_bounds, cudaStream_t st);
 cudaError_t launch_sweep_elastic(cudaStream_t st, const SweepPlan& sp, int set, const Coef& c,
                                  float dtx, float dtz, const HabcDev& h, const ElFields& a,

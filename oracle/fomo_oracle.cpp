@@ -76,6 +76,63 @@ inline int order_to_N(int fd_order) {
 inline float fmaT(float a, float b, float c) { return std::fmaf(a, b, c); }
 inline double fmaT(double a, double b, double c) { return std::fma(a, b, c); }
 
+// ---------------------------------------------------------------------------
+// Reduced-precision wavefield storage (no reference counterpart).  A stored
+// value is the FP32 result rounded to nearest-even into IEEE binary16 (with
+// subnormals, overflow to inf) or bfloat16; these restate those formats'
+// published rounding rules bit by bit so the oracle does not depend on a
+// compiler's half-precision support.
+// ---------------------------------------------------------------------------
+enum StoreKind { kStoreF32 = 0, kStoreF16 = 1, kStoreBF16 = 2 };
+
+inline float bits_f(uint32_t u) {
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+inline uint32_t f_bits(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  return u;
+}
+
+inline float round_fp16(float x) {
+  const uint32_t u = f_bits(x), sign = u & 0x80000000u, a = u & 0x7fffffffu;
+  if (a >= 0x7f800000u) return x;                              // inf, nan
+  if (a >= 0x477ff000u) return bits_f(sign | 0x7f800000u);     // >= 65520 -> inf
+  if (a >= 0x38800000u) {                                      // |x| >= 2^-14: 10-bit mantissa
+    uint32_t r = (a + 0x0fffu + ((a >> 13) & 1u)) & ~0x1fffu;
+    return bits_f(sign | r);
+  }
+  // subnormal binary16: multiples of 2^-24 (x * 2^24 is exact)
+  const float k = std::nearbyint(std::fabs(x) * 16777216.0f);
+  return bits_f(sign | f_bits(k * (1.0f / 16777216.0f)));
+}
+
+inline float round_bf16(float x) {
+  uint32_t u = f_bits(x);
+  if ((u & 0x7fffffffu) > 0x7f800000u) return x;  // nan
+  u = (u + 0x7fffu + ((u >> 16) & 1u)) & 0xffff0000u;
+  return bits_f(u);
+}
+
+inline float round_store(float x, int kind) {
+  return kind == kStoreF16 ? round_fp16(x) : (kind == kStoreBF16 ? round_bf16(x) : x);
+}
+inline double round_store(double x, int) { return x; }
+
+// Storage format and power-of-two scales of the stored velocity (sv) and
+// stress (st) fields: stored v = sv * v, stored tau = st * tau.  The scales are
+// folded into the coefficients (b * sv/st, lambda * st/sv, ...), so the FP32
+// arithmetic on scaled values equals the unscaled arithmetic times a power of
+// two; the scales only place the values inside the storage format's range.
+// Cells closer than fp32_band to a grid edge keep FP32 storage (0: none).
+struct StoreSpec {
+  int kind = kStoreF32;
+  float sv = 1.0f, st = 1.0f;
+  int fp32_band = 0;
+};
+
 // 1-based (i,j) -> linear index of a column-major (x fastest) padded grid.
 struct G2 {
   int nx, nz;
@@ -385,7 +442,7 @@ int run_elastic2d(int nx, int nz, int ns, const float* vp, const float* vs, cons
                   float dh, float dt, int nt, int nbc, int fd_order, float v_ref, int n_src,
                   const int32_t* sx, const int32_t* sz, const float* wavelet, int n_rec,
                   const int32_t* rx, const int32_t* rz, T* seis_vx, T* seis_vz, int snap_interval,
-                  T* snaps, T* final_fields) {
+                  T* snaps, T* final_fields, StoreSpec ss = StoreSpec()) {
   int N = order_to_N(fd_order);
   if (N < 0) return -2;
   int M = N, pad = nbc + M;
@@ -396,6 +453,27 @@ int run_elastic2d(int nx, int nz, int ns, const float* vp, const float* vs, cons
   std::vector<T> bx, bz, lam, lam2mu, mutxz;
   staggered_buoyancy(g, rhop, bx, bz);
   elastic_params(g, vpp, vsp, rhop, lam, lam2mu, mutxz);
+  const int sk = ss.kind;
+  const T sv = (T)ss.sv, st_ = (T)ss.st;
+  if (ss.sv != 1.0f || ss.st != 1.0f) {
+    const T rv = sv / st_, rs = st_ / sv;  // exact: powers of two
+    for (auto& a : bx) a *= rv;
+    for (auto& a : bz) a *= rv;
+    for (auto& a : lam) a *= rs;
+    for (auto& a : lam2mu) a *= rs;
+    for (auto& a : mutxz) a *= rs;
+  }
+  const int sfmt = sk, zb = ss.fp32_band, zone_f32 = zb > 0;
+  auto in_zone = [&](size_t q) {
+    const int i = (int)(q % (size_t)g.nx), j = (int)(q / (size_t)g.nx);
+    return std::min(std::min(i, g.nx - 1 - i), std::min(j, g.nz - 1 - j)) < zb;
+  };
+  auto round_all = [&](std::vector<T>& f) {
+    if (sfmt == kStoreF32) return;
+#pragma omp parallel for schedule(static)
+    for (long q = 0; q < (long)f.size(); ++q)
+      if (!zone_f32 || !in_zone((size_t)q)) f[q] = round_store(f[q], sfmt);
+  };
   Habc<T> h = init_habc<T>(pad, v_ref, dt, dh);
   std::vector<FramePt> fr = frame_points(g, h.nbc);
   Coef<T> c = coef<T>(fd_order);
@@ -414,6 +492,8 @@ int run_elastic2d(int nx, int nz, int ns, const float* vp, const float* vs, cons
       elastic_vel(g, M, c, dtx, dtz, bx.data(), bz.data(), st);
       habc_det(g, h, fr, 0, st.vx.data(), st.o1.data(), scr);
       habc_det(g, h, fr, 1, st.vz.data(), st.o2.data(), scr);
+      round_all(st.vx);  // stored v'' (the stress update reads the stored values)
+      round_all(st.vz);
       st.o1 = st.txx;
       st.o2 = st.tzz;
       st.o3 = st.txz;
@@ -421,30 +501,35 @@ int run_elastic2d(int nx, int nz, int ns, const float* vp, const float* vs, cons
       habc_det(g, h, fr, 2, st.txx.data(), st.o1.data(), scr);
       habc_det(g, h, fr, 2, st.tzz.data(), st.o2.data(), scr);
       habc_det(g, h, fr, 2, st.txz.data(), st.o3.data(), scr);
+      round_all(st.txx);
+      round_all(st.tzz);
+      round_all(st.txz);
       for (int q = 0; q < n_src; ++q) {  // batch_acq.jl:58-71, sequential in source order
         size_t p = g.at(sx[(size_t)s * n_src + q] + pad, sz[(size_t)s * n_src + q] + pad);
-        T w = (T)wavelet[(size_t)q + (size_t)n_src * (it - 1)];
-        st.txx[p] += w;
-        st.tzz[p] += w;
+        T w = (T)wavelet[(size_t)q + (size_t)n_src * (it - 1)] * st_;
+        const int k = (zone_f32 && in_zone(p)) ? kStoreF32 : sfmt;
+        st.txx[p] = round_store(st.txx[p] + w, k);
+        st.tzz[p] = round_store(st.tzz[p] + w, k);
       }
       for (int r = 0; r < n_rec; ++r) {  // batch_acq.jl:108-121
         size_t p = g.at(rx[r] + pad, rz[r] + pad);
         size_t o = (size_t)r + (size_t)n_rec * ((it - 1) + (size_t)nt * s);
-        seis_vx[o] = st.vx[p];
-        seis_vz[o] = st.vz[p];
+        seis_vx[o] = st.vx[p] / sv;
+        seis_vz[o] = st.vz[p] / sv;
       }
       if (snaps && snap_interval > 0 && it % snap_interval == 0) {
         int k = it / snap_interval - 1;
         snap_interior(g, pad, st.vz.data(), snaps + nint * ((size_t)k + (size_t)nsnap * s));
+        if (sv != T(1))
+          for (size_t q = 0; q < nint; ++q) snaps[nint * ((size_t)k + (size_t)nsnap * s) + q] /= sv;
       }
     }
-    if (final_fields) {
+    if (final_fields) {  // unscaled values of the stored fields
       T* o = final_fields + (size_t)s * 5 * ncell;
-      std::copy(st.vx.begin(), st.vx.end(), o);
-      std::copy(st.vz.begin(), st.vz.end(), o + ncell);
-      std::copy(st.txx.begin(), st.txx.end(), o + 2 * ncell);
-      std::copy(st.tzz.begin(), st.tzz.end(), o + 3 * ncell);
-      std::copy(st.txz.begin(), st.txz.end(), o + 4 * ncell);
+      const T sc[5] = {sv, sv, st_, st_, st_};
+      const std::vector<T>* F[5] = {&st.vx, &st.vz, &st.txx, &st.tzz, &st.txz};
+      for (int f = 0; f < 5; ++f)
+        for (size_t q = 0; q < ncell; ++q) o[f * ncell + q] = (*F[f])[q] / sc[f];
     }
   }
   return 0;
@@ -1059,6 +1144,29 @@ int oracle_elastic2d(int prec, int nx, int nz, int ns, const float* vp, const fl
       run_elastic2d<double>(nx, nz, ns, vp, vs, rho, dh, dt, nt, nbc, fd_order, v_ref, n_src, sx,
                             sz, wavelet, n_rec, rx, rz, (double*)seis_vx, (double*)seis_vz,
                             snap_interval, (double*)snaps, (double*)final_fields));
+}
+
+// FP32 arithmetic with wavefields stored as store_kind (0 fp32, 1 fp16,
+// 2 bf16) under power-of-two scales sv (velocities) and st (stresses).
+int oracle_elastic2d_store(int store_kind, float sv, float st, int fp32_band, int nx, int nz, int ns,
+                           const float* vp, const float* vs, const float* rho, float dh, float dt,
+                           int nt, int nbc, int fd_order, float v_ref, int n_src, const int32_t* sx,
+                           const int32_t* sz, const float* wavelet, int n_rec, const int32_t* rx,
+                           const int32_t* rz, float* seis_vx, float* seis_vz, int snap_interval,
+                           float* snaps, float* final_fields) {
+  StoreSpec ss;
+  ss.kind = store_kind;
+  ss.sv = sv;
+  ss.st = st;
+  ss.fp32_band = fp32_band;
+  return run_elastic2d<float>(nx, nz, ns, vp, vs, rho, dh, dt, nt, nbc, fd_order, v_ref, n_src,
+                              sx, sz, wavelet, n_rec, rx, rz, seis_vx, seis_vz, snap_interval,
+                              snaps, final_fields, ss);
+}
+
+// Element-wise storage rounding (checked against numpy's float16 in the tests).
+void oracle_round_store(int store_kind, const float* x, float* y, long long n) {
+  for (long long q = 0; q < n; ++q) y[q] = round_store(x[q], store_kind);
 }
 
 int oracle_acoustic2d(int prec, int nx, int nz, int ns, const float* vp, const float* rho,

@@ -46,6 +46,11 @@ def lib():
                                        C.c_float, C.c_float, C.c_int, C.c_int, C.c_int, C.c_float,
                                        C.c_int, _i32p, _i32p, _f32p, C.c_int, _i32p, _i32p,
                                        vp, vp, C.c_int, vp, vp]
+        L.oracle_elastic2d_store.restype = C.c_int
+        L.oracle_elastic2d_store.argtypes = [C.c_int, C.c_float, C.c_float, C.c_int] + \
+            L.oracle_elastic2d.argtypes[1:]
+        L.oracle_round_store.restype = None
+        L.oracle_round_store.argtypes = [C.c_int, vp, vp, C.c_longlong]
         L.oracle_acoustic2d.restype = C.c_int
         L.oracle_acoustic2d.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _f32p, _f32p,
                                         C.c_float, C.c_float, C.c_int, C.c_int, C.c_int, C.c_float,
@@ -115,9 +120,27 @@ def _src_matrix(sx, ns):
     return np.asfortranarray(a)
 
 
+STORE = {"fp32": 0, "fp16": 1, "bf16": 2}
+
+
+def round_store(x, store: str) -> np.ndarray:
+    """Round float32 values to the storage format (RNE) and back to float32."""
+    x = np.asfortranarray(np.asarray(x, dtype=np.float32))
+    y = np.empty_like(x, order="F")
+    lib().oracle_round_store(STORE[store], _ptr(x), _ptr(y), x.size)
+    return y
+
+
 def elastic2d(vp, vs, rho, dh, dt, nt, *, sx, sz, rx, rz, wavelet, nbc=50, fd_order=8,
-              v_ref=None, snap_interval=0, prec=32, n_shots=1, final=False):
-    """Elastic velocity-stress run.  ``sx``/``sz``: (n_src, n_shots).  ``wavelet``: (n_src, nt)."""
+              v_ref=None, snap_interval=0, prec=32, n_shots=1, final=False, store=None,
+              sv=1.0, st=1.0, fp32_band=0):
+    """Elastic velocity-stress run.  ``sx``/``sz``: (n_src, n_shots).  ``wavelet``: (n_src, nt).
+
+    ``store`` ("fp16"/"bf16") emulates FP32 arithmetic on wavefields stored
+    in that format under power-of-two scales ``sv`` (velocity) and ``st``
+    (stress); cells closer than ``fp32_band`` to an edge keep FP32 storage;
+    results are returned unscaled.
+    """
     vp, vs, rho = _f32(vp), _f32(vs), _f32(rho)
     nx, nz = vp.shape
     sxm, szm = _src_matrix(sx, n_shots), _src_matrix(sz, n_shots)
@@ -134,9 +157,17 @@ def elastic2d(vp, vs, rho, dh, dt, nt, *, sx, sz, rx, rz, wavelet, nbc=50, fd_or
     nxp, nzp = nx + 2 * (nbc + M), nz + 2 * (nbc + M)
     fin = np.zeros((nxp, nzp, 5, ns), dtype=T, order="F") if final else None
     vr = default_v_ref(vp) if v_ref is None else float(v_ref)
-    rc = lib().oracle_elastic2d(prec, nx, nz, ns, vp, vs, rho, dh, dt, nt, nbc, fd_order, vr,
-                                n_src, sxm, szm, w, nrec, rx, rz, _ptr(svx), _ptr(svz),
-                                snap_interval, _ptr(snaps), _ptr(fin))
+    if store is not None:
+        if prec != 32:
+            raise ValueError("storage emulation runs FP32 arithmetic")
+        rc = lib().oracle_elastic2d_store(STORE[store], sv, st, int(fp32_band), nx, nz, ns, vp, vs, rho, dh, dt,
+                                          nt, nbc, fd_order, vr, n_src, sxm, szm, w, nrec, rx,
+                                          rz, _ptr(svx), _ptr(svz), snap_interval, _ptr(snaps),
+                                          _ptr(fin))
+    else:
+        rc = lib().oracle_elastic2d(prec, nx, nz, ns, vp, vs, rho, dh, dt, nt, nbc, fd_order, vr,
+                                    n_src, sxm, szm, w, nrec, rx, rz, _ptr(svx), _ptr(svz),
+                                    snap_interval, _ptr(snaps), _ptr(fin))
     if rc != 0:
         raise RuntimeError(f"oracle_elastic2d failed: {rc}")
     return dict(seis_vx=svx, seis_vz=svz, snaps=snaps, final=fin)
