@@ -186,20 +186,16 @@ __device__ __forceinline__ void ac_vel_at(const Geo2& g, const Coef& c, float dt
   uz = vz;
 }
 
+// Velocity of time n+1 at (x, z) with the fused HABC (kernels_det.jl:22-57):
+// the shared body of the uniform-batch and uneven-batch kernels.
 template <int N>
-__global__ void __launch_bounds__(256) k_ac_vel(Geo2 g, Coef c, float dtx, float dtz, HabcDev h,
-                                                const float* __restrict__ p0,
-                                                const float* __restrict__ vx0,
-                                                const float* __restrict__ vz0,
-                                                const float* __restrict__ bx,
-                                                const float* __restrict__ bz,
-                                                float* __restrict__ vx1, float* __restrict__ vz1) {
-  int x = blockIdx.x * blockDim.x + threadIdx.x;
-  int z = blockIdx.y * blockDim.y + threadIdx.y;
-  if (x >= g.nx || z >= g.nz) return;
-  const long long so = (long long)blockIdx.z * g.plane;
-  p0 += so; vx0 += so; vz0 += so;
-  float ux, uz;
+__device__ __forceinline__ void ac_vel_cell(const Geo2& g, const Coef& c, float dtx, float dtz,
+                                            const HabcDev& h, const float* __restrict__ p0,
+                                            const float* __restrict__ vx0,
+                                            const float* __restrict__ vz0,
+                                            const float* __restrict__ bx,
+                                            const float* __restrict__ bz, int x, int z, float& ux,
+                                            float& uz) {
   ac_vel_at<N>(g, c, dtx, dtz, p0, vx0, vz0, bx, bz, x, z, ux, uz);
   long long p = (long long)z * g.ld + x;
   int sx, sz, dist;
@@ -224,6 +220,24 @@ __global__ void __launch_bounds__(256) k_ac_vel(Geo2 g, Coef c, float dtx, float
       uz = higdon_edge(wz, uz, higdon_side(h, nz_, foz, __ldg(vz0 + pn)));
     }
   }
+}
+
+template <int N>
+__global__ void __launch_bounds__(256) k_ac_vel(Geo2 g, Coef c, float dtx, float dtz, HabcDev h,
+                                                const float* __restrict__ p0,
+                                                const float* __restrict__ vx0,
+                                                const float* __restrict__ vz0,
+                                                const float* __restrict__ bx,
+                                                const float* __restrict__ bz,
+                                                float* __restrict__ vx1, float* __restrict__ vz1) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int z = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= g.nx || z >= g.nz) return;
+  const long long so = (long long)blockIdx.z * g.plane;
+  p0 += so; vx0 += so; vz0 += so;
+  float ux, uz;
+  ac_vel_cell<N>(g, c, dtx, dtz, h, p0, vx0, vz0, bx, bz, x, z, ux, uz);
+  long long p = (long long)z * g.ld + x;
   vx1[so + p] = ux;
   vz1[so + p] = uz;
 }
@@ -243,20 +257,13 @@ __device__ __forceinline__ float ac_prs_at(const Geo2& g, const Coef& c, float d
   return v;
 }
 
+// Pressure of time n+1 at (x, z) with the fused HABC.
 template <int N>
-__global__ void __launch_bounds__(256) k_ac_prs(Geo2 g, Coef c, float dtx, float dtz, HabcDev h,
-                                                const float* __restrict__ p0,
-                                                const float* __restrict__ vx1,
-                                                const float* __restrict__ vz1,
-                                                const float* __restrict__ kappa,
-                                                float* __restrict__ p1) {
-  int x = blockIdx.x * blockDim.x + threadIdx.x;
-  int z = blockIdx.y * blockDim.y + threadIdx.y;
-  if (x >= g.nx || z >= g.nz) return;
-  const long long so = (long long)blockIdx.z * g.plane;
-  p0 += so;
-  const float* vx = vx1 + so;
-  const float* vz = vz1 + so;
+__device__ __forceinline__ float ac_prs_cell(const Geo2& g, const Coef& c, float dtx, float dtz,
+                                             const HabcDev& h, const float* __restrict__ p0,
+                                             const float* __restrict__ vx,
+                                             const float* __restrict__ vz,
+                                             const float* __restrict__ kappa, int x, int z) {
   float u = ac_prs_at<N>(g, c, dtx, dtz, vx, vz, p0, kappa, x, z);
   long long p = (long long)z * g.ld + x;
   int sx, sz, dist;
@@ -276,7 +283,22 @@ __global__ void __launch_bounds__(256) k_ac_prs(Geo2 g, Coef c, float dtx, float
       u = higdon_edge(w, u, higdon_side(h, a, fo, __ldg(p0 + pn)));
     }
   }
-  p1[so + p] = u;
+  return u;
+}
+
+template <int N>
+__global__ void __launch_bounds__(256) k_ac_prs(Geo2 g, Coef c, float dtx, float dtz, HabcDev h,
+                                                const float* __restrict__ p0,
+                                                const float* __restrict__ vx1,
+                                                const float* __restrict__ vz1,
+                                                const float* __restrict__ kappa,
+                                                float* __restrict__ p1) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int z = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= g.nx || z >= g.nz) return;
+  const long long so = (long long)blockIdx.z * g.plane;
+  const float u = ac_prs_cell<N>(g, c, dtx, dtz, h, p0 + so, vx1 + so, vz1 + so, kappa, x, z);
+  p1[so + (long long)z * g.ld + x] = u;
 }
 
 // ---------------------------------------------------------------------------

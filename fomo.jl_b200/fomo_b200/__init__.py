@@ -10,6 +10,7 @@ from .api import (  # noqa: F401
     acoustic2d,
     acoustic3d,
     acoustic2d_batch,
+    acoustic2d_uneven,
     debug_medium2d,
     elastic2d,
     elastic2d_batch,

@@ -30,7 +30,7 @@ EXPORTS = (
     "fomo_version", "fomo_create", "fomo_destroy", "fomo_last_error", "fomo_set_stream",
     "fomo_trim", "fomo_check_numerics", "fomo_acoustic2d", "fomo_acoustic2d_batch",
     "fomo_elastic2d", "fomo_elastic2d_batch", "fomo_scalar2d", "fomo_debug_medium2d",
-    "fomo_scalar2d_noalloc", "fomo_acoustic3d", "fomo_elastic3d",
+    "fomo_scalar2d_noalloc", "fomo_acoustic3d", "fomo_elastic3d", "fomo_acoustic2d_uneven",
 )
 
 
@@ -56,6 +56,14 @@ class Acq3D(C.Structure):
     _fields_ = [("n_src", C.c_int32), ("sx", C.c_void_p), ("sy", C.c_void_p),
                 ("sz", C.c_void_p), ("wavelet", C.c_void_p), ("n_rec", C.c_int32),
                 ("rx", C.c_void_p), ("ry", C.c_void_p), ("rz", C.c_void_p)]
+
+
+class Shot2D(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("nz", C.c_int32), ("vp", C.c_void_p), ("rho", C.c_void_p),
+                ("n_src", C.c_int32), ("sx", C.c_void_p), ("sz", C.c_void_p),
+                ("wavelet", C.c_void_p), ("n_rec", C.c_int32), ("rx", C.c_void_p),
+                ("rz", C.c_void_p), ("v_ref", C.c_float), ("seis_p", C.c_void_p),
+                ("seis_vx", C.c_void_p), ("seis_vz", C.c_void_p)]
 
 
 class Opts(C.Structure):
@@ -111,6 +119,9 @@ def lib() -> C.CDLL:
             L.fomo_debug_medium2d.argtypes = [vp, i32, i32, i32, i32, f32, f32, vp, vp, vp, vp]
             L.fomo_scalar2d_noalloc.argtypes = [g, vp, a, vp, vp, C.c_char_p, i32]
             L.fomo_scalar2d_noalloc.restype = C.c_int
+            L.fomo_acoustic2d_uneven.argtypes = [vp, f32, f32, i32, i32, i32, i32,
+                                                 C.POINTER(Shot2D), o, s]
+            L.fomo_acoustic2d_uneven.restype = C.c_int
             g3, a3 = C.POINTER(Grid3D), C.POINTER(Acq3D)
             L.fomo_acoustic3d.argtypes = [vp, g3, vp, vp, a3, i32, i32, i32, vp, vp, vp, vp, o, s]
             L.fomo_elastic3d.argtypes = [vp, g3, vp, vp, vp, a3, i32, i32, i32, vp, vp, vp, vp,

@@ -18,7 +18,8 @@ from . import _lib as L
 
 __all__ = [
     "ArgumentError", "acoustic2d", "acoustic2d_batch", "elastic2d", "elastic2d_batch",
-    "scalar2d", "acoustic3d", "elastic3d", "ricker_wavelet", "get_fd_coefficients",
+    "scalar2d", "acoustic3d", "elastic3d", "acoustic2d_uneven", "ricker_wavelet",
+    "get_fd_coefficients",
     "get_centered_d2",
 ]
 
@@ -401,6 +402,79 @@ def scalar2d(vp, dh, dt, nt, f0, *, sx, sz, rx, rz, nbc: int = 50, fd_order: int
     ctx.check(L.lib().fomo_scalar2d(ctx.handle, C.byref(g), _ptr(vp), C.byref(acq), _ptr(seis),
                                     C.byref(o), C.byref(st)))
     return Scalar2DResult(seis, Stats(st.kernel_time_s))
+
+
+# ---------------------------------------------------------------------------
+# uneven-size batch (no reference counterpart; each shot equals acoustic2d)
+# ---------------------------------------------------------------------------
+class UnevenStats(NamedTuple):
+    kernel_time_s: float
+    n_shots: int
+    cell_updates: float
+    tile: tuple
+
+
+class Acoustic2DUnevenResult(NamedTuple):
+    shots: list  # per shot (seis_p, seis_vx, seis_vz), each (n_rec, nt)
+    stats: UnevenStats
+
+
+def acoustic2d_uneven(vps, rhos, dh, dt, nt, f0, *, sx, sz, rx, rz, nbc: int = 50,
+                      fd_order: int = 8, v_ref=None, wavelet=None,
+                      scale_source_by_dt: bool = False, device: int = 0) -> Acoustic2DUnevenResult:
+    """Many acoustic2d shots whose models differ in size, stepped together.
+
+    ``vps``/``rhos``: one (nx_s, nz_s) model per shot; ``sx``/``sz``: per shot
+    an index or a list of sources firing together; ``rx``/``rz``: per shot the
+    receiver indices; ``v_ref``: None (each shot's min positive vp), a number,
+    or one value per shot.  Each shot's seismograms equal ``acoustic2d`` on
+    that shot (equations/acoustic2d/acoustic2d.jl:47-192) bit for bit.
+    """
+    ns = len(vps)
+    if ns == 0 or len(rhos) != ns or len(sx) != ns or len(sz) != ns or len(rx) != ns \
+            or len(rz) != ns:
+        raise ArgumentError("vps, rhos, sx, sz, rx, rz need one entry per shot")
+    if fd_order not in _FD:
+        raise ValueError(f"Unsupported FD order: {fd_order}")
+    dh, dt, f0 = np.float32(dh), np.float32(dt), np.float32(f0)
+    models = [(_f32F(v), _f32F(r)) for v, r in zip(vps, rhos)]
+    vmax = max(float(v.max()) for v, _ in models)
+    vmin = min(float(_min_pos(v)) for v, _ in models)
+    _check_numerics(vmax, vmin, dh, dt, f0, fd_order)
+    w = _wavelet_row(wavelet, f0, dt, nt)
+    if scale_source_by_dt:
+        w = (w * dt).astype(np.float32)
+    keep = []  # arrays referenced by the descriptors must outlive the call
+    descs = (L.Shot2D * ns)()
+    results = []
+    for s, (vp, rho) in enumerate(models):
+        if vp.shape != rho.shape or vp.ndim != 2:
+            raise ArgumentError(f"shot {s + 1}: vp and rho must be matching 2D arrays")
+        nx, nz = vp.shape
+        sxv, szv = _i32F(np.atleast_1d(sx[s])).ravel(), _i32F(np.atleast_1d(sz[s])).ravel()
+        rxv, rzv = _i32F(rx[s]).ravel(), _i32F(rz[s]).ravel()
+        if sxv.size != szv.size or rxv.size != rzv.size:
+            raise ArgumentError(f"shot {s + 1}: coordinate lengths differ")
+        _check_geometry(nx, nz, sxv, szv, rxv, rzv)
+        wm = np.asfortranarray(np.repeat(w[None, :], sxv.size, axis=0))
+        seis = [np.zeros((rxv.size, nt), dtype=np.float32, order="F") for _ in range(3)]
+        vr = v_ref[s] if isinstance(v_ref, (list, tuple, np.ndarray)) else v_ref
+        vr = 0.0 if vr is None else float(np.float32(vr))
+        d = descs[s]
+        d.nx, d.nz, d.vp, d.rho = nx, nz, _ptr(vp), _ptr(rho)
+        d.n_src, d.sx, d.sz, d.wavelet = sxv.size, _ptr(sxv), _ptr(szv), _ptr(wm)
+        d.n_rec, d.rx, d.rz, d.v_ref = rxv.size, _ptr(rxv), _ptr(rzv), vr
+        d.seis_p, d.seis_vx, d.seis_vz = _ptr(seis[0]), _ptr(seis[1]), _ptr(seis[2])
+        keep += [vp, rho, sxv, szv, rxv, rzv, wm]
+        results.append(tuple(seis))
+    st = L.Stats()
+    ctx = L.context(device)
+    o = _opts()
+    ctx.check(L.lib().fomo_acoustic2d_uneven(ctx.handle, float(dh), float(dt), int(nt), int(nbc),
+                                             int(fd_order), ns, descs, C.byref(o), C.byref(st)))
+    del keep
+    tile = (st.sweep_config // 1000, st.sweep_config % 1000)
+    return Acoustic2DUnevenResult(results, UnevenStats(st.kernel_time_s, ns, st.cell_updates, tile))
 
 
 # ---------------------------------------------------------------------------

@@ -131,3 +131,26 @@ def elastic3d_config(nx=400, ny=400, nz=300, seed=4, vmax=5000.0):
     rx, ry = gx.ravel(order="F"), gy.ravel(order="F")
     return dict(vp=vp, vs=vs, rho=rho, dh=10.0, dt=8e-4, nt=2500, f0=12.0, fd_order=8, nbc=40,
                 sx=[nx // 2], sy=[ny // 2], sz=[10], rx=rx, ry=ry, rz=np.full(rx.size, 10))
+
+
+def uneven_batch_config(n_shots=64, seed=3, nt=2000):
+    """Uneven acoustic batch: n_shots grids with nx ~ logU(200, 2000), nz ~
+    logU(200, 800) (seed), dh 10 m, order 8, nt 2000, dt 1 ms, nbc 50; per shot
+    vp a Gaussian random field (mean 3000, std 600, correlation 300 m, clipped
+    to 1500..5000, seed+s), rho 2000; source (nx//2, 10), receivers every 2nd x
+    on z=10, 15 Hz."""
+    rng = np.random.default_rng(seed)
+    nxs = np.rint(np.exp(rng.uniform(np.log(200), np.log(2000), n_shots))).astype(int)
+    nzs = np.rint(np.exp(rng.uniform(np.log(200), np.log(800), n_shots))).astype(int)
+    vps, rhos, sx, sz, rx, rz = [], [], [], [], [], []
+    for s in range(n_shots):
+        nx, nz = int(nxs[s]), int(nzs[s])
+        vps.append(grf2d(nx, nz, 10.0, 3000.0, 600.0, 300.0, seed + s, 1500.0, 5000.0))
+        rhos.append(np.full((nx, nz), 2000.0, dtype=np.float32, order="F"))
+        sx.append(nx // 2)
+        sz.append(10)
+        r = np.arange(1, nx + 1, 2)
+        rx.append(r)
+        rz.append(np.full(r.size, 10))
+    return dict(vps=vps, rhos=rhos, dh=10.0, dt=1e-3, nt=nt, f0=15.0, fd_order=8, nbc=50,
+                sx=sx, sz=sz, rx=rx, rz=rz)

@@ -160,6 +160,36 @@ FOMO_API int fomo_elastic2d_batch(fomo_ctx* ctx, const fomo_grid2d* g, const flo
 FOMO_API int fomo_scalar2d(fomo_ctx* ctx, const fomo_grid2d* g, const float* vp, const fomo_acq* acq,
                   float* seis_u, const fomo_opts* opts, fomo_stats* stats);
 
+/* ---- uneven-size batch -----------------------------------------------------
+ * No single counterpart in the reference: acoustic2d_batch
+ * (equations/acoustic2d/batch.jl:180-261) needs one shared model, so shots on
+ * grids of different size are separate acoustic2d calls there.  Here each
+ * shot brings its own model and acquisition and all shots step together in
+ * one graph-captured run.  Every shot's seismograms equal a single
+ * fomo_acoustic2d run of that shot bit for bit. */
+typedef struct fomo_shot2d {
+  int32_t nx, nz;        /* interior grid of this shot                          */
+  const float* vp;       /* (nx, nz) host arrays                                */
+  const float* rho;
+  int32_t n_src;         /* sources firing together                             */
+  const int32_t* sx;     /* (n_src), 1-based interior indices                   */
+  const int32_t* sz;
+  const float* wavelet;  /* (n_src, nt), injected raw                           */
+  int32_t n_rec;
+  const int32_t* rx;     /* (n_rec), 1-based interior indices                   */
+  const int32_t* rz;
+  float v_ref;           /* <= 0 selects min(vp > 0) of this shot               */
+  float* seis_p;         /* (n_rec, nt) host outputs, each may be NULL          */
+  float* seis_vx;
+  float* seis_vz;
+} fomo_shot2d;
+
+/* Host arrays only (FOMO_F_DEVICE_PTRS returns FOMO_EUNSUPPORTED); FP32.
+ * stats->sweep_config = tile width * 1000 + tile height of the chosen tiles. */
+FOMO_API int fomo_acoustic2d_uneven(fomo_ctx* ctx, float dh, float dt, int32_t nt, int32_t nbc,
+                                    int32_t fd_order, int32_t n_shots, const fomo_shot2d* shots,
+                                    const fomo_opts* opts, fomo_stats* stats);
+
 /* ---- 3D solvers ------------------------------------------------------------ */
 typedef struct fomo_grid3d {
   int32_t nx, ny, nz; /* interior grid                                          */

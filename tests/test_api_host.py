@@ -95,3 +95,18 @@ def test_synthetic_layered_config(fomo):
     assert 1500 <= c["vp"].min() and c["vp"].max() <= 4500
     assert np.allclose(c["vs"], c["vp"] / 1.73, rtol=1e-6)
     assert len(np.unique(c["vp"][0])) == 12
+
+
+def test_uneven_batch_validation(fomo):
+    vp1, rho1 = _acoustic_inputs(40, 30)
+    vp2, rho2 = _acoustic_inputs(25, 35)
+    kw = dict(sx=[20, 12], sz=[3, 3], rx=[[4, 8], [5]], rz=[[3, 3], [4]])
+    with pytest.raises(fomo.ArgumentError):  # one entry per shot
+        fomo.acoustic2d_uneven([vp1, vp2], [rho1], 10.0, 1e-3, 50, 15.0, **kw)
+    with pytest.raises(fomo.ArgumentError):  # receiver outside shot 2's grid
+        fomo.acoustic2d_uneven([vp1, vp2], [rho1, rho2], 10.0, 1e-3, 50, 15.0,
+                               **dict(kw, rx=[[4], [30]], rz=[[3], [3]]))
+    with pytest.raises(fomo.ArgumentError):  # CFL over the fastest shot
+        fomo.acoustic2d_uneven([vp1, vp2 * 3], [rho1, rho2], 10.0, 1e-3, 50, 15.0, **kw)
+    with pytest.raises(ValueError):
+        fomo.acoustic2d_uneven([vp1, vp2], [rho1, rho2], 10.0, 1e-3, 50, 15.0, fd_order=7, **kw)
