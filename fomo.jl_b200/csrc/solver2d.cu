@@ -15,6 +15,12 @@
 #include "sweep2d.cuh"
 
 namespace fomo {
+// learned corrector (corrector.cu)
+cudaError_t corr_forward_device(cudaStream_t st, int h, int w, const float* u, const float* up,
+                                const float* c2, long long ld, int n_src, const int* src,
+                                const float* inj_next, const float* inj_prev,
+                                const float* params, void* scratch, float* y, bool pack);
+size_t corr_scratch_bytes(long long npix);
 namespace {
 
 enum Phys { kAcoustic = 0, kElastic = 1, kScalar = 2 };
@@ -219,9 +225,26 @@ struct Outs {
   float* snaps;
 };
 
+// Per-step extension of the scalar loop (learned correction, wavefield
+// snapshots).  correct() runs after the step and the injection of step it and
+// before the recording; u2 = u^{n+1}, u1 = u^n, u0 = u^{n-1} (padded, pitched).
+struct ScalarHook {
+  virtual ~ScalarHook() = default;
+  // wav: the run's device wavelet matrix (n_src, nt)
+  virtual int begin(fomo_ctx*, cudaStream_t, const Plan2&, const float*) { return FOMO_OK; }
+  virtual int correct(fomo_ctx*, cudaStream_t, int, float*, const float*, const float*,
+                      const float*, const Plan2&) {
+    return FOMO_OK;
+  }
+  virtual int after_step(fomo_ctx*, cudaStream_t, int, const float*, const Plan2&) { return FOMO_OK; }
+  virtual bool corrects() const { return false; }
+  virtual int launches_per_step() const { return 0; }
+};
+
 // Common run: model (vp, vs, rho per phys), acquisition, outputs.
 int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float* rho,
-          const fomo_acq* acq, Outs outs, const fomo_opts* opts, fomo_stats* stats) {
+          const fomo_acq* acq, Outs outs, const fomo_opts* opts, fomo_stats* stats,
+          ScalarHook* hook = nullptr) {
   FOMO_CU(ctx, cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
   const long long nint = (long long)P.nx * P.nz;
@@ -364,6 +387,8 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
     return cudaEventRecord(pev[2 * k + which], st);
   };
   int sweeps_per_step = 0;
+  if (hook)
+    if (int hr = hook->begin(ctx, st, P, d_wav)) return hr;
   FOMO_CU(ctx, cudaEventRecord(ctx->ev0, st));
   int A = 0, B = 1, C2 = 2;  // scalar: A = u^{n-1}, B = u^n, C2 = u^{n+1}
   for (int it = 1; it <= P.nt; ++it) {
@@ -427,10 +452,25 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
 #undef FOMO_SC_CASE
       sweeps_per_step = 1;
       FOMO_CU(ctx, prof_mark(it, 1));
-      k_inject_record<<<1, 256, 0, st>>>(it, P.nt, P.plane, P.n_src, d_src, d_wav, field(C2, 0),
-                                         nullptr, P.n_rec, d_rec, field(C2, 0), nullptr, nullptr,
-                                         d_seis[0], nullptr, nullptr);
-      launches += 2;
+      if (hook && hook->corrects()) {
+        // inject, correct u^{n+1}, then record the corrected field
+        k_inject_record<<<1, 256, 0, st>>>(it, P.nt, P.plane, P.n_src, d_src, d_wav, field(C2, 0),
+                                           nullptr, 0, d_rec, nullptr, nullptr, nullptr, nullptr,
+                                           nullptr, nullptr);
+        if (int hr = hook->correct(ctx, st, it, field(C2, 0), field(B, 0), field(A, 0), d_mat, P))
+          return hr;
+        k_inject_record<<<1, 256, 0, st>>>(it, P.nt, P.plane, 0, d_src, d_wav, nullptr, nullptr,
+                                           P.n_rec, d_rec, field(C2, 0), nullptr, nullptr,
+                                           d_seis[0], nullptr, nullptr);
+        launches += 3 + hook->launches_per_step();
+      } else {
+        k_inject_record<<<1, 256, 0, st>>>(it, P.nt, P.plane, P.n_src, d_src, d_wav, field(C2, 0),
+                                           nullptr, P.n_rec, d_rec, field(C2, 0), nullptr, nullptr,
+                                           d_seis[0], nullptr, nullptr);
+        launches += 2;
+      }
+      if (hook)
+        if (int hr = hook->after_step(ctx, st, it, field(C2, 0), P)) return hr;
     }
     FOMO_CU(ctx, cudaGetLastError());
     // snapshot of the interior (fused_kernels.jl:192-195): p (acoustic), vz (elastic)
@@ -509,6 +549,110 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
   return FOMO_OK;
 }
 
+// ---- scalar2d extensions: strided snapshots and the learned correction ----
+__global__ void k_snap_stride(const float* __restrict__ u, long long ld, int pad, int nx, int nz,
+                              int stride, int mx, float* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+  if (i >= mx || i * stride >= nx || j * stride >= nz) return;
+  out[i + (long long)mx * j] = u[(long long)(pad + j * stride) * ld + pad + i * stride];
+}
+
+// u (interior origin, pitch ld) += y (window with a margin of `mg` cells on
+// every side, row length nx + 2 mg), except within src_r cells of a source.
+__global__ void k_add_interior(float* __restrict__ u, long long ld, int nx, int nz, int mg,
+                               const float* __restrict__ y, const int* __restrict__ src, int n_src,
+                               int src_r) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, z = blockIdx.y;
+  if (x >= nx || z >= nz) return;
+  for (int q = 0; q < n_src; ++q)
+    if (abs(x - src[2 * q]) <= src_r && abs(z - src[2 * q + 1]) <= src_r) return;
+  float* p = u + (long long)z * ld + x;
+  *p = __fadd_rn(*p, y[(long long)(z + mg) * (nx + 2 * mg) + x + mg]);
+}
+
+struct SnapHook : ScalarHook {
+  int from = 1, every = 1, stride = 1, mx = 0, mz = 0, count = 0;
+  float* out = nullptr;  // device (mx, mz, count)
+  int after_step(fomo_ctx* ctx, cudaStream_t st, int it, const float* u2, const Plan2& P) override {
+    if (it < from || (it - from) % every != 0) return FOMO_OK;
+    const int k = (it - from) / every;
+    if (k >= count) return FOMO_OK;
+    k_snap_stride<<<dim3(cdiv(mx, 128), mz), 128, 0, st>>>(u2, P.ld, P.pad, P.nx, P.nz, stride, mx,
+                                                        out + (long long)k * mx * mz);
+    FOMO_CU(ctx, cudaGetLastError());
+    return FOMO_OK;
+  }
+};
+
+// The corrector sees a window reaching kCorrMargin cells into the absorbing
+// zone (its receptive field), so interior cells get real neighbours, and the
+// values injected at the sources in this and the previous step.  The
+// correction is added to interior cells except within kCorrSrcR cells of a
+// source, the cells its training targets leave out.
+constexpr int kCorrMargin = 3;
+constexpr int kCorrSrcR = 3;
+
+struct CorrHook : ScalarHook {
+  const float* params = nullptr;  // host or device (kNParam floats)
+  bool dev = false;
+  std::vector<int> src_xz;        // 0-based interior source cells
+  const float* wav = nullptr;     // device wavelet matrix (n_src, nt) of the run
+  float* d_params = nullptr;
+  float* d_y = nullptr;
+  int* d_src = nullptr;      // window coordinates
+  int* d_src_int = nullptr;  // interior coordinates
+  void* scratch = nullptr;
+  int mg = 0;
+  ~CorrHook() override {
+    if (d_params) cudaFree(d_params);
+    if (d_y) cudaFree(d_y);
+    if (d_src) cudaFree(d_src);
+    if (d_src_int) cudaFree(d_src_int);
+    if (scratch) cudaFree(scratch);
+  }
+  bool corrects() const override { return true; }
+  int launches_per_step() const override { return 5; }
+  int begin(fomo_ctx* ctx, cudaStream_t st, const Plan2& P, const float* d_wav) override {
+    wav = d_wav;
+    mg = std::min(kCorrMargin, P.pad);
+    const long long npix = (long long)(P.nx + 2 * mg) * (P.nz + 2 * mg);
+    const int np = fomo_corr_param_count();
+    FOMO_CU(ctx, cudaMalloc(&d_params, sizeof(float) * np));
+    FOMO_CU(ctx, cudaMalloc(&d_y, sizeof(float) * npix));
+    FOMO_CU(ctx, cudaMalloc(&d_src, sizeof(int) * std::max<size_t>(src_xz.size(), 2)));
+    FOMO_CU(ctx, cudaMalloc(&d_src_int, sizeof(int) * std::max<size_t>(src_xz.size(), 2)));
+    if (!src_xz.empty())
+      FOMO_CU(ctx, cudaMemcpyAsync(d_src_int, src_xz.data(), sizeof(int) * src_xz.size(),
+                                   cudaMemcpyHostToDevice, st));
+    FOMO_CU(ctx, cudaMalloc(&scratch, corr_scratch_bytes(npix)));
+    FOMO_CU(ctx, cudaMemcpyAsync(d_params, params, sizeof(float) * np,
+                                 dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+    // source cells in window coordinates (the window starts mg cells outside)
+    std::vector<int> win(src_xz);
+    for (int& v : win) v += mg;
+    if (!win.empty())
+      FOMO_CU(ctx, cudaMemcpyAsync(d_src, win.data(), sizeof(int) * win.size(),
+                                   cudaMemcpyHostToDevice, st));
+    FOMO_CU(ctx, cudaStreamSynchronize(st));  // src_xz is host memory owned by this hook
+    return FOMO_OK;
+  }
+  int correct(fomo_ctx* ctx, cudaStream_t st, int it, float* u2, const float* u1, const float* u0,
+              const float* c2, const Plan2& P) override {
+    const long long off = (long long)P.pad * P.ld + P.pad;             // interior origin
+    const long long wof = (long long)(P.pad - mg) * P.ld + (P.pad - mg);  // window origin
+    const int ns = (int)src_xz.size() / 2;
+    const float* inj_next = wav ? wav + (long long)(it - 1) * ns : nullptr;
+    const float* inj_prev = (wav && it > 1) ? wav + (long long)(it - 2) * ns : nullptr;
+    FOMO_CU(ctx, corr_forward_device(st, P.nz + 2 * mg, P.nx + 2 * mg, u1 + wof, u0 + wof,
+                                     c2 + wof, P.ld, ns, d_src, inj_next, inj_prev, d_params,
+                                     scratch, d_y, it == 1));
+    k_add_interior<<<dim3(cdiv(P.nx, 128), P.nz), 128, 0, st>>>(
+        u2 + off, P.ld, P.nx, P.nz, mg, d_y, d_src_int, ns, kCorrSrcR);
+    FOMO_CU(ctx, cudaGetLastError());
+    return FOMO_OK;
+  }
+};
+
 }  // namespace
 }  // namespace fomo
 
@@ -563,6 +707,51 @@ int fomo_scalar2d(fomo_ctx* ctx, const fomo_grid2d* g, const float* vp, const fo
   if (rc) return rc;
   Outs o{{seis_u, nullptr, nullptr}, 1, nullptr};
   return run2d(ctx, P, vp, nullptr, nullptr, acq, o, opts, stats);
+}
+
+int fomo_scalar2d_snapshots(fomo_ctx* ctx, const fomo_grid2d* g, const float* vp,
+                            const fomo_acq* acq, int32_t snap_from, int32_t snap_every,
+                            int32_t stride, float* snaps, float* seis_u, const fomo_opts* opts,
+                            fomo_stats* stats) {
+  if (!opts || !(opts->flags & FOMO_F_DEVICE_PTRS))
+    return fail(ctx, FOMO_EUNSUPPORTED, "scalar2d snapshots need FOMO_F_DEVICE_PTRS");
+  if (!g || snap_from < 1 || snap_every < 1 || stride < 1 || !snaps)
+    return fail(ctx, FOMO_EARG, "bad snapshot arguments");
+  Plan2 P;
+  int rc = make_plan(ctx, kScalar, g, acq, 0, opts, false, P);
+  if (rc) return rc;
+  SnapHook hk;
+  hk.from = snap_from;
+  hk.every = snap_every;
+  hk.stride = stride;
+  hk.mx = (g->nx + stride - 1) / stride;
+  hk.mz = (g->nz + stride - 1) / stride;
+  hk.count = g->nt >= snap_from ? (g->nt - snap_from) / snap_every + 1 : 0;
+  hk.out = snaps;
+  Outs o{{seis_u, nullptr, nullptr}, 1, nullptr};
+  return run2d(ctx, P, vp, nullptr, nullptr, acq, o, opts, stats, &hk);
+}
+
+int fomo_scalar2d_corrected(fomo_ctx* ctx, const fomo_grid2d* g, const float* vp,
+                            const fomo_acq* acq, const float* params, float* seis_u,
+                            const fomo_opts* opts, fomo_stats* stats) {
+  if (!params) return fail(ctx, FOMO_EARG, "corrector parameters are required");
+  Plan2 P;
+  int rc = make_plan(ctx, kScalar, g, acq, 0, opts, false, P);
+  if (rc) return rc;
+  CorrHook hk;
+  hk.params = params;
+  hk.dev = opts && (opts->flags & FOMO_F_DEVICE_PTRS);
+  std::vector<int32_t> hx, hz;
+  if ((rc = host_copy(ctx, acq->sx, P.n_src, P.dev, hx)) ||
+      (rc = host_copy(ctx, acq->sz, P.n_src, P.dev, hz)))
+    return rc;
+  for (int q = 0; q < P.n_src; ++q) {
+    hk.src_xz.push_back(hx[q] - 1);
+    hk.src_xz.push_back(hz[q] - 1);
+  }
+  Outs o{{seis_u, nullptr, nullptr}, 1, nullptr};
+  return run2d(ctx, P, vp, nullptr, nullptr, acq, o, opts, stats, &hk);
 }
 
 int fomo_debug_medium2d(fomo_ctx* ctx, int32_t kind, int32_t nx, int32_t nz, int32_t pad,

@@ -31,6 +31,8 @@ EXPORTS = (
     "fomo_trim", "fomo_check_numerics", "fomo_acoustic2d", "fomo_acoustic2d_batch",
     "fomo_elastic2d", "fomo_elastic2d_batch", "fomo_scalar2d", "fomo_debug_medium2d",
     "fomo_scalar2d_noalloc", "fomo_acoustic3d", "fomo_elastic3d", "fomo_acoustic2d_uneven",
+    "fomo_corr_param_count", "fomo_corr_features", "fomo_corr_target", "fomo_corr_forward",
+    "fomo_corr_gradients", "fomo_corr_adam", "fomo_scalar2d_snapshots", "fomo_scalar2d_corrected",
 )
 
 
@@ -122,6 +124,22 @@ def lib() -> C.CDLL:
             L.fomo_acoustic2d_uneven.argtypes = [vp, f32, f32, i32, i32, i32, i32,
                                                  C.POINTER(Shot2D), o, s]
             L.fomo_acoustic2d_uneven.restype = C.c_int
+            i64 = C.c_int64
+            L.fomo_corr_param_count.restype = C.c_int
+            L.fomo_corr_param_count.argtypes = []
+            L.fomo_corr_features.argtypes = [vp, i32, i32, i32, vp, vp, vp, i64, vp, i64, vp, i64,
+                                             vp, i32, vp, vp, vp, vp]
+            L.fomo_corr_target.argtypes = [vp, i32, i32, i32, i32, vp, vp, vp, vp, i64, vp, i64, vp,
+                                           i64, vp, vp, vp, i32, vp, vp]
+            L.fomo_corr_forward.argtypes = [vp, i32, i32, i32, vp, vp, vp]
+            L.fomo_corr_gradients.argtypes = [vp, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp]
+            L.fomo_corr_adam.argtypes = [vp, i32, vp, vp, vp, vp, f32, f32, f32, f32, i32]
+            L.fomo_scalar2d_snapshots.argtypes = [vp, g, vp, a, i32, i32, i32, vp, vp, o, s]
+            L.fomo_scalar2d_corrected.argtypes = [vp, g, vp, a, vp, vp, o, s]
+            for name in ("fomo_corr_features", "fomo_corr_target", "fomo_corr_forward",
+                         "fomo_corr_gradients", "fomo_corr_adam", "fomo_scalar2d_snapshots",
+                         "fomo_scalar2d_corrected"):
+                getattr(L, name).restype = C.c_int
             g3, a3 = C.POINTER(Grid3D), C.POINTER(Acq3D)
             L.fomo_acoustic3d.argtypes = [vp, g3, vp, vp, a3, i32, i32, i32, vp, vp, vp, vp, o, s]
             L.fomo_elastic3d.argtypes = [vp, g3, vp, vp, vp, a3, i32, i32, i32, vp, vp, vp, vp,
@@ -152,6 +170,13 @@ class Context:
 
     def set_stream(self, stream_ptr: int | None) -> None:
         self.check(lib().fomo_set_stream(self.handle, C.c_void_p(stream_ptr or 0)))
+
+    def use_torch_stream(self, stream) -> None:
+        """Run on a torch stream.  torch reports its legacy default stream as 0,
+        which fomo_set_stream would read as "the context's own (non-blocking)
+        stream"; pass CUDA's legacy-stream handle (1) for it instead."""
+        ptr = int(stream.cuda_stream)
+        self.check(lib().fomo_set_stream(self.handle, C.c_void_p(ptr if ptr else 1)))
 
     def close(self) -> None:
         if getattr(self, "handle", None):

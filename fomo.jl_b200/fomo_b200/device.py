@@ -33,7 +33,7 @@ def elastic2d_batch(vp, vs, rho, *, dh, dt, nt, nbc, fd_order, v_ref, sx, sz, wa
     nz, nx = vp.shape
     ns, n_src = sx.shape
     ctx = L.context(device)
-    ctx.set_stream(torch.cuda.current_stream(vp.device).cuda_stream)
+    ctx.use_torch_stream(torch.cuda.current_stream(vp.device))
     g = L.Grid2D(nx, nz, float(dh), float(dt), int(nt), int(nbc), int(fd_order), float(v_ref))
     acq = L.Acq(ns, n_src, _p(sx), _p(sz), _p(wavelet), rx.numel(), _p(rx), _p(rz))
     o = L.Opts()

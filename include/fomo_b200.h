@@ -229,6 +229,69 @@ FOMO_API int fomo_elastic3d(fomo_ctx* ctx, const fomo_grid3d* g, const float* vp
                             int32_t snap_plane, int32_t snap_index, float* seis_vx, float* seis_vy,
                             float* seis_vz, float* snaps, const fomo_opts* opts, fomo_stats* stats);
 
+/* ---- learned coarse-grid corrector ------------------------------------------
+ * No reference counterpart.  A 3-layer 3x3 CNN (6 -> 16 -> 16 -> 1 channels,
+ * bias-free, ReLU between layers; BF16 tensor-core implicit GEMM with FP32
+ * accumulation) predicts a per-step correction of u^{n+1} on a coarse grid
+ * from the features (u^n, u^{n-1}, c2 u^n, c2^2 u^n, s^{n+1}, s^n), with
+ * c2 = (vp dt / dh)^2 and s the values injected at the source cells.
+ * Parameters: fomo_corr_param_count() FP32 values, W1[9][6][16] then
+ * W2[9][16][16] then W3[9][16], index [tap = 3*dz + dx][in][out].
+ * Images are (n, h, w) with x fastest; features are BF16 (n, h, w, 16).
+ * All pointers of the fomo_corr_* calls are DEVICE pointers on the
+ * context's stream. */
+FOMO_API int fomo_corr_param_count(void);
+/* Features of n windows (h x w, row pitch ld) of the wavefields: window k
+ * starts at u_off[k] (or k*u_stride when u_off is NULL) in u and in u_prev,
+ * at c2_off[k] (or k*c2_stride) in c2; values are multiplied by scale[k]
+ * (NULL = 1).  Window k holds n_src source cells (x, z) at src[2(k n_src + q)]
+ * (window coordinates) that received inj_next[k n_src + q] in this step and
+ * inj_prev[k n_src + q] in the previous one (either may be NULL = 0). */
+FOMO_API int fomo_corr_features(fomo_ctx* ctx, int32_t n, int32_t h, int32_t w, const float* u,
+                                const float* u_prev, const float* c2, int64_t ld,
+                                const int64_t* u_off, int64_t u_stride, const int64_t* c2_off,
+                                int64_t c2_stride, const float* scale, int32_t n_src,
+                                const int32_t* src, const float* inj_next, const float* inj_prev,
+                                uint16_t* feat);
+/* Training target of the same windows: scale[k] * (u_next - (scalar2d step of
+ * (u, u_prev) + inj[k] at the window cell src[2k], src[2k+1])), using the
+ * solver's own arithmetic; mask = 0 (target 0) within max(fd_order/2, 3) of
+ * the window edge and within src_r of the source, else 1. */
+FOMO_API int fomo_corr_target(fomo_ctx* ctx, int32_t n, int32_t h, int32_t w, int32_t fd_order,
+                              const float* u, const float* u_prev, const float* u_next,
+                              const float* c2, int64_t ld, const int64_t* u_off, int64_t u_stride,
+                              const int64_t* c2_off, int64_t c2_stride, const float* scale,
+                              const int32_t* src, const float* inj, int32_t src_r, float* target,
+                              float* mask);
+FOMO_API int fomo_corr_forward(fomo_ctx* ctx, int32_t n, int32_t h, int32_t w,
+                               const uint16_t* feat, const float* params, float* y);
+/* loss = mean over pixels of (mask * (y - target))^2 (mask may be NULL) and its
+ * gradient with respect to the parameters; w % 16 == 0; y_out may be NULL. */
+FOMO_API int fomo_corr_gradients(fomo_ctx* ctx, int32_t n, int32_t h, int32_t w,
+                                 const uint16_t* feat, const float* target, const float* mask,
+                                 const float* params, float* grad, float* loss, float* y_out);
+FOMO_API int fomo_corr_adam(fomo_ctx* ctx, int32_t count, float* params, const float* grad,
+                            float* m, float* v, float lr, float beta1, float beta2, float eps,
+                            int32_t step);
+
+/* scalar2d that also writes the interior wavefield every snap_every steps from
+ * step snap_from on, sampled every `stride` cells from interior (1,1), as
+ * (ceil(nx/stride), ceil(nz/stride), count) into `snaps`.  Requires
+ * FOMO_F_DEVICE_PTRS.  Produces the training pairs of the corrector. */
+FOMO_API int fomo_scalar2d_snapshots(fomo_ctx* ctx, const fomo_grid2d* g, const float* vp,
+                                     const fomo_acq* acq, int32_t snap_from, int32_t snap_every,
+                                     int32_t stride, float* snaps, float* seis_u,
+                                     const fomo_opts* opts, fomo_stats* stats);
+/* scalar2d with the corrector applied to the interior after every step and
+ * injection (before recording); params as for fomo_corr_* (host pointer
+ * unless FOMO_F_DEVICE_PTRS).  The network sees the interior plus 3 cells of
+ * the absorbing zone; the correction is added to interior cells farther than
+ * 3 cells from every source.  All-zero parameters give fomo_scalar2d's result
+ * bit for bit. */
+FOMO_API int fomo_scalar2d_corrected(fomo_ctx* ctx, const fomo_grid2d* g, const float* vp,
+                                     const fomo_acq* acq, const float* params, float* seis_u,
+                                     const fomo_opts* opts, fomo_stats* stats);
+
 /* ---- allocation-free entry -------------------------------------------------
  * No counterpart in the reference.  scalar2d for callers that cannot allocate
  * device memory (a plugin inside a framework whose allocator owns all device

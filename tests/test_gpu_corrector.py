@@ -1,0 +1,164 @@
+"""The learned corrector's tensor-core kernels against the CPU oracle
+(oracle/corrector_ref.py): forward values and parameter gradients.
+
+The oracle in bf16 mode rounds weights, stored activations and propagated
+gradients as the GPU stores them, leaving only FP32 accumulation order: tight
+tolerance.  Against the plain float64 oracle the BF16 storage error shows:
+loose tolerance.  Also: an all-zero corrector leaves scalar2d unchanged bit
+for bit."""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(n=3, h=20, w=32, seed=0):
+    import torch
+
+    from fomo_b200 import corrector as CR
+
+    K = CR.Kernels(0)
+    rng = np.random.default_rng(seed)
+    u = rng.standard_normal((n, h, w)).astype(np.float32)
+    up = rng.standard_normal((n, h, w)).astype(np.float32)
+    c2 = rng.uniform(0.02, 0.2, (n, h, w)).astype(np.float32)
+    dev = K.dev
+    tu, tup, tc = (torch.from_numpy(a).to(dev) for a in (u, up, c2))
+    off = torch.tensor([k * h * w for k in range(n)], dtype=torch.int64, device=dev)
+    feat = K.features(int(tu.data_ptr()), int(tup.data_ptr()), int(tc.data_ptr()), w, off, off,
+                      None, n, h, w)
+    torch.cuda.synchronize()
+    # the GPU's own bf16 features are the common input of both sides
+    fnp = feat.float().cpu().numpy()[..., :6].astype(np.float64)
+    params = (rng.standard_normal(CR.param_count()) * 0.3).astype(np.float32)
+    return K, feat, fnp, params, rng
+
+
+def test_corrector_features_are_bf16_of_products():
+    from oracle import corrector_ref as R
+
+    K, feat, fnp, params, rng = _setup(n=2, h=9, w=16, seed=3)
+    rng = np.random.default_rng(3)
+    u = rng.standard_normal((2, 9, 16)).astype(np.float32)
+    up = rng.standard_normal((2, 9, 16)).astype(np.float32)
+    c2 = rng.uniform(0.02, 0.2, (2, 9, 16)).astype(np.float32)
+    ca = (c2 * u).astype(np.float32)
+    z = np.zeros_like(u)
+    want = np.stack([u, up, ca, (c2 * ca).astype(np.float32), z, z], axis=-1)
+    assert np.array_equal(fnp, R.bf16_round(want))
+
+
+def test_corrector_source_channels():
+    import torch
+
+    from oracle import corrector_ref as R
+
+    K, _, _, _, _ = _setup(n=1, h=8, w=16)
+    dev = K.dev
+    u = torch.zeros((2, 8, 16), dtype=torch.float32, device=dev)
+    c2 = torch.zeros((8, 16), dtype=torch.float32, device=dev)
+    off = torch.tensor([0, 128], dtype=torch.int64, device=dev)
+    coff = torch.zeros(2, dtype=torch.int64, device=dev)
+    src = torch.tensor([3, 5, 10, 2], dtype=torch.int32, device=dev)
+    nxt = torch.tensor([0.5, -2.0], dtype=torch.float32, device=dev)
+    prv = torch.tensor([0.25, 1.0], dtype=torch.float32, device=dev)
+    sc = torch.tensor([2.0, 1.0], dtype=torch.float32, device=dev)
+    base = int(u.data_ptr())
+    feat = K.features(base, base, int(c2.data_ptr()), 16, off, coff, sc, 2, 8, 16, src=src,
+                      inj_next=nxt, inj_prev=prv)
+    f = feat.float().cpu().numpy()
+    want = np.zeros((2, 8, 16, 16))
+    want[0, 5, 3, 4:6] = [1.0, 0.5]
+    want[1, 2, 10, 4:6] = [-2.0, 1.0]
+    assert np.array_equal(f, want)
+
+
+def test_corrector_forward_matches_oracle():
+    import torch
+
+    from oracle import corrector_ref as R
+
+    K, feat, fnp, params, _ = _setup()
+    y = K.forward(feat, torch.from_numpy(params).to(K.dev)).cpu().numpy()
+    want_bf, _ = R.forward(fnp, params, bf16=True)
+    want64, _ = R.forward(fnp, params, bf16=False)
+    assert rel_l2(y, want_bf) < 2e-3
+    assert rel_l2(y, want64) < 3e-2
+
+
+def test_corrector_gradients_match_oracle():
+    import torch
+
+    from oracle import corrector_ref as R
+
+    K, feat, fnp, params, rng = _setup(seed=1)
+    n, h, w = fnp.shape[:3]
+    target = rng.standard_normal((n, h, w)).astype(np.float32)
+    mask = (rng.uniform(size=(n, h, w)) > 0.25).astype(np.float32)
+    t = lambda a: torch.from_numpy(a).to(K.dev)  # noqa: E731
+    loss, grad = K.gradients(feat, t(target), t(mask), t(params))
+    g = grad.cpu().numpy()
+    l_bf, g_bf, _ = R.loss_and_grad(fnp, target, params, mask, bf16=True)
+    l64, g64, _ = R.loss_and_grad(fnp, target, params, mask, bf16=False)
+    assert abs(float(loss.item()) - l_bf) <= 2e-3 * l_bf
+    for lo, hi in ((0, R.N1), (R.N1, R.N1 + R.N2), (R.N1 + R.N2, R.NPARAM)):
+        assert rel_l2(g[lo:hi], g_bf[lo:hi]) < 5e-3, (lo, hi)
+        assert rel_l2(g[lo:hi], g64[lo:hi]) < 5e-2, (lo, hi)
+
+
+def test_corrector_adam_step():
+    import torch
+
+    from fomo_b200 import corrector as CR
+
+    K = CR.Kernels(0)
+    rng = np.random.default_rng(2)
+    p0 = rng.standard_normal(K.np).astype(np.float32)
+    g = rng.standard_normal(K.np).astype(np.float32)
+    p, gd = torch.from_numpy(p0.copy()).to(K.dev), torch.from_numpy(g).to(K.dev)
+    m, v = torch.zeros_like(p), torch.zeros_like(p)
+    K.adam(p, gd, m, v, 1e-2, 1)
+    # first Adam step moves every parameter by lr * sign(g) (up to eps)
+    assert np.allclose(p.cpu().numpy(), p0 - 1e-2 * np.sign(g), rtol=0, atol=1e-6)
+
+
+def test_zero_corrector_equals_plain_scalar2d(fomo):
+    from fomo_b200 import corrector as CR
+    from fomo_b200.synthetic import grf2d
+
+    vp = grf2d(70, 45, 10.0, 3000.0, 500.0, 150.0, 5, 1800.0, 4200.0)
+    kw = dict(sx=[35], sz=[6], rx=np.arange(2, 70, 3), rz=np.full(23, 4), nbc=10, fd_order=8)
+    plain = fomo.scalar2d(vp, 10.0, 1e-3, 150, 25.0, **kw).seis_u
+    zero, _ = CR.scalar2d_corrected(vp, 10.0, 1e-3, 150, 25.0,
+                                    params=np.zeros(CR.param_count(), np.float32), **kw)
+    assert np.array_equal(zero, plain)
+
+
+def test_trained_corrector_gain(fomo):
+    """Ablation: the corrector trained on solver-generated pairs of two shots
+    cuts the held-out one-step error of the coarse step (1.0 = no corrector)
+    and keeps the corrected run stable; the seismogram errors of both runs
+    against the fine run are recorded."""
+    import warnings
+
+    from fomo_b200 import corrector as CR
+
+    warnings.simplefilter("ignore")
+    K = CR.Kernels(0)
+    rng = np.random.default_rng(0)
+    cfg = dict(dh_c=10.0, dt_c=1e-3, nt_c=300, f0=25.0, nbc_c=20, fd_order=8)
+    w = CR.workload(3, 96, 64, seed=7)
+    train = CR.pairs_from_fine(K, w, [0, 1], n_pairs=1024, rng=rng, **cfg)
+    held = CR.pairs_from_fine(K, w, [2], n_pairs=256, rng=rng, **cfg)
+    params, losses = CR.train(K, train, CR.init_params(0), epochs=20, lr=1e-2)
+    assert losses[-1] < 0.5 * losses[0]
+    zero = CR.one_step_error(K, held, np.zeros(CR.param_count(), np.float32))
+    trained = CR.one_step_error(K, held, params)
+    assert zero == pytest.approx(1.0)
+    assert trained < 0.5, trained
+    r = CR.evaluate(w, [2], params, **cfg)[0]
+    print(f"one-step error {trained:.3f}; seismogram error plain {r['err_plain']:.4f} "
+          f"corrected {r['err_corrected']:.4f}")
+    assert np.isfinite(r["err_corrected"]) and r["err_corrected"] < 2 * r["err_plain"]
