@@ -12,6 +12,7 @@
 #include <tuple>
 
 #include "solver2d_kernels.cuh"
+#include "mixed2d.cuh"
 #include "sweep2d.cuh"
 
 namespace fomo {
@@ -35,6 +36,7 @@ struct Plan2 {
   bool dev;
   int snap_interval, nsnap;
   int kernel;
+  bool fp16 = false;  // elastic: binary16 wavefield storage (mixed2d.cuh)
 };
 
 int check_indices(fomo_ctx* ctx, const char* what, const int32_t* ix, const int32_t* iz,
@@ -102,8 +104,13 @@ int make_plan(fomo_ctx* ctx, Phys phys, const fomo_grid2d* g, const fomo_acq* ac
   P.nsnap = snap_interval > 0 ? P.nt / snap_interval : 0;
   P.dev = opts && (opts->flags & FOMO_F_DEVICE_PTRS);
   P.kernel = opts ? opts->kernel : FOMO_KERNEL_AUTO;
-  if (opts && opts->precision != FOMO_FP32)
-    return fail(ctx, FOMO_EUNSUPPORTED, "this solver stores FP32 only");
+  if (opts && opts->precision == FOMO_FP16 && phys == kElastic) {
+    P.fp16 = true;  // two-phase kernels with binary16 storage
+  } else if (opts && opts->precision != FOMO_FP32) {
+    return fail(ctx, FOMO_EUNSUPPORTED,
+                phys == kElastic ? "elastic2d stores FP32 or FP16 (BF16 is not accurate enough)"
+                                 : "this solver stores FP32 only");
+  }
   if ((long long)P.nxp * P.nzp > (1LL << 31))
     return fail(ctx, FOMO_EARG, "padded grid exceeds 2^31 cells");
   return FOMO_OK;
@@ -286,6 +293,8 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
   size_t o_model = P.dev ? 0 : ar.take<float>(3 * nint);
   size_t o_mat = ar.take<float>(nmat * P.plane);
   size_t o_state = ar.take<float>((long long)nsets * nfield * P.ns * P.plane);
+  size_t o_state16 = P.fp16 ? ar.take<__half>((long long)nsets * nfield * P.ns * P.plane) : 0;
+  size_t o_unpack = (P.fp16 && opts && opts->final_state) ? ar.take<float>(P.nxp * (long long)P.nzp) : 0;
   size_t o_w = ar.take<float>(hh.wtab.size());
   size_t o_src = ar.take<int32_t>(std::max<long long>(nsrc_all, 1));
   size_t o_rec = ar.take<int32_t>(std::max(P.n_rec, 1));
@@ -321,6 +330,7 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
   }
   float* d_mat = ws_ptr<float>(ctx, o_mat);
   float* d_state = ws_ptr<float>(ctx, o_state);
+  __half* d_state16 = P.fp16 ? ws_ptr<__half>(ctx, o_state16) : nullptr;
   float* d_w = ws_ptr<float>(ctx, o_w);
   int32_t* d_src = ws_ptr<int32_t>(ctx, o_src);
   int32_t* d_rec = ws_ptr<int32_t>(ctx, o_rec);
@@ -345,6 +355,12 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
                                d_mat + 2 * P.plane, d_mat + 3 * P.plane, d_mat + 4 * P.plane));
   // ---- zero state (reset!, batch.jl:30-35) ----
   FOMO_CU(ctx, cudaMemsetAsync(d_state, 0, sizeof(float) * nsets * nfield * P.ns * P.plane, st));
+  if (P.fp16) {
+    FOMO_CU(ctx, cudaMemsetAsync(d_state16, 0, sizeof(__half) * nsets * nfield * P.ns * P.plane, st));
+    // fold the storage scales into the materials (powers of two: exact)
+    k_scale<<<256, 256, 0, st>>>(d_mat, 2 * P.plane, kFp16Sv / kFp16St);
+    k_scale<<<256, 256, 0, st>>>(d_mat + 2 * P.plane, 3 * P.plane, kFp16St / kFp16Sv);
+  }
   if (!P.dev)
     for (int k = 0; k < outs.nseis; ++k)
       if (d_seis[k]) FOMO_CU(ctx, cudaMemsetAsync(d_seis[k], 0, sizeof(float) * seis_n, st));
@@ -355,9 +371,13 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
   HabcDev h{hh.q, hh.qt, hh.qxt, hh.nbc, hh.wstride, d_w};
   const float dtx = dtdh, dtz = dtdh;
   auto field = [&](int set, int f) { return d_state + ((long long)set * nfield + f) * P.ns * P.plane; };
+  auto hfield = [&](int set, int f) {
+    return HField{field(set, f), d_state16 + ((long long)set * nfield + f) * P.ns * P.plane};
+  };
 
   int kernel = P.kernel;
   if (kernel == FOMO_KERNEL_AUTO) kernel = pick_kernel_2d((int)P.phys, P.N, P.nxp, P.nzp, P.ns);
+  if (P.fp16) kernel = FOMO_KERNEL_TWO_PHASE;  // the binary16 path is two-phase
   if (kernel == FOMO_KERNEL_SINGLE_SWEEP && !sweep2d_supported((int)P.phys, P.N))
     kernel = FOMO_KERNEL_TWO_PHASE;
   ElMat emat{d_mat, d_mat + P.plane, d_mat + 2 * P.plane, d_mat + 3 * P.plane, d_mat + 4 * P.plane};
@@ -396,7 +416,19 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
     if (P.phys == kElastic) {
       ElFields a{field(A, 0), field(A, 1), field(A, 2), field(A, 3), field(A, 4)};
       const ElMat& m = emat;
-      if (kernel == FOMO_KERNEL_SINGLE_SWEEP) {
+      if (P.fp16) {
+        HSet ha{{hfield(A, 0), hfield(A, 1), hfield(A, 2), hfield(A, 3), hfield(A, 4)}};
+#define FOMO_ELH_CASE(NN)                                                                       \
+  case NN:                                                                                      \
+    k_elh_vel<NN><<<grd, blk, 0, st>>>(g, c, dtx, dtz, h, ha, m, hfield(B, 0), hfield(B, 1));   \
+    k_elh_str<NN><<<grd, blk, 0, st>>>(g, c, dtx, dtz, h, ha, hfield(B, 0), hfield(B, 1), m,    \
+                                       hfield(B, 2), hfield(B, 3), hfield(B, 4));               \
+    break;
+        switch (P.N) { FOMO_ELH_CASE(1) FOMO_ELH_CASE(2) FOMO_ELH_CASE(3) FOMO_ELH_CASE(4) FOMO_ELH_CASE(5) }
+#undef FOMO_ELH_CASE
+        launches += 2;
+        sweeps_per_step = 2;
+      } else if (kernel == FOMO_KERNEL_SINGLE_SWEEP) {
         ElOut o{field(B, 0), field(B, 1), field(B, 2), field(B, 3), field(B, 4)};
         FOMO_CU(ctx, launch_sweep_elastic(st, sp, A, c, dtx, dtz, h, a, m, o, ctx->d_flag));
         launches += 1;
@@ -414,9 +446,14 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
         sweeps_per_step = 2;
       }
       FOMO_CU(ctx, prof_mark(it, 1));
-      k_inject_record<<<P.ns, 256, 0, st>>>(it, P.nt, P.plane, P.n_src, d_src, d_wav, field(B, 2),
-                                            field(B, 3), P.n_rec, d_rec, field(B, 0), field(B, 1),
-                                            nullptr, d_seis[0], d_seis[1], nullptr);
+      if (P.fp16)
+        k_elh_inject_record<<<P.ns, 256, 0, st>>>(it, P.nt, g, P.n_src, d_src, d_wav, hfield(B, 2),
+                                                  hfield(B, 3), P.n_rec, d_rec, hfield(B, 0),
+                                                  hfield(B, 1), d_seis[0], d_seis[1]);
+      else
+        k_inject_record<<<P.ns, 256, 0, st>>>(it, P.nt, P.plane, P.n_src, d_src, d_wav, field(B, 2),
+                                              field(B, 3), P.n_rec, d_rec, field(B, 0), field(B, 1),
+                                              nullptr, d_seis[0], d_seis[1], nullptr);
       launches += 1;
     } else if (P.phys == kAcoustic) {
       const float* p0 = field(A, 2);
@@ -474,7 +511,11 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
     }
     FOMO_CU(ctx, cudaGetLastError());
     // snapshot of the interior (fused_kernels.jl:192-195): p (acoustic), vz (elastic)
-    if (d_snap && P.snap_interval > 0 && it % P.snap_interval == 0) {
+    if (P.fp16 && d_snap && P.snap_interval > 0 && it % P.snap_interval == 0) {
+      const int k = it / P.snap_interval - 1;
+      k_elh_unpack<<<dim3(cdiv(P.nx, 128), P.nz), 128, 0, st>>>(
+          g, hfield(B, 1), 0, P.pad, P.pad, P.nx, P.nz, kFp16Sv, d_snap + (long long)k * nint);
+    } else if (d_snap && P.snap_interval > 0 && it % P.snap_interval == 0) {
       int k = it / P.snap_interval - 1;
       const float* src = (P.phys == kAcoustic ? field(B, 2) : field(B, 1)) + P.pad + (long long)P.pad * P.ld;
       FOMO_CU(ctx, cudaMemcpy2DAsync(d_snap + (long long)k * nint, sizeof(float) * P.nx, src,
@@ -507,6 +548,16 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
     const long long hp = (long long)P.nxp * P.nzp;
     for (int s = 0; s < P.ns; ++s)
       for (int f = 0; f < (P.phys == kScalar ? 2 : nfield); ++f) {
+        if (P.fp16) {  // unscaled FP32 copy of the stored field
+          float* tmp = ws_ptr<float>(ctx, o_unpack);
+          k_elh_unpack<<<dim3(cdiv(P.nxp, 128), P.nzp), 128, 0, st>>>(
+              g, hfield(A, f), (long long)s * P.plane, 0, 0, P.nxp, P.nzp,
+              f < 2 ? kFp16Sv : kFp16St, tmp);
+          FOMO_CU(ctx, cudaMemcpyAsync(opts->final_state + ((long long)s * nfield + f) * hp, tmp,
+                                       sizeof(float) * hp, cudaMemcpyDeviceToHost, st));
+          FOMO_CU(ctx, cudaStreamSynchronize(st));  // tmp is reused by the next field
+          continue;
+        }
         const float* src = P.phys == kScalar ? field(f == 0 ? B : A, 0)
                                              : field(A, f) + (long long)s * P.plane;
         FOMO_CU(ctx, cudaMemcpy2DAsync(opts->final_state + ((long long)s * nfield + f) * hp,
@@ -532,10 +583,17 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
   if (nw) sweep_ms /= nw;
   if (stats) {
     stats->kernel_time_s = ms * 1e-3;
-    stats->cell_updates = (double)P.plane * P.nt * P.ns;
+    const double cells = (double)P.nxp * P.nzp;
+    stats->cell_updates = cells * P.nt * P.ns;
+    // wavefield words read + written per shot-cell, material words per cell
     double wpc = P.phys == kElastic ? 10.0 : (P.phys == kAcoustic ? 6.0 : 3.0);
     double wm = P.phys == kElastic ? 5.0 : (P.phys == kAcoustic ? 3.0 : 1.0);
-    stats->alg_bytes = 4.0 * (double)P.plane * P.nt * (wpc * P.ns + wm);
+    double wbytes = 4.0;  // bytes of a stored wavefield word
+    if (P.fp16) {         // binary16 outside the FP32 band
+      const double inner = (double)std::max(0, P.nxp - 2 * kFp16Band) * std::max(0, P.nzp - 2 * kFp16Band);
+      wbytes = (4.0 * (cells - inner) + 2.0 * inner) / cells;
+    }
+    stats->alg_bytes = (double)P.nt * cells * (wbytes * wpc * P.ns + 4.0 * wm);
     stats->n_shots = P.ns;
     stats->gpu_launches = launches;
     stats->kernel = kernel;

@@ -167,6 +167,15 @@ def _wavelet_row(wavelet, f0, dt, nt) -> np.ndarray:
     return w
 
 
+def _precision(p) -> int:
+    key = str(p).lower().lstrip(":")
+    table = {"fp32": L.FOMO_FP32, "float32": L.FOMO_FP32, "fp16": L.FOMO_FP16,
+             "float16": L.FOMO_FP16, "bf16": L.FOMO_BF16, "bfloat16": L.FOMO_BF16}
+    if key not in table:
+        raise ArgumentError(f"precision must be fp32, fp16 or bf16, got {p}")
+    return table[key]
+
+
 def _opts(kernel: int = 0, final_state: Optional[np.ndarray] = None, precision: int = 0):
     o = L.Opts()
     o.flags = 0
@@ -244,7 +253,8 @@ def elastic2d(vp, vs, rho, dh, dt, nt, f0, *, sx: Sequence[int], sz: Sequence[in
               nbc: int = 50, fd_order: int = 8, snap_interval: int = 0, boundary="habc",
               v_ref=None, sponge_factor=0.015, wavelet=None, scale_source_by_dt: bool = False,
               use_cuda_graph: bool = True, verbose: bool = True, device: int = 0,
-              kernel: int = 0, final_state: Optional[np.ndarray] = None) -> Elastic2DResult:
+              kernel: int = 0, final_state: Optional[np.ndarray] = None,
+              precision="fp32") -> Elastic2DResult:
     """2D elastic velocity-stress simulation (equations/elastic2d/elastic2d.jl:45-163)."""
     _check_boundary(boundary)
     vp, vs, rho = _f32F(vp), _f32F(vs), _f32F(rho)
@@ -270,7 +280,7 @@ def elastic2d(vp, vs, rho, dh, dt, nt, f0, *, sx: Sequence[int], sz: Sequence[in
     ctx = L.context(device)
     g = _grid(nx, nz, dh, dt, nt, nbc, fd_order, v_ref)
     acq = _acq(sxv.reshape(-1, 1, order="F"), szv.reshape(-1, 1, order="F"), wm, rxv, rzv)
-    o = _opts(kernel, final_state)
+    o = _opts(kernel, final_state, _precision(precision))
     ctx.check(L.lib().fomo_elastic2d(ctx.handle, C.byref(g), _ptr(vp), _ptr(vs), _ptr(rho),
                                      C.byref(acq), int(snap_interval), _ptr(seis[0]),
                                      _ptr(seis[1]), _ptr(snaps), C.byref(o), C.byref(st)))
@@ -339,8 +349,12 @@ def acoustic2d_batch(vp, rho, dh, dt, nt, f0, *, sx, sz, rx, rz, nbc: int = 50,
 def elastic2d_batch(vp, vs, rho, dh, dt, nt, f0, *, sx, sz, rx, rz, nbc: int = 50,
                     fd_order: int = 8, v_ref=None, wavelet=None,
                     scale_source_by_dt: bool = False, verbose: bool = True, device: int = 0,
-                    kernel: int = 0, final_state=None) -> Elastic2DBatchResult:
-    """Multi-shot elastic run on one shared model (equations/elastic2d/batch.jl:197-261)."""
+                    kernel: int = 0, final_state=None, precision="fp32") -> Elastic2DBatchResult:
+    """Multi-shot elastic run on one shared model (equations/elastic2d/batch.jl:197-261).
+
+    ``precision="fp16"`` stores the wavefields in binary16 (FP32 arithmetic,
+    FP32 storage in a 32-cell band at the grid edges); no reference
+    counterpart."""
     vp, vs, rho = _f32F(vp), _f32F(vs), _f32F(rho)
     nx, nz = vp.shape
     dh, dt, f0 = np.float32(dh), np.float32(dt), np.float32(f0)
@@ -352,7 +366,7 @@ def elastic2d_batch(vp, vs, rho, dh, dt, nt, f0, *, sx, sz, rx, rz, nbc: int = 5
     ctx = L.context(device)
     g = _grid(nx, nz, dh, dt, nt, nbc, fd_order, v_ref)
     acq = _acq(sxd, szd, wm, rxv, rzv)
-    o = _opts(kernel, final_state)
+    o = _opts(kernel, final_state, _precision(precision))
     ctx.check(L.lib().fomo_elastic2d_batch(ctx.handle, C.byref(g), _ptr(vp), _ptr(vs), _ptr(rho),
                                            C.byref(acq), _ptr(seis[0]), _ptr(seis[1]),
                                            C.byref(o), C.byref(st)))
