@@ -10,6 +10,11 @@ timed region.  Multi-GPU (torchrun): every rank runs its own 32 shots (shots
 are independent, no data-path collective), time = max over ranks.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Secondary workloads (one JSON line each, same keys; not the default line):
+    --workload elastic-fp16   the same batch with binary16 wavefield storage
+    --workload uneven         64 acoustic shots on grids of uneven size (graph run)
+    --workload elastic3d      elastic3d 400x400x300, nbc 40, order 8 (nt from --nt)
 """
 from __future__ import annotations
 
@@ -266,7 +271,7 @@ def ours(args, cfg):
 
     h_vp, h_vs, h_rho = pinned(cfg["vp"]), pinned(cfg["vs"]), pinned(cfg["rho"])
     ctx = L.context(local)
-    ctx.set_stream(stream.cuda_stream)
+    ctx.use_torch_stream(stream)
     kw = dict(sx=cfg["sx"], sz=cfg["sz"], rx=cfg["rx"], rz=cfg["rz"], nbc=cfg["nbc"],
               fd_order=cfg["fd_order"], device=local, kernel=kernel)
     import warnings
@@ -325,6 +330,109 @@ def ours(args, cfg):
         torch.distributed.destroy_process_group()
 
 
+def secondary(args):
+    """Secondary workloads through the public API: `value` from the library's
+    CUDA-event time of the time loop, `e2e` from torch events around the call
+    (host arrays in, seismograms out)."""
+    import warnings
+
+    import torch
+
+    import fomo_b200 as F
+
+    warnings.simplefilter("ignore")
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    peak, peak_kind = _peaks()
+    if args.workload == "uneven":
+        from fomo_b200.synthetic import uneven_batch_config
+
+        c = uneven_batch_config(nt=args.nt if args.nt != 3000 else 2000)
+        ns = len(c["vps"])
+        desc = (f"acoustic2d uneven batch: {ns} shots, nx ~ logU(200,2000), nz ~ logU(200,800), "
+                f"dh 10 m, dt 1 ms, nt {c['nt']}, order 8, nbc 50, GRF vp; one graph-captured run")
+
+        def run():
+            r = F.acoustic2d_uneven(c["vps"], c["rhos"], c["dh"], c["dt"], c["nt"], c["f0"],
+                                    sx=c["sx"], sz=c["sz"], rx=c["rx"], rz=c["rz"], nbc=c["nbc"],
+                                    fd_order=c["fd_order"], device=local)
+            return r, r.stats.kernel_time_s, r.stats.cell_updates, 36.0 * r.stats.cell_updates, 3 * c["nt"]
+        unit, metric, per = "shots/s", "shots/s", ns
+        h2d = sum(2 * v.nbytes for v in c["vps"])
+        d2h = sum(3 * r.size * c["nt"] * 4 for r in c["rx"])
+        dtype = "f32"
+    elif args.workload == "elastic3d":
+        from fomo_b200.synthetic import elastic3d_config
+
+        c = elastic3d_config()
+        nt = args.nt if args.nt != 3000 else 200
+        desc = (f"elastic3d: 400x400x300 (padded 488x488x388), dh 10 m, dt 0.8 ms, nt {nt} of 2500, "
+                "order 8, nbc 40, 3D GRF vp, vacuum top, 200x200 receivers")
+
+        def run():
+            r = F.elastic3d(c["vp"], c["vs"], c["rho"], c["dh"], c["dt"], nt, c["f0"], sx=c["sx"],
+                            sy=c["sy"], sz=c["sz"], rx=c["rx"], ry=c["ry"], rz=c["rz"], nbc=c["nbc"],
+                            fd_order=c["fd_order"], device=local)
+            s = F.api.last_stats
+            return r, s.kernel_time_s, s.cell_updates, s.alg_bytes, s.gpu_launches
+        unit, metric, per = "Gcell-updates/s", "Gcell-updates/s", None
+        h2d = 3 * c["vp"].nbytes
+        d2h = 3 * c["rx"].size * nt * 4
+        dtype = "f32"
+    else:  # elastic-fp16
+        from fomo_b200.synthetic import elastic_batch_config
+
+        c = elastic_batch_config(n_shots=args.shots)
+        c["nt"] = args.nt
+        ns = c["sx"].size
+        desc = WORKLOAD.replace("elastic2d_batch fp32", "elastic2d_batch fp16-storage/fp32-accumulate")
+
+        def run():
+            r = F.elastic2d_batch(c["vp"], c["vs"], c["rho"], c["dh"], c["dt"], c["nt"], c["f0"],
+                                  sx=c["sx"], sz=c["sz"], rx=c["rx"], rz=c["rz"], nbc=c["nbc"],
+                                  fd_order=c["fd_order"], precision="fp16", device=local)
+            s = F.api.last_stats
+            return r, s.kernel_time_s, s.cell_updates, s.alg_bytes, s.gpu_launches
+        unit, metric, per = "shots/s", "shots/s", ns
+        h2d = 3 * c["vp"].nbytes
+        d2h = 2 * c["rx"].size * c["nt"] * ns * 4
+        dtype = "fp16-storage/f32"
+    for _ in range(args.warmup):
+        run()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    kt, cells, algb, launches = [], 0.0, 0.0, 0
+    with ClockSampler(local) as clk:
+        ev[0].record(stream)
+        for _ in range(args.steps):
+            _, t, cells, algb, nl = run()
+            kt.append(t)
+            launches += int(nl)
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+    wall = ev[0].elapsed_time(ev[1]) / args.steps * 1e-3
+    t = float(np.mean(kt))
+    if per is None:
+        value, e2e = cells / t / 1e9, cells / wall / 1e9
+    else:
+        value, e2e = per / t, per / wall
+    achieved = algb / t / 1e9
+    line = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": dtype, "data": "synthetic",
+            "config": {"workload": desc, "secondary": args.workload},
+            "gcell_updates_per_s": cells / t / 1e9,
+            "e2e": {"value": e2e, "unit": unit, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "kernel": "whole time loop (library CUDA events)"},
+            "gpu_launches": launches, "clocks": clk.summary()}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -336,7 +444,16 @@ def main():
     ap.add_argument("--nt", type=int, default=3000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", choices=["elastic-batch", "elastic-fp16", "uneven", "elastic3d"],
+                    default="elastic-batch")
     args = ap.parse_args()
+    if args.workload != "elastic-batch":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "reference arm is measured on "
+                              "the default elastic-batch workload only"}))
+            return
+        secondary(args)
+        return
     from fomo_b200.synthetic import elastic_batch_config
 
     cfg = elastic_batch_config(n_shots=args.shots)

@@ -28,6 +28,18 @@ class ArgumentError(ValueError):
     """Invalid input, raised before any launch (Julia's ArgumentError)."""
 
 
+# The library's fomo_stats of the most recent solver call in this process
+# (kernel time, cell updates, algorithmic bytes, launches): diagnostics beyond
+# the reference's result fields.
+last_stats = None
+
+
+def _remember(st):
+    global last_stats
+    last_stats = st
+    return st
+
+
 # utils/FD_utils.jl:5-11 (Float32 values of the reference's literals)
 _FD = {
     2: [1.0],
@@ -246,6 +258,7 @@ def acoustic2d(vp, rho, dh, dt, nt, f0, *, sx: Sequence[int], sz: Sequence[int],
     ctx.check(L.lib().fomo_acoustic2d(ctx.handle, C.byref(g), _ptr(vp), _ptr(rho), C.byref(acq),
                                       int(snap_interval), _ptr(seis[0]), _ptr(seis[1]),
                                       _ptr(seis[2]), _ptr(snaps), C.byref(o), C.byref(st)))
+    _remember(st)
     return Acoustic2DResult(seis[0], seis[1], seis[2], _snap_list(snaps), Stats(st.kernel_time_s))
 
 
@@ -284,6 +297,7 @@ def elastic2d(vp, vs, rho, dh, dt, nt, f0, *, sx: Sequence[int], sz: Sequence[in
     ctx.check(L.lib().fomo_elastic2d(ctx.handle, C.byref(g), _ptr(vp), _ptr(vs), _ptr(rho),
                                      C.byref(acq), int(snap_interval), _ptr(seis[0]),
                                      _ptr(seis[1]), _ptr(snaps), C.byref(o), C.byref(st)))
+    _remember(st)
     return Elastic2DResult(seis[0], seis[1], _snap_list(snaps), Stats(st.kernel_time_s))
 
 
@@ -343,6 +357,7 @@ def acoustic2d_batch(vp, rho, dh, dt, nt, f0, *, sx, sz, rx, rz, nbc: int = 50,
     ctx.check(L.lib().fomo_acoustic2d_batch(ctx.handle, C.byref(g), _ptr(vp), _ptr(rho),
                                             C.byref(acq), _ptr(seis[0]), _ptr(seis[1]),
                                             _ptr(seis[2]), C.byref(o), C.byref(st)))
+    _remember(st)
     return Acoustic2DBatchResult(seis[0], seis[1], seis[2], BatchStats(st.kernel_time_s, ns))
 
 
@@ -370,6 +385,7 @@ def elastic2d_batch(vp, vs, rho, dh, dt, nt, f0, *, sx, sz, rx, rz, nbc: int = 5
     ctx.check(L.lib().fomo_elastic2d_batch(ctx.handle, C.byref(g), _ptr(vp), _ptr(vs), _ptr(rho),
                                            C.byref(acq), _ptr(seis[0]), _ptr(seis[1]),
                                            C.byref(o), C.byref(st)))
+    _remember(st)
     return Elastic2DBatchResult(seis[0], seis[1], BatchStats(st.kernel_time_s, ns))
 
 
@@ -415,6 +431,7 @@ def scalar2d(vp, dh, dt, nt, f0, *, sx, sz, rx, rz, nbc: int = 50, fd_order: int
     o = _opts(kernel, final_state)
     ctx.check(L.lib().fomo_scalar2d(ctx.handle, C.byref(g), _ptr(vp), C.byref(acq), _ptr(seis),
                                     C.byref(o), C.byref(st)))
+    _remember(st)
     return Scalar2DResult(seis, Stats(st.kernel_time_s))
 
 
@@ -486,6 +503,7 @@ def acoustic2d_uneven(vps, rhos, dh, dt, nt, f0, *, sx, sz, rx, rz, nbc: int = 5
     o = _opts()
     ctx.check(L.lib().fomo_acoustic2d_uneven(ctx.handle, float(dh), float(dt), int(nt), int(nbc),
                                              int(fd_order), ns, descs, C.byref(o), C.byref(st)))
+    _remember(st)
     del keep
     tile = (st.sweep_config // 1000, st.sweep_config % 1000)
     return Acoustic2DUnevenResult(results, UnevenStats(st.kernel_time_s, ns, st.cell_updates, tile))
@@ -545,6 +563,7 @@ def _run3d(elastic, vp, vs, rho, dh, dt, nt, f0, sx, sy, sz, rx, ry, rz, nbc, fd
                                      _ptr(seis[1]), _ptr(seis[2]), _ptr(snaps), C.byref(o),
                                      C.byref(st))
     ctx.check(rc)
+    _remember(st)
     return seis[0], seis[1], seis[2], _snap_list(snaps)
 
 
