@@ -828,6 +828,400 @@ __global__ void __launch_bounds__(kX2Threads, 1)
   }
 }
 
+// ===========================================================================
+// Register-window single sweep (the "rw" variants).
+//
+// 128 threads; thread t owns the column pair XV + 2t, +1 and takes two rows
+// per iteration through all four stages, so it keeps both z-derivative
+// windows in registers: txz/tzz rows zv-M .. zv+M+1 for v', and v''x/v''z rows
+// q-M .. q+M+1 for s' (q = zv-3-M).  Shared memory holds only what crosses
+// columns: the x-derivative rows and the Higdon x-neighbours.  The stress of
+// time n arrives by TMA in three small streams of 2-row boxes (rows zv+M for
+// the window, rows zv for the x-derivatives, rows q for the old values), so a
+// CTA needs about 100 KB and two fit on an SM.  Materials are read from L2
+// one iteration ahead.  Per iteration i (zv = zv0 + 2i):
+//   A: v'(zv, zv+1)        s'(q, q+1)
+//   B: v''(zv-1, zv)       s''(q-1, q)      (Higdon on frame cells; outputs)
+// Same canonical per-cell arithmetic as every other kernel (bit-identical).
+// ===========================================================================
+constexpr int kRWThreads = 128;
+
+template <int N, int P>
+struct RWShape {
+  static constexpr int TN = x2_tn(N), HV = x2_hv(N);
+  static constexpr int NZ = P + 1;                  // z / x stream slots
+  static constexpr int NO = P + 2;                  // old-stress / A.v stream slots (and barriers)
+  static constexpr int LVV = (N + 2 + 1) & ~1;      // v'' rows kept for the s' x-derivatives
+  static constexpr int O_Z = 0;                          // [NZ][txz, tzz][2][W]   rows zv+M, +1
+  static constexpr int O_X = O_Z + NZ * 4 * kX2W;        // [NZ][txx, txz][2][W]   rows zv, zv+1
+  static constexpr int O_O = O_X + NZ * 4 * kX2W;        // [NO][txx, tzz, txz][2][W] rows q, q+1
+  static constexpr int O_V = O_O + NO * 6 * kX2W;        // [NO][vx, vz][2][W]     rows zv, zv+1
+  static constexpr int O_VP = O_V + NO * 4 * kX2W;       // [vx, vz][4][W]  v'
+  static constexpr int O_VV = O_VP + 8 * kX2W;           // [vx, vz][LVV][W] v''
+  static constexpr int O_SP = O_VV + 2 * LVV * kX2W;     // [xx, zz, xz][4][W] s'
+  static constexpr int O_WT = O_SP + 12 * kX2W;          // [3][wstride] weights
+};
+
+template <int N, int P>
+__global__ void __launch_bounds__(kRWThreads, 2)
+    k_el_sweep_rw(const __grid_constant__ CUtensorMap tm_xx, const __grid_constant__ CUtensorMap tm_zz,
+                  const __grid_constant__ CUtensorMap tm_xz, const __grid_constant__ CUtensorMap tm_vx,
+                  const __grid_constant__ CUtensorMap tm_vz, SweepGeom gm, Coef c, float dtx,
+                  float dtz, HabcDev h, ElMat m, ElOut o, const long long* __restrict__ bounds,
+                  int* __restrict__ err) {
+  using S = RWShape<N, P>;
+  constexpr int W = kX2W, M = N, TN = S::TN, HV = S::HV;
+  constexpr int NZ = S::NZ, NO = S::NO, LVV = S::LVV;
+  constexpr int WN = 2 * M + 2;  // window rows
+  extern __shared__ __align__(128) float sm[];
+  float* s_z = sm + S::O_Z;
+  float* s_x = sm + S::O_X;
+  float* s_o = sm + S::O_O;
+  float* s_v = sm + S::O_V;
+  float* s_vp = sm + S::O_VP;
+  float* s_vv = sm + S::O_VV;
+  float* s_sp = sm + S::O_SP;
+  float* s_wt = sm + S::O_WT;
+  const int nwt = (3 * h.wstride + 31) & ~31;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sm + S::O_WT + nwt);  // [NO]
+
+  const int tid = threadIdx.x, sc = 2 * tid;
+  const int TX = gm.TX, WV = TX + 2 * HV;
+  const Geo2 g2{gm.nx, gm.nz, gm.ld, M, gm.nbc, gm.plane};
+  for (int k = tid; k < S::O_WT; k += kRWThreads) sm[k] = 0.0f;
+  for (int k = tid; k < 3 * h.wstride; k += kRWThreads) s_wt[k] = __ldg(h.wtab + k);
+  if (tid == 0) {
+    for (int k = 0; k < NO; ++k) mbar_init(&bars[k], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  auto wsm = [&](int kind, int dist) {
+    return dist < h.wstride ? s_wt[kind * h.wstride + dist] : 1.0f;
+  };
+  auto interior = [&](int x, int z) { return x >= M && x < gm.nx - M && z >= M && z < gm.nz - M; };
+  const bool do_v = sc < WV;
+  const bool do_s = sc >= HV - 2 && sc < HV + TX + 2;
+  const bool do_o = sc >= HV && sc < HV + TX;
+
+  const long long r_lo = bounds[blockIdx.x];
+  const long long r_hi = bounds[blockIdx.x + 1];
+  int gb = 0;  // batches this CTA has consumed (ring slot / barrier phase base)
+  bool live = true;
+  for (long long r = r_lo; r < r_hi;) {
+    const long long item = r / gm.nz;
+    const int za = (int)(r - item * gm.nz);
+    const int zb = (int)min((long long)gm.nz, za + (r_hi - r));
+    r += zb - za;
+    const int strip = (int)(item % gm.nstrip);
+    const int shot = (int)(item / gm.nstrip);
+    const long long so = (long long)shot * gm.plane;
+    const int X0 = strip * TX, XV = X0 - HV, XT = XV - TN;
+    const int xc = XV + sc;
+    // M warm-up iterations fill the txz/tzz window before the first needed v' row
+    const int zv0 = za - 2 - 3 * M;
+    const int I = (zb - za + 4 + 4 * M + 1) / 2 + 1;
+    auto issue = [&](int k) {
+      const int gk = gb + k, zs = gk % NZ, os = gk % NO;
+      uint64_t* bar = &bars[os];
+      mbar_expect_tx(bar, 9u * 2u * W * 4u);
+      const int zr = zv0 + 2 * k;
+      tma_load_3d(s_z + (zs * 2 + 0) * 2 * W, &tm_xz, XT, zr + M, shot, bar);
+      tma_load_3d(s_z + (zs * 2 + 1) * 2 * W, &tm_zz, XT, zr + M, shot, bar);
+      tma_load_3d(s_x + (zs * 2 + 0) * 2 * W, &tm_xx, XT, zr, shot, bar);
+      tma_load_3d(s_x + (zs * 2 + 1) * 2 * W, &tm_xz, XT, zr, shot, bar);
+      tma_load_3d(s_o + (os * 3 + 0) * 2 * W, &tm_xx, XT, zr - 3 - M, shot, bar);
+      tma_load_3d(s_o + (os * 3 + 1) * 2 * W, &tm_zz, XT, zr - 3 - M, shot, bar);
+      tma_load_3d(s_o + (os * 3 + 2) * 2 * W, &tm_xz, XT, zr - 3 - M, shot, bar);
+      tma_load_3d(s_v + (os * 2 + 0) * 2 * W, &tm_vx, XV, zr, shot, bar);
+      tma_load_3d(s_v + (os * 2 + 1) * 2 * W, &tm_vz, XV, zr, shot, bar);
+    };
+    __syncthreads();  // the previous segment's readers are done with every ring
+    if (tid == 0 && live) {
+      fence_proxy_async();
+      for (int k = 0; k <= P && k < I; ++k) issue(k);
+    }
+    // register state
+    float wxz[WN][2], wzz[WN][2], wvx[WN][2], wvz[WN][2];
+#pragma unroll
+    for (int k = 0; k < WN; ++k)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) wxz[k][e] = wzz[k][e] = wvx[k][e] = wvz[k][e] = 0.0f;
+    float vpp[2][2][2], spp[3][2][2];  // previous iteration's v' / s' rows [field][row][cell]
+#pragma unroll
+    for (int f = 0; f < 2; ++f)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) vpp[f][k >> 1][k & 1] = 0.0f;
+#pragma unroll
+    for (int f = 0; f < 3; ++f)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) spp[f][k >> 1][k & 1] = 0.0f;
+    // materials of iteration i, loaded during iteration i-1
+    float mbx[2][2], mbz[2][2], mla[2][2], ml2[2][2], mmu[2][2];
+    auto load_mat = [&](int zv) {
+#pragma unroll
+      for (int rr = 0; rr < 2; ++rr) {
+        const int zr = zv + rr, zq = zv - 3 - M + rr;
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int x = xc + e;
+          const bool xin = x >= 0 && x < gm.nx;
+          const bool vin = do_v && xin && zr >= 0 && zr < gm.nz;
+          const bool sin_ = do_s && xin && zq >= 0 && zq < gm.nz;
+          const long long pv = (long long)zr * gm.ld + x, ps = (long long)zq * gm.ld + x;
+          mbx[rr][e] = vin ? __ldg(m.bx + pv) : 0.0f;
+          mbz[rr][e] = vin ? __ldg(m.bz + pv) : 0.0f;
+          mla[rr][e] = sin_ ? __ldg(m.lam + ps) : 0.0f;
+          ml2[rr][e] = sin_ ? __ldg(m.l2m + ps) : 0.0f;
+          mmu[rr][e] = sin_ ? __ldg(m.mut + ps) : 0.0f;
+        }
+      }
+    };
+    load_mat(zv0);
+
+    for (int i = 0; i < I; ++i) {
+      const int zv = zv0 + 2 * i, q = zv - 3 - M;
+      const int gi = gb + i, zs = gi % NZ, os = gi % NO, osp = (gi + NO - 1) % NO;
+      if (live)
+        live = mbar_wait_bounded(&bars[os], (uint32_t)((gi / NO) & 1), err) && live;
+      // ---------------- stage A ----------------
+      // new window rows zv+M, zv+M+1 of txz and tzz
+#pragma unroll
+      for (int rr = 0; rr < 2; ++rr) {
+        const float2 a = *reinterpret_cast<const float2*>(s_z + ((zs * 2 + 0) * 2 + rr) * W + sc + TN);
+        const float2 b = *reinterpret_cast<const float2*>(s_z + ((zs * 2 + 1) * 2 + rr) * W + sc + TN);
+        wxz[2 * M + rr][0] = a.x;
+        wxz[2 * M + rr][1] = a.y;
+        wzz[2 * M + rr][0] = b.x;
+        wzz[2 * M + rr][1] = b.y;
+      }
+      float vpc[2][2][2];  // v' rows zv, zv+1 [field][row][cell]
+      if (do_v) {
+#pragma unroll
+        for (int rr = 0; rr < 2; ++rr) {
+          const int zr = zv + rr;
+          float xw[4 * ((N + 1) / 2) + 2];
+          float dxx[2], dxzx[2];
+          load_xwin<N>(s_x + ((zs * 2 + 0) * 2 + rr) * W, sc + TN, xw);
+          dxx[0] = xdm<N>(xw, 0, c);
+          dxx[1] = xdm<N>(xw, 1, c);
+          load_xwin<N>(s_x + ((zs * 2 + 1) * 2 + rr) * W, sc + TN, xw);
+          dxzx[0] = xdp<N>(xw, 0, c);
+          dxzx[1] = xdp<N>(xw, 1, c);
+          const float2 ox = *reinterpret_cast<const float2*>(s_v + ((os * 2 + 0) * 2 + rr) * W + sc);
+          const float2 oz = *reinterpret_cast<const float2*>(s_v + ((os * 2 + 1) * 2 + rr) * W + sc);
+          const float vo[2][2] = {{ox.x, ox.y}, {oz.x, oz.y}};
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            float dxzz = 0.0f, dzz = 0.0f;
+#pragma unroll
+            for (int l = 1; l <= N; ++l) {
+              dxzz = __fmaf_rn(c.a[l - 1], __fsub_rn(wxz[rr + M + l - 1][e], wxz[rr + M - l][e]), dxzz);
+              dzz = __fmaf_rn(c.a[l - 1], __fsub_rn(wzz[rr + M + l][e], wzz[rr + M - l + 1][e]), dzz);
+            }
+            float ux = vo[0][e], uz = vo[1][e];
+            if (interior(xc + e, zr)) {
+              ux = __fmaf_rn(mbx[rr][e], __fmaf_rn(dtx, dxx[e], __fmul_rn(dtz, dxzz)), ux);
+              uz = __fmaf_rn(mbz[rr][e], __fmaf_rn(dtx, dxzx[e], __fmul_rn(dtz, dzz)), uz);
+            }
+            vpc[0][rr][e] = ux;
+            vpc[1][rr][e] = uz;
+          }
+          const int pr = (2 * i + rr) & 3;  // v' ring row of zr
+          *reinterpret_cast<float2*>(s_vp + pr * W + sc) = make_float2(vpc[0][rr][0], vpc[0][rr][1]);
+          *reinterpret_cast<float2*>(s_vp + (4 + pr) * W + sc) =
+              make_float2(vpc[1][rr][0], vpc[1][rr][1]);
+        }
+      }
+      // shift the txz / tzz window by two rows for the next iteration
+#pragma unroll
+      for (int k = 0; k < 2 * M; ++k)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          wxz[k][e] = wxz[k + 2][e];
+          wzz[k][e] = wzz[k + 2][e];
+        }
+      float spc[3][2][2];  // s' rows q, q+1 [field][row][cell]
+      if (do_s) {
+#pragma unroll
+        for (int rr = 0; rr < 2; ++rr) {
+          const int zq = q + rr;
+          const int vb = (2 * i - 2 - M + rr + 2 * LVV) % LVV;  // v'' ring row of zq
+          float xw[4 * ((N + 1) / 2) + 2];
+          float dvxdx[2], dvzdx[2];
+          load_xwin<N>(s_vv + vb * W, sc, xw);
+          dvxdx[0] = xdp<N>(xw, 0, c);
+          dvxdx[1] = xdp<N>(xw, 1, c);
+          load_xwin<N>(s_vv + (LVV + vb) * W, sc, xw);
+          dvzdx[0] = xdm<N>(xw, 0, c);
+          dvzdx[1] = xdm<N>(xw, 1, c);
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            float dvxdz = 0.0f, dvzdz = 0.0f;
+#pragma unroll
+            for (int l = 1; l <= N; ++l) {
+              dvxdz = __fmaf_rn(c.a[l - 1], __fsub_rn(wvx[rr + M + l][e], wvx[rr + M - l + 1][e]), dvxdz);
+              dvzdz = __fmaf_rn(c.a[l - 1], __fsub_rn(wvz[rr + M + l - 1][e], wvz[rr + M - l][e]), dvzdz);
+            }
+            float sxx = s_o[((os * 3 + 0) * 2 + rr) * W + sc + TN + e];
+            float szz = s_o[((os * 3 + 1) * 2 + rr) * W + sc + TN + e];
+            float sxz = s_o[((os * 3 + 2) * 2 + rr) * W + sc + TN + e];
+            if (interior(xc + e, zq)) {
+              const float ex = __fmul_rn(dvxdx[e], dtx), ez = __fmul_rn(dvzdz, dtz);
+              sxx = __fadd_rn(sxx, __fmaf_rn(ml2[rr][e], ex, __fmul_rn(mla[rr][e], ez)));
+              szz = __fadd_rn(szz, __fmaf_rn(mla[rr][e], ex, __fmul_rn(ml2[rr][e], ez)));
+              sxz = __fmaf_rn(mmu[rr][e], __fmaf_rn(dvxdz, dtz, __fmul_rn(dvzdx[e], dtx)), sxz);
+            }
+            spc[0][rr][e] = sxx;
+            spc[1][rr][e] = szz;
+            spc[2][rr][e] = sxz;
+          }
+          const int sr = (2 * i + rr) & 3;  // s' ring row of zq
+#pragma unroll
+          for (int f = 0; f < 3; ++f)
+            *reinterpret_cast<float2*>(s_sp + (4 * f + sr) * W + sc) =
+                make_float2(spc[f][rr][0], spc[f][rr][1]);
+        }
+      }
+      __syncthreads();
+
+      // ---------------- stage B ----------------
+      // v'' rows zv-1 (rr = 0) and zv (rr = 1); v' rows zv-2 .. zv+1 are in vpp / vpc
+      float vvn[2][2][2];
+      if (do_v) {
+#pragma unroll
+        for (int rr = 0; rr < 2; ++rr) {
+          const int qv = zv - 1 + rr;
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+#pragma unroll
+            for (int f = 0; f < 2; ++f) vvn[f][rr][e] = rr ? vpc[f][0][e] : vpp[f][1][e];
+            int sx, sz, dist;
+            if (!frame2(g2, xc + e, qv, sx, sz, dist)) continue;
+            const int col = sc + e;
+            const int coln = min(max(col + sx, 0), W - 1);
+            // A.v rows zv-2, zv-1 (previous pair slot) and zv, zv+1 (this pair); row qv:
+            const int orow = rr ? 0 : 1;
+            const int prow = (2 * i - 1 + rr) & 3;  // v' ring row of qv
+            // z-neighbour row qv + sz: A.v and v'
+            // row qv + sz: zv-2 / zv-1 sit in the previous pair's slot, zv / zv+1 in this one
+            const bool up = sz > 0;
+            const int ozs = up ? os : osp;
+            const int ozr = rr;
+#pragma unroll
+            for (int f = 0; f < 2; ++f) {
+              const float* fo = s_v + (((rr ? os : osp) * 2 + f) * 2 + orow) * W;
+              const float fop = fo[col];
+              const float w = wsm(f, dist);
+              const float* fzo = s_v + ((ozs * 2 + f) * 2 + ozr) * W;
+              const float vz_n = rr ? (up ? vpc[f][1][e] : vpp[f][1][e]) : (up ? vpc[f][0][e] : vpp[f][0][e]);
+              const float vx_n = s_vp[(4 * f + prow) * W + coln];
+              if (sx != 0 && sz != 0)
+                vvn[f][rr][e] = higdon_corner(w, vvn[f][rr][e], higdon_side(h, vx_n, fop, fo[coln]),
+                                              higdon_side(h, vz_n, fop, fzo[col]));
+              else if (sx != 0)
+                vvn[f][rr][e] = higdon_edge(w, vvn[f][rr][e], higdon_side(h, vx_n, fop, fo[coln]));
+              else
+                vvn[f][rr][e] = higdon_edge(w, vvn[f][rr][e], higdon_side(h, vz_n, fop, fzo[col]));
+            }
+          }
+          const int vw = (2 * i + rr) % LVV;  // v'' ring row of qv
+          *reinterpret_cast<float2*>(s_vv + vw * W + sc) = make_float2(vvn[0][rr][0], vvn[0][rr][1]);
+          *reinterpret_cast<float2*>(s_vv + (LVV + vw) * W + sc) =
+              make_float2(vvn[1][rr][0], vvn[1][rr][1]);
+          if (do_o && qv >= za && qv < zb && xc < gm.nx) {
+            const long long p = so + (long long)qv * gm.ld + xc;
+            if (xc + 1 < gm.nx) {
+              *reinterpret_cast<float2*>(o.vx + p) = make_float2(vvn[0][rr][0], vvn[0][rr][1]);
+              *reinterpret_cast<float2*>(o.vz + p) = make_float2(vvn[1][rr][0], vvn[1][rr][1]);
+            } else {
+              o.vx[p] = vvn[0][rr][0];
+              o.vz[p] = vvn[1][rr][0];
+            }
+          }
+        }
+      }
+      // the v'' window advances: rows q-M+2 .. q+M+1, then the new rows zv-1, zv
+#pragma unroll
+      for (int k = 0; k < 2 * M; ++k)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          wvx[k][e] = wvx[k + 2][e];
+          wvz[k][e] = wvz[k + 2][e];
+        }
+#pragma unroll
+      for (int rr = 0; rr < 2; ++rr)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          wvx[2 * M + rr][e] = do_v ? vvn[0][rr][e] : 0.0f;
+          wvz[2 * M + rr][e] = do_v ? vvn[1][rr][e] : 0.0f;
+        }
+      // s'' rows q-1 (rr = 0) and q (rr = 1); s' rows q-2 .. q+1 are in spp / spc
+      if (do_o) {
+#pragma unroll
+        for (int rr = 0; rr < 2; ++rr) {
+          const int qs = q - 1 + rr;
+          if (qs < za || qs >= zb || xc >= gm.nx) continue;
+          float v[3][2];
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+#pragma unroll
+            for (int f = 0; f < 3; ++f) v[f][e] = rr ? spc[f][0][e] : spp[f][1][e];
+            int sx, sz, dist;
+            if (!frame2(g2, xc + e, qs, sx, sz, dist)) continue;
+            const int col = sc + e;
+            const int coln = min(max(col + sx, 0), W - 1);
+            const int srow = (2 * i - 1 + rr) & 3;  // s' ring row of qs
+            const bool up = sz > 0;
+            // old stress rows: q-2, q-1 in the previous pair slot, q, q+1 in this one
+            const int oso = rr ? os : osp, oro = rr ? 0 : 1;  // row qs
+            const int osz = up ? os : osp, orz = rr;         // row qs + sz
+            const float w = wsm(2, dist);
+#pragma unroll
+            for (int f = 0; f < 3; ++f) {
+              const float* fo = s_o + ((oso * 3 + f) * 2 + oro) * W + TN;
+              const float* fzo = s_o + ((osz * 3 + f) * 2 + orz) * W + TN;
+              const float fop = fo[col];
+              const float sz_n = rr ? (up ? spc[f][1][e] : spp[f][1][e]) : (up ? spc[f][0][e] : spp[f][0][e]);
+              const float sx_n = s_sp[(4 * f + srow) * W + coln];
+              if (sx != 0 && sz != 0)
+                v[f][e] = higdon_corner(w, v[f][e], higdon_side(h, sx_n, fop, fo[coln]),
+                                        higdon_side(h, sz_n, fop, fzo[col]));
+              else if (sx != 0)
+                v[f][e] = higdon_edge(w, v[f][e], higdon_side(h, sx_n, fop, fo[coln]));
+              else
+                v[f][e] = higdon_edge(w, v[f][e], higdon_side(h, sz_n, fop, fzo[col]));
+            }
+          }
+          const long long p = so + (long long)qs * gm.ld + xc;
+          float* out[3] = {o.txx, o.tzz, o.txz};
+#pragma unroll
+          for (int f = 0; f < 3; ++f) {
+            if (xc + 1 < gm.nx)
+              *reinterpret_cast<float2*>(out[f] + p) = make_float2(v[f][0], v[f][1]);
+            else
+              out[f][p] = v[f][0];
+          }
+        }
+      }
+#pragma unroll
+      for (int f = 0; f < 2; ++f)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) vpp[f][k >> 1][k & 1] = do_v ? vpc[f][k >> 1][k & 1] : 0.0f;
+#pragma unroll
+      for (int f = 0; f < 3; ++f)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) spp[f][k >> 1][k & 1] = do_s ? spc[f][k >> 1][k & 1] : 0.0f;
+      load_mat(zv + 2);
+      __syncthreads();
+      if (tid == 0 && live && i + 1 + P < I) {
+        fence_proxy_async();
+        issue(i + 1 + P);
+      }
+    }
+    gb += I;
+  }
+}
+
 // ---- host side --------------------------------------------------------------
 PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 std::once_flag g_encode_once;
@@ -866,6 +1260,16 @@ size_t x2_smem_bytes(int wstride) {
 constexpr int kX2P[] = {1, 2, 3};
 constexpr int kNumX2 = sizeof(kX2P) / sizeof(kX2P[0]);
 #define FOMO_X2_VARIANTS(X, NN) X(0, NN, 1) X(1, NN, 2) X(2, NN, 3)
+// register-window variants: prefetch depth in row pairs
+constexpr int kRWP[] = {1, 2};
+constexpr int kNumRW = sizeof(kRWP) / sizeof(kRWP[0]);
+#define FOMO_RW_VARIANTS(X, NN) X(0, NN, 1) X(1, NN, 2)
+
+template <int N, int P>
+size_t rw_smem_bytes(int wstride) {
+  using S = RWShape<N, P>;
+  return (size_t)(S::O_WT + ((3 * wstride + 31) & ~31)) * 4 + sizeof(uint64_t) * S::NO;
+}
 
 struct Variant {
   int NT, R, P;
@@ -935,6 +1339,47 @@ cudaError_t launch_x2_n(cudaStream_t st, const SweepPlan& sp, int set, const Coe
   return cudaErrorInvalidValue;
 }
 
+template <int N, int P>
+cudaError_t launch_rw(cudaStream_t st, const SweepPlan& sp, int set, const Coef& c, float dtx,
+                      float dtz, const HabcDev& h, const ElMat& m, const ElOut& o, int* err) {
+  auto kern = k_el_sweep_rw<N, P>;
+  static std::atomic<int> attr_set{0};
+  if (!attr_set.load(std::memory_order_acquire)) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kMaxDynSmem);
+    if (e != cudaSuccess) return e;
+    attr_set.store(1, std::memory_order_release);
+  }
+  if (sp.smem > (size_t)kMaxDynSmem) return cudaErrorInvalidValue;
+  kern<<<(unsigned)sp.grid, kRWThreads, sp.smem, st>>>(sp.tm[set][0], sp.tm[set][1], sp.tm[set][2],
+                                                        sp.tm[set][3], sp.tm[set][4], sp.gm, c, dtx,
+                                                        dtz, h, m, o, sp.d_bounds, err);
+  return cudaGetLastError();
+}
+
+template <int N>
+cudaError_t launch_rw_n(cudaStream_t st, const SweepPlan& sp, int set, const Coef& c, float dtx,
+                        float dtz, const HabcDev& h, const ElMat& m, const ElOut& o, int* err) {
+#define FOMO_LAUNCH_RW(V, NN, PP) \
+  case V: return launch_rw<NN, PP>(st, sp, set, c, dtx, dtz, h, m, o, err);
+  switch (sp.variant - kNumVariants - kNumX2) { FOMO_RW_VARIANTS(FOMO_LAUNCH_RW, N) }
+#undef FOMO_LAUNCH_RW
+  return cudaErrorInvalidValue;
+}
+
+size_t rw_smem_for(int N, int v, int wstride) {
+#define FOMO_SMEM_RW(V, NN, PP) \
+  case V: return rw_smem_bytes<NN, PP>(wstride);
+#define FOMO_SMEM_RWN(NN)                              \
+  case NN:                                             \
+    switch (v) { FOMO_RW_VARIANTS(FOMO_SMEM_RW, NN) }  \
+    break;
+  switch (N) { FOMO_SMEM_RWN(1) FOMO_SMEM_RWN(2) FOMO_SMEM_RWN(3) FOMO_SMEM_RWN(4) FOMO_SMEM_RWN(5) }
+#undef FOMO_SMEM_RWN
+#undef FOMO_SMEM_RW
+  return 0;
+}
+
 size_t x2_smem_for(int N, int v2, int wstride) {
 #define FOMO_SMEM_X2(V, NN, PP) \
   case V: return x2_smem_bytes<NN, PP>(wstride);
@@ -973,7 +1418,7 @@ int pick_kernel_2d(int phys, int N, int nxp, int nzp, int ns) {
 
 bool sweep2d_supported(int phys, int N) { return phys == 1 && N >= 1 && N <= 5 && encoder(); }
 
-int sweep_num_variants() { return kNumVariants + kNumX2; }
+int sweep_num_variants() { return kNumVariants + kNumX2 + kNumRW; }
 
 // Builds the work decomposition and the six tensor maps (3 stress fields x 2
 // ping-pong sets).  variant selects (threads, rows per chunk, prefetch depth);
@@ -983,14 +1428,16 @@ cudaError_t make_sweep_plan(SweepPlan& sp, int N, int variant, int TX, int per_s
                             long long* d_bounds, cudaStream_t st) {
   auto enc = encoder();
   if (!enc) return cudaErrorNotSupported;
-  if (variant < 0 || variant >= kNumVariants + kNumX2 || per_sm < 1) return cudaErrorInvalidValue;
-  const bool x2 = variant >= kNumVariants;
+  if (variant < 0 || variant >= kNumVariants + kNumX2 + kNumRW || per_sm < 1)
+    return cudaErrorInvalidValue;
+  const bool rw = variant >= kNumVariants + kNumX2;
+  const bool x2 = variant >= kNumVariants;  // both 256-wide TMA-box families
   int W = 0, R = 2;
   if (x2) {
     if (TX < 8 || TX > x2_txmax(N) || (TX & 3)) return cudaErrorInvalidValue;
     W = kX2W;
-    sp.family = 1;
-    sp.P = kX2P[variant - kNumVariants];
+    sp.family = rw ? 2 : 1;
+    sp.P = rw ? kRWP[variant - kNumVariants - kNumX2] : kX2P[variant - kNumVariants];
   } else {
     const int NT = kVariants[variant].NT;
     R = kVariants[variant].R;
@@ -1013,8 +1460,9 @@ cudaError_t make_sweep_plan(SweepPlan& sp, int N, int variant, int TX, int per_s
   sp.gm.W = W;
   sp.gm.nstrip = (g.nx + TX - 1) / TX;
   sp.gm.ns = ns;
-  sp.smem = x2 ? x2_smem_for(N, variant - kNumVariants, g.nbc + 3)
-             : smem_for(N, variant, W, g.nbc + 3);
+  sp.smem = rw   ? rw_smem_for(N, variant - kNumVariants - kNumX2, g.nbc + 3)
+             : x2 ? x2_smem_for(N, variant - kNumVariants, g.nbc + 3)
+                  : smem_for(N, variant, W, g.nbc + 3);
   const int bps = sweep_blocks_per_sm(sp);
   if (bps < 1) return cudaErrorInvalidConfiguration;
   int dev = 0, nsm = 148;
@@ -1116,7 +1564,32 @@ int occ_x2(const SweepPlan& sp) {
   return nb;
 }
 
+template <int N, int P>
+int occ_rw(const SweepPlan& sp) {
+  int nb = 0;
+  cudaFuncSetAttribute(k_el_sweep_rw<N, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       kMaxDynSmem);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_el_sweep_rw<N, P>, kRWThreads,
+                                                    sp.smem) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return nb;
+}
+
 int sweep_blocks_per_sm(const SweepPlan& sp) {
+  if (sp.family == 2) {
+#define FOMO_OCC_RW(V, NN, PP) \
+  case V: return occ_rw<NN, PP>(sp);
+#define FOMO_OCC_RWN(NN)                                                              \
+  case NN:                                                                            \
+    switch (sp.variant - kNumVariants - kNumX2) { FOMO_RW_VARIANTS(FOMO_OCC_RW, NN) } \
+    break;
+    switch (sp.N) { FOMO_OCC_RWN(1) FOMO_OCC_RWN(2) FOMO_OCC_RWN(3) FOMO_OCC_RWN(4) FOMO_OCC_RWN(5) }
+#undef FOMO_OCC_RWN
+#undef FOMO_OCC_RW
+    return 0;
+  }
   if (sp.family == 1) {
 #define FOMO_OCC_X2(V, NN, PP) \
   case V: return occ_x2<NN, PP>(sp);
@@ -1144,6 +1617,16 @@ int sweep_blocks_per_sm(const SweepPlan& sp) {
 cudaError_t launch_sweep_elastic(cudaStream_t st, const SweepPlan& sp, int set, const Coef& c,
                                  float dtx, float dtz, const HabcDev& h, const ElFields& a,
                                  const ElMat& m, const ElOut& o, int* err) {
+  if (sp.family == 2) {
+    switch (sp.N) {
+      case 1: return launch_rw_n<1>(st, sp, set, c, dtx, dtz, h, m, o, err);
+      case 2: return launch_rw_n<2>(st, sp, set, c, dtx, dtz, h, m, o, err);
+      case 3: return launch_rw_n<3>(st, sp, set, c, dtx, dtz, h, m, o, err);
+      case 4: return launch_rw_n<4>(st, sp, set, c, dtx, dtz, h, m, o, err);
+      case 5: return launch_rw_n<5>(st, sp, set, c, dtx, dtz, h, m, o, err);
+    }
+    return cudaErrorInvalidValue;
+  }
   if (sp.family == 1) {
     switch (sp.N) {
       case 1: return launch_x2_n<1>(st, sp, set, c, dtx, dtz, h, m, o, err);

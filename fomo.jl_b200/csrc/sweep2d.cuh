@@ -21,7 +21,7 @@ constexpr int kMaxGrid = 4096;
 
 struct SweepPlan {
   int N = 0, variant = 0;
-  int family = 0;            // 0: column-per-thread kernel, 1: pair-blocked kernel
+  int family = 0;            // 0: column-per-thread, 1: pair-blocked, 2: register-window
   int P = 0;                 // pair-blocked: prefetch depth (row pairs)
   int per_sm = 1, grid = 1;  // persistent CTAs per SM, grid size
   float frame_weight = 1.0f; // extra cost of a frame cell in the row-range split

@@ -16,7 +16,8 @@ KERNELS = [1, 2]  # two-phase, single-sweep
 
 
 SWEEP_CONFIGS = ["0,112,3", "1,144,1", "2,80,2", "2,20,4", "3,112,2", "0,64,1",
-                 "4,224,1", "5,100,1", "6,40,1", "5,8,1"]  # variant,TX,CTAs per SM
+                 "4,224,1", "5,100,1", "6,40,1", "5,8,1",
+                 "7,224,2", "8,196,2", "8,40,2", "7,8,1"]  # variant,TX,CTAs per SM
 
 
 @pytest.fixture
