@@ -354,13 +354,16 @@ int run_uneven(fomo_ctx* ctx, float dh, float dt, int nt, int nbc, int fd_order,
   FOMO_CU(ctx, cudaStreamSynchronize(st));
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
-  FOMO_CU(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  // Capture on the context's own stream: the caller's stream may be the
+  // legacy default stream, which cannot be captured.  Replay on the caller's.
+  const cudaStream_t cs = ctx->own_stream;
+  FOMO_CU(ctx, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
   for (int it = 1; it <= nt; ++it) {
     const int A = (it - 1) & 1;
-    launch_step_n(N, st, nblk, t, d_tab, d_tiles, d_state, d_mat, c, dtdh, d_w, zone, wstride, A);
-    k_uinject_record<<<ns, 256, 0, st>>>(d_tab, d_state, d_src, d_wav, d_rec, d_seis, it, nt, 1 - A);
+    launch_step_n(N, cs, nblk, t, d_tab, d_tiles, d_state, d_mat, c, dtdh, d_w, zone, wstride, A);
+    k_uinject_record<<<ns, 256, 0, cs>>>(d_tab, d_state, d_src, d_wav, d_rec, d_seis, it, nt, 1 - A);
   }
-  cudaError_t ce = cudaStreamEndCapture(st, &graph);
+  cudaError_t ce = cudaStreamEndCapture(cs, &graph);
   if (ce != cudaSuccess) return cuda_fail(ctx, ce, "capture of the uneven-batch run");
   ce = cudaGraphInstantiate(&exec, graph, 0);
   if (ce != cudaSuccess) {

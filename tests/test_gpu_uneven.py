@@ -73,3 +73,20 @@ def test_uneven_rerun_deterministic(fomo):
     for x, y in zip(a.shots, b.shots):
         for u, v in zip(x, y):
             assert np.array_equal(u, v)
+
+
+def test_uneven_on_legacy_default_stream(fomo):
+    """The run is captured into a graph; a context borrowing the legacy default
+    stream (what torch's default stream maps to) must still work."""
+    import torch
+
+    from fomo_b200 import _lib as L
+
+    ctx = L.context(0)
+    ctx.use_torch_stream(torch.cuda.current_stream())
+    vps, rhos, sx, sz, rx, rz = _shots(seed=2)
+    a = fomo.acoustic2d_uneven(vps, rhos, 10.0, 1e-3, 40, 20.0, sx=sx, sz=sz, rx=rx, rz=rz, nbc=6)
+    ctx.set_stream(None)
+    b = fomo.acoustic2d_uneven(vps, rhos, 10.0, 1e-3, 40, 20.0, sx=sx, sz=sz, rx=rx, rz=rz, nbc=6)
+    for x, y in zip(a.shots, b.shots):
+        assert np.array_equal(x[0], y[0])
