@@ -284,6 +284,12 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
   }
   HabcHost hh = make_habc(P.pad, P.v_ref, P.dt, P.dh);
 
+  int kernel = P.kernel;
+  if (kernel == FOMO_KERNEL_AUTO) kernel = pick_kernel_2d((int)P.phys, P.N, P.nxp, P.nzp, P.ns);
+  if (P.fp16) kernel = FOMO_KERNEL_TWO_PHASE;  // the binary16 path is two-phase
+  if (kernel == FOMO_KERNEL_SINGLE_SWEEP && !sweep2d_supported((int)P.phys, P.N))
+    kernel = FOMO_KERNEL_TWO_PHASE;
+
   // ---- workspace layout ----
   const int nmat = P.phys == kElastic ? 5 : (P.phys == kAcoustic ? 3 : 1);
   const int nfield = P.phys == kElastic ? 5 : (P.phys == kAcoustic ? 3 : 1);
@@ -302,6 +308,8 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
   size_t o_seis = P.dev ? 0 : ar.take<float>(std::max<long long>(outs.nseis * seis_n, 1));
   size_t o_snap = (!P.dev && outs.snaps && P.nsnap) ? ar.take<float>(P.nsnap * nint) : 0;
   size_t o_bounds = ar.take<long long>(kMaxGrid + 1);
+  const bool sweep = kernel == FOMO_KERNEL_SINGLE_SWEEP;
+  size_t o_pack = sweep ? ar.take<float>(sweep_pack_floats(P.nxp, P.nzp)) : 0;
   if ((rc = ensure_workspace(ctx, ar.off))) return rc;
 
   const float* d_vp = vp;
@@ -375,14 +383,10 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
     return HField{field(set, f), d_state16 + ((long long)set * nfield + f) * P.ns * P.plane};
   };
 
-  int kernel = P.kernel;
-  if (kernel == FOMO_KERNEL_AUTO) kernel = pick_kernel_2d((int)P.phys, P.N, P.nxp, P.nzp, P.ns);
-  if (P.fp16) kernel = FOMO_KERNEL_TWO_PHASE;  // the binary16 path is two-phase
-  if (kernel == FOMO_KERNEL_SINGLE_SWEEP && !sweep2d_supported((int)P.phys, P.N))
-    kernel = FOMO_KERNEL_TWO_PHASE;
   ElMat emat{d_mat, d_mat + P.plane, d_mat + 2 * P.plane, d_mat + 3 * P.plane, d_mat + 4 * P.plane};
   SweepPlan sp;
-  if (kernel == FOMO_KERNEL_SINGLE_SWEEP) {
+  if (sweep) {
+    FOMO_CU(ctx, build_sweep_pack(st, g, emat, ws_ptr<float>(ctx, o_pack)));
     float* sets[2][5] = {{field(0, 2), field(0, 3), field(0, 4), field(0, 0), field(0, 1)},
                          {field(1, 2), field(1, 3), field(1, 4), field(1, 0), field(1, 1)}};
     rc = tune_sweep(ctx, st, sp, P.N, g, P.ns, sets, c, dtx, dtz, h, emat,

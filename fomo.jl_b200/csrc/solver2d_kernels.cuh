@@ -36,6 +36,10 @@ struct ElMat {
   const float* lam;
   const float* l2m;
   const float* mut;
+  // Padded, column-pair-interleaved copy of the five planes read by the lean
+  // single sweep (layout in sweep2d.cuh); null where that kernel is not used.
+  const float* pack = nullptr;
+  int pack_pitch = 0;  // column pairs per pack row
 };
 
 template <int N>

@@ -1222,6 +1222,923 @@ __global__ void __launch_bounds__(kRWThreads, 2)
   }
 }
 
+// ===========================================================================
+// Lean register-window sweep (the "rl" variants).
+//
+// The same two-stage march as k_el_sweep_rw (2x2 cells per thread, both
+// z-derivative windows in registers, three TMA stress streams, same canonical
+// arithmetic, bit-identical results), with the per-cell bookkeeping moved out
+// of the inner loop:
+//   - the HABC frame and interior tests split into per-column constants of the
+//     thread (computed once per segment) and per-row values that are the same
+//     for the whole CTA (computed once per row);
+//   - materials come from a padded, column-pair-interleaved pack (six vector
+//     loads per row pair, no bounds tests, pointers advanced by two rows);
+//   - ring slots advance by counters instead of divisions;
+//   - NT threads (64 or 128; 256 / NT CTAs per SM keep two warps on each
+//     scheduler) and a TMA row of W = 2 (NT + TN) floats (at most 256), so
+//     narrower CTAs can cover a grid with fewer idle lanes.
+// ===========================================================================
+// TMA row width: 2 (NT + TN) rounded up to 16 floats (every ring row pair
+// then starts on a 128-byte boundary), at most 256 (the TMA box limit).
+__host__ __device__ constexpr int rl_w(int N, int NT) {
+  return ((2 * (NT + x2_tn(N)) + 15) & ~15) < 256 ? ((2 * (NT + x2_tn(N)) + 15) & ~15) : 256;
+}
+__host__ __device__ constexpr int rl_txmax(int N, int NT) {
+  // v' columns [0, TX + 2HV) on the threads; tau columns [-TN, W - TN) cover them +- N
+  return ((2 * NT - 2 * x2_hv(N)) < (rl_w(N, NT) - x2_tn(N) - N - 2 * x2_hv(N))
+              ? (2 * NT - 2 * x2_hv(N))
+              : (rl_w(N, NT) - x2_tn(N) - N - 2 * x2_hv(N))) &
+         ~3;
+}
+
+template <int N, int NT, int P>
+struct RLShape {
+  static constexpr int W = rl_w(N, NT);
+  static constexpr int TN = x2_tn(N), HV = x2_hv(N);
+  static constexpr int NZ = P + 1;                 // z / x stream slots
+  static constexpr int NO = P + 2;                 // old-stress / A.v stream slots (and barriers)
+  static constexpr int LVV = N + 2 <= 4 ? 4 : 8;   // v'' ring rows (a power of two >= N + 2)
+  static constexpr int O_Z = 0;                    // [NZ][txz, tzz][2][W]   rows zv+M, +1
+  static constexpr int O_X = O_Z + NZ * 4 * W;     // [NZ][txx, txz][2][W]   rows zv, zv+1
+  static constexpr int O_O = O_X + NZ * 4 * W;     // [NO][txx, tzz, txz][2][W] rows q, q+1
+  static constexpr int O_V = O_O + NO * 6 * W;     // [NO][vx, vz][2][W]     rows zv, zv+1
+  static constexpr int O_VP = O_V + NO * 4 * W;    // [vx, vz][4][W]  v'
+  static constexpr int O_VV = O_VP + 8 * W;        // [vx, vz][LVV][W] v''
+  static constexpr int O_SP = O_VV + 2 * LVV * W;  // [xx, zz, xz][4][W] s'
+  static constexpr int O_WT = O_SP + 12 * W;       // [3][wstride] weights
+};
+
+template <int N, int NT, int P>
+__global__ void __launch_bounds__(NT, 256 / NT)
+    k_el_sweep_rl(const __grid_constant__ CUtensorMap tm_xx, const __grid_constant__ CUtensorMap tm_zz,
+                  const __grid_constant__ CUtensorMap tm_xz, const __grid_constant__ CUtensorMap tm_vx,
+                  const __grid_constant__ CUtensorMap tm_vz, SweepGeom gm, Coef c, float dtx,
+                  float dtz, HabcDev h, MatPack mp, ElOut o, const long long* __restrict__ bounds,
+                  int* __restrict__ err) {
+  using S = RLShape<N, NT, P>;
+  constexpr int W = S::W, M = N, TN = S::TN, HV = S::HV;
+  constexpr int NZ = S::NZ, NO = S::NO, LVV = S::LVV;
+  constexpr int WN = 2 * M + 2;  // window rows
+  extern __shared__ __align__(128) float sm[];
+  float* s_z = sm + S::O_Z;
+  float* s_x = sm + S::O_X;
+  float* s_o = sm + S::O_O;
+  float* s_v = sm + S::O_V;
+  float* s_vp = sm + S::O_VP;
+  float* s_vv = sm + S::O_VV;
+  float* s_sp = sm + S::O_SP;
+  float* s_wt = sm + S::O_WT;
+  const int nwt = (3 * h.wstride + 31) & ~31;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sm + S::O_WT + nwt);  // [NO]
+
+  const int tid = threadIdx.x, sc = 2 * tid;
+  const int TX = gm.TX, WV = TX + 2 * HV;
+  const int nx = gm.nx, nz = gm.nz, nbc = gm.nbc;
+  for (int k = tid; k < S::O_WT; k += NT) sm[k] = 0.0f;
+  for (int k = tid; k < 3 * h.wstride; k += NT) s_wt[k] = __ldg(h.wtab + k);
+  if (tid == 0) {
+    for (int k = 0; k < NO; ++k) mbar_init(&bars[k], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  auto wsm = [&](int kind, int dist) {
+    return dist < h.wstride ? s_wt[kind * h.wstride + dist] : 1.0f;
+  };
+  // Row classification (kernels_fused.jl:28-52, interior of fused_kernels.jl:48):
+  // frame rows 1..nz-2; Higdon side +1 (top band) / -1 (bottom band) / 0.
+  auto zside = [&](int z) { return z <= nbc ? 1 : (z >= nz - 1 - nbc ? -1 : 0); };
+  auto zframe = [&](int z) { return z >= 1 && z <= nz - 2; };
+  auto zinner = [&](int z) { return z >= M && z < nz - M; };
+  auto zdist = [&](int z) { return min(z, nz - 1 - z); };
+  const bool do_v = sc < WV;
+  const bool do_s = sc >= HV - 2 && sc < HV + TX + 2;
+  const bool do_o = sc >= HV && sc < HV + TX;
+  const long long mrow = 2LL * mp.pitch;  // pack step per iteration (two rows)
+
+  const long long r_lo = bounds[blockIdx.x];
+  const long long r_hi = bounds[blockIdx.x + 1];
+  int gb = 0;  // batches this CTA has consumed (ring slot / barrier phase base)
+  bool live = true;
+  for (long long r = r_lo; r < r_hi;) {
+    const long long item = r / nz;
+    const int za = (int)(r - item * nz);
+    const int zb = (int)min((long long)nz, za + (r_hi - r));
+    r += zb - za;
+    const int strip = (int)(item % gm.nstrip);
+    const int shot = (int)(item / gm.nstrip);
+    const int X0 = strip * TX, XV = X0 - HV, XT = XV - TN;
+    const int xc = XV + sc;
+    // per-column constants of this thread's two cells
+    bool xin[2], xfr[2];
+    int xsd[2], xds[2], xcn[2];
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const int x = xc + e;
+      xin[e] = x >= M && x < nx - M;
+      xsd[e] = x <= nbc ? 1 : (x >= nx - 1 - nbc ? -1 : 0);
+      xfr[e] = x >= 1 && x <= nx - 2;
+      xds[e] = min(x, nx - 1 - x);
+      xcn[e] = min(max(sc + e + xsd[e], 0), W - 1);
+    }
+    // a cell of this thread lies in a left/right Higdon band on every frame row
+    const bool xband = (xfr[0] && xsd[0] != 0) || (xfr[1] && xsd[1] != 0);
+    const bool o_any = do_o && xc < nx, o_pair = xc + 1 < nx;
+    float* const ob[5] = {o.vx, o.vz, o.txx, o.tzz, o.txz};
+    const long long obase = (long long)shot * gm.plane + xc;
+    // M warm-up iterations fill the txz/tzz window before the first needed v' row
+    const int zv0 = za - 2 - 3 * M;
+    const int I = (zb - za + 4 + 4 * M + 1) / 2 + 1;
+    auto issue = [&](int k) {
+      const int gk = gb + k, zs = gk % NZ, os = gk % NO;
+      uint64_t* bar = &bars[os];
+      mbar_expect_tx(bar, 9u * 2u * W * 4u);
+      const int zr = zv0 + 2 * k;
+      tma_load_3d(s_z + (zs * 4 + 0) * W, &tm_xz, XT, zr + M, shot, bar);
+      tma_load_3d(s_z + (zs * 4 + 2) * W, &tm_zz, XT, zr + M, shot, bar);
+      tma_load_3d(s_x + (zs * 4 + 0) * W, &tm_xx, XT, zr, shot, bar);
+      tma_load_3d(s_x + (zs * 4 + 2) * W, &tm_xz, XT, zr, shot, bar);
+      tma_load_3d(s_o + (os * 6 + 0) * W, &tm_xx, XT, zr - 3 - M, shot, bar);
+      tma_load_3d(s_o + (os * 6 + 2) * W, &tm_zz, XT, zr - 3 - M, shot, bar);
+      tma_load_3d(s_o + (os * 6 + 4) * W, &tm_xz, XT, zr - 3 - M, shot, bar);
+      tma_load_3d(s_v + (os * 4 + 0) * W, &tm_vx, XV, zr, shot, bar);
+      tma_load_3d(s_v + (os * 4 + 2) * W, &tm_vz, XV, zr, shot, bar);
+    };
+    __syncthreads();  // the previous segment's readers are done with every ring
+    if (tid == 0 && live) {
+      fence_proxy_async();
+      for (int k = 0; k <= P && k < I; ++k) issue(k);
+    }
+    // register state
+    float wxz[WN][2], wzz[WN][2], wvx[WN][2], wvz[WN][2];
+#pragma unroll
+    for (int k = 0; k < WN; ++k)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) wxz[k][e] = wzz[k][e] = wvx[k][e] = wvz[k][e] = 0.0f;
+    float vpp[2][2][2], spp[3][2][2];  // previous iteration's v' / s' rows [field][row][cell]
+#pragma unroll
+    for (int f = 0; f < 2; ++f)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) vpp[f][k >> 1][k & 1] = 0.0f;
+#pragma unroll
+    for (int f = 0; f < 3; ++f)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) spp[f][k >> 1][k & 1] = 0.0f;
+    // materials of iteration i (rows zv, zv+1 for v'; q, q+1 for s'), loaded during i-1
+    const long long pcol = (xc >> 1) + kPackColPad / 2;
+    const float4* pv = mp.v + (long long)(zv0 + kPackRowPad) * mp.pitch + pcol;
+    const float4* pl = mp.l + (long long)(zv0 - 3 - M + kPackRowPad) * mp.pitch + pcol;
+    const float2* pu = mp.mu + (long long)(zv0 - 3 - M + kPackRowPad) * mp.pitch + pcol;
+    float4 mv[2], ml[2];
+    float2 mu[2];
+    auto load_mat = [&]() {
+#pragma unroll
+      for (int rr = 0; rr < 2; ++rr) {
+        mv[rr] = __ldg(pv + rr * mp.pitch);
+        ml[rr] = __ldg(pl + rr * mp.pitch);
+        mu[rr] = __ldg(pu + rr * mp.pitch);
+      }
+      pv += mrow;
+      pl += mrow;
+      pu += mrow;
+    };
+    load_mat();
+    // ring slots of iteration i: zs = (gb+i) % NZ, os = (gb+i) % NO, osp = (gb+i-1) % NO
+    int zs = gb % NZ, os = gb % NO, osp = (gb + NO - 1) % NO;
+    uint32_t ph = (uint32_t)((gb / NO) & 1);
+
+    for (int i = 0; i < I; ++i) {
+      const int zv = zv0 + 2 * i, q = zv - 3 - M;
+      if (live) live = mbar_wait_bounded(&bars[os], ph, err) && live;
+      const float bxv[2][2] = {{mv[0].x, mv[0].y}, {mv[1].x, mv[1].y}};
+      const float bzv[2][2] = {{mv[0].z, mv[0].w}, {mv[1].z, mv[1].w}};
+      const float lav[2][2] = {{ml[0].x, ml[0].y}, {ml[1].x, ml[1].y}};
+      const float l2v[2][2] = {{ml[0].z, ml[0].w}, {ml[1].z, ml[1].w}};
+      const float muv[2][2] = {{mu[0].x, mu[0].y}, {mu[1].x, mu[1].y}};
+      // ---------------- stage A ----------------
+      // new window rows zv+M, zv+M+1 of txz and tzz
+#pragma unroll
+      for (int rr = 0; rr < 2; ++rr) {
+        const float2 a = *reinterpret_cast<const float2*>(s_z + (zs * 4 + rr) * W + sc + TN);
+        const float2 b = *reinterpret_cast<const float2*>(s_z + (zs * 4 + 2 + rr) * W + sc + TN);
+        wxz[2 * M + rr][0] = a.x;
+        wxz[2 * M + rr][1] = a.y;
+        wzz[2 * M + rr][0] = b.x;
+        wzz[2 * M + rr][1] = b.y;
+      }
+      float vpc[2][2][2];  // v' rows zv, zv+1 [field][row][cell]
+      if (do_v) {
+#pragma unroll
+        for (int rr = 0; rr < 2; ++rr) {
+          const bool zin = zinner(zv + rr);
+          float xw[4 * ((N + 1) / 2) + 2];
+          float dxx[2], dxzx[2];
+          load_xwin<N>(s_x + (zs * 4 + rr) * W, sc + TN, xw);
+          dxx[0] = xdm<N>(xw, 0, c);
+          dxx[1] = xdm<N>(xw, 1, c);
+          load_xwin<N>(s_x + (zs * 4 + 2 + rr) * W, sc + TN, xw);
+          dxzx[0] = xdp<N>(xw, 0, c);
+          dxzx[1] = xdp<N>(xw, 1, c);
+          const float2 ox = *reinterpret_cast<const float2*>(s_v + (os * 4 + rr) * W + sc);
+          const float2 oz = *reinterpret_cast<const float2*>(s_v + (os * 4 + 2 + rr) * W + sc);
+          const float vo[2][2] = {{ox.x, ox.y}, {oz.x, oz.y}};
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            float dxzz = 0.0f, dzz = 0.0f;
+#pragma unroll
+            for (int l = 1; l <= N; ++l) {
+              dxzz = __fmaf_rn(c.a[l - 1], __fsub_rn(wxz[rr + M + l - 1][e], wxz[rr + M - l][e]), dxzz);
+              dzz = __fmaf_rn(c.a[l - 1], __fsub_rn(wzz[rr + M + l][e], wzz[rr + M - l + 1][e]), dzz);
+            }
+            float ux = vo[0][e], uz = vo[1][e];
+            if (zin && xin[e]) {
+              ux = __fmaf_rn(bxv[rr][e], __fmaf_rn(dtx, dxx[e], __fmul_rn(dtz, dxzz)), ux);
+              uz = __fmaf_rn(bzv[rr][e], __fmaf_rn(dtx, dxzx[e], __fmul_rn(dtz, dzz)), uz);
+            }
+            vpc[0][rr][e] = ux;
+            vpc[1][rr][e] = uz;
+          }
+          const int pr = (2 * i + rr) & 3;  // v' ring row of zv + rr
+          *reinterpret_cast<float2*>(s_vp + pr * W + sc) = make_float2(vpc[0][rr][0], vpc[0][rr][1]);
+          *reinterpret_cast<float2*>(s_vp + (4 + pr) * W + sc) =
+              make_float2(vpc[1][rr][0], vpc[1][rr][1]);
+        }
+      }
+      // shift the txz / tzz window by two rows for the next iteration
+#pragma unroll
+      for (int k = 0; k < 2 * M; ++k)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          wxz[k][e] = wxz[k + 2][e];
+          wzz[k][e] = wzz[k + 2][e];
+        }
+      float spc[3][2][2];  // s' rows q, q+1 [field][row][cell]
+      if (do_s) {
+#pragma unroll
+        for (int rr = 0; rr < 2; ++rr) {
+          const bool zin = zinner(q + rr);
+          const int vb = (2 * i - 2 - M + rr) & (LVV - 1);  // v'' ring row of q + rr
+          float xw[4 * ((N + 1) / 2) + 2];
+          float dvxdx[2], dvzdx[2];
+          load_xwin<N>(s_vv + vb * W, sc, xw);
+          dvxdx[0] = xdp<N>(xw, 0, c);
+          dvxdx[1] = xdp<N>(xw, 1, c);
+          load_xwin<N>(s_vv + (LVV + vb) * W, sc, xw);
+          dvzdx[0] = xdm<N>(xw, 0, c);
+          dvzdx[1] = xdm<N>(xw, 1, c);
+          const float2 oxx = *reinterpret_cast<const float2*>(s_o + (os * 6 + 0 + rr) * W + sc + TN);
+          const float2 ozz = *reinterpret_cast<const float2*>(s_o + (os * 6 + 2 + rr) * W + sc + TN);
+          const float2 oxz = *reinterpret_cast<const float2*>(s_o + (os * 6 + 4 + rr) * W + sc + TN);
+          const float so_[3][2] = {{oxx.x, oxx.y}, {ozz.x, ozz.y}, {oxz.x, oxz.y}};
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            float dvxdz = 0.0f, dvzdz = 0.0f;
+#pragma unroll
+            for (int l = 1; l <= N; ++l) {
+              dvxdz = __fmaf_rn(c.a[l - 1], __fsub_rn(wvx[rr + M + l][e], wvx[rr + M - l + 1][e]), dvxdz);
+              dvzdz = __fmaf_rn(c.a[l - 1], __fsub_rn(wvz[rr + M + l - 1][e], wvz[rr + M - l][e]), dvzdz);
+            }
+            float sxx = so_[0][e], szz = so_[1][e], sxz = so_[2][e];
+            if (zin && xin[e]) {
+              const float ex = __fmul_rn(dvxdx[e], dtx), ez = __fmul_rn(dvzdz, dtz);
+              sxx = __fadd_rn(sxx, __fmaf_rn(l2v[rr][e], ex, __fmul_rn(lav[rr][e], ez)));
+              szz = __fadd_rn(szz, __fmaf_rn(lav[rr][e], ex, __fmul_rn(l2v[rr][e], ez)));
+              sxz = __fmaf_rn(muv[rr][e], __fmaf_rn(dvxdz, dtz, __fmul_rn(dvzdx[e], dtx)), sxz);
+            }
+            spc[0][rr][e] = sxx;
+            spc[1][rr][e] = szz;
+            spc[2][rr][e] = sxz;
+          }
+          const int sr = (2 * i + rr) & 3;  // s' ring row of q + rr
+#pragma unroll
+          for (int f = 0; f < 3; ++f)
+            *reinterpret_cast<float2*>(s_sp + (4 * f + sr) * W + sc) =
+                make_float2(spc[f][rr][0], spc[f][rr][1]);
+        }
+      }
+      __syncthreads();
+
+      // ---------------- stage B ----------------
+      // v'' rows zv-1 (rr = 0) and zv (rr = 1); v' rows zv-2 .. zv+1 are in vpp / vpc
+      float vvn[2][2][2];
+      if (do_v) {
+#pragma unroll
+        for (int rr = 0; rr < 2; ++rr) {
+          const int qv = zv - 1 + rr;
+#pragma unroll
+          for (int f = 0; f < 2; ++f)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) vvn[f][rr][e] = rr ? vpc[f][0][e] : vpp[f][1][e];
+          const int zsd = zside(qv);
+          if (zframe(qv) && (zsd != 0 || xband)) {
+            const int zd = zdist(qv);
+            const int prow = (2 * i - 1 + rr) & 3;  // v' ring row of qv
+            // A.v rows zv-2, zv-1 sit in the previous pair's slot, zv, zv+1 in this one
+            const int orow = rr ? 0 : 1;
+            const int oslot = rr ? os : osp;
+            const int zslot = zsd > 0 ? os : osp;  // slot of row qv + zsd (row index rr)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+              if (!xfr[e] || (xsd[e] == 0 && zsd == 0)) continue;
+              const int col = sc + e, coln = xcn[e];
+              const int dist = min(xds[e], zd);
+#pragma unroll
+              for (int f = 0; f < 2; ++f) {
+                const float* fo = s_v + (oslot * 4 + 2 * f + orow) * W;
+                const float fop = fo[col];
+                const float w = wsm(f, dist);
+                const float vz_n = rr ? (zsd > 0 ? vpc[f][1][e] : vpp[f][1][e])
+                                      : (zsd > 0 ? vpc[f][0][e] : vpp[f][0][e]);
+                if (xsd[e] != 0 && zsd != 0)
+                  vvn[f][rr][e] = higdon_corner(
+                      w, vvn[f][rr][e],
+                      higdon_side(h, s_vp[(4 * f + prow) * W + coln], fop, fo[coln]),
+                      higdon_side(h, vz_n, fop, s_v[(zslot * 4 + 2 * f + rr) * W + col]));
+                else if (xsd[e] != 0)
+                  vvn[f][rr][e] = higdon_edge(
+                      w, vvn[f][rr][e],
+                      higdon_side(h, s_vp[(4 * f + prow) * W + coln], fop, fo[coln]));
+                else
+                  vvn[f][rr][e] = higdon_edge(
+                      w, vvn[f][rr][e],
+                      higdon_side(h, vz_n, fop, s_v[(zslot * 4 + 2 * f + rr) * W + col]));
+              }
+            }
+          }
+          const int vw = (2 * i + rr) & (LVV - 1);  // v'' ring row of qv
+          *reinterpret_cast<float2*>(s_vv + vw * W + sc) = make_float2(vvn[0][rr][0], vvn[0][rr][1]);
+          *reinterpret_cast<float2*>(s_vv + (LVV + vw) * W + sc) =
+              make_float2(vvn[1][rr][0], vvn[1][rr][1]);
+          if (o_any && qv >= za && qv < zb) {
+            const long long p = obase + (long long)qv * gm.ld;
+            if (o_pair) {
+              *reinterpret_cast<float2*>(ob[0] + p) = make_float2(vvn[0][rr][0], vvn[0][rr][1]);
+              *reinterpret_cast<float2*>(ob[1] + p) = make_float2(vvn[1][rr][0], vvn[1][rr][1]);
+            } else {
+              ob[0][p] = vvn[0][rr][0];
+              ob[1][p] = vvn[1][rr][0];
+            }
+          }
+        }
+      }
+      // the v'' window advances: rows q-M+2 .. q+M+1, then the new rows zv-1, zv
+#pragma unroll
+      for (int k = 0; k < 2 * M; ++k)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          wvx[k][e] = wvx[k + 2][e];
+          wvz[k][e] = wvz[k + 2][e];
+        }
+#pragma unroll
+      for (int rr = 0; rr < 2; ++rr)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          wvx[2 * M + rr][e] = vvn[0][rr][e];
+          wvz[2 * M + rr][e] = vvn[1][rr][e];
+        }
+      // s'' rows q-1 (rr = 0) and q (rr = 1); s' rows q-2 .. q+1 are in spp / spc
+      if (o_any) {
+#pragma unroll
+        for (int rr = 0; rr < 2; ++rr) {
+          const int qs = q - 1 + rr;
+          if (qs < za || qs >= zb) continue;
+          float v[3][2];
+#pragma unroll
+          for (int f = 0; f < 3; ++f)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) v[f][e] = rr ? spc[f][0][e] : spp[f][1][e];
+          const int zsd = zside(qs);
+          if (zframe(qs) && (zsd != 0 || xband)) {
+            const int zd = zdist(qs);
+            const int srow = (2 * i - 1 + rr) & 3;  // s' ring row of qs
+            // old stress rows: q-2, q-1 in the previous pair slot, q, q+1 in this one
+            const int oso = rr ? os : osp, oro = rr ? 0 : 1;  // row qs
+            const int osz = zsd > 0 ? os : osp;              // row qs + zsd (row index rr)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+              if (!xfr[e] || (xsd[e] == 0 && zsd == 0)) continue;
+              const int col = sc + e, coln = xcn[e];
+              const float w = wsm(2, min(xds[e], zd));
+#pragma unroll
+              for (int f = 0; f < 3; ++f) {
+                const float* fo = s_o + (oso * 6 + 2 * f + oro) * W + TN;
+                const float fop = fo[col];
+                const float sz_n = rr ? (zsd > 0 ? spc[f][1][e] : spp[f][1][e])
+                                      : (zsd > 0 ? spc[f][0][e] : spp[f][0][e]);
+                if (xsd[e] != 0 && zsd != 0)
+                  v[f][e] = higdon_corner(
+                      w, v[f][e], higdon_side(h, s_sp[(4 * f + srow) * W + coln], fop, fo[coln]),
+                      higdon_side(h, sz_n, fop, s_o[(osz * 6 + 2 * f + rr) * W + TN + col]));
+                else if (xsd[e] != 0)
+                  v[f][e] = higdon_edge(
+                      w, v[f][e], higdon_side(h, s_sp[(4 * f + srow) * W + coln], fop, fo[coln]));
+                else
+                  v[f][e] = higdon_edge(
+                      w, v[f][e],
+                      higdon_side(h, sz_n, fop, s_o[(osz * 6 + 2 * f + rr) * W + TN + col]));
+              }
+            }
+          }
+          const long long p = obase + (long long)qs * gm.ld;
+#pragma unroll
+          for (int f = 0; f < 3; ++f) {
+            if (o_pair)
+              *reinterpret_cast<float2*>(ob[2 + f] + p) = make_float2(v[f][0], v[f][1]);
+            else
+              ob[2 + f][p] = v[f][0];
+          }
+        }
+      }
+#pragma unroll
+      for (int f = 0; f < 2; ++f)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) vpp[f][k >> 1][k & 1] = vpc[f][k >> 1][k & 1];
+#pragma unroll
+      for (int f = 0; f < 3; ++f)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) spp[f][k >> 1][k & 1] = spc[f][k >> 1][k & 1];
+      load_mat();
+      __syncthreads();
+      if (tid == 0 && live && i + 1 + P < I) {
+        fence_proxy_async();
+        issue(i + 1 + P);
+      }
+      zs = zs + 1 == NZ ? 0 : zs + 1;
+      osp = os;
+      os = os + 1 == NO ? 0 : os + 1;
+      ph ^= os == 0 ? 1u : 0u;
+    }
+    gb += I;
+  }
+}
+
+// ===========================================================================
+// Warp-specialized register-window sweep (the "ws" variants).
+//
+// The lean sweep's work split by role: NV "velocity" threads hold the txz/tzz
+// z-windows and produce v', v'' (HABC, B.v); NV "stress" threads hold the
+// v''x/v''z z-windows and produce s', s'' (HABC, B.stress).  Each role runs
+// its own loop, so a thread keeps only its role's state (about half the
+// registers of k_el_sweep_rl) and more warps fit on an SM to hide the latency
+// of the dependent FMA chains.  The roles meet at a named CTA barrier twice per
+// row pair, in the same sequence in both loops; the v'' rows a stress thread
+// needs in its window come from the shared v'' ring, written one iteration
+// earlier by the velocity threads of the same columns.  Same canonical
+// arithmetic, bit-identical results.
+// ===========================================================================
+__device__ __forceinline__ void cta_bar(int nthreads) {
+  asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
+}
+
+template <int N, int NV, int P, int MINB>
+__global__ void __launch_bounds__(2 * NV, MINB)
+    k_el_sweep_ws(const __grid_constant__ CUtensorMap tm_xx, const __grid_constant__ CUtensorMap tm_zz,
+                  const __grid_constant__ CUtensorMap tm_xz, const __grid_constant__ CUtensorMap tm_vx,
+                  const __grid_constant__ CUtensorMap tm_vz, SweepGeom gm, Coef c, float dtx,
+                  float dtz, HabcDev h, MatPack mp, ElOut o, const long long* __restrict__ bounds,
+                  int* __restrict__ err) {
+  using S = RLShape<N, NV, P>;
+  constexpr int NT = 2 * NV;
+  constexpr int W = S::W, M = N, TN = S::TN, HV = S::HV;
+  constexpr int NZ = S::NZ, NO = S::NO, LVV = S::LVV;
+  constexpr int WN = 2 * M + 2;  // window rows
+  extern __shared__ __align__(128) float sm[];
+  float* s_z = sm + S::O_Z;
+  float* s_x = sm + S::O_X;
+  float* s_o = sm + S::O_O;
+  float* s_v = sm + S::O_V;
+  float* s_vp = sm + S::O_VP;
+  float* s_vv = sm + S::O_VV;
+  float* s_sp = sm + S::O_SP;
+  float* s_wt = sm + S::O_WT;
+  const int nwt = (3 * h.wstride + 31) & ~31;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sm + S::O_WT + nwt);  // [NO]
+
+  const int tid = threadIdx.x;
+  const bool vel = tid < NV;  // warp-uniform role
+  const int sc = 2 * (vel ? tid : tid - NV);
+  const int TX = gm.TX, WV = TX + 2 * HV;
+  const int nx = gm.nx, nz = gm.nz, nbc = gm.nbc;
+  for (int k = tid; k < S::O_WT; k += NT) sm[k] = 0.0f;
+  for (int k = tid; k < 3 * h.wstride; k += NT) s_wt[k] = __ldg(h.wtab + k);
+  if (tid == 0) {
+    for (int k = 0; k < NO; ++k) mbar_init(&bars[k], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  auto wsm = [&](int kind, int dist) {
+    return dist < h.wstride ? s_wt[kind * h.wstride + dist] : 1.0f;
+  };
+  // Row classification (kernels_fused.jl:28-52, interior of fused_kernels.jl:48)
+  auto zside = [&](int z) { return z <= nbc ? 1 : (z >= nz - 1 - nbc ? -1 : 0); };
+  auto zframe = [&](int z) { return z >= 1 && z <= nz - 2; };
+  auto zinner = [&](int z) { return z >= M && z < nz - M; };
+  auto zdist = [&](int z) { return min(z, nz - 1 - z); };
+  const bool do_v = sc < WV;
+  const bool do_s = sc >= HV - 2 && sc < HV + TX + 2;
+  const bool do_o = sc >= HV && sc < HV + TX;
+  const long long mrow = 2LL * mp.pitch;  // pack step per iteration (two rows)
+  const long long r_lo = bounds[blockIdx.x];
+  const long long r_hi = bounds[blockIdx.x + 1];
+
+  // One segment = a run of rows [za, zb) of one (shot, strip); both roles walk
+  // the same segments and iterations.
+  struct Seg {
+    int za, zb, shot, XV, XT, xc, zv0, I;
+    bool xin[2], xfr[2], xband, o_any, o_pair;
+    int xsd[2], xds[2], xcn[2];
+    long long obase;
+  };
+  auto segment = [&](long long& r, Seg& g) {
+    const long long item = r / nz;
+    g.za = (int)(r - item * nz);
+    g.zb = (int)min((long long)nz, g.za + (r_hi - r));
+    r += g.zb - g.za;
+    const int strip = (int)(item % gm.nstrip);
+    g.shot = (int)(item / gm.nstrip);
+    g.XV = strip * TX - HV;
+    g.XT = g.XV - TN;
+    g.xc = g.XV + sc;
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const int x = g.xc + e;
+      g.xin[e] = x >= M && x < nx - M;
+      g.xsd[e] = x <= nbc ? 1 : (x >= nx - 1 - nbc ? -1 : 0);
+      g.xfr[e] = x >= 1 && x <= nx - 2;
+      g.xds[e] = min(x, nx - 1 - x);
+      g.xcn[e] = min(max(sc + e + g.xsd[e], 0), W - 1);
+    }
+    g.xband = (g.xfr[0] && g.xsd[0] != 0) || (g.xfr[1] && g.xsd[1] != 0);
+    g.o_any = do_o && g.xc < nx;
+    g.o_pair = g.xc + 1 < nx;
+    g.obase = (long long)g.shot * gm.plane + g.xc;
+    g.zv0 = g.za - 2 - 3 * M;  // M warm-up iterations fill the windows
+    g.I = (g.zb - g.za + 4 + 4 * M + 1) / 2 + 1;
+  };
+
+  if (vel) {
+    // ======================= velocity role =======================
+    int gb = 0;
+    bool live = true;
+    for (long long r = r_lo; r < r_hi;) {
+      Seg g;
+      segment(r, g);
+      auto issue = [&](int k) {
+        const int gk = gb + k, zs = gk % NZ, os = gk % NO;
+        uint64_t* bar = &bars[os];
+        mbar_expect_tx(bar, 9u * 2u * W * 4u);
+        const int zr = g.zv0 + 2 * k;
+        tma_load_3d(s_z + (zs * 4 + 0) * W, &tm_xz, g.XT, zr + M, g.shot, bar);
+        tma_load_3d(s_z + (zs * 4 + 2) * W, &tm_zz, g.XT, zr + M, g.shot, bar);
+        tma_load_3d(s_x + (zs * 4 + 0) * W, &tm_xx, g.XT, zr, g.shot, bar);
+        tma_load_3d(s_x + (zs * 4 + 2) * W, &tm_xz, g.XT, zr, g.shot, bar);
+        tma_load_3d(s_o + (os * 6 + 0) * W, &tm_xx, g.XT, zr - 3 - M, g.shot, bar);
+        tma_load_3d(s_o + (os * 6 + 2) * W, &tm_zz, g.XT, zr - 3 - M, g.shot, bar);
+        tma_load_3d(s_o + (os * 6 + 4) * W, &tm_xz, g.XT, zr - 3 - M, g.shot, bar);
+        tma_load_3d(s_v + (os * 4 + 0) * W, &tm_vx, g.XV, zr, g.shot, bar);
+        tma_load_3d(s_v + (os * 4 + 2) * W, &tm_vz, g.XV, zr, g.shot, bar);
+      };
+      cta_bar(NT);  // the previous segment's readers are done with every ring
+      if (tid == 0 && live) {
+        fence_proxy_async();
+        for (int k = 0; k <= P && k < g.I; ++k) issue(k);
+      }
+      float wxz[WN][2], wzz[WN][2];
+#pragma unroll
+      for (int k = 0; k < WN; ++k)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) wxz[k][e] = wzz[k][e] = 0.0f;
+      float vpp[2][2][2];  // previous iteration's v' rows [field][row][cell]
+#pragma unroll
+      for (int f = 0; f < 2; ++f)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) vpp[f][k >> 1][k & 1] = 0.0f;
+      const long long pcol = (g.xc >> 1) + kPackColPad / 2;
+      const float4* pv = mp.v + (long long)(g.zv0 + kPackRowPad) * mp.pitch + pcol;
+      float4 mv[2];
+      mv[0] = __ldg(pv);
+      mv[1] = __ldg(pv + mp.pitch);
+      pv += mrow;
+      int zs = gb % NZ, os = gb % NO, osp = (gb + NO - 1) % NO;
+      uint32_t ph = (uint32_t)((gb / NO) & 1);
+      for (int i = 0; i < g.I; ++i) {
+        const int zv = g.zv0 + 2 * i;
+        if (live) live = mbar_wait_bounded(&bars[os], ph, err) && live;
+        const float bxv[2][2] = {{mv[0].x, mv[0].y}, {mv[1].x, mv[1].y}};
+        const float bzv[2][2] = {{mv[0].z, mv[0].w}, {mv[1].z, mv[1].w}};
+#pragma unroll
+        for (int rr = 0; rr < 2; ++rr) {
+          const float2 a = *reinterpret_cast<const float2*>(s_z + (zs * 4 + rr) * W + sc + TN);
+          const float2 b = *reinterpret_cast<const float2*>(s_z + (zs * 4 + 2 + rr) * W + sc + TN);
+          wxz[2 * M + rr][0] = a.x;
+          wxz[2 * M + rr][1] = a.y;
+          wzz[2 * M + rr][0] = b.x;
+          wzz[2 * M + rr][1] = b.y;
+        }
+        float vpc[2][2][2];  // v' rows zv, zv+1 [field][row][cell]
+        if (do_v) {
+#pragma unroll
+          for (int rr = 0; rr < 2; ++rr) {
+            const bool zin = zinner(zv + rr);
+            float xw[4 * ((N + 1) / 2) + 2];
+            float dxx[2], dxzx[2];
+            load_xwin<N>(s_x + (zs * 4 + rr) * W, sc + TN, xw);
+            dxx[0] = xdm<N>(xw, 0, c);
+            dxx[1] = xdm<N>(xw, 1, c);
+            load_xwin<N>(s_x + (zs * 4 + 2 + rr) * W, sc + TN, xw);
+            dxzx[0] = xdp<N>(xw, 0, c);
+            dxzx[1] = xdp<N>(xw, 1, c);
+            const float2 ox = *reinterpret_cast<const float2*>(s_v + (os * 4 + rr) * W + sc);
+            const float2 oz = *reinterpret_cast<const float2*>(s_v + (os * 4 + 2 + rr) * W + sc);
+            const float vo[2][2] = {{ox.x, ox.y}, {oz.x, oz.y}};
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+              float dxzz = 0.0f, dzz = 0.0f;
+#pragma unroll
+              for (int l = 1; l <= N; ++l) {
+                dxzz = __fmaf_rn(c.a[l - 1], __fsub_rn(wxz[rr + M + l - 1][e], wxz[rr + M - l][e]), dxzz);
+                dzz = __fmaf_rn(c.a[l - 1], __fsub_rn(wzz[rr + M + l][e], wzz[rr + M - l + 1][e]), dzz);
+              }
+              float ux = vo[0][e], uz = vo[1][e];
+              if (zin && g.xin[e]) {
+                ux = __fmaf_rn(bxv[rr][e], __fmaf_rn(dtx, dxx[e], __fmul_rn(dtz, dxzz)), ux);
+                uz = __fmaf_rn(bzv[rr][e], __fmaf_rn(dtx, dxzx[e], __fmul_rn(dtz, dzz)), uz);
+              }
+              vpc[0][rr][e] = ux;
+              vpc[1][rr][e] = uz;
+            }
+            const int pr = (2 * i + rr) & 3;  // v' ring row of zv + rr
+            *reinterpret_cast<float2*>(s_vp + pr * W + sc) = make_float2(vpc[0][rr][0], vpc[0][rr][1]);
+            *reinterpret_cast<float2*>(s_vp + (4 + pr) * W + sc) =
+                make_float2(vpc[1][rr][0], vpc[1][rr][1]);
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < 2 * M; ++k)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            wxz[k][e] = wxz[k + 2][e];
+            wzz[k][e] = wzz[k + 2][e];
+          }
+        cta_bar(NT);
+        // v'' rows zv-1 (rr = 0) and zv (rr = 1); v' rows zv-2 .. zv+1 are in vpp / vpc
+        if (do_v) {
+#pragma unroll
+          for (int rr = 0; rr < 2; ++rr) {
+            const int qv = zv - 1 + rr;
+            float vvn[2][2];
+#pragma unroll
+            for (int f = 0; f < 2; ++f)
+#pragma unroll
+              for (int e = 0; e < 2; ++e) vvn[f][e] = rr ? vpc[f][0][e] : vpp[f][1][e];
+            const int zsd = zside(qv);
+            if (zframe(qv) && (zsd != 0 || g.xband)) {
+              const int zd = zdist(qv);
+              const int prow = (2 * i - 1 + rr) & 3;  // v' ring row of qv
+              // A.v rows zv-2, zv-1 sit in the previous pair's slot, zv, zv+1 in this one
+              const int orow = rr ? 0 : 1;
+              const int oslot = rr ? os : osp;
+              const int zslot = zsd > 0 ? os : osp;  // slot of row qv + zsd (row index rr)
+#pragma unroll
+              for (int e = 0; e < 2; ++e) {
+                if (!g.xfr[e] || (g.xsd[e] == 0 && zsd == 0)) continue;
+                const int col = sc + e, coln = g.xcn[e];
+                const int dist = min(g.xds[e], zd);
+#pragma unroll
+                for (int f = 0; f < 2; ++f) {
+                  const float* fo = s_v + (oslot * 4 + 2 * f + orow) * W;
+                  const float fop = fo[col];
+                  const float w = wsm(f, dist);
+                  const float vz_n = rr ? (zsd > 0 ? vpc[f][1][e] : vpp[f][1][e])
+                                        : (zsd > 0 ? vpc[f][0][e] : vpp[f][0][e]);
+                  if (g.xsd[e] != 0 && zsd != 0)
+                    vvn[f][e] = higdon_corner(
+                        w, vvn[f][e], higdon_side(h, s_vp[(4 * f + prow) * W + coln], fop, fo[coln]),
+                        higdon_side(h, vz_n, fop, s_v[(zslot * 4 + 2 * f + rr) * W + col]));
+                  else if (g.xsd[e] != 0)
+                    vvn[f][e] = higdon_edge(
+                        w, vvn[f][e], higdon_side(h, s_vp[(4 * f + prow) * W + coln], fop, fo[coln]));
+                  else
+                    vvn[f][e] = higdon_edge(
+                        w, vvn[f][e],
+                        higdon_side(h, vz_n, fop, s_v[(zslot * 4 + 2 * f + rr) * W + col]));
+                }
+              }
+            }
+            const int vw = (2 * i + rr) & (LVV - 1);  // v'' ring row of qv
+            *reinterpret_cast<float2*>(s_vv + vw * W + sc) = make_float2(vvn[0][0], vvn[0][1]);
+            *reinterpret_cast<float2*>(s_vv + (LVV + vw) * W + sc) = make_float2(vvn[1][0], vvn[1][1]);
+            if (g.o_any && qv >= g.za && qv < g.zb) {
+              const long long p = g.obase + (long long)qv * gm.ld;
+              if (g.o_pair) {
+                *reinterpret_cast<float2*>(o.vx + p) = make_float2(vvn[0][0], vvn[0][1]);
+                *reinterpret_cast<float2*>(o.vz + p) = make_float2(vvn[1][0], vvn[1][1]);
+              } else {
+                o.vx[p] = vvn[0][0];
+                o.vz[p] = vvn[1][0];
+              }
+            }
+          }
+        }
+#pragma unroll
+        for (int f = 0; f < 2; ++f)
+#pragma unroll
+          for (int k = 0; k < 4; ++k) vpp[f][k >> 1][k & 1] = vpc[f][k >> 1][k & 1];
+        mv[0] = __ldg(pv);
+        mv[1] = __ldg(pv + mp.pitch);
+        pv += mrow;
+        cta_bar(NT);
+        if (tid == 0 && live && i + 1 + P < g.I) {
+          fence_proxy_async();
+          issue(i + 1 + P);
+        }
+        zs = zs + 1 == NZ ? 0 : zs + 1;
+        osp = os;
+        os = os + 1 == NO ? 0 : os + 1;
+        ph ^= os == 0 ? 1u : 0u;
+      }
+      gb += g.I;
+    }
+  } else {
+    // ======================== stress role ========================
+    int gb = 0;
+    bool live = true;
+    for (long long r = r_lo; r < r_hi;) {
+      Seg g;
+      segment(r, g);
+      cta_bar(NT);  // pairs with the velocity role's segment barrier
+      float wvx[WN][2], wvz[WN][2];
+#pragma unroll
+      for (int k = 0; k < WN; ++k)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) wvx[k][e] = wvz[k][e] = 0.0f;
+      float spp[3][2][2];  // previous iteration's s' rows [field][row][cell]
+#pragma unroll
+      for (int f = 0; f < 3; ++f)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) spp[f][k >> 1][k & 1] = 0.0f;
+      const long long pcol = (g.xc >> 1) + kPackColPad / 2;
+      const long long prow0 = (long long)(g.zv0 - 3 - M + kPackRowPad) * mp.pitch + pcol;
+      const float4* pl = mp.l + prow0;
+      const float2* pu = mp.mu + prow0;
+      float4 ml[2];
+      float2 mu[2];
+      ml[0] = __ldg(pl);
+      ml[1] = __ldg(pl + mp.pitch);
+      mu[0] = __ldg(pu);
+      mu[1] = __ldg(pu + mp.pitch);
+      pl += mrow;
+      pu += mrow;
+      int os = gb % NO, osp = (gb + NO - 1) % NO;
+      uint32_t ph = (uint32_t)((gb / NO) & 1);
+      for (int i = 0; i < g.I; ++i) {
+        const int zv = g.zv0 + 2 * i, q = zv - 3 - M;
+        if (live) live = mbar_wait_bounded(&bars[os], ph, err) && live;
+        const float lav[2][2] = {{ml[0].x, ml[0].y}, {ml[1].x, ml[1].y}};
+        const float l2v[2][2] = {{ml[0].z, ml[0].w}, {ml[1].z, ml[1].w}};
+        const float muv[2][2] = {{mu[0].x, mu[0].y}, {mu[1].x, mu[1].y}};
+        // the v'' window advances by two rows: rows q-M .. q+M-1 move down, and
+        // v'' rows q+M, q+M+1 (= zv-3, zv-2, written by the velocity role in
+        // the previous iteration) enter at the top
+
+        if (i > 0) {
+#pragma unroll
+          for (int k = 0; k < 2 * M; ++k)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+              wvx[k][e] = wvx[k + 2][e];
+              wvz[k][e] = wvz[k + 2][e];
+            }
+#pragma unroll
+          for (int rr = 0; rr < 2; ++rr) {
+            const int vr = (2 * i - 2 + rr) & (LVV - 1);
+            const float2 a = *reinterpret_cast<const float2*>(s_vv + vr * W + sc);
+            const float2 b = *reinterpret_cast<const float2*>(s_vv + (LVV + vr) * W + sc);
+            wvx[2 * M + rr][0] = a.x;
+            wvx[2 * M + rr][1] = a.y;
+            wvz[2 * M + rr][0] = b.x;
+            wvz[2 * M + rr][1] = b.y;
+          }
+        }
+        float spc[3][2][2];  // s' rows q, q+1 [field][row][cell]
+        if (do_s) {
+#pragma unroll
+          for (int rr = 0; rr < 2; ++rr) {
+            const bool zin = zinner(q + rr);
+            const int vb = (2 * i - 2 - M + rr) & (LVV - 1);  // v'' ring row of q + rr
+            float xw[4 * ((N + 1) / 2) + 2];
+            float dvxdx[2], dvzdx[2];
+            load_xwin<N>(s_vv + vb * W, sc, xw);
+            dvxdx[0] = xdp<N>(xw, 0, c);
+            dvxdx[1] = xdp<N>(xw, 1, c);
+            load_xwin<N>(s_vv + (LVV + vb) * W, sc, xw);
+            dvzdx[0] = xdm<N>(xw, 0, c);
+            dvzdx[1] = xdm<N>(xw, 1, c);
+            const float2 oxx = *reinterpret_cast<const float2*>(s_o + (os * 6 + 0 + rr) * W + sc + TN);
+            const float2 ozz = *reinterpret_cast<const float2*>(s_o + (os * 6 + 2 + rr) * W + sc + TN);
+            const float2 oxz = *reinterpret_cast<const float2*>(s_o + (os * 6 + 4 + rr) * W + sc + TN);
+            const float so_[3][2] = {{oxx.x, oxx.y}, {ozz.x, ozz.y}, {oxz.x, oxz.y}};
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+              float dvxdz = 0.0f, dvzdz = 0.0f;
+#pragma unroll
+              for (int l = 1; l <= N; ++l) {
+                dvxdz = __fmaf_rn(c.a[l - 1], __fsub_rn(wvx[rr + M + l][e], wvx[rr + M - l + 1][e]), dvxdz);
+                dvzdz = __fmaf_rn(c.a[l - 1], __fsub_rn(wvz[rr + M + l - 1][e], wvz[rr + M - l][e]), dvzdz);
+              }
+              float sxx = so_[0][e], szz = so_[1][e], sxz = so_[2][e];
+              if (zin && g.xin[e]) {
+                const float ex = __fmul_rn(dvxdx[e], dtx), ez = __fmul_rn(dvzdz, dtz);
+                sxx = __fadd_rn(sxx, __fmaf_rn(l2v[rr][e], ex, __fmul_rn(lav[rr][e], ez)));
+                szz = __fadd_rn(szz, __fmaf_rn(lav[rr][e], ex, __fmul_rn(l2v[rr][e], ez)));
+                sxz = __fmaf_rn(muv[rr][e], __fmaf_rn(dvxdz, dtz, __fmul_rn(dvzdx[e], dtx)), sxz);
+              }
+              spc[0][rr][e] = sxx;
+              spc[1][rr][e] = szz;
+              spc[2][rr][e] = sxz;
+            }
+            const int sr = (2 * i + rr) & 3;  // s' ring row of q + rr
+#pragma unroll
+            for (int f = 0; f < 3; ++f)
+              *reinterpret_cast<float2*>(s_sp + (4 * f + sr) * W + sc) =
+                  make_float2(spc[f][rr][0], spc[f][rr][1]);
+          }
+        }
+        cta_bar(NT);
+        // s'' rows q-1 (rr = 0) and q (rr = 1); s' rows q-2 .. q+1 are in spp / spc
+        if (g.o_any) {
+#pragma unroll
+          for (int rr = 0; rr < 2; ++rr) {
+            const int qs = q - 1 + rr;
+            if (qs < g.za || qs >= g.zb) continue;
+            float v[3][2];
+#pragma unroll
+            for (int f = 0; f < 3; ++f)
+#pragma unroll
+              for (int e = 0; e < 2; ++e) v[f][e] = rr ? spc[f][0][e] : spp[f][1][e];
+            const int zsd = zside(qs);
+            if (zframe(qs) && (zsd != 0 || g.xband)) {
+              const int zd = zdist(qs);
+              const int srow = (2 * i - 1 + rr) & 3;  // s' ring row of qs
+              // old stress rows: q-2, q-1 in the previous pair slot, q, q+1 in this one
+              const int oso = rr ? os : osp, oro = rr ? 0 : 1;  // row qs
+              const int osz = zsd > 0 ? os : osp;              // row qs + zsd (row index rr)
+#pragma unroll
+              for (int e = 0; e < 2; ++e) {
+                if (!g.xfr[e] || (g.xsd[e] == 0 && zsd == 0)) continue;
+                const int col = sc + e, coln = g.xcn[e];
+                const float w = wsm(2, min(g.xds[e], zd));
+#pragma unroll
+                for (int f = 0; f < 3; ++f) {
+                  const float* fo = s_o + (oso * 6 + 2 * f + oro) * W + TN;
+                  const float fop = fo[col];
+                  const float sz_n = rr ? (zsd > 0 ? spc[f][1][e] : spp[f][1][e])
+                                        : (zsd > 0 ? spc[f][0][e] : spp[f][0][e]);
+                  if (g.xsd[e] != 0 && zsd != 0)
+                    v[f][e] = higdon_corner(
+                        w, v[f][e], higdon_side(h, s_sp[(4 * f + srow) * W + coln], fop, fo[coln]),
+                        higdon_side(h, sz_n, fop, s_o[(osz * 6 + 2 * f + rr) * W + TN + col]));
+                  else if (g.xsd[e] != 0)
+                    v[f][e] = higdon_edge(
+                        w, v[f][e], higdon_side(h, s_sp[(4 * f + srow) * W + coln], fop, fo[coln]));
+                  else
+                    v[f][e] = higdon_edge(
+                        w, v[f][e],
+                        higdon_side(h, sz_n, fop, s_o[(osz * 6 + 2 * f + rr) * W + TN + col]));
+                }
+              }
+            }
+            const long long p = g.obase + (long long)qs * gm.ld;
+            float* out[3] = {o.txx, o.tzz, o.txz};
+#pragma unroll
+            for (int f = 0; f < 3; ++f) {
+              if (g.o_pair)
+                *reinterpret_cast<float2*>(out[f] + p) = make_float2(v[f][0], v[f][1]);
+              else
+                out[f][p] = v[f][0];
+            }
+          }
+        }
+#pragma unroll
+        for (int f = 0; f < 3; ++f)
+#pragma unroll
+          for (int k = 0; k < 4; ++k) spp[f][k >> 1][k & 1] = spc[f][k >> 1][k & 1];
+        ml[0] = __ldg(pl);
+        ml[1] = __ldg(pl + mp.pitch);
+        mu[0] = __ldg(pu);
+        mu[1] = __ldg(pu + mp.pitch);
+        pl += mrow;
+        pu += mrow;
+        cta_bar(NT);
+        osp = os;
+        os = os + 1 == NO ? 0 : os + 1;
+        ph ^= os == 0 ? 1u : 0u;
+      }
+      gb += g.I;
+    }
+  }
+}
+
 // ---- host side --------------------------------------------------------------
 PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 std::once_flag g_encode_once;
@@ -1264,6 +2181,25 @@ constexpr int kNumX2 = sizeof(kX2P) / sizeof(kX2P[0]);
 constexpr int kRWP[] = {1, 2};
 constexpr int kNumRW = sizeof(kRWP) / sizeof(kRWP[0]);
 #define FOMO_RW_VARIANTS(X, NN) X(0, NN, 1) X(1, NN, 2)
+
+// lean register-window variants: (threads, prefetch depth in row pairs)
+constexpr int kRLNT[] = {128, 128, 64, 64};
+constexpr int kRLP[] = {1, 2, 1, 2};
+constexpr int kNumRL = sizeof(kRLP) / sizeof(kRLP[0]);
+#define FOMO_RL_VARIANTS(X, NN) X(0, NN, 128, 1) X(1, NN, 128, 2) X(2, NN, 64, 1) X(3, NN, 64, 2)
+
+template <int N, int NT, int P>
+size_t rl_smem_bytes(int wstride) {
+  using S = RLShape<N, NT, P>;
+  return (size_t)(S::O_WT + ((3 * wstride + 31) & ~31)) * 4 + sizeof(uint64_t) * S::NO;
+}
+
+// warp-specialized variants: (threads per role, prefetch depth, CTAs per SM)
+constexpr int kWSNV[] = {128, 64, 64, 128};
+constexpr int kWSP[] = {1, 1, 1, 2};
+constexpr int kNumWS = sizeof(kWSP) / sizeof(kWSP[0]);
+#define FOMO_WS_VARIANTS(X, NN) \
+  X(0, NN, 128, 1, 2) X(1, NN, 64, 1, 4) X(2, NN, 64, 1, 3) X(3, NN, 128, 2, 2)
 
 template <int N, int P>
 size_t rw_smem_bytes(int wstride) {
@@ -1367,6 +2303,114 @@ cudaError_t launch_rw_n(cudaStream_t st, const SweepPlan& sp, int set, const Coe
   return cudaErrorInvalidValue;
 }
 
+template <int N, int NT, int P>
+cudaError_t launch_rl(cudaStream_t st, const SweepPlan& sp, int set, const Coef& c, float dtx,
+                      float dtz, const HabcDev& h, const ElMat& m, const ElOut& o, int* err) {
+  auto kern = k_el_sweep_rl<N, NT, P>;
+  static std::atomic<int> attr_set{0};
+  if (!attr_set.load(std::memory_order_acquire)) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kMaxDynSmem);
+    if (e != cudaSuccess) return e;
+    attr_set.store(1, std::memory_order_release);
+  }
+  if (sp.smem > (size_t)kMaxDynSmem || !m.pack || m.pack_pitch < 1) return cudaErrorInvalidValue;
+  const long long cells = (long long)(sp.gm.nz + 2 * kPackRowPad) * m.pack_pitch;
+  const MatPack mp{reinterpret_cast<const float4*>(m.pack),
+                   reinterpret_cast<const float4*>(m.pack) + cells,
+                   reinterpret_cast<const float2*>(m.pack + 8 * cells), m.pack_pitch};
+  kern<<<(unsigned)sp.grid, NT, sp.smem, st>>>(sp.tm[set][0], sp.tm[set][1], sp.tm[set][2],
+                                                sp.tm[set][3], sp.tm[set][4], sp.gm, c, dtx, dtz, h,
+                                                mp, o, sp.d_bounds, err);
+  return cudaGetLastError();
+}
+
+template <int N>
+cudaError_t launch_rl_n(cudaStream_t st, const SweepPlan& sp, int set, const Coef& c, float dtx,
+                        float dtz, const HabcDev& h, const ElMat& m, const ElOut& o, int* err) {
+#define FOMO_LAUNCH_RL(V, NN, NT, PP) \
+  case V: return launch_rl<NN, NT, PP>(st, sp, set, c, dtx, dtz, h, m, o, err);
+  switch (sp.variant - kNumVariants - kNumX2 - kNumRW) { FOMO_RL_VARIANTS(FOMO_LAUNCH_RL, N) }
+#undef FOMO_LAUNCH_RL
+  return cudaErrorInvalidValue;
+}
+
+template <int N, int NV, int P, int MINB>
+cudaError_t launch_ws(cudaStream_t st, const SweepPlan& sp, int set, const Coef& c, float dtx,
+                      float dtz, const HabcDev& h, const ElMat& m, const ElOut& o, int* err) {
+  auto kern = k_el_sweep_ws<N, NV, P, MINB>;
+  static std::atomic<int> attr_set{0};
+  if (!attr_set.load(std::memory_order_acquire)) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kMaxDynSmem);
+    if (e != cudaSuccess) return e;
+    attr_set.store(1, std::memory_order_release);
+  }
+  if (sp.smem > (size_t)kMaxDynSmem || !m.pack || m.pack_pitch < 1) return cudaErrorInvalidValue;
+  const long long cells = (long long)(sp.gm.nz + 2 * kPackRowPad) * m.pack_pitch;
+  const MatPack mp{reinterpret_cast<const float4*>(m.pack),
+                   reinterpret_cast<const float4*>(m.pack) + cells,
+                   reinterpret_cast<const float2*>(m.pack + 8 * cells), m.pack_pitch};
+  kern<<<(unsigned)sp.grid, 2 * NV, sp.smem, st>>>(sp.tm[set][0], sp.tm[set][1], sp.tm[set][2],
+                                                    sp.tm[set][3], sp.tm[set][4], sp.gm, c, dtx,
+                                                    dtz, h, mp, o, sp.d_bounds, err);
+  return cudaGetLastError();
+}
+
+template <int N>
+cudaError_t launch_ws_n(cudaStream_t st, const SweepPlan& sp, int set, const Coef& c, float dtx,
+                        float dtz, const HabcDev& h, const ElMat& m, const ElOut& o, int* err) {
+#define FOMO_LAUNCH_WS(V, NN, NV, PP, MB) \
+  case V: return launch_ws<NN, NV, PP, MB>(st, sp, set, c, dtx, dtz, h, m, o, err);
+  switch (sp.variant - kNumVariants - kNumX2 - kNumRW - kNumRL) {
+    FOMO_WS_VARIANTS(FOMO_LAUNCH_WS, N)
+  }
+#undef FOMO_LAUNCH_WS
+  return cudaErrorInvalidValue;
+}
+
+size_t ws_smem_for(int N, int v, int wstride) {
+#define FOMO_SMEM_WS(V, NN, NV, PP, MB) \
+  case V: return rl_smem_bytes<NN, NV, PP>(wstride);
+#define FOMO_SMEM_WSN(NN)                              \
+  case NN:                                             \
+    switch (v) { FOMO_WS_VARIANTS(FOMO_SMEM_WS, NN) }  \
+    break;
+  switch (N) { FOMO_SMEM_WSN(1) FOMO_SMEM_WSN(2) FOMO_SMEM_WSN(3) FOMO_SMEM_WSN(4) FOMO_SMEM_WSN(5) }
+#undef FOMO_SMEM_WSN
+#undef FOMO_SMEM_WS
+  return 0;
+}
+
+size_t rl_smem_for(int N, int v, int wstride) {
+#define FOMO_SMEM_RL(V, NN, NT, PP) \
+  case V: return rl_smem_bytes<NN, NT, PP>(wstride);
+#define FOMO_SMEM_RLN(NN)                              \
+  case NN:                                             \
+    switch (v) { FOMO_RL_VARIANTS(FOMO_SMEM_RL, NN) }  \
+    break;
+  switch (N) { FOMO_SMEM_RLN(1) FOMO_SMEM_RLN(2) FOMO_SMEM_RLN(3) FOMO_SMEM_RLN(4) FOMO_SMEM_RLN(5) }
+#undef FOMO_SMEM_RLN
+#undef FOMO_SMEM_RL
+  return 0;
+}
+
+// Copies the five elastic planes into the lean sweep's material pack.
+__global__ void k_sweep_pack(int nx, int nz, int ld, ElMat m, float4* pv, float4* pl, float2* pu,
+                             int pitch, long long cells) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < cells;
+       k += (long long)gridDim.x * blockDim.x) {
+    const int z = (int)(k / pitch) - kPackRowPad;
+    const int x = 2 * ((int)(k % pitch) - kPackColPad / 2);
+    auto at = [&](const float* a, int xx) {
+      return z >= 0 && z < nz && xx >= 0 && xx < nx ? a[(long long)z * ld + xx] : 0.0f;
+    };
+    pv[k] = make_float4(at(m.bx, x), at(m.bx, x + 1), at(m.bz, x), at(m.bz, x + 1));
+    pl[k] = make_float4(at(m.lam, x), at(m.lam, x + 1), at(m.l2m, x), at(m.l2m, x + 1));
+    pu[k] = make_float2(at(m.mut, x), at(m.mut, x + 1));
+  }
+}
+
 size_t rw_smem_for(int N, int v, int wstride) {
 #define FOMO_SMEM_RW(V, NN, PP) \
   case V: return rw_smem_bytes<NN, PP>(wstride);
@@ -1418,7 +2462,25 @@ int pick_kernel_2d(int phys, int N, int nxp, int nzp, int ns) {
 
 bool sweep2d_supported(int phys, int N) { return phys == 1 && N >= 1 && N <= 5 && encoder(); }
 
-int sweep_num_variants() { return kNumVariants + kNumX2 + kNumRW; }
+int sweep_num_variants() { return kNumVariants + kNumX2 + kNumRW + kNumRL + kNumWS; }
+
+int sweep_pack_pitch(int nx) { return ((nx + 2 * 128 + kPackColPad) / 2 + 16) & ~15; }
+
+size_t sweep_pack_floats(int nx, int nz) {
+  return (size_t)(nz + 2 * kPackRowPad) * sweep_pack_pitch(nx) * 10;
+}
+
+cudaError_t build_sweep_pack(cudaStream_t st, const Geo2& g, ElMat& m, float* dst) {
+  if (!dst || (reinterpret_cast<uintptr_t>(dst) & 15)) return cudaErrorInvalidValue;
+  const int pitch = sweep_pack_pitch(g.nx);
+  const long long cells = (long long)(g.nz + 2 * kPackRowPad) * pitch;
+  float4* pv = reinterpret_cast<float4*>(dst);
+  k_sweep_pack<<<1184, 256, 0, st>>>(g.nx, g.nz, g.ld, m, pv, pv + cells,
+                                     reinterpret_cast<float2*>(dst + 8 * cells), pitch, cells);
+  m.pack = dst;
+  m.pack_pitch = pitch;
+  return cudaGetLastError();
+}
 
 // Builds the work decomposition and the six tensor maps (3 stress fields x 2
 // ping-pong sets).  variant selects (threads, rows per chunk, prefetch depth);
@@ -1428,12 +2490,25 @@ cudaError_t make_sweep_plan(SweepPlan& sp, int N, int variant, int TX, int per_s
                             long long* d_bounds, cudaStream_t st) {
   auto enc = encoder();
   if (!enc) return cudaErrorNotSupported;
-  if (variant < 0 || variant >= kNumVariants + kNumX2 + kNumRW || per_sm < 1)
-    return cudaErrorInvalidValue;
-  const bool rw = variant >= kNumVariants + kNumX2;
-  const bool x2 = variant >= kNumVariants;  // both 256-wide TMA-box families
+  if (variant < 0 || variant >= sweep_num_variants() || per_sm < 1) return cudaErrorInvalidValue;
+  const bool ws = variant >= kNumVariants + kNumX2 + kNumRW + kNumRL;
+  const bool rl = !ws && variant >= kNumVariants + kNumX2 + kNumRW;
+  const bool rw = !ws && !rl && variant >= kNumVariants + kNumX2;
+  const bool x2 = variant >= kNumVariants;  // the 2-row TMA-box families
   int W = 0, R = 2;
-  if (x2) {
+  if (ws) {
+    const int v = variant - kNumVariants - kNumX2 - kNumRW - kNumRL;
+    if (TX < 8 || TX > rl_txmax(N, kWSNV[v]) || (TX & 3)) return cudaErrorInvalidValue;
+    W = rl_w(N, kWSNV[v]);
+    sp.family = 4;
+    sp.P = kWSP[v];
+  } else if (rl) {
+    const int v = variant - kNumVariants - kNumX2 - kNumRW;
+    if (TX < 8 || TX > rl_txmax(N, kRLNT[v]) || (TX & 3)) return cudaErrorInvalidValue;
+    W = rl_w(N, kRLNT[v]);
+    sp.family = 3;
+    sp.P = kRLP[v];
+  } else if (x2) {
     if (TX < 8 || TX > x2_txmax(N) || (TX & 3)) return cudaErrorInvalidValue;
     W = kX2W;
     sp.family = rw ? 2 : 1;
@@ -1460,7 +2535,9 @@ cudaError_t make_sweep_plan(SweepPlan& sp, int N, int variant, int TX, int per_s
   sp.gm.W = W;
   sp.gm.nstrip = (g.nx + TX - 1) / TX;
   sp.gm.ns = ns;
-  sp.smem = rw   ? rw_smem_for(N, variant - kNumVariants - kNumX2, g.nbc + 3)
+  sp.smem = ws   ? ws_smem_for(N, variant - kNumVariants - kNumX2 - kNumRW - kNumRL, g.nbc + 3)
+             : rl ? rl_smem_for(N, variant - kNumVariants - kNumX2 - kNumRW, g.nbc + 3)
+             : rw ? rw_smem_for(N, variant - kNumVariants - kNumX2, g.nbc + 3)
              : x2 ? x2_smem_for(N, variant - kNumVariants, g.nbc + 3)
                   : smem_for(N, variant, W, g.nbc + 3);
   const int bps = sweep_blocks_per_sm(sp);
@@ -1525,7 +2602,10 @@ int sweep_tx_candidates(int variant, int N, int nx, int* out, int max_out) {
   int n = 0;
   if (variant >= kNumVariants) {
     // the widest strip, and the narrowest strip with the same strip count
-    const int tmax = x2_txmax(N);
+    const int v = variant - kNumVariants - kNumX2 - kNumRW;
+    const int tmax = v >= kNumRL ? rl_txmax(N, kWSNV[v - kNumRL])
+                     : v >= 0    ? rl_txmax(N, kRLNT[v])
+                                 : x2_txmax(N);
     if (tmax >= 8 && n < max_out) out[n++] = tmax;
     const int ns = (nx + tmax - 1) / tmax;
     const int tbal = (((nx + ns - 1) / ns) + 3) & ~3;
@@ -1577,7 +2657,58 @@ int occ_rw(const SweepPlan& sp) {
   return nb;
 }
 
+template <int N, int NT, int P>
+int occ_rl(const SweepPlan& sp) {
+  int nb = 0;
+  cudaFuncSetAttribute(k_el_sweep_rl<N, NT, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       kMaxDynSmem);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_el_sweep_rl<N, NT, P>, NT, sp.smem) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return nb;
+}
+
+template <int N, int NV, int P, int MINB>
+int occ_ws(const SweepPlan& sp) {
+  int nb = 0;
+  auto kern = k_el_sweep_ws<N, NV, P, MINB>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, 2 * NV, sp.smem) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return nb;
+}
+
 int sweep_blocks_per_sm(const SweepPlan& sp) {
+  if (sp.family == 4) {
+#define FOMO_OCC_WS(V, NN, NV, PP, MB) \
+  case V: return occ_ws<NN, NV, PP, MB>(sp);
+#define FOMO_OCC_WSN(NN)                                                         \
+  case NN:                                                                       \
+    switch (sp.variant - kNumVariants - kNumX2 - kNumRW - kNumRL) {              \
+      FOMO_WS_VARIANTS(FOMO_OCC_WS, NN)                                          \
+    }                                                                            \
+    break;
+    switch (sp.N) { FOMO_OCC_WSN(1) FOMO_OCC_WSN(2) FOMO_OCC_WSN(3) FOMO_OCC_WSN(4) FOMO_OCC_WSN(5) }
+#undef FOMO_OCC_WSN
+#undef FOMO_OCC_WS
+    return 0;
+  }
+  if (sp.family == 3) {
+#define FOMO_OCC_RL(V, NN, NT, PP) \
+  case V: return occ_rl<NN, NT, PP>(sp);
+#define FOMO_OCC_RLN(NN)                                                                        \
+  case NN:                                                                                      \
+    switch (sp.variant - kNumVariants - kNumX2 - kNumRW) { FOMO_RL_VARIANTS(FOMO_OCC_RL, NN) } \
+    break;
+    switch (sp.N) { FOMO_OCC_RLN(1) FOMO_OCC_RLN(2) FOMO_OCC_RLN(3) FOMO_OCC_RLN(4) FOMO_OCC_RLN(5) }
+#undef FOMO_OCC_RLN
+#undef FOMO_OCC_RL
+    return 0;
+  }
   if (sp.family == 2) {
 #define FOMO_OCC_RW(V, NN, PP) \
   case V: return occ_rw<NN, PP>(sp);
@@ -1617,6 +2748,26 @@ int sweep_blocks_per_sm(const SweepPlan& sp) {
 cudaError_t launch_sweep_elastic(cudaStream_t st, const SweepPlan& sp, int set, const Coef& c,
                                  float dtx, float dtz, const HabcDev& h, const ElFields& a,
                                  const ElMat& m, const ElOut& o, int* err) {
+  if (sp.family == 4) {
+    switch (sp.N) {
+      case 1: return launch_ws_n<1>(st, sp, set, c, dtx, dtz, h, m, o, err);
+      case 2: return launch_ws_n<2>(st, sp, set, c, dtx, dtz, h, m, o, err);
+      case 3: return launch_ws_n<3>(st, sp, set, c, dtx, dtz, h, m, o, err);
+      case 4: return launch_ws_n<4>(st, sp, set, c, dtx, dtz, h, m, o, err);
+      case 5: return launch_ws_n<5>(st, sp, set, c, dtx, dtz, h, m, o, err);
+    }
+    return cudaErrorInvalidValue;
+  }
+  if (sp.family == 3) {
+    switch (sp.N) {
+      case 1: return launch_rl_n<1>(st, sp, set, c, dtx, dtz, h, m, o, err);
+      case 2: return launch_rl_n<2>(st, sp, set, c, dtx, dtz, h, m, o, err);
+      case 3: return launch_rl_n<3>(st, sp, set, c, dtx, dtz, h, m, o, err);
+      case 4: return launch_rl_n<4>(st, sp, set, c, dtx, dtz, h, m, o, err);
+      case 5: return launch_rl_n<5>(st, sp, set, c, dtx, dtz, h, m, o, err);
+    }
+    return cudaErrorInvalidValue;
+  }
   if (sp.family == 2) {
     switch (sp.N) {
       case 1: return launch_rw_n<1>(st, sp, set, c, dtx, dtz, h, m, o, err);

@@ -19,9 +19,33 @@ struct SweepGeom {
 // Upper bound on the persistent grid (size of the row-range table).
 constexpr int kMaxGrid = 4096;
 
+// Material pack of the lean single sweep: the five elastic planes copied into
+// column-pair-interleaved rows with kPackRowPad zero rows above and below the
+// grid and kPackColPad zero columns to its left (room for every row and column
+// a CTA reads, so the kernel loads without bounds tests).  Element (z, pair p)
+// of each region sits at (z + kPackRowPad) * pitch + p + kPackColPad / 2:
+//   v : float4 {bx(2p), bx(2p+1), bz(2p), bz(2p+1)}
+//   l : float4 {lam(2p), lam(2p+1), l2m(2p), l2m(2p+1)}
+//   mu: float2 {mut(2p), mut(2p+1)}
+constexpr int kPackRowPad = 32;
+constexpr int kPackColPad = 8;
+struct MatPack {
+  const float4* v;
+  const float4* l;
+  const float2* mu;
+  int pitch;  // column pairs per row
+};
+// Pairs per pack row and floats of the whole pack for a padded nx x nz grid.
+int sweep_pack_pitch(int nx);
+size_t sweep_pack_floats(int nx, int nz);
+// Fills the pack at dst (16-byte aligned, sweep_pack_floats floats) from m's
+// planes and records it in m (pack, pack_pitch).
+cudaError_t build_sweep_pack(cudaStream_t st, const Geo2& g, ElMat& m, float* dst);
+
 struct SweepPlan {
   int N = 0, variant = 0;
-  int family = 0;            // 0: column-per-thread, 1: pair-blocked, 2: register-window
+  int family = 0;            // 0: column-per-thread, 1: pair-blocked, 2: register-window,
+                             // 3: lean register-window, 4: warp-specialized
   int P = 0;                 // pair-blocked: prefetch depth (row pairs)
   int per_sm = 1, grid = 1;  // persistent CTAs per SM, grid size
   float frame_weight = 1.0f; // extra cost of a frame cell in the row-range split
