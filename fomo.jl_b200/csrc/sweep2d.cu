@@ -1252,13 +1252,13 @@ __host__ __device__ constexpr int rl_txmax(int N, int NT) {
          ~3;
 }
 
-template <int N, int NT, int P>
+template <int N, int NT, int P, int LV = (N + 2 <= 4 ? 4 : 8)>
 struct RLShape {
   static constexpr int W = rl_w(N, NT);
   static constexpr int TN = x2_tn(N), HV = x2_hv(N);
   static constexpr int NZ = P + 1;                 // z / x stream slots
   static constexpr int NO = P + 2;                 // old-stress / A.v stream slots (and barriers)
-  static constexpr int LVV = N + 2 <= 4 ? 4 : 8;   // v'' ring rows (a power of two >= N + 2)
+  static constexpr int LVV = LV;                   // v'' ring rows (a power of two >= N + 2)
   static constexpr int O_Z = 0;                    // [NZ][txz, tzz][2][W]   rows zv+M, +1
   static constexpr int O_X = O_Z + NZ * 4 * W;     // [NZ][txx, txz][2][W]   rows zv, zv+1
   static constexpr int O_O = O_X + NZ * 4 * W;     // [NO][txx, tzz, txz][2][W] rows q, q+1
@@ -1686,19 +1686,30 @@ __global__ void __launch_bounds__(NT, 256 / NT)
 // earlier by the velocity threads of the same columns.  Same canonical
 // arithmetic, bit-identical results.
 // ===========================================================================
-__device__ __forceinline__ void cta_bar(int nthreads) {
-  asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
+__device__ __forceinline__ void cta_bar(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+// v'' ring depth of the warp-specialized sweep.  With SPLIT the ring is deep
+// enough (>= N + 4 rows) that the rows the stress role reads in stage A never
+// share a slot with the rows the velocity role writes in stage B of the same
+// iteration, so the mid-iteration barrier only has to order each role with
+// itself.
+__host__ __device__ constexpr int ws_lvv(int N, bool split) {
+  return split ? (N + 4 <= 8 ? 8 : 16) : (N + 2 <= 4 ? 4 : 8);
 }
 
-template <int N, int NV, int P, int MINB>
+template <int N, int NV, int P, int MINB, bool SPLIT>
 __global__ void __launch_bounds__(2 * NV, MINB)
     k_el_sweep_ws(const __grid_constant__ CUtensorMap tm_xx, const __grid_constant__ CUtensorMap tm_zz,
                   const __grid_constant__ CUtensorMap tm_xz, const __grid_constant__ CUtensorMap tm_vx,
                   const __grid_constant__ CUtensorMap tm_vz, SweepGeom gm, Coef c, float dtx,
                   float dtz, HabcDev h, MatPack mp, ElOut o, const long long* __restrict__ bounds,
                   int* __restrict__ err) {
-  using S = RLShape<N, NV, P>;
+  using S = RLShape<N, NV, P, ws_lvv(N, SPLIT)>;
   constexpr int NT = 2 * NV;
+  // mid-iteration barrier: per role (ids 2, 3) when SPLIT, else the whole CTA (id 1)
+  const int mid_id = SPLIT ? (threadIdx.x < NV ? 2 : 3) : 1;
+  constexpr int mid_n = SPLIT ? NV : NT;
   constexpr int W = S::W, M = N, TN = S::TN, HV = S::HV;
   constexpr int NZ = S::NZ, NO = S::NO, LVV = S::LVV;
   constexpr int WN = 2 * M + 2;  // window rows
@@ -1798,7 +1809,7 @@ __global__ void __launch_bounds__(2 * NV, MINB)
         tma_load_3d(s_v + (os * 4 + 0) * W, &tm_vx, g.XV, zr, g.shot, bar);
         tma_load_3d(s_v + (os * 4 + 2) * W, &tm_vz, g.XV, zr, g.shot, bar);
       };
-      cta_bar(NT);  // the previous segment's readers are done with every ring
+      cta_bar(1, NT);  // the previous segment's readers are done with every ring
       if (tid == 0 && live) {
         fence_proxy_async();
         for (int k = 0; k <= P && k < g.I; ++k) issue(k);
@@ -1880,7 +1891,7 @@ __global__ void __launch_bounds__(2 * NV, MINB)
             wxz[k][e] = wxz[k + 2][e];
             wzz[k][e] = wzz[k + 2][e];
           }
-        cta_bar(NT);
+        cta_bar(mid_id, mid_n);
         // v'' rows zv-1 (rr = 0) and zv (rr = 1); v' rows zv-2 .. zv+1 are in vpp / vpc
         if (do_v) {
 #pragma unroll
@@ -1894,34 +1905,28 @@ __global__ void __launch_bounds__(2 * NV, MINB)
             const int zsd = zside(qv);
             if (zframe(qv) && (zsd != 0 || g.xband)) {
               const int zd = zdist(qv);
-              const int prow = (2 * i - 1 + rr) & 3;  // v' ring row of qv
-              // A.v rows zv-2, zv-1 sit in the previous pair's slot, zv, zv+1 in this one
-              const int orow = rr ? 0 : 1;
-              const int oslot = rr ? os : osp;
-              const int zslot = zsd > 0 ? os : osp;  // slot of row qv + zsd (row index rr)
+              // row bases (field f at + f * stride): A.v row qv (rows zv-2, zv-1 sit in
+              // the previous pair's slot, zv, zv+1 in this one), A.v row qv + zsd, v' row qv
+              const float* vo_r = s_v + ((rr ? os : osp) * 4 + (rr ? 0 : 1)) * W;
+              const float* vz_r = s_v + ((zsd > 0 ? os : osp) * 4 + rr) * W;
+              const float* vp_r = s_vp + ((2 * i - 1 + rr) & 3) * W;
 #pragma unroll
               for (int e = 0; e < 2; ++e) {
-                if (!g.xfr[e] || (g.xsd[e] == 0 && zsd == 0)) continue;
+                const bool fr = g.xfr[e] && (g.xsd[e] != 0 || zsd != 0);
+                const bool corner = g.xsd[e] != 0 && zsd != 0, xs = g.xsd[e] != 0;
                 const int col = sc + e, coln = g.xcn[e];
                 const int dist = min(g.xds[e], zd);
 #pragma unroll
                 for (int f = 0; f < 2; ++f) {
-                  const float* fo = s_v + (oslot * 4 + 2 * f + orow) * W;
-                  const float fop = fo[col];
                   const float w = wsm(f, dist);
+                  const float fop = vo_r[f * 2 * W + col];
                   const float vz_n = rr ? (zsd > 0 ? vpc[f][1][e] : vpp[f][1][e])
                                         : (zsd > 0 ? vpc[f][0][e] : vpp[f][0][e]);
-                  if (g.xsd[e] != 0 && zsd != 0)
-                    vvn[f][e] = higdon_corner(
-                        w, vvn[f][e], higdon_side(h, s_vp[(4 * f + prow) * W + coln], fop, fo[coln]),
-                        higdon_side(h, vz_n, fop, s_v[(zslot * 4 + 2 * f + rr) * W + col]));
-                  else if (g.xsd[e] != 0)
-                    vvn[f][e] = higdon_edge(
-                        w, vvn[f][e], higdon_side(h, s_vp[(4 * f + prow) * W + coln], fop, fo[coln]));
-                  else
-                    vvn[f][e] = higdon_edge(
-                        w, vvn[f][e],
-                        higdon_side(h, vz_n, fop, s_v[(zslot * 4 + 2 * f + rr) * W + col]));
+                  const float hx = higdon_side(h, vp_r[f * 4 * W + coln], fop, vo_r[f * 2 * W + coln]);
+                  const float hz = higdon_side(h, vz_n, fop, vz_r[f * 2 * W + col]);
+                  const float res = corner ? higdon_corner(w, vvn[f][e], hx, hz)
+                                           : higdon_edge(w, vvn[f][e], xs ? hx : hz);
+                  vvn[f][e] = fr ? res : vvn[f][e];
                 }
               }
             }
@@ -1947,7 +1952,7 @@ __global__ void __launch_bounds__(2 * NV, MINB)
         mv[0] = __ldg(pv);
         mv[1] = __ldg(pv + mp.pitch);
         pv += mrow;
-        cta_bar(NT);
+        cta_bar(1, NT);
         if (tid == 0 && live && i + 1 + P < g.I) {
           fence_proxy_async();
           issue(i + 1 + P);
@@ -1966,7 +1971,7 @@ __global__ void __launch_bounds__(2 * NV, MINB)
     for (long long r = r_lo; r < r_hi;) {
       Seg g;
       segment(r, g);
-      cta_bar(NT);  // pairs with the velocity role's segment barrier
+      cta_bar(1, NT);  // pairs with the velocity role's segment barrier
       float wvx[WN][2], wvz[WN][2];
 #pragma unroll
       for (int k = 0; k < WN; ++k)
@@ -2064,7 +2069,7 @@ __global__ void __launch_bounds__(2 * NV, MINB)
                   make_float2(spc[f][rr][0], spc[f][rr][1]);
           }
         }
-        cta_bar(NT);
+        cta_bar(mid_id, mid_n);
         // s'' rows q-1 (rr = 0) and q (rr = 1); s' rows q-2 .. q+1 are in spp / spc
         if (g.o_any) {
 #pragma unroll
@@ -2079,32 +2084,27 @@ __global__ void __launch_bounds__(2 * NV, MINB)
             const int zsd = zside(qs);
             if (zframe(qs) && (zsd != 0 || g.xband)) {
               const int zd = zdist(qs);
-              const int srow = (2 * i - 1 + rr) & 3;  // s' ring row of qs
-              // old stress rows: q-2, q-1 in the previous pair slot, q, q+1 in this one
-              const int oso = rr ? os : osp, oro = rr ? 0 : 1;  // row qs
-              const int osz = zsd > 0 ? os : osp;              // row qs + zsd (row index rr)
+              // row bases (field f at + f * stride): old stress row qs (rows q-2, q-1 in
+              // the previous pair slot, q, q+1 in this one), row qs + zsd, s' row qs
+              const float* so_r = s_o + ((rr ? os : osp) * 6 + (rr ? 0 : 1)) * W + TN;
+              const float* sz_r = s_o + ((zsd > 0 ? os : osp) * 6 + rr) * W + TN;
+              const float* sp_r = s_sp + ((2 * i - 1 + rr) & 3) * W;
 #pragma unroll
               for (int e = 0; e < 2; ++e) {
-                if (!g.xfr[e] || (g.xsd[e] == 0 && zsd == 0)) continue;
+                const bool fr = g.xfr[e] && (g.xsd[e] != 0 || zsd != 0);
+                const bool corner = g.xsd[e] != 0 && zsd != 0, xs = g.xsd[e] != 0;
                 const int col = sc + e, coln = g.xcn[e];
                 const float w = wsm(2, min(g.xds[e], zd));
 #pragma unroll
                 for (int f = 0; f < 3; ++f) {
-                  const float* fo = s_o + (oso * 6 + 2 * f + oro) * W + TN;
-                  const float fop = fo[col];
+                  const float fop = so_r[f * 2 * W + col];
                   const float sz_n = rr ? (zsd > 0 ? spc[f][1][e] : spp[f][1][e])
                                         : (zsd > 0 ? spc[f][0][e] : spp[f][0][e]);
-                  if (g.xsd[e] != 0 && zsd != 0)
-                    v[f][e] = higdon_corner(
-                        w, v[f][e], higdon_side(h, s_sp[(4 * f + srow) * W + coln], fop, fo[coln]),
-                        higdon_side(h, sz_n, fop, s_o[(osz * 6 + 2 * f + rr) * W + TN + col]));
-                  else if (g.xsd[e] != 0)
-                    v[f][e] = higdon_edge(
-                        w, v[f][e], higdon_side(h, s_sp[(4 * f + srow) * W + coln], fop, fo[coln]));
-                  else
-                    v[f][e] = higdon_edge(
-                        w, v[f][e],
-                        higdon_side(h, sz_n, fop, s_o[(osz * 6 + 2 * f + rr) * W + TN + col]));
+                  const float hx = higdon_side(h, sp_r[f * 4 * W + coln], fop, so_r[f * 2 * W + coln]);
+                  const float hz = higdon_side(h, sz_n, fop, sz_r[f * 2 * W + col]);
+                  const float res = corner ? higdon_corner(w, v[f][e], hx, hz)
+                                           : higdon_edge(w, v[f][e], xs ? hx : hz);
+                  v[f][e] = fr ? res : v[f][e];
                 }
               }
             }
@@ -2129,7 +2129,7 @@ __global__ void __launch_bounds__(2 * NV, MINB)
         mu[1] = __ldg(pu + mp.pitch);
         pl += mrow;
         pu += mrow;
-        cta_bar(NT);
+        cta_bar(1, NT);
         osp = os;
         os = os + 1 == NO ? 0 : os + 1;
         ph ^= os == 0 ? 1u : 0u;
@@ -2188,18 +2188,20 @@ constexpr int kRLP[] = {1, 2, 1, 2};
 constexpr int kNumRL = sizeof(kRLP) / sizeof(kRLP[0]);
 #define FOMO_RL_VARIANTS(X, NN) X(0, NN, 128, 1) X(1, NN, 128, 2) X(2, NN, 64, 1) X(3, NN, 64, 2)
 
-template <int N, int NT, int P>
+template <int N, int NT, int P, int LV = (N + 2 <= 4 ? 4 : 8)>
 size_t rl_smem_bytes(int wstride) {
-  using S = RLShape<N, NT, P>;
+  using S = RLShape<N, NT, P, LV>;
   return (size_t)(S::O_WT + ((3 * wstride + 31) & ~31)) * 4 + sizeof(uint64_t) * S::NO;
 }
 
 // warp-specialized variants: (threads per role, prefetch depth, CTAs per SM)
+// (threads per role, prefetch depth, CTAs per SM, role-local mid-iteration barrier)
 constexpr int kWSNV[] = {128, 64, 64, 128};
-constexpr int kWSP[] = {1, 1, 1, 2};
+constexpr int kWSP[] = {1, 1, 1, 1};
 constexpr int kNumWS = sizeof(kWSP) / sizeof(kWSP[0]);
 #define FOMO_WS_VARIANTS(X, NN) \
-  X(0, NN, 128, 1, 2) X(1, NN, 64, 1, 4) X(2, NN, 64, 1, 3) X(3, NN, 128, 2, 2)
+  X(0, NN, 128, 1, 2, true) X(1, NN, 64, 1, 4, false) X(2, NN, 64, 1, 3, true) \
+  X(3, NN, 128, 1, 2, false)
 
 template <int N, int P>
 size_t rw_smem_bytes(int wstride) {
@@ -2335,10 +2337,10 @@ cudaError_t launch_rl_n(cudaStream_t st, const SweepPlan& sp, int set, const Coe
   return cudaErrorInvalidValue;
 }
 
-template <int N, int NV, int P, int MINB>
+template <int N, int NV, int P, int MINB, bool SPLIT>
 cudaError_t launch_ws(cudaStream_t st, const SweepPlan& sp, int set, const Coef& c, float dtx,
                       float dtz, const HabcDev& h, const ElMat& m, const ElOut& o, int* err) {
-  auto kern = k_el_sweep_ws<N, NV, P, MINB>;
+  auto kern = k_el_sweep_ws<N, NV, P, MINB, SPLIT>;
   static std::atomic<int> attr_set{0};
   if (!attr_set.load(std::memory_order_acquire)) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2360,8 +2362,8 @@ cudaError_t launch_ws(cudaStream_t st, const SweepPlan& sp, int set, const Coef&
 template <int N>
 cudaError_t launch_ws_n(cudaStream_t st, const SweepPlan& sp, int set, const Coef& c, float dtx,
                         float dtz, const HabcDev& h, const ElMat& m, const ElOut& o, int* err) {
-#define FOMO_LAUNCH_WS(V, NN, NV, PP, MB) \
-  case V: return launch_ws<NN, NV, PP, MB>(st, sp, set, c, dtx, dtz, h, m, o, err);
+#define FOMO_LAUNCH_WS(V, NN, NV, PP, MB, SP) \
+  case V: return launch_ws<NN, NV, PP, MB, SP>(st, sp, set, c, dtx, dtz, h, m, o, err);
   switch (sp.variant - kNumVariants - kNumX2 - kNumRW - kNumRL) {
     FOMO_WS_VARIANTS(FOMO_LAUNCH_WS, N)
   }
@@ -2370,8 +2372,8 @@ cudaError_t launch_ws_n(cudaStream_t st, const SweepPlan& sp, int set, const Coe
 }
 
 size_t ws_smem_for(int N, int v, int wstride) {
-#define FOMO_SMEM_WS(V, NN, NV, PP, MB) \
-  case V: return rl_smem_bytes<NN, NV, PP>(wstride);
+#define FOMO_SMEM_WS(V, NN, NV, PP, MB, SP) \
+  case V: return rl_smem_bytes<NN, NV, PP, ws_lvv(NN, SP)>(wstride);
 #define FOMO_SMEM_WSN(NN)                              \
   case NN:                                             \
     switch (v) { FOMO_WS_VARIANTS(FOMO_SMEM_WS, NN) }  \
@@ -2670,10 +2672,10 @@ int occ_rl(const SweepPlan& sp) {
   return nb;
 }
 
-template <int N, int NV, int P, int MINB>
+template <int N, int NV, int P, int MINB, bool SPLIT>
 int occ_ws(const SweepPlan& sp) {
   int nb = 0;
-  auto kern = k_el_sweep_ws<N, NV, P, MINB>;
+  auto kern = k_el_sweep_ws<N, NV, P, MINB, SPLIT>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, 2 * NV, sp.smem) != cudaSuccess) {
     cudaGetLastError();
@@ -2684,8 +2686,8 @@ int occ_ws(const SweepPlan& sp) {
 
 int sweep_blocks_per_sm(const SweepPlan& sp) {
   if (sp.family == 4) {
-#define FOMO_OCC_WS(V, NN, NV, PP, MB) \
-  case V: return occ_ws<NN, NV, PP, MB>(sp);
+#define FOMO_OCC_WS(V, NN, NV, PP, MB, SP) \
+  case V: return occ_ws<NN, NV, PP, MB, SP>(sp);
 #define FOMO_OCC_WSN(NN)                                                         \
   case NN:                                                                       \
     switch (sp.variant - kNumVariants - kNumX2 - kNumRW - kNumRL) {              \
