@@ -1757,6 +1757,7 @@ __global__ void __launch_bounds__(2 * NV, MINB)
   struct Seg {
     int za, zb, shot, XV, XT, xc, zv0, I;
     bool xin[2], xfr[2], xband, o_any, o_pair;
+    bool xedge[2];  // frame cell of a left/right band (on rows outside the z bands)
     int xsd[2], xds[2], xcn[2];
     long long obase;
   };
@@ -1779,7 +1780,9 @@ __global__ void __launch_bounds__(2 * NV, MINB)
       g.xds[e] = min(x, nx - 1 - x);
       g.xcn[e] = min(max(sc + e + g.xsd[e], 0), W - 1);
     }
-    g.xband = (g.xfr[0] && g.xsd[0] != 0) || (g.xfr[1] && g.xsd[1] != 0);
+    g.xedge[0] = g.xfr[0] && g.xsd[0] != 0;
+    g.xedge[1] = g.xfr[1] && g.xsd[1] != 0;
+    g.xband = g.xedge[0] || g.xedge[1];
     g.o_any = do_o && g.xc < nx;
     g.o_pair = g.xc + 1 < nx;
     g.obase = (long long)g.shot * gm.plane + g.xc;
@@ -1819,6 +1822,15 @@ __global__ void __launch_bounds__(2 * NV, MINB)
       for (int k = 0; k < WN; ++k)
 #pragma unroll
         for (int e = 0; e < 2; ++e) wxz[k][e] = wzz[k][e] = 0.0f;
+      // HABC weights of the x-band cells on rows outside the z bands (dist = xds there)
+      float wxb[2][2];
+#pragma unroll
+      for (int f = 0; f < 2; ++f)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) wxb[f][e] = wsm(f, g.xds[e]);
+      // output rows zv-1 (iteration 0) onwards, advanced two rows per iteration
+      float* ovx = o.vx + g.obase + (long long)(g.zv0 - 1) * gm.ld;
+      float* ovz = o.vz + g.obase + (long long)(g.zv0 - 1) * gm.ld;
       float vpp[2][2][2];  // previous iteration's v' rows [field][row][cell]
 #pragma unroll
       for (int f = 0; f < 2; ++f)
@@ -1903,7 +1915,44 @@ __global__ void __launch_bounds__(2 * NV, MINB)
 #pragma unroll
               for (int e = 0; e < 2; ++e) vvn[f][e] = rr ? vpc[f][0][e] : vpp[f][1][e];
             const int zsd = zside(qv);
-            if (zframe(qv) && (zsd != 0 || g.xband)) {
+            const bool zfr = zframe(qv);
+            if (zfr && zsd != 0 && !g.xband) {
+              // z band, no x band on this thread: z-side edge on its frame cells
+              const int zd = zdist(qv);
+              const float* vo_r = s_v + ((rr ? os : osp) * 4 + (rr ? 0 : 1)) * W + sc;
+              const float* vz_r = s_v + ((zsd > 0 ? os : osp) * 4 + rr) * W + sc;
+#pragma unroll
+              for (int f = 0; f < 2; ++f) {
+                const float w = wsm(f, zd);
+                const float2 fo = *reinterpret_cast<const float2*>(vo_r + f * 2 * W);
+                const float2 fz = *reinterpret_cast<const float2*>(vz_r + f * 2 * W);
+                const float fo_[2] = {fo.x, fo.y}, fz_[2] = {fz.x, fz.y};
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                  const float vz_n = rr ? (zsd > 0 ? vpc[f][1][e] : vpp[f][1][e])
+                                        : (zsd > 0 ? vpc[f][0][e] : vpp[f][0][e]);
+                  const float res = higdon_edge(w, vvn[f][e], higdon_side(h, vz_n, fo_[e], fz_[e]));
+                  vvn[f][e] = g.xfr[e] ? res : vvn[f][e];
+                }
+              }
+            } else if (zfr && zsd == 0 && g.xband) {
+              // x band outside the z bands: x-side edge on the band cells
+              const float* vo_r = s_v + ((rr ? os : osp) * 4 + (rr ? 0 : 1)) * W;
+              const float* vp_r = s_vp + ((2 * i - 1 + rr) & 3) * W;
+#pragma unroll
+              for (int e = 0; e < 2; ++e) {
+                const int col = sc + e, coln = g.xcn[e];
+#pragma unroll
+                for (int f = 0; f < 2; ++f) {
+                  const float fop = vo_r[f * 2 * W + col];
+                  const float res = higdon_edge(
+                      wxb[f][e], vvn[f][e],
+                      higdon_side(h, vp_r[f * 4 * W + coln], fop, vo_r[f * 2 * W + coln]));
+                  vvn[f][e] = g.xedge[e] ? res : vvn[f][e];
+                }
+              }
+            } else if (zfr && zsd != 0) {
+              // z band and x band: corners, edges of both kinds
               const int zd = zdist(qv);
               // row bases (field f at + f * stride): A.v row qv (rows zv-2, zv-1 sit in
               // the previous pair's slot, zv, zv+1 in this one), A.v row qv + zsd, v' row qv
@@ -1912,8 +1961,8 @@ __global__ void __launch_bounds__(2 * NV, MINB)
               const float* vp_r = s_vp + ((2 * i - 1 + rr) & 3) * W;
 #pragma unroll
               for (int e = 0; e < 2; ++e) {
-                const bool fr = g.xfr[e] && (g.xsd[e] != 0 || zsd != 0);
-                const bool corner = g.xsd[e] != 0 && zsd != 0, xs = g.xsd[e] != 0;
+                const bool fr = g.xfr[e];
+                const bool corner = g.xsd[e] != 0, xs = g.xsd[e] != 0;
                 const int col = sc + e, coln = g.xcn[e];
                 const int dist = min(g.xds[e], zd);
 #pragma unroll
@@ -1934,17 +1983,20 @@ __global__ void __launch_bounds__(2 * NV, MINB)
             *reinterpret_cast<float2*>(s_vv + vw * W + sc) = make_float2(vvn[0][0], vvn[0][1]);
             *reinterpret_cast<float2*>(s_vv + (LVV + vw) * W + sc) = make_float2(vvn[1][0], vvn[1][1]);
             if (g.o_any && qv >= g.za && qv < g.zb) {
-              const long long p = g.obase + (long long)qv * gm.ld;
+              float* px = rr ? ovx + gm.ld : ovx;
+              float* pz = rr ? ovz + gm.ld : ovz;
               if (g.o_pair) {
-                *reinterpret_cast<float2*>(o.vx + p) = make_float2(vvn[0][0], vvn[0][1]);
-                *reinterpret_cast<float2*>(o.vz + p) = make_float2(vvn[1][0], vvn[1][1]);
+                *reinterpret_cast<float2*>(px) = make_float2(vvn[0][0], vvn[0][1]);
+                *reinterpret_cast<float2*>(pz) = make_float2(vvn[1][0], vvn[1][1]);
               } else {
-                o.vx[p] = vvn[0][0];
-                o.vz[p] = vvn[1][0];
+                *px = vvn[0][0];
+                *pz = vvn[1][0];
               }
             }
           }
         }
+        ovx += 2 * gm.ld;
+        ovz += 2 * gm.ld;
 #pragma unroll
         for (int f = 0; f < 2; ++f)
 #pragma unroll
@@ -1977,6 +2029,14 @@ __global__ void __launch_bounds__(2 * NV, MINB)
       for (int k = 0; k < WN; ++k)
 #pragma unroll
         for (int e = 0; e < 2; ++e) wvx[k][e] = wvz[k][e] = 0.0f;
+      float wxb[2];  // HABC weights of the x-band cells outside the z bands
+#pragma unroll
+      for (int e = 0; e < 2; ++e) wxb[e] = wsm(2, g.xds[e]);
+      // output rows q-1 (iteration 0) onwards, advanced two rows per iteration
+      float* ot[3];
+      ot[0] = o.txx + g.obase + (long long)(g.zv0 - 4 - M) * gm.ld;
+      ot[1] = o.tzz + g.obase + (long long)(g.zv0 - 4 - M) * gm.ld;
+      ot[2] = o.txz + g.obase + (long long)(g.zv0 - 4 - M) * gm.ld;
       float spp[3][2][2];  // previous iteration's s' rows [field][row][cell]
 #pragma unroll
       for (int f = 0; f < 3; ++f)
@@ -2082,7 +2142,43 @@ __global__ void __launch_bounds__(2 * NV, MINB)
 #pragma unroll
               for (int e = 0; e < 2; ++e) v[f][e] = rr ? spc[f][0][e] : spp[f][1][e];
             const int zsd = zside(qs);
-            if (zframe(qs) && (zsd != 0 || g.xband)) {
+            const bool zfr = zframe(qs);
+            if (zfr && zsd != 0 && !g.xband) {
+              // z band, no x band on this thread: z-side edge on its frame cells
+              const float w = wsm(2, zdist(qs));
+              const float* so_r = s_o + ((rr ? os : osp) * 6 + (rr ? 0 : 1)) * W + TN + sc;
+              const float* sz_r = s_o + ((zsd > 0 ? os : osp) * 6 + rr) * W + TN + sc;
+#pragma unroll
+              for (int f = 0; f < 3; ++f) {
+                const float2 fo = *reinterpret_cast<const float2*>(so_r + f * 2 * W);
+                const float2 fz = *reinterpret_cast<const float2*>(sz_r + f * 2 * W);
+                const float fo_[2] = {fo.x, fo.y}, fz_[2] = {fz.x, fz.y};
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                  const float sz_n = rr ? (zsd > 0 ? spc[f][1][e] : spp[f][1][e])
+                                        : (zsd > 0 ? spc[f][0][e] : spp[f][0][e]);
+                  const float res = higdon_edge(w, v[f][e], higdon_side(h, sz_n, fo_[e], fz_[e]));
+                  v[f][e] = g.xfr[e] ? res : v[f][e];
+                }
+              }
+            } else if (zfr && zsd == 0 && g.xband) {
+              // x band outside the z bands: x-side edge on the band cells
+              const float* so_r = s_o + ((rr ? os : osp) * 6 + (rr ? 0 : 1)) * W + TN;
+              const float* sp_r = s_sp + ((2 * i - 1 + rr) & 3) * W;
+#pragma unroll
+              for (int e = 0; e < 2; ++e) {
+                const int col = sc + e, coln = g.xcn[e];
+#pragma unroll
+                for (int f = 0; f < 3; ++f) {
+                  const float fop = so_r[f * 2 * W + col];
+                  const float res = higdon_edge(
+                      wxb[e], v[f][e],
+                      higdon_side(h, sp_r[f * 4 * W + coln], fop, so_r[f * 2 * W + coln]));
+                  v[f][e] = g.xedge[e] ? res : v[f][e];
+                }
+              }
+            } else if (zfr && zsd != 0) {
+              // z band and x band: corners, edges of both kinds
               const int zd = zdist(qs);
               // row bases (field f at + f * stride): old stress row qs (rows q-2, q-1 in
               // the previous pair slot, q, q+1 in this one), row qs + zsd, s' row qs
@@ -2091,8 +2187,8 @@ __global__ void __launch_bounds__(2 * NV, MINB)
               const float* sp_r = s_sp + ((2 * i - 1 + rr) & 3) * W;
 #pragma unroll
               for (int e = 0; e < 2; ++e) {
-                const bool fr = g.xfr[e] && (g.xsd[e] != 0 || zsd != 0);
-                const bool corner = g.xsd[e] != 0 && zsd != 0, xs = g.xsd[e] != 0;
+                const bool fr = g.xfr[e];
+                const bool corner = g.xsd[e] != 0, xs = g.xsd[e] != 0;
                 const int col = sc + e, coln = g.xcn[e];
                 const float w = wsm(2, min(g.xds[e], zd));
 #pragma unroll
@@ -2108,17 +2204,18 @@ __global__ void __launch_bounds__(2 * NV, MINB)
                 }
               }
             }
-            const long long p = g.obase + (long long)qs * gm.ld;
-            float* out[3] = {o.txx, o.tzz, o.txz};
 #pragma unroll
             for (int f = 0; f < 3; ++f) {
+              float* pt = rr ? ot[f] + gm.ld : ot[f];
               if (g.o_pair)
-                *reinterpret_cast<float2*>(out[f] + p) = make_float2(v[f][0], v[f][1]);
+                *reinterpret_cast<float2*>(pt) = make_float2(v[f][0], v[f][1]);
               else
-                out[f][p] = v[f][0];
+                *pt = v[f][0];
             }
           }
         }
+#pragma unroll
+        for (int f = 0; f < 3; ++f) ot[f] += 2 * gm.ld;
 #pragma unroll
         for (int f = 0; f < 3; ++f)
 #pragma unroll
@@ -2196,12 +2293,12 @@ size_t rl_smem_bytes(int wstride) {
 
 // warp-specialized variants: (threads per role, prefetch depth, CTAs per SM)
 // (threads per role, prefetch depth, CTAs per SM, role-local mid-iteration barrier)
-constexpr int kWSNV[] = {128, 64, 64, 128};
-constexpr int kWSP[] = {1, 1, 1, 1};
+constexpr int kWSNV[] = {128, 64, 64, 64};
+constexpr int kWSP[] = {1, 1, 1, 2};
 constexpr int kNumWS = sizeof(kWSP) / sizeof(kWSP[0]);
 #define FOMO_WS_VARIANTS(X, NN) \
   X(0, NN, 128, 1, 2, true) X(1, NN, 64, 1, 4, false) X(2, NN, 64, 1, 3, true) \
-  X(3, NN, 128, 1, 2, false)
+  X(3, NN, 64, 2, 3, true)
 
 template <int N, int P>
 size_t rw_smem_bytes(int wstride) {
@@ -2551,8 +2648,12 @@ cudaError_t make_sweep_plan(SweepPlan& sp, int N, int variant, int TX, int per_s
   const long long rows = (long long)sp.gm.nstrip * ns * g.nz;
   sp.grid = (int)std::max(1LL, std::min({(long long)sp.per_sm * nsm, rows, (long long)kMaxGrid}));
   sp.frame_weight = frame_weight;
-  // Cost-balanced split of the flattened (strip, shot, row) space: a row of a
-  // strip costs 1 + frame_weight * (fraction of its cells in the HABC frame).
+  // Cost-balanced split of the flattened (strip, shot, row) space.  A row of a
+  // strip costs 1 + frame_weight * (fraction of its cells in the HABC frame),
+  // and every z-segment a CTA starts (its first row, and each new (shot, strip)
+  // item inside its range) costs the warm-up rows that fill the register
+  // windows.  The smallest per-CTA budget whose greedy split needs at most
+  // `grid` CTAs is found by bisection.
   {
     std::vector<double> strip_frac(sp.gm.nstrip);
     for (int k = 0; k < sp.gm.nstrip; ++k) {
@@ -2561,23 +2662,64 @@ cudaError_t make_sweep_plan(SweepPlan& sp, int N, int variant, int TX, int per_s
         nf += (x >= 1 && x <= g.nx - 2 && (x <= g.nbc || x >= g.nx - 1 - g.nbc)) ? 1 : 0;
       strip_frac[k] = (double)nf / TX;
     }
-    auto row_cost = [&](int strip, int z) {
-      const bool band = z >= 1 && z <= g.nz - 2 && (z <= g.nbc || z >= g.nz - 1 - g.nbc);
-      return 1.0 + frame_weight * (band ? 1.0 : strip_frac[strip]);
-    };
-    double shot_cost = 0.0;
+    // cost of each row of each strip, and the prefix sums along z
+    std::vector<double> pre((size_t)sp.gm.nstrip * (g.nz + 1), 0.0);
     for (int k = 0; k < sp.gm.nstrip; ++k)
-      for (int z = 0; z < g.nz; ++z) shot_cost += row_cost(k, z);
-    const double total = shot_cost * ns;
-    std::vector<long long> b(sp.grid + 1, rows);
-    b[0] = 0;
-    double acc = 0.0;
-    int next = 1;
-    for (long long r = 0; r < rows && next < sp.grid; ++r) {
-      const long long item = r / g.nz;
-      acc += row_cost((int)(item % sp.gm.nstrip), (int)(r - item * g.nz));
-      while (next < sp.grid && acc >= total * next / sp.grid) b[next++] = r + 1;
+      for (int z = 0; z < g.nz; ++z) {
+        const bool band = z >= 1 && z <= g.nz - 2 && (z <= g.nbc || z >= g.nz - 1 - g.nbc);
+        const double c = 1.0 + frame_weight * (band ? 1.0 : strip_frac[k]);
+        pre[(size_t)k * (g.nz + 1) + z + 1] = pre[(size_t)k * (g.nz + 1) + z] + c;
+      }
+    const double warm = x2 ? 4.0 * N + 7.0 : 2.0 * N + 2.0;
+    auto cost = [&](long long r0, long long r1) {  // rows [r0, r1) of one item
+      const long long item = r0 / g.nz;
+      const int k = (int)(item % sp.gm.nstrip);
+      const double* pk = pre.data() + (size_t)k * (g.nz + 1);
+      return pk[r1 - item * g.nz] - pk[r0 - item * g.nz];
+    };
+    // greedy split under budget B; fills b when given, returns the CTAs used
+    auto split = [&](double B, std::vector<long long>* b) {
+      long long r = 0;
+      int used = 0;
+      while (r < rows) {
+        if (b && used < (int)b->size() - 1) (*b)[used] = r;
+        ++used;
+        double acc = 0.0;
+        bool first = true;
+        while (r < rows) {
+          const long long item_end = (r / g.nz + 1) * g.nz;
+          const double seg = warm + cost(r, item_end);
+          if (acc + seg <= B) {  // the rest of this item fits
+            acc += seg;
+            r = item_end;
+            first = false;
+            continue;
+          }
+          // take as many rows of this item as fit (at least one for a fresh CTA)
+          long long lo = r, hi = item_end;  // largest e in (r, item_end] with warm + cost <= B - acc
+          while (hi - lo > 1) {
+            const long long mid = (lo + hi) / 2;
+            if (acc + warm + cost(r, mid) <= B) lo = mid;
+            else hi = mid;
+          }
+          if (lo == r && first) lo = r + 1;
+          r = lo;
+          break;
+        }
+      }
+      return used;
+    };
+    double total = 0.0;
+    for (long long it = 0; it < rows / g.nz; ++it) total += warm + cost(it * g.nz, (it + 1) * g.nz);
+    double lo = total / sp.grid, hi = total + warm;
+    for (int k = 0; k < 40 && hi - lo > 1e-3 * lo; ++k) {
+      const double mid = 0.5 * (lo + hi);
+      if (split(mid, nullptr) <= sp.grid) hi = mid;
+      else lo = mid;
     }
+    std::vector<long long> b(sp.grid + 1, rows);
+    split(hi, &b);
+    b[sp.grid] = rows;
     cudaError_t e = cudaMemcpyAsync(d_bounds, b.data(), sizeof(long long) * b.size(),
                                     cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return e;

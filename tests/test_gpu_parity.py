@@ -19,8 +19,8 @@ SWEEP_CONFIGS = ["0,112,3", "1,144,1", "2,80,2", "2,20,4", "3,112,2", "0,64,1",
                  "4,224,1", "5,100,1", "6,40,1", "5,8,1",
                  "7,224,2", "8,196,2", "8,40,2", "7,8,1",
                  "9,224,2", "10,176,2", "11,112,4", "12,100,4", "11,8,1", "9,40,1",
-                 "12,60,3", "13,224,2", "14,112,4", "15,100,3", "16,176,2", "14,8,1",
-                 "13,40,1"]  # variant,TX,CTAs per SM
+                 "12,60,3", "13,224,2", "14,112,4", "15,100,3", "16,112,3", "14,8,1",
+                 "13,40,1", "16,20,2"]  # variant,TX,CTAs per SM
 
 
 @pytest.fixture
