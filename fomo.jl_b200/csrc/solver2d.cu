@@ -147,7 +147,7 @@ int tune_sweep(fomo_ctx* ctx, cudaStream_t st, SweepPlan& sp, int N, const Geo2&
   // FOMO_SWEEP_CONFIG="variant,TX,ctas_per_sm" pins the configuration (tests, sweeps)
   if (const char* env = std::getenv("FOMO_SWEEP_CONFIG")) {
     int v = 0, tx = 0, per_sm = 0;
-    float fw = 1.0f;
+    float fw = kFrameWeight;
     const int nr = std::sscanf(env, "%d,%d,%d,%f", &v, &tx, &per_sm, &fw);
     if (nr >= 3 && v >= 0 && v < sweep_num_variants() && per_sm >= 1) {
       FOMO_CU(ctx, make_sweep_plan(sp, N, v, tx, per_sm, g, ns, sets, fw, d_bounds, st));
@@ -170,7 +170,7 @@ int tune_sweep(fomo_ctx* ctx, cudaStream_t st, SweepPlan& sp, int N, const Geo2&
   FOMO_CU(ctx, cudaEventCreate(&e0));
   FOMO_CU(ctx, cudaEventCreate(&e1));
   float best = 1e30f;
-  TuneVal bv{-1, 0, 0, 1.0f};
+  TuneVal bv{-1, 0, 0, kFrameWeight};
   auto time_plan = [&](const SweepPlan& cand, float& ms) -> int {
     FOMO_CU(ctx, launch_sweep_elastic(st, cand, 0, c, dtx, dtz, h, a, m, o, ctx->d_flag));
     FOMO_CU(ctx, cudaEventRecord(e0, st));
@@ -186,25 +186,26 @@ int tune_sweep(fomo_ctx* ctx, cudaStream_t st, SweepPlan& sp, int N, const Geo2&
     int ntx = sweep_tx_candidates(v, N, g.nx, txs, 4);
     for (int k = 0; k < ntx; ++k) {
       SweepPlan cand;
-      if (make_sweep_plan(cand, N, v, txs[k], 64, g, ns, sets, 1.0f, d_bounds, st) != cudaSuccess)
+      if (make_sweep_plan(cand, N, v, txs[k], 64, g, ns, sets, kFrameWeight, d_bounds, st) !=
+          cudaSuccess)
         continue;
       const int full = cand.per_sm;  // all resident CTAs; also try one fewer
       for (int per_sm = full; per_sm >= 1 && per_sm >= full - 1; --per_sm) {
-        if (make_sweep_plan(cand, N, v, txs[k], per_sm, g, ns, sets, 1.0f, d_bounds, st) !=
-            cudaSuccess)
+        if (make_sweep_plan(cand, N, v, txs[k], per_sm, g, ns, sets, kFrameWeight, d_bounds,
+                            st) != cudaSuccess)
           continue;
         float ms = 0.0f;
         if (int rc = time_plan(cand, ms)) return rc;
         if (ms < best) {
           best = ms;
-          bv = TuneVal{v, txs[k], per_sm, 1.0f};
+          bv = TuneVal{v, txs[k], per_sm, kFrameWeight};
         }
       }
     }
   }
   // then the cost weight of frame cells for the row-range split
   if (bv.variant >= 0)
-    for (float fw : {0.0f, 0.5f, 2.0f, 3.0f}) {
+    for (float fw : {0.0f, 0.07f, 0.3f, 0.6f, 1.2f}) {
       SweepPlan cand;
       if (make_sweep_plan(cand, N, bv.variant, bv.TX, bv.per_sm, g, ns, sets, fw, d_bounds, st) !=
           cudaSuccess)

@@ -2648,11 +2648,14 @@ cudaError_t make_sweep_plan(SweepPlan& sp, int N, int variant, int TX, int per_s
   const long long rows = (long long)sp.gm.nstrip * ns * g.nz;
   sp.grid = (int)std::max(1LL, std::min({(long long)sp.per_sm * nsm, rows, (long long)kMaxGrid}));
   sp.frame_weight = frame_weight;
-  // Cost-balanced split of the flattened (strip, shot, row) space.  A row of a
-  // strip costs 1 + frame_weight * (fraction of its cells in the HABC frame),
-  // and every z-segment a CTA starts (its first row, and each new (shot, strip)
-  // item inside its range) costs the warm-up rows that fill the register
-  // windows.  The smallest per-CTA budget whose greedy split needs at most
+  // Cost-balanced split of the flattened (strip, shot, row) space.  A row costs
+  // 1 + frame_weight * (b + s + b * s), b = 1 on a z-band row, s = 1 in a strip
+  // that holds x-band columns (every warp of such a strip takes the Higdon
+  // path); every z-segment a CTA starts (its first row, and each new (shot,
+  // strip) item inside its range) costs the warm-up rows that fill the
+  // register windows.  (Fitted to per-CTA timings of the warp-specialized
+  // sweep at order 10: 1.13 / 1.20 / 1.52 for b, s, both, and 31 rows per
+  // segment.)  The smallest per-CTA budget whose greedy split needs at most
   // `grid` CTAs is found by bisection.
   {
     std::vector<double> strip_frac(sp.gm.nstrip);
@@ -2667,10 +2670,11 @@ cudaError_t make_sweep_plan(SweepPlan& sp, int N, int variant, int TX, int per_s
     for (int k = 0; k < sp.gm.nstrip; ++k)
       for (int z = 0; z < g.nz; ++z) {
         const bool band = z >= 1 && z <= g.nz - 2 && (z <= g.nbc || z >= g.nz - 1 - g.nbc);
-        const double c = 1.0 + frame_weight * (band ? 1.0 : strip_frac[k]);
+        const double xs = strip_frac[k] > 0.0 ? 1.0 : 0.0, zb = band ? 1.0 : 0.0;
+        const double c = 1.0 + frame_weight * (zb + xs + zb * xs);
         pre[(size_t)k * (g.nz + 1) + z + 1] = pre[(size_t)k * (g.nz + 1) + z] + c;
       }
-    const double warm = x2 ? 4.0 * N + 7.0 : 2.0 * N + 2.0;
+    const double warm = x2 ? 4.0 * N + 11.0 : 2.0 * N + 2.0;
     auto cost = [&](long long r0, long long r1) {  // rows [r0, r1) of one item
       const long long item = r0 / g.nz;
       const int k = (int)(item % sp.gm.nstrip);

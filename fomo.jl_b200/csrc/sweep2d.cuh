@@ -18,6 +18,9 @@ struct SweepGeom {
 
 // Upper bound on the persistent grid (size of the row-range table).
 constexpr int kMaxGrid = 4096;
+// Default extra cost of a frame row in the row-range split (the autotuner
+// searches around it).
+constexpr float kFrameWeight = 0.15f;
 
 // Material pack of the lean single sweep: the five elastic planes copied into
 // column-pair-interleaved rows with kPackRowPad zero rows above and below the
