@@ -1863,29 +1863,34 @@ __global__ void __launch_bounds__(2 * NV, MINB)
 #pragma unroll
           for (int rr = 0; rr < 2; ++rr) {
             const bool zin = zinner(zv + rr);
-            float xw[4 * ((N + 1) / 2) + 2];
-            float dxx[2], dxzx[2];
-            load_xwin<N>(s_x + (zs * 4 + rr) * W, sc + TN, xw);
-            dxx[0] = xdm<N>(xw, 0, c);
-            dxx[1] = xdm<N>(xw, 1, c);
-            load_xwin<N>(s_x + (zs * 4 + 2 + rr) * W, sc + TN, xw);
-            dxzx[0] = xdp<N>(xw, 0, c);
-            dxzx[1] = xdp<N>(xw, 1, c);
+            constexpr int E = (N + 1) / 2;
+            float xa[4 * E + 2], xb[4 * E + 2];  // txx and txz rows zv + rr around the pair
+            load_xwin<N>(s_x + (zs * 4 + rr) * W, sc + TN, xa);
+            load_xwin<N>(s_x + (zs * 4 + 2 + rr) * W, sc + TN, xb);
             const float2 ox = *reinterpret_cast<const float2*>(s_v + (os * 4 + rr) * W + sc);
             const float2 oz = *reinterpret_cast<const float2*>(s_v + (os * 4 + 2 + rr) * W + sc);
             const float vo[2][2] = {{ox.x, ox.y}, {oz.x, oz.y}};
+            // the eight derivative sums of the row pair, advanced together term by term
+            // (each sum keeps the canonical order l = 1..N)
+            float dxx[2] = {0.0f, 0.0f}, dxzx[2] = {0.0f, 0.0f};
+            float dxzz[2] = {0.0f, 0.0f}, dzz[2] = {0.0f, 0.0f};
+#pragma unroll
+            for (int l = 1; l <= N; ++l) {
+              const float a = c.a[l - 1];
+#pragma unroll
+              for (int e = 0; e < 2; ++e) {
+                dxx[e] = __fmaf_rn(a, __fsub_rn(xa[2 * E + e + l - 1], xa[2 * E + e - l]), dxx[e]);
+                dxzx[e] = __fmaf_rn(a, __fsub_rn(xb[2 * E + e + l], xb[2 * E + e - l + 1]), dxzx[e]);
+                dxzz[e] = __fmaf_rn(a, __fsub_rn(wxz[rr + M + l - 1][e], wxz[rr + M - l][e]), dxzz[e]);
+                dzz[e] = __fmaf_rn(a, __fsub_rn(wzz[rr + M + l][e], wzz[rr + M - l + 1][e]), dzz[e]);
+              }
+            }
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
-              float dxzz = 0.0f, dzz = 0.0f;
-#pragma unroll
-              for (int l = 1; l <= N; ++l) {
-                dxzz = __fmaf_rn(c.a[l - 1], __fsub_rn(wxz[rr + M + l - 1][e], wxz[rr + M - l][e]), dxzz);
-                dzz = __fmaf_rn(c.a[l - 1], __fsub_rn(wzz[rr + M + l][e], wzz[rr + M - l + 1][e]), dzz);
-              }
               float ux = vo[0][e], uz = vo[1][e];
               if (zin && g.xin[e]) {
-                ux = __fmaf_rn(bxv[rr][e], __fmaf_rn(dtx, dxx[e], __fmul_rn(dtz, dxzz)), ux);
-                uz = __fmaf_rn(bzv[rr][e], __fmaf_rn(dtx, dxzx[e], __fmul_rn(dtz, dzz)), uz);
+                ux = __fmaf_rn(bxv[rr][e], __fmaf_rn(dtx, dxx[e], __fmul_rn(dtz, dxzz[e])), ux);
+                uz = __fmaf_rn(bzv[rr][e], __fmaf_rn(dtx, dxzx[e], __fmul_rn(dtz, dzz[e])), uz);
               }
               vpc[0][rr][e] = ux;
               vpc[1][rr][e] = uz;
@@ -2091,32 +2096,37 @@ __global__ void __launch_bounds__(2 * NV, MINB)
           for (int rr = 0; rr < 2; ++rr) {
             const bool zin = zinner(q + rr);
             const int vb = (2 * i - 2 - M + rr) & (LVV - 1);  // v'' ring row of q + rr
-            float xw[4 * ((N + 1) / 2) + 2];
-            float dvxdx[2], dvzdx[2];
-            load_xwin<N>(s_vv + vb * W, sc, xw);
-            dvxdx[0] = xdp<N>(xw, 0, c);
-            dvxdx[1] = xdp<N>(xw, 1, c);
-            load_xwin<N>(s_vv + (LVV + vb) * W, sc, xw);
-            dvzdx[0] = xdm<N>(xw, 0, c);
-            dvzdx[1] = xdm<N>(xw, 1, c);
+            constexpr int E = (N + 1) / 2;
+            float xa[4 * E + 2], xb[4 * E + 2];  // v''x and v''z rows q + rr around the pair
+            load_xwin<N>(s_vv + vb * W, sc, xa);
+            load_xwin<N>(s_vv + (LVV + vb) * W, sc, xb);
             const float2 oxx = *reinterpret_cast<const float2*>(s_o + (os * 6 + 0 + rr) * W + sc + TN);
             const float2 ozz = *reinterpret_cast<const float2*>(s_o + (os * 6 + 2 + rr) * W + sc + TN);
             const float2 oxz = *reinterpret_cast<const float2*>(s_o + (os * 6 + 4 + rr) * W + sc + TN);
             const float so_[3][2] = {{oxx.x, oxx.y}, {ozz.x, ozz.y}, {oxz.x, oxz.y}};
+            // the eight derivative sums of the row pair, advanced together term by term
+            // (each sum keeps the canonical order l = 1..N)
+            float dvxdx[2] = {0.0f, 0.0f}, dvzdx[2] = {0.0f, 0.0f};
+            float dvxdz[2] = {0.0f, 0.0f}, dvzdz[2] = {0.0f, 0.0f};
+#pragma unroll
+            for (int l = 1; l <= N; ++l) {
+              const float a = c.a[l - 1];
+#pragma unroll
+              for (int e = 0; e < 2; ++e) {
+                dvxdx[e] = __fmaf_rn(a, __fsub_rn(xa[2 * E + e + l], xa[2 * E + e - l + 1]), dvxdx[e]);
+                dvzdx[e] = __fmaf_rn(a, __fsub_rn(xb[2 * E + e + l - 1], xb[2 * E + e - l]), dvzdx[e]);
+                dvxdz[e] = __fmaf_rn(a, __fsub_rn(wvx[rr + M + l][e], wvx[rr + M - l + 1][e]), dvxdz[e]);
+                dvzdz[e] = __fmaf_rn(a, __fsub_rn(wvz[rr + M + l - 1][e], wvz[rr + M - l][e]), dvzdz[e]);
+              }
+            }
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
-              float dvxdz = 0.0f, dvzdz = 0.0f;
-#pragma unroll
-              for (int l = 1; l <= N; ++l) {
-                dvxdz = __fmaf_rn(c.a[l - 1], __fsub_rn(wvx[rr + M + l][e], wvx[rr + M - l + 1][e]), dvxdz);
-                dvzdz = __fmaf_rn(c.a[l - 1], __fsub_rn(wvz[rr + M + l - 1][e], wvz[rr + M - l][e]), dvzdz);
-              }
               float sxx = so_[0][e], szz = so_[1][e], sxz = so_[2][e];
               if (zin && g.xin[e]) {
-                const float ex = __fmul_rn(dvxdx[e], dtx), ez = __fmul_rn(dvzdz, dtz);
+                const float ex = __fmul_rn(dvxdx[e], dtx), ez = __fmul_rn(dvzdz[e], dtz);
                 sxx = __fadd_rn(sxx, __fmaf_rn(l2v[rr][e], ex, __fmul_rn(lav[rr][e], ez)));
                 szz = __fadd_rn(szz, __fmaf_rn(lav[rr][e], ex, __fmul_rn(l2v[rr][e], ez)));
-                sxz = __fmaf_rn(muv[rr][e], __fmaf_rn(dvxdz, dtz, __fmul_rn(dvzdx[e], dtx)), sxz);
+                sxz = __fmaf_rn(muv[rr][e], __fmaf_rn(dvxdz[e], dtz, __fmul_rn(dvzdx[e], dtx)), sxz);
               }
               spc[0][rr][e] = sxx;
               spc[1][rr][e] = szz;
