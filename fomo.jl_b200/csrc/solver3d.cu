@@ -18,14 +18,17 @@
 
 namespace fomo {
 
-// Injection then recording, one block per shot (2D and 3D; linear indices).
+// Injection and recording of one 3D step (linear indices).  The injected
+// fields (p, or txx/tyy/tzz) are never the recorded ones (vx, vy, vz), so the
+// recording needs no ordering after the injection and runs over all blocks;
+// block 0 injects.
 __global__ void k_inject_record3(int it, int nt, int n_src, const int* __restrict__ src_lin,
                                  const float* __restrict__ wav, float* inj0, float* inj1,
                                  float* inj2, int n_rec, const int* __restrict__ rec_lin,
                                  const float* rec0, const float* rec1, const float* rec2,
                                  float* __restrict__ s0, float* __restrict__ s1,
                                  float* __restrict__ s2) {
-  if (threadIdx.x == 0) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
     for (int q = 0; q < n_src; ++q) {
       const long long p = src_lin[q];
       const float w = wav[(long long)(it - 1) * n_src + q];
@@ -34,9 +37,8 @@ __global__ void k_inject_record3(int it, int nt, int n_src, const int* __restric
       if (inj2) inj2[p] = __fadd_rn(inj2[p], w);
     }
   }
-  __syncthreads();
   const long long ob = (long long)n_rec * (it - 1);
-  for (int r = threadIdx.x; r < n_rec; r += blockDim.x) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n_rec; r += gridDim.x * blockDim.x) {
     const long long p = rec_lin[r];
     s0[ob + r] = rec0[p];
     s1[ob + r] = rec1[p];
@@ -240,38 +242,6 @@ __device__ __forceinline__ void frame3_xyz(const Geo3& g, const Frame3& fr, long
   }
 }
 
-// kernels_3d.jl:186-240 evaluated from read-only inputs: mean of the active
-// directions' Higdon side terms.
-__device__ __forceinline__ float habc3_value(const Geo3& g, const HabcDev& h, int kind,
-                                             const float* __restrict__ f,
-                                             const float* __restrict__ fo, int x, int y, int z) {
-  const long long q = x + g.sy * y + g.sz * z;
-  const int sx = x <= g.nbc ? 1 : (x >= g.nx - 1 - g.nbc ? -1 : 0);
-  const int sy = y <= g.nbc ? 1 : (y >= g.ny - 1 - g.nbc ? -1 : 0);
-  const int sz = z <= g.nbc ? 1 : (z >= g.nz - 1 - g.nbc ? -1 : 0);
-  const float fop = __ldg(fo + q);
-  float sum = 0.0f;
-  int nd = 0;
-  if (sx) {
-    const long long nb = q + sx;
-    sum = __fadd_rn(sum, higdon_side(h, __ldg(f + nb), fop, __ldg(fo + nb)));
-    ++nd;
-  }
-  if (sy) {
-    const long long nb = q + sy * g.sy;
-    sum = __fadd_rn(sum, higdon_side(h, __ldg(f + nb), fop, __ldg(fo + nb)));
-    ++nd;
-  }
-  if (sz) {
-    const long long nb = q + sz * g.sz;
-    sum = __fadd_rn(sum, higdon_side(h, __ldg(f + nb), fop, __ldg(fo + nb)));
-    ++nd;
-  }
-  const int dist = min(min(min(x, g.nx - 1 - x), min(y, g.ny - 1 - y)), min(z, g.nz - 1 - z));
-  const float w = habc_weight(h, kind, dist);
-  return __fmaf_rn(w, __ldg(f + q), __fdiv_rn(__fmul_rn(__fsub_rn(1.0f, w), sum), (float)nd));
-}
-
 struct FieldSet3 {
   const float* f[6];
   const float* fo[6];
@@ -282,24 +252,69 @@ struct FieldOut3 {
   float* f[6];
 };
 
-__global__ void k_habc3_pass1(Geo3 g, Frame3 fr, HabcDev h, FieldSet3 fs,
-                              float* __restrict__ scr) {
-  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= fr.total) return;
-  int x, y, z;
-  frame3_xyz(g, fr, idx, x, y, z);
-  for (int k = 0; k < fs.n; ++k)
-    scr[k * fr.total + idx] = habc3_value(g, h, fs.kind[k], fs.f[k], fs.fo[k], x, y, z);
-}
-
-__global__ void k_habc3_pass2(Geo3 g, Frame3 fr, int n, FieldOut3 fo,
-                              const float* __restrict__ scr) {
+// Pass 1: the Higdon value of every frame cell of NF fields into scratch --
+// kernels_3d.jl:186-240 evaluated from read-only inputs: the mean of the
+// active directions' side terms, blended with the weight ramp.  The cell's
+// sides, distance and neighbour offsets are shared by its fields.
+template <int NF>
+__global__ void __launch_bounds__(256) k_habc3_pass1(Geo3 g, Frame3 fr, HabcDev h, FieldSet3 fs,
+                                                     float* __restrict__ scr) {
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= fr.total) return;
   int x, y, z;
   frame3_xyz(g, fr, idx, x, y, z);
   const long long q = x + g.sy * y + g.sz * z;
-  for (int k = 0; k < n; ++k) fo.f[k][q] = scr[k * fr.total + idx];
+  const int sx = x <= g.nbc ? 1 : (x >= g.nx - 1 - g.nbc ? -1 : 0);
+  const int sy = y <= g.nbc ? 1 : (y >= g.ny - 1 - g.nbc ? -1 : 0);
+  const int sz = z <= g.nbc ? 1 : (z >= g.nz - 1 - g.nbc ? -1 : 0);
+  const int nd = (sx != 0) + (sy != 0) + (sz != 0);
+  const long long nbx = q + sx, nby = q + sy * g.sy, nbz = q + sz * g.sz;
+  const int dist = min(min(min(x, g.nx - 1 - x), min(y, g.ny - 1 - y)), min(z, g.nz - 1 - z));
+#pragma unroll
+  for (int k = 0; k < NF; ++k) {
+    const float* f = fs.f[k];
+    const float* fo = fs.fo[k];
+    const float fop = __ldg(fo + q);
+    float sum = 0.0f;
+    if (sx) sum = __fadd_rn(sum, higdon_side(h, __ldg(f + nbx), fop, __ldg(fo + nbx)));
+    if (sy) sum = __fadd_rn(sum, higdon_side(h, __ldg(f + nby), fop, __ldg(fo + nby)));
+    if (sz) sum = __fadd_rn(sum, higdon_side(h, __ldg(f + nbz), fop, __ldg(fo + nbz)));
+    const float w = habc_weight(h, fs.kind[k], dist);
+    scr[k * fr.total + idx] =
+        __fmaf_rn(w, __ldg(f + q), __fdiv_rn(__fmul_rn(__fsub_rn(1.0f, w), sum), (float)nd));
+  }
+}
+
+// Pass 2: scratch back into the NF fields.
+template <int NF>
+__global__ void __launch_bounds__(256) k_habc3_pass2(Geo3 g, Frame3 fr, FieldOut3 fo,
+                                                     const float* __restrict__ scr) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= fr.total) return;
+  int x, y, z;
+  frame3_xyz(g, fr, idx, x, y, z);
+  const long long q = x + g.sy * y + g.sz * z;
+#pragma unroll
+  for (int k = 0; k < NF; ++k) fo.f[k][q] = scr[k * fr.total + idx];
+}
+
+// Both passes for NF = 1, 3 or 6 fields.
+inline void habc3_passes(cudaStream_t st, unsigned fblocks, const Geo3& g, const Frame3& fr,
+                         const HabcDev& h, const FieldSet3& fs, const FieldOut3& fo, float* scr) {
+  switch (fs.n) {
+    case 1:
+      k_habc3_pass1<1><<<fblocks, 256, 0, st>>>(g, fr, h, fs, scr);
+      k_habc3_pass2<1><<<fblocks, 256, 0, st>>>(g, fr, fo, scr);
+      break;
+    case 3:
+      k_habc3_pass1<3><<<fblocks, 256, 0, st>>>(g, fr, h, fs, scr);
+      k_habc3_pass2<3><<<fblocks, 256, 0, st>>>(g, fr, fo, scr);
+      break;
+    default:
+      k_habc3_pass1<6><<<fblocks, 256, 0, st>>>(g, fr, h, fs, scr);
+      k_habc3_pass2<6><<<fblocks, 256, 0, st>>>(g, fr, fo, scr);
+      break;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -542,6 +557,7 @@ int run3d(fomo_ctx* ctx, bool elastic, const fomo_grid3d* gp, const float* vp, c
   HabcDev h{hh.q, hh.qt, hh.qxt, hh.nbc, hh.wstride, d_w};
   const float dtdh = gp->dt / gp->dh;
   const unsigned fblocks = (unsigned)std::max<long long>(1, (fr.total + 255) / 256);
+  const unsigned rec_blocks = (unsigned)std::min(1184, std::max(1, (acq->n_rec + 255) / 256));
   int A = 0, B = 1, launches = 0;
   FOMO_CU(ctx, cudaEventRecord(ctx->ev0, st));
   for (int it = 1; it <= nt; ++it) {
@@ -579,8 +595,7 @@ int run3d(fomo_ctx* ctx, bool elastic, const fomo_grid3d* gp, const float* vp, c
         fs.kind[k] = k;
         fo.f[k] = field(B, k);
       }
-      k_habc3_pass1<<<fblocks, 256, 0, st>>>(g, fr, h, fs, d_scr);
-      k_habc3_pass2<<<fblocks, 256, 0, st>>>(g, fr, 3, fo, d_scr);
+      habc3_passes(st, fblocks, g, fr, h, fs, fo, d_scr);
     }
     // stress / pressure phase
     if (elastic) {
@@ -618,11 +633,10 @@ int run3d(fomo_ctx* ctx, bool elastic, const fomo_grid3d* gp, const float* vp, c
         fs.kind[k] = 3;
         fo.f[k] = field(B, 3 + k);
       }
-      k_habc3_pass1<<<fblocks, 256, 0, st>>>(g, fr, h, fs, d_scr);
-      k_habc3_pass2<<<fblocks, 256, 0, st>>>(g, fr, fs.n, fo, d_scr);
+      habc3_passes(st, fblocks, g, fr, h, fs, fo, d_scr);
     }
     // inject (p | txx,tyy,tzz), record vx vy vz (acoustic3d.jl:171-176, elastic3d.jl:139-147)
-    k_inject_record3<<<1, 256, 0, st>>>(it, nt, acq->n_src, d_src, d_wav, field(B, 3),
+    k_inject_record3<<<rec_blocks, 256, 0, st>>>(it, nt, acq->n_src, d_src, d_wav, field(B, 3),
                                         elastic ? field(B, 4) : nullptr,
                                         elastic ? field(B, 5) : nullptr, acq->n_rec, d_rec,
                                         field(B, 0), field(B, 1), field(B, 2), d_seis[0],
