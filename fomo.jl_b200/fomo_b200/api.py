@@ -516,7 +516,7 @@ _PLANES = {"xz": 0, "xy": 1, "yz": 2}
 
 
 def _run3d(elastic, vp, vs, rho, dh, dt, nt, f0, sx, sy, sz, rx, ry, rz, nbc, fd_order,
-           snap_interval, snap_plane, snap_index, v_ref, wavelet, device, final_state):
+           snap_interval, snap_plane, snap_index, v_ref, wavelet, device, final_state, kernel=0):
     vp, rho = _f32F(vp), _f32F(rho)
     vs = _f32F(vs) if elastic else None
     if vp.ndim != 3:
@@ -551,7 +551,7 @@ def _run3d(elastic, vp, vs, rho, dh, dt, nt, f0, sx, sy, sz, rx, ry, rz, nbc, fd
     g = L.Grid3D(nx, ny, nz, float(dh), float(dt), int(nt), int(nbc), int(fd_order), float(v_ref))
     acq = L.Acq3D(sxv.size, _ptr(sxv), _ptr(syv), _ptr(szv), _ptr(wm), rxv.size, _ptr(rxv),
                   _ptr(ryv), _ptr(rzv))
-    o = _opts(0, final_state)
+    o = _opts(kernel, final_state)
     if elastic:
         rc = L.lib().fomo_elastic3d(ctx.handle, C.byref(g), _ptr(vp), _ptr(vs), _ptr(rho),
                                     C.byref(acq), int(snap_interval), plane, int(snap_index),
@@ -584,14 +584,16 @@ def acoustic3d(vp, rho, dh, dt, nt, f0, *, sx, sy, sz, rx, ry, rz, nbc: int = 50
 def elastic3d(vp, vs, rho, dh, dt, nt, f0, *, sx, sy, sz, rx, ry, rz, nbc: int = 50,
               fd_order: int = 8, snap_interval: int = 0, snap_plane="xz", snap_index: int = 0,
               v_ref=None, wavelet=None, device: int = 0,
-              final_state: Optional[np.ndarray] = None):
+              final_state: Optional[np.ndarray] = None, kernel: int = 0):
     """3D elastic simulation (equations/elastic3d/elastic3d.jl:37-165).
 
     Returns ``(seis_vx, seis_vy, seis_vz, snaps)``; sources inject into txx,
-    tyy and tzz; snapshots hold vz.
+    tyy and tzz; snapshots hold vz.  ``kernel``: 0 or 3 = z-marching updates,
+    1 = per-cell updates (identical results).
     """
     return _run3d(True, vp, vs, rho, dh, dt, nt, f0, sx, sy, sz, rx, ry, rz, nbc, fd_order,
-                  snap_interval, snap_plane, snap_index, v_ref, wavelet, device, final_state)
+                  snap_interval, snap_plane, snap_index, v_ref, wavelet, device, final_state,
+                  kernel)
 
 
 def debug_medium2d(kind: str, vp, vs, rho, pad: int, dt=1.0, dh=1.0, device: int = 0):

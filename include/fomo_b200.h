@@ -63,6 +63,9 @@ extern "C" {
 #define FOMO_KERNEL_AUTO 0
 #define FOMO_KERNEL_TWO_PHASE 1    /* velocity sweep + stress sweep per step      */
 #define FOMO_KERNEL_SINGLE_SWEEP 2 /* one fused sweep per step (z-marching tiles) */
+#define FOMO_KERNEL_ZMARCH 3       /* 3D: z-marching velocity and stress updates;  */
+                                   /* TWO_PHASE = per-cell updates; AUTO = z-marching */
+                                   /* velocity + per-cell stress (stats: AUTO)        */
 
 typedef struct fomo_ctx fomo_ctx;
 

@@ -86,6 +86,30 @@ def test_elastic3d_bitwise(fomo, oracle, fd_order):
     assert np.array_equal(fin, o["final"])
 
 
+@pytest.mark.parametrize("fd_order", [2, 8, 10])
+def test_elastic3d_zmarch_equals_per_cell(fomo, fd_order):
+    """The z-marching updates (several 32x8 tiles and z-chunks, ragged edges)
+    equal the per-cell kernels bit for bit, wavefields included, in both the
+    all-z-marching form (kernel 3) and the default mix (kernel 0)."""
+    nx, ny, nz, nt, nbc = 61, 23, 45, 40, 5
+    vp, vs, rho = _model3d(nx, ny, nz, seed=40 + fd_order, fluid_pocket=True)
+    sx, sy, sz, rx, ry, rz = _acq(nx, ny, nz)
+    kw = dict(sx=sx, sy=sy, sz=sz, rx=rx, ry=ry, rz=rz, nbc=nbc, fd_order=fd_order)
+    shape = _final_shape(nx, ny, nz, nbc, fd_order, 9)
+    f_pc = np.zeros(shape, np.float32, order="F")
+    b = fomo.elastic3d(vp, vs, rho, 10.0, 8e-4, nt, 25.0, final_state=f_pc, kernel=1, **kw)
+    assert fomo.api.last_stats.kernel == 1
+    assert np.abs(f_pc).max() > 0
+    for kernel in (3, 0):
+        f_zm = np.zeros(shape, np.float32, order="F")
+        a = fomo.elastic3d(vp, vs, rho, 10.0, 8e-4, nt, 25.0, final_state=f_zm, kernel=kernel,
+                           **kw)
+        assert fomo.api.last_stats.kernel == kernel
+        for k in range(3):
+            assert np.array_equal(a[k], b[k])
+        assert np.array_equal(f_zm, f_pc)
+
+
 @pytest.mark.parametrize("kind", ["acoustic", "elastic"])
 def test_3d_error_vs_fp64(fomo, oracle, kind):
     nx, ny, nz, nt, nbc = 24, 22, 20, 120, 8
