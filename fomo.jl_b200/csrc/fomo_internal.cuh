@@ -79,6 +79,13 @@ struct HabcDev {
   const float* wtab;
 };
 
+// FP16 wavefield storage (elastic2d, mixed2d.cuh and the sweep's binary16
+// form): cells within kFp16Band of the padded grid's edge stay FP32; stored
+// velocities are scaled by kFp16Sv, stresses by kFp16St (powers of two).
+constexpr int kFp16Band = 32;
+constexpr float kFp16Sv = 4194304.0f;  // 2^22
+constexpr float kFp16St = 1.0f;
+
 // Padded 2D geometry (0-based x in [0,nx), z in [0,nz)).
 struct Geo2 {
   int nx, nz;      // padded

@@ -18,10 +18,6 @@
 
 namespace fomo {
 
-constexpr int kFp16Band = 32;
-constexpr float kFp16Sv = 4194304.0f;  // 2^22
-constexpr float kFp16St = 1.0f;
-
 struct HField {  // one wavefield of one ping-pong set, all shots (shot offset = shot * plane)
   float* f32;    // cells of the band
   __half* f16;   // other cells

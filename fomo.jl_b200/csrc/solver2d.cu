@@ -127,9 +127,9 @@ float min_positive(const std::vector<float>& v) {
 // z-segments) candidate on the problem itself and keeps the fastest; the
 // choice is cached per (N, padded grid, shots) for the process.
 struct TuneKey {
-  int N, nx, nz, ns;
+  int N, nx, nz, ns, h16;
   bool operator<(const TuneKey& o) const {
-    return std::tie(N, nx, nz, ns) < std::tie(o.N, o.nx, o.nz, o.ns);
+    return std::tie(N, nx, nz, ns, h16) < std::tie(o.N, o.nx, o.nz, o.ns, o.h16);
   }
 };
 struct TuneVal {
@@ -139,18 +139,24 @@ struct TuneVal {
 std::mutex g_tune_mu;
 std::map<TuneKey, TuneVal> g_tune;
 
+// sets16 / o16: the binary16 arrays (set-major, sweep field order) and the
+// binary16 outputs of set 1 for the binary16 storage form; null for FP32.
 template <class FieldFn>
 int tune_sweep(fomo_ctx* ctx, cudaStream_t st, SweepPlan& sp, int N, const Geo2& g, int ns,
                float* const sets[2][5], const Coef& c, float dtx, float dtz, const HabcDev& h,
-               const ElMat& m, FieldFn field, long long* d_bounds) {
-  const TuneKey key{N, g.nx, g.nz, ns};
+               const ElMat& m, FieldFn field, long long* d_bounds, __half* const* sets16 = nullptr,
+               const ElOut16* o16 = nullptr) {
+  const bool h16 = sets16 != nullptr;
+  const TuneKey key{N, g.nx, g.nz, ns, h16 ? 1 : 0};
   // FOMO_SWEEP_CONFIG="variant,TX,ctas_per_sm" pins the configuration (tests, sweeps)
   if (const char* env = std::getenv("FOMO_SWEEP_CONFIG")) {
     int v = 0, tx = 0, per_sm = 0;
     float fw = kFrameWeight;
     const int nr = std::sscanf(env, "%d,%d,%d,%f", &v, &tx, &per_sm, &fw);
     if (nr >= 3 && v >= 0 && v < sweep_num_variants() && per_sm >= 1) {
-      FOMO_CU(ctx, make_sweep_plan(sp, N, v, tx, per_sm, g, ns, sets, fw, d_bounds, st));
+      if (sweep_variant_h16(v) != h16)
+        return fail(ctx, FOMO_EARG, "FOMO_SWEEP_CONFIG names a variant of the other storage form");
+      FOMO_CU(ctx, make_sweep_plan(sp, N, v, tx, per_sm, g, ns, sets, fw, d_bounds, st, sets16));
       return FOMO_OK;
     }
     return fail(ctx, FOMO_EARG, "bad FOMO_SWEEP_CONFIG (want variant,TX,ctas_per_sm[,frame_weight])");
@@ -160,7 +166,7 @@ int tune_sweep(fomo_ctx* ctx, cudaStream_t st, SweepPlan& sp, int N, const Geo2&
     auto it = g_tune.find(key);
     if (it != g_tune.end()) {
       FOMO_CU(ctx, make_sweep_plan(sp, N, it->second.variant, it->second.TX, it->second.per_sm, g,
-                                   ns, sets, it->second.frame_weight, d_bounds, st));
+                                   ns, sets, it->second.frame_weight, d_bounds, st, sets16));
       return FOMO_OK;
     }
   }
@@ -172,27 +178,28 @@ int tune_sweep(fomo_ctx* ctx, cudaStream_t st, SweepPlan& sp, int N, const Geo2&
   float best = 1e30f;
   TuneVal bv{-1, 0, 0, kFrameWeight};
   auto time_plan = [&](const SweepPlan& cand, float& ms) -> int {
-    FOMO_CU(ctx, launch_sweep_elastic(st, cand, 0, c, dtx, dtz, h, a, m, o, ctx->d_flag));
+    FOMO_CU(ctx, launch_sweep_elastic(st, cand, 0, c, dtx, dtz, h, a, m, o, ctx->d_flag, o16));
     FOMO_CU(ctx, cudaEventRecord(e0, st));
     for (int r = 0; r < 3; ++r)
-      FOMO_CU(ctx, launch_sweep_elastic(st, cand, 0, c, dtx, dtz, h, a, m, o, ctx->d_flag));
+      FOMO_CU(ctx, launch_sweep_elastic(st, cand, 0, c, dtx, dtz, h, a, m, o, ctx->d_flag, o16));
     FOMO_CU(ctx, cudaEventRecord(e1, st));
     FOMO_CU(ctx, cudaEventSynchronize(e1));
     FOMO_CU(ctx, cudaEventElapsedTime(&ms, e0, e1));
     return FOMO_OK;
   };
   for (int v = 0; v < sweep_num_variants(); ++v) {
+    if (sweep_variant_h16(v) != h16) continue;
     int txs[4];
     int ntx = sweep_tx_candidates(v, N, g.nx, txs, 4);
     for (int k = 0; k < ntx; ++k) {
       SweepPlan cand;
-      if (make_sweep_plan(cand, N, v, txs[k], 64, g, ns, sets, kFrameWeight, d_bounds, st) !=
-          cudaSuccess)
+      if (make_sweep_plan(cand, N, v, txs[k], 64, g, ns, sets, kFrameWeight, d_bounds, st,
+                          sets16) != cudaSuccess)
         continue;
       const int full = cand.per_sm;  // all resident CTAs; also try one fewer
       for (int per_sm = full; per_sm >= 1 && per_sm >= full - 1; --per_sm) {
         if (make_sweep_plan(cand, N, v, txs[k], per_sm, g, ns, sets, kFrameWeight, d_bounds,
-                            st) != cudaSuccess)
+                            st, sets16) != cudaSuccess)
           continue;
         float ms = 0.0f;
         if (int rc = time_plan(cand, ms)) return rc;
@@ -207,8 +214,8 @@ int tune_sweep(fomo_ctx* ctx, cudaStream_t st, SweepPlan& sp, int N, const Geo2&
   if (bv.variant >= 0)
     for (float fw : {0.0f, 0.07f, 0.3f, 0.6f, 1.2f}) {
       SweepPlan cand;
-      if (make_sweep_plan(cand, N, bv.variant, bv.TX, bv.per_sm, g, ns, sets, fw, d_bounds, st) !=
-          cudaSuccess)
+      if (make_sweep_plan(cand, N, bv.variant, bv.TX, bv.per_sm, g, ns, sets, fw, d_bounds, st,
+                          sets16) != cudaSuccess)
         continue;
       float ms = 0.0f;
       if (int rc = time_plan(cand, ms)) return rc;
@@ -221,7 +228,7 @@ int tune_sweep(fomo_ctx* ctx, cudaStream_t st, SweepPlan& sp, int N, const Geo2&
   cudaEventDestroy(e1);
   if (bv.variant < 0) return fail(ctx, FOMO_ECUDA, "no single-sweep configuration fits");
   FOMO_CU(ctx, make_sweep_plan(sp, N, bv.variant, bv.TX, bv.per_sm, g, ns, sets, bv.frame_weight,
-                               d_bounds, st));
+                               d_bounds, st, sets16));
   std::lock_guard<std::mutex> lk(g_tune_mu);
   g_tune[key] = bv;
   return FOMO_OK;
@@ -287,7 +294,6 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
 
   int kernel = P.kernel;
   if (kernel == FOMO_KERNEL_AUTO) kernel = pick_kernel_2d((int)P.phys, P.N, P.nxp, P.nzp, P.ns);
-  if (P.fp16) kernel = FOMO_KERNEL_TWO_PHASE;  // the binary16 path is two-phase
   if (kernel == FOMO_KERNEL_SINGLE_SWEEP && !sweep2d_supported((int)P.phys, P.N))
     kernel = FOMO_KERNEL_TWO_PHASE;
 
@@ -390,12 +396,25 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
     FOMO_CU(ctx, build_sweep_pack(st, g, emat, ws_ptr<float>(ctx, o_pack)));
     float* sets[2][5] = {{field(0, 2), field(0, 3), field(0, 4), field(0, 0), field(0, 1)},
                          {field(1, 2), field(1, 3), field(1, 4), field(1, 0), field(1, 1)}};
+    __half* sets16[10];
+    ElOut16 o16{};
+    if (P.fp16) {
+      const int order[5] = {2, 3, 4, 0, 1};  // txx, tzz, txz, vx, vz
+      for (int s2 = 0; s2 < 2; ++s2)
+        for (int f = 0; f < 5; ++f) sets16[s2 * 5 + f] = hfield(s2, order[f]).f16;
+      o16 = ElOut16{hfield(1, 0).f16, hfield(1, 1).f16, hfield(1, 2).f16, hfield(1, 3).f16,
+                    hfield(1, 4).f16};
+    }
     rc = tune_sweep(ctx, st, sp, P.N, g, P.ns, sets, c, dtx, dtz, h, emat,
                     [&](int set, int f) { return field(set, f); },
-                    ws_ptr<long long>(ctx, o_bounds));
+                    ws_ptr<long long>(ctx, o_bounds), P.fp16 ? sets16 : nullptr,
+                    P.fp16 ? &o16 : nullptr);
     if (rc) return rc;
     // the tuning launches ran on the zero state; restore it
     FOMO_CU(ctx, cudaMemsetAsync(d_state, 0, sizeof(float) * nsets * nfield * P.ns * P.plane, st));
+    if (P.fp16)
+      FOMO_CU(ctx, cudaMemsetAsync(d_state16, 0, sizeof(__half) * nsets * nfield * P.ns * P.plane,
+                                   st));
   }
   FOMO_CU(ctx, cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), st));
 
@@ -421,7 +440,14 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
     if (P.phys == kElastic) {
       ElFields a{field(A, 0), field(A, 1), field(A, 2), field(A, 3), field(A, 4)};
       const ElMat& m = emat;
-      if (P.fp16) {
+      if (P.fp16 && kernel == FOMO_KERNEL_SINGLE_SWEEP) {
+        ElOut o{field(B, 0), field(B, 1), field(B, 2), field(B, 3), field(B, 4)};
+        const ElOut16 o16{hfield(B, 0).f16, hfield(B, 1).f16, hfield(B, 2).f16, hfield(B, 3).f16,
+                          hfield(B, 4).f16};
+        FOMO_CU(ctx, launch_sweep_elastic(st, sp, A, c, dtx, dtz, h, a, m, o, ctx->d_flag, &o16));
+        launches += 1;
+        sweeps_per_step = 1;
+      } else if (P.fp16) {
         HSet ha{{hfield(A, 0), hfield(A, 1), hfield(A, 2), hfield(A, 3), hfield(A, 4)}};
 #define FOMO_ELH_CASE(NN)                                                                       \
   case NN:                                                                                      \

@@ -1252,10 +1252,20 @@ __host__ __device__ constexpr int rl_txmax(int N, int NT) {
          ~3;
 }
 
-template <int N, int NT, int P, int LV = (N + 2 <= 4 ? 4 : 8)>
+// binary16 form: 8-column halos so that every TMA x coordinate of a binary16
+// row is a multiple of 8 elements (16 bytes)
+__host__ __device__ constexpr int rl_w16(int NT) {
+  return ((2 * (NT + 8) + 15) & ~15) < 256 ? ((2 * (NT + 8) + 15) & ~15) : 256;
+}
+__host__ __device__ constexpr int rl_txmax16(int N, int NT) {
+  return ((2 * NT - 16) < (rl_w16(NT) - 8 - N - 16) ? (2 * NT - 16) : (rl_w16(NT) - 8 - N - 16)) &
+         ~7;
+}
+
+template <int N, int NT, int P, int LV = (N + 2 <= 4 ? 4 : 8), bool H16 = false>
 struct RLShape {
-  static constexpr int W = rl_w(N, NT);
-  static constexpr int TN = x2_tn(N), HV = x2_hv(N);
+  static constexpr int W = H16 ? rl_w16(NT) : rl_w(N, NT);
+  static constexpr int TN = H16 ? 8 : x2_tn(N), HV = H16 ? 8 : x2_hv(N);
   static constexpr int NZ = P + 1;                 // z / x stream slots
   static constexpr int NO = P + 2;                 // old-stress / A.v stream slots (and barriers)
   static constexpr int LVV = LV;                   // v'' ring rows (a power of two >= N + 2)
@@ -1266,7 +1276,12 @@ struct RLShape {
   static constexpr int O_VP = O_V + NO * 4 * W;    // [vx, vz][4][W]  v'
   static constexpr int O_VV = O_VP + 8 * W;        // [vx, vz][LVV][W] v''
   static constexpr int O_SP = O_VV + 2 * LVV * W;  // [xx, zz, xz][4][W] s'
-  static constexpr int O_WT = O_SP + 12 * W;       // [3][wstride] weights
+  // binary16 staging boxes (2 rows of W halves, each box on a 128-byte boundary):
+  // z [NZ][txz, tzz], x [NZ][txx, txz], o [NO][txx, tzz, txz], v [NO][vx, vz]
+  static constexpr int NB16 = H16 ? 4 * NZ + 5 * NO : 0;
+  static constexpr int HB = ((4 * W + 127) & ~127) / 4;  // floats per staging box
+  static constexpr int O_H = O_SP + 12 * W;
+  static constexpr int O_WT = O_H + NB16 * HB;     // [3][wstride] weights
 };
 
 template <int N, int NT, int P>
@@ -1698,14 +1713,23 @@ __host__ __device__ constexpr int ws_lvv(int N, bool split) {
   return split ? (N + 4 <= 8 ? 8 : 16) : (N + 2 <= 4 ? 4 : 8);
 }
 
-template <int N, int NV, int P, int MINB, bool SPLIT>
+template <int N, int NV, int P, int MINB, bool SPLIT, bool H16>
 __global__ void __launch_bounds__(2 * NV, MINB)
     k_el_sweep_ws(const __grid_constant__ CUtensorMap tm_xx, const __grid_constant__ CUtensorMap tm_zz,
                   const __grid_constant__ CUtensorMap tm_xz, const __grid_constant__ CUtensorMap tm_vx,
-                  const __grid_constant__ CUtensorMap tm_vz, SweepGeom gm, Coef c, float dtx,
-                  float dtz, HabcDev h, MatPack mp, ElOut o, const long long* __restrict__ bounds,
-                  int* __restrict__ err) {
-  using S = RLShape<N, NV, P, ws_lvv(N, SPLIT)>;
+                  const __grid_constant__ CUtensorMap tm_vz, const __grid_constant__ CUtensorMap th_xx,
+                  const __grid_constant__ CUtensorMap th_zz, const __grid_constant__ CUtensorMap th_xz,
+                  const __grid_constant__ CUtensorMap th_vx, const __grid_constant__ CUtensorMap th_vz,
+                  SweepGeom gm, Coef c, float dtx, float dtz, HabcDev h, MatPack mp, ElOut o,
+                  ElOut16 o16, const long long* __restrict__ bounds, int* __restrict__ err) {
+  // H16: binary16 storage outside the kFp16Band-wide FP32 band (th_* map the
+  // binary16 arrays, o16 receives them); TMA brings the binary16 rows into
+  // staging boxes (and the FP32 rows where the band reaches), each role widens
+  // the rows it reads into the FP32 rings, and stored values are rounded to
+  // binary16 outside the band -- the velocities the stress role reads included,
+  // as they would be read back from storage.
+  using S = RLShape<N, NV, P, ws_lvv(N, SPLIT), H16>;
+  static_assert(!H16 || (S::TN % 8 == 0 && S::HV % 8 == 0), "binary16 TMA x must be 8-aligned");
   constexpr int NT = 2 * NV;
   // mid-iteration barrier: per role (ids 2, 3) when SPLIT, else the whole CTA (id 1)
   const int mid_id = SPLIT ? (threadIdx.x < NV ? 2 : 3) : 1;
@@ -1724,6 +1748,8 @@ __global__ void __launch_bounds__(2 * NV, MINB)
   float* s_wt = sm + S::O_WT;
   const int nwt = (3 * h.wstride + 31) & ~31;
   uint64_t* bars = reinterpret_cast<uint64_t*>(sm + S::O_WT + nwt);  // [NO]
+  float* s_h = sm + S::O_H;  // binary16 staging boxes
+  auto hbox = [&](int b) { return s_h + b * S::HB; };
 
   const int tid = threadIdx.x;
   const bool vel = tid < NV;  // warp-uniform role
@@ -1745,6 +1771,38 @@ __global__ void __launch_bounds__(2 * NV, MINB)
   auto zframe = [&](int z) { return z >= 1 && z <= nz - 2; };
   auto zinner = [&](int z) { return z >= M && z < nz - M; };
   auto zdist = [&](int z) { return min(z, nz - 1 - z); };
+  // FP32 band of the binary16 storage: rows (and columns) within kFp16Band of
+  // the edge; rows outside the grid count as band (TMA fills them with zeros)
+  auto zband16 = [&](int z) { return z < kFp16Band || z >= nz - kFp16Band; };
+  auto xband16 = [&](int x) { return x < kFp16Band || x >= nx - kFp16Band; };
+  // Widens binary16 rows y0, y0+1 of a staging box into the FP32 rows at dst
+  // (columns x0 + c) outside the band; every thread of the role takes column
+  // pairs c = 2t, 2t + 2 NV, ...
+  auto widen = [&](float* dst, const float* box, int x0, int y0) {
+#pragma unroll
+    for (int rr = 0; rr < 2; ++rr) {
+      if (zband16(y0 + rr)) continue;
+      const __half* src = reinterpret_cast<const __half*>(box) + rr * W;
+      float* d = dst + rr * W;
+#pragma unroll
+      for (int c0 = 0; c0 < W; c0 += 2 * NV) {
+        const int cc = c0 + sc;
+        if (cc < W) {
+          const float2 v = __half22float2(*reinterpret_cast<const __half2*>(src + cc));
+          const bool b0 = xband16(x0 + cc), b1 = xband16(x0 + cc + 1);
+          if (!b0 && !b1) *reinterpret_cast<float2*>(d + cc) = v;
+          else {
+            if (!b0) d[cc] = v.x;
+            if (!b1) d[cc + 1] = v.y;
+          }
+        }
+      }
+    }
+  };
+  // the value as stored: rounded to binary16 outside the band
+  auto stored = [&](float v, bool band) {
+    return (H16 && !band) ? __half2float(__float2half_rn(v)) : v;
+  };
   const bool do_v = sc < WV;
   const bool do_s = sc >= HV - 2 && sc < HV + TX + 2;
   const bool do_o = sc >= HV && sc < HV + TX;
@@ -1800,17 +1858,70 @@ __global__ void __launch_bounds__(2 * NV, MINB)
       auto issue = [&](int k) {
         const int gk = gb + k, zs = gk % NZ, os = gk % NO;
         uint64_t* bar = &bars[os];
-        mbar_expect_tx(bar, 9u * 2u * W * 4u);
         const int zr = g.zv0 + 2 * k;
-        tma_load_3d(s_z + (zs * 4 + 0) * W, &tm_xz, g.XT, zr + M, g.shot, bar);
-        tma_load_3d(s_z + (zs * 4 + 2) * W, &tm_zz, g.XT, zr + M, g.shot, bar);
-        tma_load_3d(s_x + (zs * 4 + 0) * W, &tm_xx, g.XT, zr, g.shot, bar);
-        tma_load_3d(s_x + (zs * 4 + 2) * W, &tm_xz, g.XT, zr, g.shot, bar);
-        tma_load_3d(s_o + (os * 6 + 0) * W, &tm_xx, g.XT, zr - 3 - M, g.shot, bar);
-        tma_load_3d(s_o + (os * 6 + 2) * W, &tm_zz, g.XT, zr - 3 - M, g.shot, bar);
-        tma_load_3d(s_o + (os * 6 + 4) * W, &tm_xz, g.XT, zr - 3 - M, g.shot, bar);
-        tma_load_3d(s_v + (os * 4 + 0) * W, &tm_vx, g.XV, zr, g.shot, bar);
-        tma_load_3d(s_v + (os * 4 + 2) * W, &tm_vz, g.XV, zr, g.shot, bar);
+        if constexpr (!H16) {
+          mbar_expect_tx(bar, 9u * 2u * W * 4u);
+          tma_load_3d(s_z + (zs * 4 + 0) * W, &tm_xz, g.XT, zr + M, g.shot, bar);
+          tma_load_3d(s_z + (zs * 4 + 2) * W, &tm_zz, g.XT, zr + M, g.shot, bar);
+          tma_load_3d(s_x + (zs * 4 + 0) * W, &tm_xx, g.XT, zr, g.shot, bar);
+          tma_load_3d(s_x + (zs * 4 + 2) * W, &tm_xz, g.XT, zr, g.shot, bar);
+          tma_load_3d(s_o + (os * 6 + 0) * W, &tm_xx, g.XT, zr - 3 - M, g.shot, bar);
+          tma_load_3d(s_o + (os * 6 + 2) * W, &tm_zz, g.XT, zr - 3 - M, g.shot, bar);
+          tma_load_3d(s_o + (os * 6 + 4) * W, &tm_xz, g.XT, zr - 3 - M, g.shot, bar);
+          tma_load_3d(s_v + (os * 4 + 0) * W, &tm_vx, g.XV, zr, g.shot, bar);
+          tma_load_3d(s_v + (os * 4 + 2) * W, &tm_vz, g.XV, zr, g.shot, bar);
+        } else {
+          // per stream (z, x, o, v): binary16 rows unless both rows are band
+          // rows; FP32 rows where a row or a column of the box is band
+          const int ys[4] = {zr + M, zr, zr - 3 - M, zr};
+          const bool xt = xband16(g.XT) || xband16(g.XT + W - 1);
+          const bool xv = xband16(g.XV) || xband16(g.XV + W - 1);
+          bool n16[4], n32[4];
+          uint32_t bytes = 0;
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            const bool b0 = zband16(ys[t]), b1 = zband16(ys[t] + 1);
+            n16[t] = !(b0 && b1);
+            n32[t] = (t == 3 ? xv : xt) || b0 || b1;
+            const uint32_t nf = t == 2 ? 3u : 2u;
+            bytes += nf * ((n16[t] ? 4u * W : 0u) + (n32[t] ? 8u * W : 0u));
+          }
+          mbar_expect_tx(bar, bytes);
+          if (n32[0]) {
+            tma_load_3d(s_z + (zs * 4 + 0) * W, &tm_xz, g.XT, ys[0], g.shot, bar);
+            tma_load_3d(s_z + (zs * 4 + 2) * W, &tm_zz, g.XT, ys[0], g.shot, bar);
+          }
+          if (n16[0]) {
+            tma_load_3d(hbox(zs * 2 + 0), &th_xz, g.XT, ys[0], g.shot, bar);
+            tma_load_3d(hbox(zs * 2 + 1), &th_zz, g.XT, ys[0], g.shot, bar);
+          }
+          if (n32[1]) {
+            tma_load_3d(s_x + (zs * 4 + 0) * W, &tm_xx, g.XT, ys[1], g.shot, bar);
+            tma_load_3d(s_x + (zs * 4 + 2) * W, &tm_xz, g.XT, ys[1], g.shot, bar);
+          }
+          if (n16[1]) {
+            tma_load_3d(hbox(2 * NZ + zs * 2 + 0), &th_xx, g.XT, ys[1], g.shot, bar);
+            tma_load_3d(hbox(2 * NZ + zs * 2 + 1), &th_xz, g.XT, ys[1], g.shot, bar);
+          }
+          if (n32[2]) {
+            tma_load_3d(s_o + (os * 6 + 0) * W, &tm_xx, g.XT, ys[2], g.shot, bar);
+            tma_load_3d(s_o + (os * 6 + 2) * W, &tm_zz, g.XT, ys[2], g.shot, bar);
+            tma_load_3d(s_o + (os * 6 + 4) * W, &tm_xz, g.XT, ys[2], g.shot, bar);
+          }
+          if (n16[2]) {
+            tma_load_3d(hbox(4 * NZ + os * 3 + 0), &th_xx, g.XT, ys[2], g.shot, bar);
+            tma_load_3d(hbox(4 * NZ + os * 3 + 1), &th_zz, g.XT, ys[2], g.shot, bar);
+            tma_load_3d(hbox(4 * NZ + os * 3 + 2), &th_xz, g.XT, ys[2], g.shot, bar);
+          }
+          if (n32[3]) {
+            tma_load_3d(s_v + (os * 4 + 0) * W, &tm_vx, g.XV, ys[3], g.shot, bar);
+            tma_load_3d(s_v + (os * 4 + 2) * W, &tm_vz, g.XV, ys[3], g.shot, bar);
+          }
+          if (n16[3]) {
+            tma_load_3d(hbox(4 * NZ + 3 * NO + os * 2 + 0), &th_vx, g.XV, ys[3], g.shot, bar);
+            tma_load_3d(hbox(4 * NZ + 3 * NO + os * 2 + 1), &th_vz, g.XV, ys[3], g.shot, bar);
+          }
+        }
       };
       cta_bar(1, NT);  // the previous segment's readers are done with every ring
       if (tid == 0 && live) {
@@ -1847,6 +1958,15 @@ __global__ void __launch_bounds__(2 * NV, MINB)
       for (int i = 0; i < g.I; ++i) {
         const int zv = g.zv0 + 2 * i;
         if (live) live = mbar_wait_bounded(&bars[os], ph, err) && live;
+        if constexpr (H16) {
+          widen(s_z + (zs * 4 + 0) * W, hbox(zs * 2 + 0), g.XT, zv + M);
+          widen(s_z + (zs * 4 + 2) * W, hbox(zs * 2 + 1), g.XT, zv + M);
+          widen(s_x + (zs * 4 + 0) * W, hbox(2 * NZ + zs * 2 + 0), g.XT, zv);
+          widen(s_x + (zs * 4 + 2) * W, hbox(2 * NZ + zs * 2 + 1), g.XT, zv);
+          widen(s_v + (os * 4 + 0) * W, hbox(4 * NZ + 3 * NO + os * 2 + 0), g.XV, zv);
+          widen(s_v + (os * 4 + 2) * W, hbox(4 * NZ + 3 * NO + os * 2 + 1), g.XV, zv);
+          cta_bar(4, NV);  // the role's widened rows are complete
+        }
         const float bxv[2][2] = {{mv[0].x, mv[0].y}, {mv[1].x, mv[1].y}};
         const float bzv[2][2] = {{mv[0].z, mv[0].w}, {mv[1].z, mv[1].w}};
 #pragma unroll
@@ -1984,18 +2104,45 @@ __global__ void __launch_bounds__(2 * NV, MINB)
                 }
               }
             }
+            bool bnd[2] = {true, true};
+            if constexpr (H16) {
+              const bool zb16 = zband16(qv);
+#pragma unroll
+              for (int e = 0; e < 2; ++e) {
+                bnd[e] = zb16 || xband16(g.xc + e);
+#pragma unroll
+                for (int f = 0; f < 2; ++f) vvn[f][e] = stored(vvn[f][e], bnd[e]);
+              }
+            }
             const int vw = (2 * i + rr) & (LVV - 1);  // v'' ring row of qv
             *reinterpret_cast<float2*>(s_vv + vw * W + sc) = make_float2(vvn[0][0], vvn[0][1]);
             *reinterpret_cast<float2*>(s_vv + (LVV + vw) * W + sc) = make_float2(vvn[1][0], vvn[1][1]);
             if (g.o_any && qv >= g.za && qv < g.zb) {
               float* px = rr ? ovx + gm.ld : ovx;
               float* pz = rr ? ovz + gm.ld : ovz;
-              if (g.o_pair) {
-                *reinterpret_cast<float2*>(px) = make_float2(vvn[0][0], vvn[0][1]);
-                *reinterpret_cast<float2*>(pz) = make_float2(vvn[1][0], vvn[1][1]);
+              if constexpr (!H16) {
+                if (g.o_pair) {
+                  *reinterpret_cast<float2*>(px) = make_float2(vvn[0][0], vvn[0][1]);
+                  *reinterpret_cast<float2*>(pz) = make_float2(vvn[1][0], vvn[1][1]);
+                } else {
+                  *px = vvn[0][0];
+                  *pz = vvn[1][0];
+                }
               } else {
-                *px = vvn[0][0];
-                *pz = vvn[1][0];
+                // the binary16 arrays run parallel to the FP32 ones (same index)
+                __half* hx = o16.vx + (px - o.vx);
+                __half* hz = o16.vz + (pz - o.vz);
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                  if (e == 1 && !g.o_pair) break;
+                  if (bnd[e]) {
+                    px[e] = vvn[0][e];
+                    pz[e] = vvn[1][e];
+                  } else {
+                    hx[e] = __float2half_rn(vvn[0][e]);
+                    hz[e] = __float2half_rn(vvn[1][e]);
+                  }
+                }
               }
             }
           }
@@ -2064,6 +2211,12 @@ __global__ void __launch_bounds__(2 * NV, MINB)
       for (int i = 0; i < g.I; ++i) {
         const int zv = g.zv0 + 2 * i, q = zv - 3 - M;
         if (live) live = mbar_wait_bounded(&bars[os], ph, err) && live;
+        if constexpr (H16) {
+          widen(s_o + (os * 6 + 0) * W, hbox(4 * NZ + os * 3 + 0), g.XT, q);
+          widen(s_o + (os * 6 + 2) * W, hbox(4 * NZ + os * 3 + 1), g.XT, q);
+          widen(s_o + (os * 6 + 4) * W, hbox(4 * NZ + os * 3 + 2), g.XT, q);
+          cta_bar(5, NV);  // the role's widened rows are complete
+        }
         const float lav[2][2] = {{ml[0].x, ml[0].y}, {ml[1].x, ml[1].y}};
         const float l2v[2][2] = {{ml[0].z, ml[0].w}, {ml[1].z, ml[1].w}};
         const float muv[2][2] = {{mu[0].x, mu[0].y}, {mu[1].x, mu[1].y}};
@@ -2214,13 +2367,30 @@ __global__ void __launch_bounds__(2 * NV, MINB)
                 }
               }
             }
+            if constexpr (!H16) {
 #pragma unroll
-            for (int f = 0; f < 3; ++f) {
-              float* pt = rr ? ot[f] + gm.ld : ot[f];
-              if (g.o_pair)
-                *reinterpret_cast<float2*>(pt) = make_float2(v[f][0], v[f][1]);
-              else
-                *pt = v[f][0];
+              for (int f = 0; f < 3; ++f) {
+                float* pt = rr ? ot[f] + gm.ld : ot[f];
+                if (g.o_pair)
+                  *reinterpret_cast<float2*>(pt) = make_float2(v[f][0], v[f][1]);
+                else
+                  *pt = v[f][0];
+              }
+            } else {
+              __half* const oh[3] = {o16.txx, o16.tzz, o16.txz};
+              float* const of[3] = {o.txx, o.tzz, o.txz};
+              const bool zb16 = zband16(qs);
+#pragma unroll
+              for (int e = 0; e < 2; ++e) {
+                if (e == 1 && !g.o_pair) break;
+                const bool bnd = zb16 || xband16(g.xc + e);
+#pragma unroll
+                for (int f = 0; f < 3; ++f) {
+                  float* pt = (rr ? ot[f] + gm.ld : ot[f]) + e;
+                  if (bnd) *pt = v[f][e];
+                  else oh[f][pt - of[f]] = __float2half_rn(v[f][e]);
+                }
+              }
             }
           }
         }
@@ -2295,20 +2465,23 @@ constexpr int kRLP[] = {1, 2, 1, 2};
 constexpr int kNumRL = sizeof(kRLP) / sizeof(kRLP[0]);
 #define FOMO_RL_VARIANTS(X, NN) X(0, NN, 128, 1) X(1, NN, 128, 2) X(2, NN, 64, 1) X(3, NN, 64, 2)
 
-template <int N, int NT, int P, int LV = (N + 2 <= 4 ? 4 : 8)>
+template <int N, int NT, int P, int LV = (N + 2 <= 4 ? 4 : 8), bool H16 = false>
 size_t rl_smem_bytes(int wstride) {
-  using S = RLShape<N, NT, P, LV>;
+  using S = RLShape<N, NT, P, LV, H16>;
   return (size_t)(S::O_WT + ((3 * wstride + 31) & ~31)) * 4 + sizeof(uint64_t) * S::NO;
 }
 
 // warp-specialized variants: (threads per role, prefetch depth, CTAs per SM)
 // (threads per role, prefetch depth, CTAs per SM, role-local mid-iteration barrier)
-constexpr int kWSNV[] = {128, 64, 64, 64};
-constexpr int kWSP[] = {1, 1, 1, 2};
+constexpr int kWSNV[] = {128, 64, 64, 64, 64, 64};
+constexpr int kWSP[] = {1, 1, 1, 2, 1, 1};
+constexpr bool kWSH16[] = {false, false, false, false, true, true};  // binary16 storage form
 constexpr int kNumWS = sizeof(kWSP) / sizeof(kWSP[0]);
-#define FOMO_WS_VARIANTS(X, NN) \
-  X(0, NN, 128, 1, 2, true) X(1, NN, 64, 1, 4, false) X(2, NN, 64, 1, 3, true) \
-  X(3, NN, 64, 2, 3, true)
+#define FOMO_WS_VARIANTS(X, NN)                                                           \
+  X(0, NN, 128, 1, 2, true, false) X(1, NN, 64, 1, 4, false, false)                      \
+  X(2, NN, 64, 1, 3, true, false) X(3, NN, 64, 2, 3, true, false) X(4, NN, 64, 1, 3, true, \
+                                                                      true)                \
+  X(5, NN, 64, 1, 2, true, true)
 
 template <int N, int P>
 size_t rw_smem_bytes(int wstride) {
@@ -2444,10 +2617,11 @@ cudaError_t launch_rl_n(cudaStream_t st, const SweepPlan& sp, int set, const Coe
   return cudaErrorInvalidValue;
 }
 
-template <int N, int NV, int P, int MINB, bool SPLIT>
+template <int N, int NV, int P, int MINB, bool SPLIT, bool H16>
 cudaError_t launch_ws(cudaStream_t st, const SweepPlan& sp, int set, const Coef& c, float dtx,
-                      float dtz, const HabcDev& h, const ElMat& m, const ElOut& o, int* err) {
-  auto kern = k_el_sweep_ws<N, NV, P, MINB, SPLIT>;
+                      float dtz, const HabcDev& h, const ElMat& m, const ElOut& o,
+                      const ElOut16* o16, int* err) {
+  auto kern = k_el_sweep_ws<N, NV, P, MINB, SPLIT, H16>;
   static std::atomic<int> attr_set{0};
   if (!attr_set.load(std::memory_order_acquire)) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2456,21 +2630,26 @@ cudaError_t launch_ws(cudaStream_t st, const SweepPlan& sp, int set, const Coef&
     attr_set.store(1, std::memory_order_release);
   }
   if (sp.smem > (size_t)kMaxDynSmem || !m.pack || m.pack_pitch < 1) return cudaErrorInvalidValue;
+  if (H16 && (!sp.h16 || !o16)) return cudaErrorInvalidValue;
   const long long cells = (long long)(sp.gm.nz + 2 * kPackRowPad) * m.pack_pitch;
   const MatPack mp{reinterpret_cast<const float4*>(m.pack),
                    reinterpret_cast<const float4*>(m.pack) + cells,
                    reinterpret_cast<const float2*>(m.pack + 8 * cells), m.pack_pitch};
+  const CUtensorMap* th = H16 ? sp.tm16[set] : sp.tm[set];  // unused by the FP32 form
+  const ElOut16 oh = o16 ? *o16 : ElOut16{};
   kern<<<(unsigned)sp.grid, 2 * NV, sp.smem, st>>>(sp.tm[set][0], sp.tm[set][1], sp.tm[set][2],
-                                                    sp.tm[set][3], sp.tm[set][4], sp.gm, c, dtx,
-                                                    dtz, h, mp, o, sp.d_bounds, err);
+                                                    sp.tm[set][3], sp.tm[set][4], th[0], th[1],
+                                                    th[2], th[3], th[4], sp.gm, c, dtx, dtz, h, mp,
+                                                    o, oh, sp.d_bounds, err);
   return cudaGetLastError();
 }
 
 template <int N>
 cudaError_t launch_ws_n(cudaStream_t st, const SweepPlan& sp, int set, const Coef& c, float dtx,
-                        float dtz, const HabcDev& h, const ElMat& m, const ElOut& o, int* err) {
-#define FOMO_LAUNCH_WS(V, NN, NV, PP, MB, SP) \
-  case V: return launch_ws<NN, NV, PP, MB, SP>(st, sp, set, c, dtx, dtz, h, m, o, err);
+                        float dtz, const HabcDev& h, const ElMat& m, const ElOut& o,
+                        const ElOut16* o16, int* err) {
+#define FOMO_LAUNCH_WS(V, NN, NV, PP, MB, SP, HH) \
+  case V: return launch_ws<NN, NV, PP, MB, SP, HH>(st, sp, set, c, dtx, dtz, h, m, o, o16, err);
   switch (sp.variant - kNumVariants - kNumX2 - kNumRW - kNumRL) {
     FOMO_WS_VARIANTS(FOMO_LAUNCH_WS, N)
   }
@@ -2479,8 +2658,8 @@ cudaError_t launch_ws_n(cudaStream_t st, const SweepPlan& sp, int set, const Coe
 }
 
 size_t ws_smem_for(int N, int v, int wstride) {
-#define FOMO_SMEM_WS(V, NN, NV, PP, MB, SP) \
-  case V: return rl_smem_bytes<NN, NV, PP, ws_lvv(NN, SP)>(wstride);
+#define FOMO_SMEM_WS(V, NN, NV, PP, MB, SP, HH) \
+  case V: return rl_smem_bytes<NN, NV, PP, ws_lvv(NN, SP), HH>(wstride);
 #define FOMO_SMEM_WSN(NN)                              \
   case NN:                                             \
     switch (v) { FOMO_WS_VARIANTS(FOMO_SMEM_WS, NN) }  \
@@ -2594,9 +2773,14 @@ cudaError_t build_sweep_pack(cudaStream_t st, const Geo2& g, ElMat& m, float* ds
 // Builds the work decomposition and the six tensor maps (3 stress fields x 2
 // ping-pong sets).  variant selects (threads, rows per chunk, prefetch depth);
 // TX is the strip width (multiple of 4).
+bool sweep_variant_h16(int variant) {
+  const int v = variant - kNumVariants - kNumX2 - kNumRW - kNumRL;
+  return v >= 0 && v < kNumWS && kWSH16[v];
+}
+
 cudaError_t make_sweep_plan(SweepPlan& sp, int N, int variant, int TX, int per_sm, const Geo2& g,
                             int ns, float* const sets[2][5], float frame_weight,
-                            long long* d_bounds, cudaStream_t st) {
+                            long long* d_bounds, cudaStream_t st, __half* const* sets16) {
   auto enc = encoder();
   if (!enc) return cudaErrorNotSupported;
   if (variant < 0 || variant >= sweep_num_variants() || per_sm < 1) return cudaErrorInvalidValue;
@@ -2605,24 +2789,36 @@ cudaError_t make_sweep_plan(SweepPlan& sp, int N, int variant, int TX, int per_s
   const bool rw = !ws && !rl && variant >= kNumVariants + kNumX2;
   const bool x2 = variant >= kNumVariants;  // the 2-row TMA-box families
   int W = 0, R = 2;
+  sp.h16 = false;
   if (ws) {
     const int v = variant - kNumVariants - kNumX2 - kNumRW - kNumRL;
-    if (TX < 8 || TX > rl_txmax(N, kWSNV[v]) || (TX & 3)) return cudaErrorInvalidValue;
-    W = rl_w(N, kWSNV[v]);
+    if (kWSH16[v]) {
+      // binary16 rows: every TMA x coordinate (strip * TX - 8 - 8, strip * TX - 8)
+      // must be a multiple of 8 elements
+      if (!sets16 || TX < 8 || TX > rl_txmax16(N, kWSNV[v]) || (TX & 7))
+        return cudaErrorInvalidValue;
+      W = rl_w16(kWSNV[v]);
+      sp.h16 = true;
+    } else {
+      if (sets16 || TX < 8 || TX > rl_txmax(N, kWSNV[v]) || (TX & 3)) return cudaErrorInvalidValue;
+      W = rl_w(N, kWSNV[v]);
+    }
     sp.family = 4;
     sp.P = kWSP[v];
   } else if (rl) {
+    if (sets16) return cudaErrorInvalidValue;
     const int v = variant - kNumVariants - kNumX2 - kNumRW;
     if (TX < 8 || TX > rl_txmax(N, kRLNT[v]) || (TX & 3)) return cudaErrorInvalidValue;
     W = rl_w(N, kRLNT[v]);
     sp.family = 3;
     sp.P = kRLP[v];
   } else if (x2) {
-    if (TX < 8 || TX > x2_txmax(N) || (TX & 3)) return cudaErrorInvalidValue;
+    if (sets16 || TX < 8 || TX > x2_txmax(N) || (TX & 3)) return cudaErrorInvalidValue;
     W = kX2W;
     sp.family = rw ? 2 : 1;
     sp.P = rw ? kRWP[variant - kNumVariants - kNumX2] : kX2P[variant - kNumVariants];
   } else {
+    if (sets16) return cudaErrorInvalidValue;
     const int NT = kVariants[variant].NT;
     R = kVariants[variant].R;
     const int M = N, HS = halo_x(M);
@@ -2752,6 +2948,13 @@ cudaError_t make_sweep_plan(SweepPlan& sp, int N, int variant, int TX, int per_s
                        strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
       if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+      if (sp.h16) {
+        cuuint64_t strides16[2] = {(cuuint64_t)g.ld * 2, (cuuint64_t)g.plane * 2};
+        r = enc(&sp.tm16[s][f], CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3, sets16[s * 5 + f], dims,
+                strides16, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+      }
     }
   return cudaSuccess;
 }
@@ -2761,9 +2964,18 @@ int sweep_tx_candidates(int variant, int N, int nx, int* out, int max_out) {
   if (variant >= kNumVariants) {
     // the widest strip, and the narrowest strip with the same strip count
     const int v = variant - kNumVariants - kNumX2 - kNumRW;
-    const int tmax = v >= kNumRL ? rl_txmax(N, kWSNV[v - kNumRL])
-                     : v >= 0    ? rl_txmax(N, kRLNT[v])
-                                 : x2_txmax(N);
+    const bool h16 = v >= kNumRL && kWSH16[v - kNumRL];
+    const int tmax = h16           ? rl_txmax16(N, kWSNV[v - kNumRL])
+                     : v >= kNumRL ? rl_txmax(N, kWSNV[v - kNumRL])
+                     : v >= 0      ? rl_txmax(N, kRLNT[v])
+                                   : x2_txmax(N);
+    if (h16) {  // strip widths of binary16 rows are multiples of 8
+      if (tmax >= 8 && n < max_out) out[n++] = tmax;
+      const int ns = (nx + tmax - 1) / tmax;
+      const int tbal = (((nx + ns - 1) / ns) + 7) & ~7;
+      if (tbal >= 8 && tbal < tmax && n < max_out) out[n++] = tbal;
+      return n;
+    }
     if (tmax >= 8 && n < max_out) out[n++] = tmax;
     const int ns = (nx + tmax - 1) / tmax;
     const int tbal = (((nx + ns - 1) / ns) + 3) & ~3;
@@ -2828,10 +3040,10 @@ int occ_rl(const SweepPlan& sp) {
   return nb;
 }
 
-template <int N, int NV, int P, int MINB, bool SPLIT>
+template <int N, int NV, int P, int MINB, bool SPLIT, bool H16>
 int occ_ws(const SweepPlan& sp) {
   int nb = 0;
-  auto kern = k_el_sweep_ws<N, NV, P, MINB, SPLIT>;
+  auto kern = k_el_sweep_ws<N, NV, P, MINB, SPLIT, H16>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, 2 * NV, sp.smem) != cudaSuccess) {
     cudaGetLastError();
@@ -2842,8 +3054,8 @@ int occ_ws(const SweepPlan& sp) {
 
 int sweep_blocks_per_sm(const SweepPlan& sp) {
   if (sp.family == 4) {
-#define FOMO_OCC_WS(V, NN, NV, PP, MB, SP) \
-  case V: return occ_ws<NN, NV, PP, MB, SP>(sp);
+#define FOMO_OCC_WS(V, NN, NV, PP, MB, SP, HH) \
+  case V: return occ_ws<NN, NV, PP, MB, SP, HH>(sp);
 #define FOMO_OCC_WSN(NN)                                                         \
   case NN:                                                                       \
     switch (sp.variant - kNumVariants - kNumX2 - kNumRW - kNumRL) {              \
@@ -2905,14 +3117,15 @@ int sweep_blocks_per_sm(const SweepPlan& sp) {
 
 cudaError_t launch_sweep_elastic(cudaStream_t st, const SweepPlan& sp, int set, const Coef& c,
                                  float dtx, float dtz, const HabcDev& h, const ElFields& a,
-                                 const ElMat& m, const ElOut& o, int* err) {
+                                 const ElMat& m, const ElOut& o, int* err, const ElOut16* o16) {
+  if (sp.h16 != (o16 != nullptr)) return cudaErrorInvalidValue;
   if (sp.family == 4) {
     switch (sp.N) {
-      case 1: return launch_ws_n<1>(st, sp, set, c, dtx, dtz, h, m, o, err);
-      case 2: return launch_ws_n<2>(st, sp, set, c, dtx, dtz, h, m, o, err);
-      case 3: return launch_ws_n<3>(st, sp, set, c, dtx, dtz, h, m, o, err);
-      case 4: return launch_ws_n<4>(st, sp, set, c, dtx, dtz, h, m, o, err);
-      case 5: return launch_ws_n<5>(st, sp, set, c, dtx, dtz, h, m, o, err);
+      case 1: return launch_ws_n<1>(st, sp, set, c, dtx, dtz, h, m, o, o16, err);
+      case 2: return launch_ws_n<2>(st, sp, set, c, dtx, dtz, h, m, o, o16, err);
+      case 3: return launch_ws_n<3>(st, sp, set, c, dtx, dtz, h, m, o, o16, err);
+      case 4: return launch_ws_n<4>(st, sp, set, c, dtx, dtz, h, m, o, o16, err);
+      case 5: return launch_ws_n<5>(st, sp, set, c, dtx, dtz, h, m, o, o16, err);
     }
     return cudaErrorInvalidValue;
   }

@@ -2,6 +2,7 @@
 // the kernel-family choice of the autotuner.
 #pragma once
 #include <cuda.h>
+#include <cuda_fp16.h>
 
 #include "solver2d_kernels.cuh"
 
@@ -45,6 +46,16 @@ size_t sweep_pack_floats(int nx, int nz);
 // planes and records it in m (pack, pack_pitch).
 cudaError_t build_sweep_pack(cudaStream_t st, const Geo2& g, ElMat& m, float* dst);
 
+// Binary16 arrays of the output set (binary16 storage form; same index space
+// as the FP32 arrays, which keep the band cells).
+struct ElOut16 {
+  __half* vx;
+  __half* vz;
+  __half* txx;
+  __half* tzz;
+  __half* txz;
+};
+
 struct SweepPlan {
   int N = 0, variant = 0;
   int family = 0;            // 0: column-per-thread, 1: pair-blocked, 2: register-window,
@@ -56,6 +67,8 @@ struct SweepPlan {
   size_t smem = 0;
   SweepGeom gm{};
   CUtensorMap tm[2][5];  // [ping-pong set][txx, tzz, txz, vx, vz]
+  bool h16 = false;      // binary16 storage form (tm16 maps the binary16 arrays)
+  CUtensorMap tm16[2][5];
 };
 
 // Kernel family for a problem (FOMO_KERNEL_TWO_PHASE / _SINGLE_SWEEP).
@@ -70,12 +83,18 @@ int sweep_tx_candidates(int variant, int N, int nx, int* out, int max_out);
 // estimated cost (frame cells weigh 1 + frame_weight); the row-range table is
 // written to d_bounds (kMaxGrid + 1 entries) on stream st.
 // sets: per ping-pong set the fields txx, tzz, txz, vx, vz.
+// sets16: for the binary16 variants, the binary16 arrays [set * 5 + field] in
+// the order of sets (null for the FP32 variants).
 cudaError_t make_sweep_plan(SweepPlan& sp, int N, int variant, int TX, int per_sm, const Geo2& g,
                             int ns, float* const sets[2][5], float frame_weight,
-                            long long* d_bounds, cudaStream_t st);
+                            long long* d_bounds, cudaStream_t st, __half* const* sets16 = nullptr);
+// o16: the binary16 output arrays, for (and only for) a binary16 plan.
 cudaError_t launch_sweep_elastic(cudaStream_t st, const SweepPlan& sp, int set, const Coef& c,
                                  float dtx, float dtz, const HabcDev& h, const ElFields& a,
-                                 const ElMat& m, const ElOut& o, int* err);
+                                 const ElMat& m, const ElOut& o, int* err,
+                                 const ElOut16* o16 = nullptr);
+// Is a variant the binary16 storage form?
+bool sweep_variant_h16(int variant);
 // Resident CTAs per SM for a plan (occupancy API).
 int sweep_blocks_per_sm(const SweepPlan& sp);
 

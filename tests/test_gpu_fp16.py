@@ -17,9 +17,11 @@ def _case():
     return vp, vs, rho
 
 
-# nbc 30: the Higdon zone lies inside the FP32 band; nbc 60: it reaches past it
+# nbc 30: the Higdon zone lies inside the FP32 band; nbc 60: it reaches past it.
+# kernel 1: two-phase binary16 kernels; 2: the single sweep's binary16 form.
+@pytest.mark.parametrize("kernel", [1, 2])
 @pytest.mark.parametrize("fd_order,nbc", [(4, 30), (10, 30), (8, 60)])
-def test_fp16_batch_bitwise_vs_emulation(fomo, oracle, fd_order, nbc):
+def test_fp16_batch_bitwise_vs_emulation(fomo, oracle, fd_order, nbc, kernel):
     vp, vs, rho = _case()
     nt = 400
     rx = np.arange(1, 121, 4)
@@ -30,7 +32,9 @@ def test_fp16_batch_bitwise_vs_emulation(fomo, oracle, fd_order, nbc):
     nxp, nzp = 120 + 2 * (nbc + M), 70 + 2 * (nbc + M)
     fin = np.zeros((nxp, nzp, 5, 2), np.float32, order="F")
     r = fomo.elastic2d_batch(vp, vs, rho, 5.0, 5e-4, nt, 20.0, sx=sx, sz=sz, rx=rx, rz=rz,
-                             nbc=nbc, fd_order=fd_order, precision="fp16", final_state=fin)
+                             nbc=nbc, fd_order=fd_order, precision="fp16", final_state=fin,
+                             kernel=kernel)
+    assert fomo.api.last_stats.kernel == kernel
     w = fomo.ricker_wavelet(20.0, 5e-4, nt).reshape(1, -1)
     kw = dict(sx=sx.T, sz=sz.T, rx=rx, rz=rz, wavelet=w, nbc=nbc, fd_order=fd_order, n_shots=2)
     o = oracle.elastic2d(vp, vs, rho, 5.0, 5e-4, nt, final=True, store="fp16", sv=SV, st=ST,
@@ -42,6 +46,33 @@ def test_fp16_batch_bitwise_vs_emulation(fomo, oracle, fd_order, nbc):
     for k, name in ((r.seis_vx, "seis_vx"), (r.seis_vz, "seis_vz")):
         e = rel_l2(k, ref[name])
         assert 1e-6 < e < 2e-2, (name, e)
+
+
+# variant,TX,CTAs per SM of the sweep's binary16 form: several strips (first and
+# last touch the FP32 columns), segment boundaries inside the z band
+@pytest.mark.parametrize("cfg", ["17,112,3", "18,56,2", "17,8,1", "18,40,1"])
+def test_fp16_sweep_configs_bitwise(fomo, oracle, monkeypatch, cfg):
+    from fomo_b200.synthetic import layered_elastic
+
+    monkeypatch.setenv("FOMO_SWEEP_CONFIG", cfg)
+    vp, vs, rho = layered_elastic(260, 90, n_layers=6, seed=21)
+    nt, nbc, fd_order = 150, 40, 10
+    rx = np.arange(1, 261, 6)
+    rz = np.full(rx.size, 4)
+    sx = np.array([[20], [240]])
+    sz = np.array([[4], [80]])
+    M = fd_order // 2
+    fin = np.zeros((260 + 2 * (nbc + M), 90 + 2 * (nbc + M), 5, 2), np.float32, order="F")
+    r = fomo.elastic2d_batch(vp, vs, rho, 5.0, 5e-4, nt, 20.0, sx=sx, sz=sz, rx=rx, rz=rz,
+                             nbc=nbc, fd_order=fd_order, precision="fp16", final_state=fin,
+                             kernel=2)
+    w = fomo.ricker_wavelet(20.0, 5e-4, nt).reshape(1, -1)
+    o = oracle.elastic2d(vp, vs, rho, 5.0, 5e-4, nt, sx=sx.T, sz=sz.T, rx=rx, rz=rz, wavelet=w,
+                         nbc=nbc, fd_order=fd_order, n_shots=2, final=True, store="fp16", sv=SV,
+                         st=ST, fp32_band=BAND)
+    assert np.array_equal(r.seis_vx, o["seis_vx"])
+    assert np.array_equal(r.seis_vz, o["seis_vz"])
+    assert np.array_equal(fin, o["final"])
 
 
 def test_fp16_single_equals_batch_and_snapshots(fomo, oracle):
