@@ -6,8 +6,9 @@ One "step" is one full elastic2d_batch run of the 32-shot batch (3000 time
 steps).  `value` is shots/s with model, acquisition and outputs resident in
 HBM (device entry point); `e2e` is the same metric through the public API
 with pinned host inputs, the H2D copies and the seismogram D2H inside the
-timed region.  Multi-GPU (torchrun): every rank runs its own 32 shots (shots
-are independent, no data-path collective), time = max over ranks.
+timed region.  Multi-GPU (torchrun): the job is 32 x N shots and every rank
+runs its own 32 (shots are independent, no data-path collective), time = max
+over ranks.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -116,6 +117,32 @@ def _dist():
     return world, rank, local
 
 
+def rank_config(shots_per_rank, world, rank):
+    """This rank's share of the job: the batch workload of shots_per_rank * world
+    shots (sources evenly along the surface), of which rank r runs shots
+    r * shots_per_rank .. (r + 1) * shots_per_rank - 1.  Shots are independent,
+    so the ranks need no data-path collective (weak scaling)."""
+    from fomo_b200.synthetic import elastic_batch_config
+
+    cfg = elastic_batch_config(n_shots=shots_per_rank * world)
+    lo = rank * shots_per_rank
+    cfg["sx"] = cfg["sx"][lo:lo + shots_per_rank].copy()
+    cfg["sz"] = cfg["sz"][lo:lo + shots_per_rank].copy()
+    return cfg
+
+
+def max_over_ranks(x, world, device):
+    """The maximum of x over all ranks (the job's time is its slowest rank's)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def cpu_baseline(cfg, target_s=12.0, threads=None):
     """The FP32 CPU oracle (OpenMP, all host threads) on a bounded sample:
     all 32 shots for a reduced number of time steps, scaled linearly to nt."""
@@ -216,13 +243,6 @@ def ours(args, cfg):
         if world > 1:
             torch.distributed.barrier()
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
-
     for _ in range(args.warmup):
         st = step()
     torch.cuda.synchronize()
@@ -242,7 +262,7 @@ def ours(args, cfg):
         torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
-    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, dev)
     clocks = clk.summary()
     value = ns * world / (ms * 1e-3)
     cells = st.cell_updates
@@ -289,7 +309,7 @@ def ours(args, cfg):
         e3.record(stream)
         torch.cuda.synchronize()
     barrier()
-    e2e_ms = max_over_ranks(e2.elapsed_time(e3) / args.steps)
+    e2e_ms = max_over_ranks(e2.elapsed_time(e3) / args.steps, world, dev)
     h2d = 3 * cfg["vp"].size * 4 + nt * 4 + 4 * 2 * (ns + nrec)
     d2h = r.seis_vx.nbytes + r.seis_vz.nbytes
 
@@ -454,9 +474,8 @@ def main():
             return
         secondary(args)
         return
-    from fomo_b200.synthetic import elastic_batch_config
-
-    cfg = elastic_batch_config(n_shots=args.shots)
+    world, rank, _ = _dist()
+    cfg = rank_config(args.shots, world, rank)
     cfg["nt"] = args.nt
     if args.no_cpu:
         os.environ["FOMO_BENCH_NO_CPU"] = "1"
