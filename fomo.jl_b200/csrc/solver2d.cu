@@ -315,6 +315,7 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
   size_t o_seis = P.dev ? 0 : ar.take<float>(std::max<long long>(outs.nseis * seis_n, 1));
   size_t o_snap = (!P.dev && outs.snaps && P.nsnap) ? ar.take<float>(P.nsnap * nint) : 0;
   size_t o_bounds = ar.take<long long>(kMaxGrid + 1);
+  size_t o_it = ar.take<int>(1);  // device step index of replayed chunks
   const bool sweep = kernel == FOMO_KERNEL_SINGLE_SWEEP;
   size_t o_pack = sweep ? ar.take<float>(sweep_pack_floats(P.nxp, P.nzp)) : 0;
   if ((rc = ensure_workspace(ctx, ar.off))) return rc;
@@ -435,7 +436,89 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
     if (int hr = hook->begin(ctx, st, P, d_wav)) return hr;
   FOMO_CU(ctx, cudaEventRecord(ctx->ev0, st));
   int A = 0, B = 1, C2 = 2;  // scalar: A = u^{n-1}, B = u^n, C2 = u^{n+1}
-  for (int it = 1; it <= P.nt; ++it) {
+  // Acoustic runs on small grids are bound by launch latency.  A chunk of K
+  // steps (velocity, pressure, inject/record; the interior snapshot where the
+  // step is a multiple of snap_interval; the advance of a device step index)
+  // is captured once and replayed; the remaining steps launch one by one.  K
+  // is even (a chunk returns the ping-pong buffers to their start) and a
+  // multiple of snap_interval, so every replay runs the same node sequence.
+  // Results are identical to step-by-step launches (FOMO_F_STEP_LAUNCH).
+  int it_first = 1;
+  cudaGraphExec_t chunk_exec = nullptr;
+  struct ExecGuard {  // the chunk's replays finish before it is destroyed, on every return path
+    cudaGraphExec_t& e;
+    cudaStream_t s;
+    ~ExecGuard() {
+      if (e) {
+        cudaStreamSynchronize(s);
+        cudaGraphExecDestroy(e);
+      }
+    }
+  } exec_guard{chunk_exec, st};
+  {
+    const bool chunks_ok = P.phys == kAcoustic && !P.fp16 && !hook && !prof &&
+                           !(opts && (opts->flags & FOMO_F_STEP_LAUNCH));
+    const int si = (d_snap && P.snap_interval > 0) ? P.snap_interval : 0;
+    int K = 0;
+    if (chunks_ok) {
+      if (si == 0) {
+        K = 64;
+      } else if (si <= 256) {
+        K = si * std::max(1, (64 + si / 2) / si);
+        if (K & 1) K *= 2;
+      }
+    }
+    const int nchunk = K > 0 ? P.nt / K : 0;
+    if (nchunk >= 2) {
+      int* d_it = ws_ptr<int>(ctx, o_it);
+      FOMO_CU(ctx, cudaMemsetAsync(d_it, 0, sizeof(int), st));
+      const cudaStream_t cs = ctx->own_stream;  // the caller's may be uncapturable
+      const float* bx = d_mat;
+      const float* bz = d_mat + P.plane;
+      const float* kap = d_mat + 2 * P.plane;
+      cudaGraph_t graph = nullptr;
+      cudaError_t ce = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+      if (ce == cudaSuccess) {
+        int a = A, b = B, nodes = 0;
+        for (int j = 0; j < K; ++j) {
+#define FOMO_ACC_CASE(NN)                                                                         \
+  case NN:                                                                                        \
+    k_ac_vel<NN><<<grd, blk, 0, cs>>>(g, c, dtx, dtz, h, field(a, 2), field(a, 0), field(a, 1),  \
+                                      bx, bz, field(b, 0), field(b, 1));                          \
+    k_ac_prs<NN><<<grd, blk, 0, cs>>>(g, c, dtx, dtz, h, field(a, 2), field(b, 0), field(b, 1),  \
+                                      kap, field(b, 2));                                          \
+    break;
+          switch (P.N) { FOMO_ACC_CASE(1) FOMO_ACC_CASE(2) FOMO_ACC_CASE(3) FOMO_ACC_CASE(4) FOMO_ACC_CASE(5) }
+#undef FOMO_ACC_CASE
+          k_inject_record_at<<<P.ns, 256, 0, cs>>>(d_it, j, P.nt, P.plane, P.n_src, d_src, d_wav,
+                                                   field(b, 2), nullptr, P.n_rec, d_rec,
+                                                   field(b, 2), field(b, 0), field(b, 1),
+                                                   d_seis[0], d_seis[1], d_seis[2]);
+          nodes += 3;
+          if (si && (j + 1) % si == 0) {
+            k_snap_at<<<dim3(cdiv(P.nx, 128), P.nz), 128, 0, cs>>>(
+                d_it, j, si, field(b, 2) + P.pad + (long long)P.pad * P.ld, P.ld, P.nx, P.nz,
+                d_snap);
+            ++nodes;
+          }
+          std::swap(a, b);
+        }
+        k_step_add<<<1, 1, 0, cs>>>(d_it, K);
+        ++nodes;
+        ce = cudaStreamEndCapture(cs, &graph);
+        if (ce == cudaSuccess) ce = cudaGraphInstantiate(&chunk_exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        for (int k = 0; ce == cudaSuccess && k < nchunk; ++k) ce = cudaGraphLaunch(chunk_exec, st);
+        if (ce == cudaSuccess) {
+          launches += nchunk * nodes;
+          it_first = nchunk * K + 1;
+        }
+      }
+      if (ce != cudaSuccess)
+        return fail(ctx, FOMO_ECUDA, std::string("replayed step chunk: ") + cudaGetErrorString(ce));
+    }
+  }
+  for (int it = it_first; it <= P.nt; ++it) {
     FOMO_CU(ctx, prof_mark(it, 0));
     if (P.phys == kElastic) {
       ElFields a{field(A, 0), field(A, 1), field(A, 2), field(A, 3), field(A, 4)};

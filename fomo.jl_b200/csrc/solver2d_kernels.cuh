@@ -374,12 +374,63 @@ __global__ void __launch_bounds__(256) k_sc_step(Geo2 g, D2Coef c, HabcDev h,
 //   inj0/inj1: fields receiving the wavelet (acoustic p; elastic txx,tzz;
 //              scalar u).  rec0..2: recorded fields (null = skip).
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ void inject_record_body(int it, int nt, long long plane, int n_src,
+                                                   const int* __restrict__ src_lin,
+                                                   const float* __restrict__ wav, float* inj0,
+                                                   float* inj1, int n_rec,
+                                                   const int* __restrict__ rec_lin,
+                                                   const float* rec0, const float* rec1,
+                                                   const float* rec2, float* __restrict__ s0,
+                                                   float* __restrict__ s1, float* __restrict__ s2);
+
 static __global__ void k_inject_record(int it, int nt, long long plane, int n_src,
                                 const int* __restrict__ src_lin, const float* __restrict__ wav,
                                 float* inj0, float* inj1, int n_rec,
                                 const int* __restrict__ rec_lin, const float* rec0,
                                 const float* rec1, const float* rec2, float* __restrict__ s0,
                                 float* __restrict__ s1, float* __restrict__ s2) {
+  inject_record_body(it, nt, plane, n_src, src_lin, wav, inj0, inj1, n_rec, rec_lin, rec0, rec1,
+                     rec2, s0, s1, s2);
+}
+
+// The same for step *it0 + j + 1: inside a captured chunk of steps the step
+// index lives in device memory (it0 = steps completed before the chunk).
+static __global__ void k_inject_record_at(const int* __restrict__ it0, int j, int nt,
+                                          long long plane, int n_src,
+                                          const int* __restrict__ src_lin,
+                                          const float* __restrict__ wav, float* inj0, float* inj1,
+                                          int n_rec, const int* __restrict__ rec_lin,
+                                          const float* rec0, const float* rec1, const float* rec2,
+                                          float* __restrict__ s0, float* __restrict__ s1,
+                                          float* __restrict__ s2) {
+  inject_record_body(*it0 + j + 1, nt, plane, n_src, src_lin, wav, inj0, inj1, n_rec, rec_lin,
+                     rec0, rec1, rec2, s0, s1, s2);
+}
+
+// Interior snapshot (nx x nz, x fastest) of step *it0 + j + 1 when that step
+// is a multiple of snap_interval (fused_kernels.jl:192-195).
+static __global__ void k_snap_at(const int* __restrict__ it0, int j, int snap_interval,
+                                 const float* __restrict__ src, long long ld, int nx, int nz,
+                                 float* __restrict__ snaps) {
+  const int it = *it0 + j + 1;
+  if (it % snap_interval) return;
+  float* dst = snaps + (long long)(it / snap_interval - 1) * nx * nz;
+  const int z = blockIdx.y;
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < nx; x += gridDim.x * blockDim.x)
+    dst[(long long)z * nx + x] = src[(long long)z * ld + x];
+}
+
+// Advances the device step index by the chunk length.
+static __global__ void k_step_add(int* it0, int k) { *it0 += k; }
+
+__device__ __forceinline__ void inject_record_body(int it, int nt, long long plane, int n_src,
+                                                   const int* __restrict__ src_lin,
+                                                   const float* __restrict__ wav, float* inj0,
+                                                   float* inj1, int n_rec,
+                                                   const int* __restrict__ rec_lin,
+                                                   const float* rec0, const float* rec1,
+                                                   const float* rec2, float* __restrict__ s0,
+                                                   float* __restrict__ s1, float* __restrict__ s2) {
   const int s = blockIdx.x;
   const long long so = (long long)s * plane;
   if (threadIdx.x == 0) {

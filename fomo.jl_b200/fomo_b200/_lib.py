@@ -22,6 +22,7 @@ FOMO_EUNSUPPORTED = -5
 
 FOMO_F_DEVICE_PTRS = 1
 FOMO_F_PROFILE = 2
+FOMO_F_STEP_LAUNCH = 4
 FOMO_FP32, FOMO_FP16, FOMO_BF16 = 0, 1, 2
 FOMO_KERNEL_AUTO, FOMO_KERNEL_TWO_PHASE, FOMO_KERNEL_SINGLE_SWEEP = 0, 1, 2
 

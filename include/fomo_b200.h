@@ -53,6 +53,8 @@ extern "C" {
 /* fomo_opts.flags */
 #define FOMO_F_DEVICE_PTRS 1u /* every array argument is a device pointer */
 #define FOMO_F_PROFILE 2u     /* time the sweep kernels of a window of steps  */
+#define FOMO_F_STEP_LAUNCH 4u /* launch every time step from the host (no      */
+                              /* replayed CUDA-graph chunks; same results)      */
 
 /* fomo_opts.precision: storage format of wavefields and material arrays */
 #define FOMO_FP32 0

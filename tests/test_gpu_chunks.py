@@ -1,0 +1,100 @@
+"""Acoustic runs replay captured chunks of time steps (CUDA graphs with a device
+step index); the results must equal step-by-step launches bit for bit."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture
+def step_launch(monkeypatch, fomo):
+    """Calls made through this fixture's function launch every step from the host."""
+    from fomo_b200 import _lib as L
+
+    orig = fomo.api._opts
+
+    def run(fn, *a, **kw):
+        def opts(*oa, **okw):
+            o = orig(*oa, **okw)
+            o.flags |= L.FOMO_F_STEP_LAUNCH
+            return o
+
+        monkeypatch.setattr(fomo.api, "_opts", opts)
+        try:
+            return fn(*a, **kw)
+        finally:
+            monkeypatch.setattr(fomo.api, "_opts", orig)
+
+    return run
+
+
+def _model():
+    from fomo_b200.synthetic import two_layer
+
+    vp, rho = two_layer(90, 60)
+    vp = vp.copy(order="F")
+    vp[:, 0] = 0.0
+    rho = rho.copy(order="F")
+    rho[:, 0] = 0.0
+    return vp, rho
+
+
+def test_acoustic2d_chunks_equal_step_launches(fomo, step_launch):
+    """Snapshots every 50 steps, 230 steps: four replayed 50-step chunks and a
+    30-step remainder launched step by step."""
+    vp, rho = _model()
+    nt, nbc, order = 230, 12, 8
+    rx = np.arange(1, 91, 3)
+    rz = np.full(rx.size, 8)
+    kw = dict(sx=[45], sz=[10], rx=rx, rz=rz, nbc=nbc, fd_order=order, snap_interval=50)
+    shape = (90 + 2 * (nbc + 4), 60 + 2 * (nbc + 4), 3)
+    fa = np.zeros(shape, np.float32, order="F")
+    fb = np.zeros(shape, np.float32, order="F")
+    a = fomo.acoustic2d(vp, rho, 10.0, 1e-3, nt, 15.0, final_state=fa, **kw)
+    la = fomo.api.last_stats.gpu_launches
+    b = step_launch(fomo.acoustic2d, vp, rho, 10.0, 1e-3, nt, 15.0, final_state=fb, **kw)
+    lb = fomo.api.last_stats.gpu_launches
+    for x, y in ((a.seis_p, b.seis_p), (a.seis_vx, b.seis_vx), (a.seis_vz, b.seis_vz)):
+        assert np.array_equal(x, y)
+    assert len(a.snaps) == len(b.snaps) == 4
+    for x, y in zip(a.snaps, b.snaps):
+        assert np.array_equal(x, y)
+    assert np.array_equal(fa, fb)
+    assert np.abs(a.seis_p).max() > 0
+    # per chunk the replay adds a snapshot kernel and the step-index node (the
+    # step-by-step path copies snapshots with cudaMemcpy2DAsync)
+    assert la == lb + 8
+
+
+def test_acoustic2d_batch_chunks_equal_step_launches(fomo, step_launch):
+    """Two shots, no snapshots, 200 steps: three 64-step chunks and 8 single steps."""
+    vp, rho = _model()
+    nt = 200
+    rx = np.arange(1, 91, 4)
+    rz = np.full(rx.size, 6)
+    kw = dict(sx=[[20], [70]], sz=[[10], [30]], rx=rx, rz=rz, nbc=10, fd_order=6)
+    a = fomo.acoustic2d_batch(vp, rho, 10.0, 1e-3, nt, 15.0, **kw)
+    b = step_launch(fomo.acoustic2d_batch, vp, rho, 10.0, 1e-3, nt, 15.0, **kw)
+    for x, y in ((a.seis_p, b.seis_p), (a.seis_vx, b.seis_vx), (a.seis_vz, b.seis_vz)):
+        assert np.array_equal(x, y)
+    assert not np.array_equal(a.seis_p[:, :, 0], a.seis_p[:, :, 1])
+
+
+def test_acoustic2d_chunks_on_legacy_default_stream(fomo):
+    """The chunk is captured on the context's own stream, so a context that
+    borrows the legacy default stream (torch's default) still replays it."""
+    import torch
+
+    from fomo_b200 import _lib as L
+
+    vp, rho = _model()
+    kw = dict(sx=[45], sz=[10], rx=np.arange(1, 91, 5), rz=np.full(18, 8), nbc=10, fd_order=8)
+    ctx = L.context(0)
+    ctx.use_torch_stream(torch.cuda.current_stream())
+    try:
+        a = fomo.acoustic2d(vp, rho, 10.0, 1e-3, 150, 15.0, **kw)
+    finally:
+        ctx.set_stream(None)
+    b = fomo.acoustic2d(vp, rho, 10.0, 1e-3, 150, 15.0, **kw)
+    assert np.array_equal(a.seis_p, b.seis_p)
+    assert np.array_equal(a.seis_vz, b.seis_vz)
