@@ -436,13 +436,14 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
     if (int hr = hook->begin(ctx, st, P, d_wav)) return hr;
   FOMO_CU(ctx, cudaEventRecord(ctx->ev0, st));
   int A = 0, B = 1, C2 = 2;  // scalar: A = u^{n-1}, B = u^n, C2 = u^{n+1}
-  // Acoustic runs on small grids are bound by launch latency.  A chunk of K
-  // steps (velocity, pressure, inject/record; the interior snapshot where the
-  // step is a multiple of snap_interval; the advance of a device step index)
-  // is captured once and replayed; the remaining steps launch one by one.  K
-  // is even (a chunk returns the ping-pong buffers to their start) and a
-  // multiple of snap_interval, so every replay runs the same node sequence.
-  // Results are identical to step-by-step launches (FOMO_F_STEP_LAUNCH).
+  // Acoustic and scalar runs on small grids are bound by launch latency.  A
+  // chunk of K steps (the updates, inject/record; the interior snapshot where
+  // the step is a multiple of snap_interval; the advance of a device step
+  // index) is captured once and replayed; the remaining steps launch one by
+  // one.  K is a multiple of the buffer rotation (2 acoustic, 3 scalar: a chunk
+  // returns the buffers to their start) and of snap_interval, so every replay
+  // runs the same node sequence.  Results are identical to step-by-step
+  // launches (FOMO_F_STEP_LAUNCH).
   int it_first = 1;
   cudaGraphExec_t chunk_exec = nullptr;
   struct ExecGuard {  // the chunk's replays finish before it is destroyed, on every return path
@@ -456,16 +457,18 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
     }
   } exec_guard{chunk_exec, st};
   {
-    const bool chunks_ok = P.phys == kAcoustic && !P.fp16 && !hook && !prof &&
+    const bool scalar = P.phys == kScalar;
+    const bool chunks_ok = (P.phys == kAcoustic || scalar) && !P.fp16 && !hook && !prof &&
                            !(opts && (opts->flags & FOMO_F_STEP_LAUNCH));
-    const int si = (d_snap && P.snap_interval > 0) ? P.snap_interval : 0;
+    const int si = (!scalar && d_snap && P.snap_interval > 0) ? P.snap_interval : 0;
+    const int period = scalar ? 3 : 2;  // buffer rotation: scalar u^{n-1}, u^n, u^{n+1}
     int K = 0;
-    if (chunks_ok) {
+    if (chunks_ok && (scalar ? !d_snap : true)) {
       if (si == 0) {
-        K = 64;
+        K = 64 / period * period;
       } else if (si <= 256) {
         K = si * std::max(1, (64 + si / 2) / si);
-        if (K & 1) K *= 2;
+        if (K % period) K *= period;
       }
     }
     const int nchunk = K > 0 ? P.nt / K : 0;
@@ -478,7 +481,38 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
       const float* kap = d_mat + 2 * P.plane;
       cudaGraph_t graph = nullptr;
       cudaError_t ce = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
-      if (ce == cudaSuccess) {
+      if (ce == cudaSuccess && scalar) {
+        D2Coef dc;
+        dc.two_c0 = 2.0f * kD2C0[P.N];
+        for (int l = 0; l < 5; ++l) dc.d[l] = kD2[P.N][l];
+        int a = A, b = B, n = C2, nodes = 0;
+        for (int j = 0; j < K; ++j) {
+#define FOMO_SCC_CASE(NN)                                                                 \
+  case NN:                                                                                \
+    k_sc_step<NN><<<grd, blk, 0, cs>>>(g, dc, h, field(b, 0), field(a, 0), d_mat, field(n, 0)); \
+    break;
+          switch (P.N) { FOMO_SCC_CASE(1) FOMO_SCC_CASE(2) FOMO_SCC_CASE(3) FOMO_SCC_CASE(4) FOMO_SCC_CASE(5) }
+#undef FOMO_SCC_CASE
+          k_inject_record_at<<<1, 256, 0, cs>>>(d_it, j, P.nt, P.plane, P.n_src, d_src, d_wav,
+                                                field(n, 0), nullptr, P.n_rec, d_rec, field(n, 0),
+                                                nullptr, nullptr, d_seis[0], nullptr, nullptr);
+          nodes += 2;
+          const int t = a;
+          a = b;
+          b = n;
+          n = t;
+        }
+        k_step_add<<<1, 1, 0, cs>>>(d_it, K);
+        ++nodes;
+        ce = cudaStreamEndCapture(cs, &graph);
+        if (ce == cudaSuccess) ce = cudaGraphInstantiate(&chunk_exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        for (int k = 0; ce == cudaSuccess && k < nchunk; ++k) ce = cudaGraphLaunch(chunk_exec, st);
+        if (ce == cudaSuccess) {
+          launches += nchunk * nodes;
+          it_first = nchunk * K + 1;
+        }
+      } else if (ce == cudaSuccess) {
         int a = A, b = B, nodes = 0;
         for (int j = 0; j < K; ++j) {
 #define FOMO_ACC_CASE(NN)                                                                         \

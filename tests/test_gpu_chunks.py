@@ -98,3 +98,17 @@ def test_acoustic2d_chunks_on_legacy_default_stream(fomo):
     b = fomo.acoustic2d(vp, rho, 10.0, 1e-3, 150, 15.0, **kw)
     assert np.array_equal(a.seis_p, b.seis_p)
     assert np.array_equal(a.seis_vz, b.seis_vz)
+
+
+def test_scalar2d_chunks_equal_step_launches(fomo, step_launch):
+    """scalar2d rotates three buffers: 200 steps are three 63-step chunks and
+    11 single steps."""
+    from fomo_b200.synthetic import two_layer
+
+    vp, _ = two_layer(80, 50)
+    rx = np.arange(1, 81, 3)
+    kw = dict(sx=[40], sz=[12], rx=rx, rz=np.full(rx.size, 6), nbc=10, fd_order=8)
+    a = fomo.scalar2d(vp, 10.0, 1e-3, 200, 15.0, **kw)
+    b = step_launch(fomo.scalar2d, vp, 10.0, 1e-3, 200, 15.0, **kw)
+    assert np.array_equal(a.seis_u, b.seis_u)
+    assert np.abs(a.seis_u).max() > 0
