@@ -520,34 +520,40 @@ inline Frame3 make_frame3(const Geo3& g) {
   return f;
 }
 
-__device__ __forceinline__ void frame3_xyz(const Geo3& g, const Frame3& fr, long long idx, int& x,
+// idx -> (x, y, z) in 32-bit arithmetic (the host keeps frames below 2^31 cells)
+__device__ __forceinline__ void frame3_xyz(const Geo3& g, const Frame3& fr, long long idx_, int& x,
                                            int& y, int& z) {
-  if (idx < 2 * fr.slab) {
-    const long long t = idx < fr.slab ? idx : idx - fr.slab;
-    const long long plane = (long long)fr.Wx * fr.Wy;
-    const int kz = (int)(t / plane);
-    const long long r = t - kz * plane;
-    y = 1 + (int)(r / fr.Wx);
-    x = 1 + (int)(r % fr.Wx);
-    z = idx < fr.slab ? 1 + kz : g.nz - 1 - g.nbc + kz;
+  const unsigned idx = (unsigned)idx_;
+  const unsigned slab = (unsigned)fr.slab, wx = (unsigned)fr.Wx;
+  if (idx < 2u * slab) {
+    const unsigned t = idx < slab ? idx : idx - slab;
+    const unsigned plane = wx * (unsigned)fr.Wy;
+    const unsigned kz = t / plane;
+    const unsigned r = t - kz * plane;
+    const unsigned jy = r / wx;
+    y = 1 + (int)jy;
+    x = 1 + (int)(r - jy * wx);
+    z = idx < slab ? 1 + (int)kz : g.nz - 1 - g.nbc + (int)kz;
     return;
   }
-  const long long t = idx - 2 * fr.slab;
-  const int kz = (int)(t / fr.ring);
-  long long r = t - (long long)kz * fr.ring;
-  z = g.nbc + 1 + kz;
-  const long long band = (long long)fr.Wx * g.nbc;
-  if (r < 2 * band) {  // y bands
-    const long long u = r < band ? r : r - band;
-    const int jy = (int)(u / fr.Wx);
-    x = 1 + (int)(u % fr.Wx);
-    y = r < band ? 1 + jy : g.ny - 1 - g.nbc + jy;
+  const unsigned t = idx - 2u * slab;
+  const unsigned ring = (unsigned)fr.ring;
+  const unsigned kz = t / ring;
+  const unsigned r = t - kz * ring;
+  z = g.nbc + 1 + (int)kz;
+  const unsigned band = wx * (unsigned)g.nbc;
+  if (r < 2u * band) {  // y bands
+    const unsigned u = r < band ? r : r - band;
+    const unsigned jy = u / wx;
+    x = 1 + (int)(u - jy * wx);
+    y = r < band ? 1 + (int)jy : g.ny - 1 - g.nbc + (int)jy;
   } else {  // x bands of the middle y rows
-    const long long u = r - 2 * band;
-    const int jy = (int)(u / (2 * g.nbc));
-    const int ix = (int)(u % (2 * g.nbc));
-    y = g.nbc + 1 + jy;
-    x = ix < g.nbc ? 1 + ix : g.nx - 1 - g.nbc + (ix - g.nbc);
+    const unsigned u = r - 2u * band;
+    const unsigned nb2 = 2u * (unsigned)g.nbc;
+    const unsigned jy = u / nb2;
+    const unsigned ix = u - jy * nb2;
+    y = g.nbc + 1 + (int)jy;
+    x = ix < (unsigned)g.nbc ? 1 + (int)ix : g.nx - 1 - g.nbc + ((int)ix - g.nbc);
   }
 }
 
@@ -793,6 +799,8 @@ int run3d(fomo_ctx* ctx, bool elastic, const fomo_grid3d* gp, const float* vp, c
   const int nfield = elastic ? 9 : 4;  // vx vy vz (txx tyy tzz txy txz tyz | p)
   const int nmat = elastic ? 8 : 4;
   const Frame3 fr = make_frame3(g);
+  if (fr.total >= (1LL << 31))  // the frame enumeration uses 32-bit indices
+    return fail(ctx, FOMO_EARG, "3D grid too large: the HABC frame exceeds 2^31 cells");
   const int nphase_max = elastic ? 6 : 3;
   const long long seis_n = (long long)acq->n_rec * nt;
   const long long snap_sz = snap_plane == 0 ? (long long)nx * nz
