@@ -16,6 +16,7 @@ Secondary workloads (one JSON line each, same keys; not the default line):
     --workload elastic-fp16   the same batch with binary16 wavefield storage
     --workload uneven         64 acoustic shots on grids of uneven size (graph run)
     --workload elastic3d      elastic3d 400x400x300, nbc 40, order 8 (nt from --nt)
+    --workload readme         steps/s on the grids of Fomo's published throughput table
 """
 from __future__ import annotations
 
@@ -453,6 +454,53 @@ def secondary(args):
         print(json.dumps(line), flush=True)
 
 
+# Fomo's published throughput (README.md "Performance & Reproducibility", RTX 3060,
+# Float32, HABC, fd_order 8, nbc 50): steps/s per interior grid.
+README_STEPS = {
+    "acoustic2d": {(240, 200): 25000, (500, 400): 11800, (1000, 800): 4400, (2000, 1600): 1300},
+    "scalar2d": {(240, 200): 24400, (500, 400): 23800, (1000, 800): 11800, (2000, 1600): 4100},
+    "elastic2d": {(240, 200): 17000, (500, 400): 7700, (1000, 800): 2600},
+}
+
+
+def readme_grids(args):
+    """Steps/s of the single-shot solvers on the reference's published grids, with
+    the setup of its benchmark scripts (test/bench_fused.jl, bench_batch_v2.jl):
+    dh 10 m, dt 1 ms, 15 Hz, vp 3000 m/s over 3800 m/s below mid-depth, rho 2200,
+    vs = vp / 1.8, source at (nx/2, 8), receivers every 5th x at depth 6, nbc 50,
+    order 8.  Steps/s from the library's CUDA-event time of the time loop."""
+    import warnings
+
+    import fomo_b200 as F
+
+    warnings.simplefilter("ignore")
+    nt = args.nt if args.nt != 3000 else 1000
+    for eq, table in README_STEPS.items():
+        for (nx, nz), ref in table.items():
+            vp = np.full((nx, nz), 3000.0, np.float32, order="F")
+            vp[:, nz // 2 - 1:] = 3800.0
+            rho = np.full((nx, nz), 2200.0, np.float32, order="F")
+            rx = np.arange(10, nx - 9, 5)
+            kw = dict(sx=[nx // 2], sz=[8], rx=rx, rz=np.full(rx.size, 6), nbc=50, fd_order=8)
+
+            def run():
+                if eq == "acoustic2d":
+                    return F.acoustic2d(vp, rho, 10.0, 1e-3, nt, 15.0, **kw).stats.kernel_time_s
+                if eq == "scalar2d":
+                    return F.scalar2d(vp, 10.0, 1e-3, nt, 15.0, **kw).stats.kernel_time_s
+                vs = (vp / np.float32(1.8)).astype(np.float32)
+                return F.elastic2d(vp, vs, rho, 10.0, 1e-3, nt, 15.0, **kw).stats.kernel_time_s
+
+            for _ in range(max(1, args.warmup)):
+                run()
+            t = float(np.median([run() for _ in range(max(1, args.steps))]))
+            sps = nt / t
+            print(json.dumps({"workload": "reference README grids", "equation": eq,
+                              "grid": [nx, nz], "nt": nt, "steps_per_s": sps,
+                              "reference_rtx3060_steps_per_s": ref, "ratio": sps / ref,
+                              "device": "B200", "dtype": "f32"}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -464,9 +512,17 @@ def main():
     ap.add_argument("--nt", type=int, default=3000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", choices=["elastic-batch", "elastic-fp16", "uneven", "elastic3d"],
+    ap.add_argument("--workload", choices=["elastic-batch", "elastic-fp16", "uneven", "elastic3d",
+                                           "readme"],
                     default="elastic-batch")
     args = ap.parse_args()
+    if args.workload == "readme":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference's README grids "
+                              "are compared against its published RTX 3060 figures"}))
+            return
+        readme_grids(args)
+        return
     if args.workload != "elastic-batch":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "reference arm is measured on "

@@ -436,8 +436,8 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
     if (int hr = hook->begin(ctx, st, P, d_wav)) return hr;
   FOMO_CU(ctx, cudaEventRecord(ctx->ev0, st));
   int A = 0, B = 1, C2 = 2;  // scalar: A = u^{n-1}, B = u^n, C2 = u^{n+1}
-  // Acoustic and scalar runs on small grids are bound by launch latency.  A
-  // chunk of K steps (the updates, inject/record; the interior snapshot where
+  // Acoustic, scalar and two-phase elastic runs on small grids are bound by
+  // launch latency.  A chunk of K steps (the updates, inject/record; the interior snapshot where
   // the step is a multiple of snap_interval; the advance of a device step
   // index) is captured once and replayed; the remaining steps launch one by
   // one.  K is a multiple of the buffer rotation (2 acoustic, 3 scalar: a chunk
@@ -458,8 +458,9 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
   } exec_guard{chunk_exec, st};
   {
     const bool scalar = P.phys == kScalar;
-    const bool chunks_ok = (P.phys == kAcoustic || scalar) && !P.fp16 && !hook && !prof &&
-                           !(opts && (opts->flags & FOMO_F_STEP_LAUNCH));
+    const bool elastic = P.phys == kElastic;
+    const bool chunks_ok = (!elastic || kernel == FOMO_KERNEL_TWO_PHASE) && !P.fp16 && !hook &&
+                           !prof && !(opts && (opts->flags & FOMO_F_STEP_LAUNCH));
     const int si = (!scalar && d_snap && P.snap_interval > 0) ? P.snap_interval : 0;
     const int period = scalar ? 3 : 2;  // buffer rotation: scalar u^{n-1}, u^n, u^{n+1}
     int K = 0;
@@ -501,6 +502,42 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
           a = b;
           b = n;
           n = t;
+        }
+        k_step_add<<<1, 1, 0, cs>>>(d_it, K);
+        ++nodes;
+        ce = cudaStreamEndCapture(cs, &graph);
+        if (ce == cudaSuccess) ce = cudaGraphInstantiate(&chunk_exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        for (int k = 0; ce == cudaSuccess && k < nchunk; ++k) ce = cudaGraphLaunch(chunk_exec, st);
+        if (ce == cudaSuccess) {
+          launches += nchunk * nodes;
+          it_first = nchunk * K + 1;
+        }
+      } else if (ce == cudaSuccess && elastic) {
+        const ElMat& m = emat;
+        int a = A, b = B, nodes = 0;
+        for (int j = 0; j < K; ++j) {
+          ElFields fa{field(a, 0), field(a, 1), field(a, 2), field(a, 3), field(a, 4)};
+#define FOMO_ELC_CASE(NN)                                                                     \
+  case NN:                                                                                    \
+    k_el_vel<NN><<<grd, blk, 0, cs>>>(g, c, dtx, dtz, h, fa, m, field(b, 0), field(b, 1));    \
+    k_el_str<NN><<<grd, blk, 0, cs>>>(g, c, dtx, dtz, h, fa, field(b, 0), field(b, 1), m,     \
+                                      field(b, 2), field(b, 3), field(b, 4));                 \
+    break;
+          switch (P.N) { FOMO_ELC_CASE(1) FOMO_ELC_CASE(2) FOMO_ELC_CASE(3) FOMO_ELC_CASE(4) FOMO_ELC_CASE(5) }
+#undef FOMO_ELC_CASE
+          k_inject_record_at<<<P.ns, 256, 0, cs>>>(d_it, j, P.nt, P.plane, P.n_src, d_src, d_wav,
+                                                   field(b, 2), field(b, 3), P.n_rec, d_rec,
+                                                   field(b, 0), field(b, 1), nullptr, d_seis[0],
+                                                   d_seis[1], nullptr);
+          nodes += 3;
+          if (si && (j + 1) % si == 0) {
+            k_snap_at<<<dim3(cdiv(P.nx, 128), P.nz), 128, 0, cs>>>(
+                d_it, j, si, field(b, 1) + P.pad + (long long)P.pad * P.ld, P.ld, P.nx, P.nz,
+                d_snap);
+            ++nodes;
+          }
+          std::swap(a, b);
         }
         k_step_add<<<1, 1, 0, cs>>>(d_it, K);
         ++nodes;

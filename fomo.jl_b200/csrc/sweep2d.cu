@@ -2740,12 +2740,16 @@ size_t smem_for(int N, int variant, int W, int wstride) {
 
 }  // namespace
 
+// The single sweep pays off on large batches; a small problem gives each CTA
+// only a few rows, and the z-segment warm-up then dominates.  Measured (order
+// 8, one shot): 240x200 two-phase 61 k vs sweep 36 k steps/s, 1000x800 24.9 k vs
+// 22.6 k; the 32-shot 1170x670 batch (25 M cell-shots) 0.49 vs 1.0 ms per step
+// for the sweep.
 int pick_kernel_2d(int phys, int N, int nxp, int nzp, int ns) {
   (void)N;
-  (void)nxp;
-  (void)nzp;
-  (void)ns;
-  return phys == 1 && encoder() ? FOMO_KERNEL_SINGLE_SWEEP : FOMO_KERNEL_TWO_PHASE;
+  const double work = (double)nxp * nzp * ns;  // cell-updates per step
+  return phys == 1 && encoder() && work >= 4.0e6 ? FOMO_KERNEL_SINGLE_SWEEP
+                                                  : FOMO_KERNEL_TWO_PHASE;
 }
 
 bool sweep2d_supported(int phys, int N) { return phys == 1 && N >= 1 && N <= 5 && encoder(); }

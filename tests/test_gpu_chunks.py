@@ -112,3 +112,22 @@ def test_scalar2d_chunks_equal_step_launches(fomo, step_launch):
     b = step_launch(fomo.scalar2d, vp, 10.0, 1e-3, 200, 15.0, **kw)
     assert np.array_equal(a.seis_u, b.seis_u)
     assert np.abs(a.seis_u).max() > 0
+
+
+def test_elastic2d_two_phase_chunks_equal_step_launches(fomo, step_launch):
+    """Two-phase elastic2d with vz snapshots every 40 steps, 190 steps: two
+    80-step chunks and 30 single steps."""
+    from fomo_b200.synthetic import layered_elastic
+
+    vp, vs, rho = layered_elastic(70, 50, n_layers=4, seed=5)
+    rx = np.arange(1, 71, 3)
+    kw = dict(sx=[35], sz=[6], rx=rx, rz=np.full(rx.size, 5), nbc=10, fd_order=8,
+              snap_interval=40, kernel=1)
+    a = fomo.elastic2d(vp, vs, rho, 5.0, 5e-4, 190, 20.0, **kw)
+    b = step_launch(fomo.elastic2d, vp, vs, rho, 5.0, 5e-4, 190, 20.0, **kw)
+    assert np.array_equal(a.seis_vx, b.seis_vx)
+    assert np.array_equal(a.seis_vz, b.seis_vz)
+    assert len(a.snaps) == 4
+    for x, y in zip(a.snaps, b.snaps):
+        assert np.array_equal(x, y)
+    assert np.abs(a.seis_vz).max() > 0
