@@ -16,8 +16,8 @@ physical point source: the coarse raw wavelet is the fine one times
 (dh_fine / dh_coarse)^2, because a point source of strength w on a grid of
 spacing dh injects w * dh^2 worth of source density.
 
-The plain fine-grid method stays the fallback and the judge of the error
-(``evaluate``).
+The plain fine-grid method stays the fallback and the reference that the
+error is measured against (``evaluate``).
 """
 from __future__ import annotations
 

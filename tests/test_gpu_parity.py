@@ -3,7 +3,7 @@
 The kernels spell out the oracle's rounding sequence, so FP32 results are
 compared BIT-EXACTLY (seismograms, snapshots, final wavefields, device-prepared
 materials).  The FP64 oracle of the same scheme gives the reported error
-(tolerance 1e-5 relative L2, the north-star parity bar).
+(tolerance 1e-5 relative L2).
 """
 import numpy as np
 import pytest
