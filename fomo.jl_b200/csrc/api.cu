@@ -90,6 +90,16 @@ HabcHost make_habc(int pad, float v_ref, float dt, float dh) {
   return h;
 }
 
+std::vector<float> sponge_table(int nbc, float factor) {
+  std::vector<float> t((size_t)std::max(nbc, 0));
+  for (int d = 0; d < nbc; ++d) {
+    const float r = factor * (float)(nbc - d);
+    const float rr = r * r;
+    t[(size_t)d] = (float)std::exp(-(double)rr);
+  }
+  return t;
+}
+
 }  // namespace fomo
 
 using namespace fomo;

@@ -71,7 +71,12 @@ struct HabcHost {
   int wstride;
 };
 HabcHost make_habc(int pad, float v_ref, float dt, float dh);
+// Cerjan sponge damping by distance to the padded edge, d = 0 .. nbc-1
+// (boundary/sponge.jl:31-48): exp(-r^2), r = factor * (nbc - d) in float32, the
+// exponential in double rounded once to float32.
+std::vector<float> sponge_table(int nbc, float factor);
 
+// In sponge mode nbc is the user's layer count and wtab the sponge_table.
 struct HabcDev {
   float q, qt, qxt;
   int nbc;

@@ -37,6 +37,8 @@ struct Plan2 {
   int snap_interval, nsnap;
   int kernel;
   bool fp16 = false;  // elastic: binary16 wavefield storage (mixed2d.cuh)
+  bool sponge = false;  // boundary = :sponge (FOMO_F_SPONGE) instead of HABC
+  float sponge_factor = 0.015f;
 };
 
 int check_indices(fomo_ctx* ctx, const char* what, const int32_t* ix, const int32_t* iz,
@@ -110,6 +112,17 @@ int make_plan(fomo_ctx* ctx, Phys phys, const fomo_grid2d* g, const fomo_acq* ac
     return fail(ctx, FOMO_EUNSUPPORTED,
                 phys == kElastic ? "elastic2d stores FP32 or FP16 (BF16 is not accurate enough)"
                                  : "this solver stores FP32 only");
+  }
+  if (opts && (opts->flags & FOMO_F_SPONGE)) {  // acoustic2d.jl:65-87, elastic2d.jl:63-87
+    if (phys == kScalar)
+      return fail(ctx, FOMO_EUNSUPPORTED, "scalar2d has no sponge boundary (HABC only)");
+    if (P.fp16) return fail(ctx, FOMO_EUNSUPPORTED, "the sponge boundary stores FP32 only");
+    if (P.kernel == FOMO_KERNEL_SINGLE_SWEEP)
+      return fail(ctx, FOMO_EUNSUPPORTED, "the sponge boundary runs the two-phase kernels");
+    if (!(opts->sponge_factor >= 0.0f) || !std::isfinite(opts->sponge_factor))
+      return fail(ctx, FOMO_EARG, "sponge_factor must be finite and >= 0");
+    P.sponge = true;
+    P.sponge_factor = opts->sponge_factor;
   }
   if ((long long)P.nxp * P.nzp > (1LL << 31))
     return fail(ctx, FOMO_EARG, "padded grid exceeds 2^31 cells");
@@ -284,6 +297,7 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
   for (int r = 0; r < P.n_rec; ++r) rec_lin[r] = (hrx[r] - 1 + P.pad) + P.ld * (hrz[r] - 1 + P.pad);
 
   // ---- v_ref default: minimum(vp > 0) (acoustic2d.jl:55) ----
+  if (P.sponge && !(P.v_ref > 0.0f)) P.v_ref = 1.0f;  // v_ref is ignored with the sponge
   if (!(P.v_ref > 0.0f)) {
     std::vector<float> hvp;
     if ((rc = host_copy(ctx, vp, nint, P.dev, hvp))) return rc;
@@ -293,6 +307,7 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
   HabcHost hh = make_habc(P.pad, P.v_ref, P.dt, P.dh);
 
   int kernel = P.kernel;
+  if (P.sponge) kernel = FOMO_KERNEL_TWO_PHASE;
   if (kernel == FOMO_KERNEL_AUTO) kernel = pick_kernel_2d((int)P.phys, P.N, P.nxp, P.nzp, P.ns);
   if (kernel == FOMO_KERNEL_SINGLE_SWEEP && !sweep2d_supported((int)P.phys, P.N))
     kernel = FOMO_KERNEL_TWO_PHASE;
@@ -308,6 +323,8 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
   size_t o_state = ar.take<float>((long long)nsets * nfield * P.ns * P.plane);
   size_t o_state16 = P.fp16 ? ar.take<__half>((long long)nsets * nfield * P.ns * P.plane) : 0;
   size_t o_unpack = (P.fp16 && opts && opts->final_state) ? ar.take<float>(P.nxp * (long long)P.nzp) : 0;
+  const std::vector<float> damp = P.sponge ? sponge_table(P.nbc, P.sponge_factor) : std::vector<float>();
+  if (P.sponge) hh.wtab = damp.empty() ? std::vector<float>(1, 1.0f) : damp;
   size_t o_w = ar.take<float>(hh.wtab.size());
   size_t o_src = ar.take<int32_t>(std::max<long long>(nsrc_all, 1));
   size_t o_rec = ar.take<int32_t>(std::max(P.n_rec, 1));
@@ -384,7 +401,7 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
   Geo2 g{P.nxp, P.nzp, P.ld, P.M, hh.nbc, P.plane};
   Coef c;
   for (int l = 0; l < 5; ++l) c.a[l] = kFD[P.N][l];
-  HabcDev h{hh.q, hh.qt, hh.qxt, hh.nbc, hh.wstride, d_w};
+  HabcDev h{hh.q, hh.qt, hh.qxt, P.sponge ? P.nbc : hh.nbc, hh.wstride, d_w};
   const float dtx = dtdh, dtz = dtdh;
   auto field = [&](int set, int f) { return d_state + ((long long)set * nfield + f) * P.ns * P.plane; };
   auto hfield = [&](int set, int f) {
@@ -518,13 +535,23 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
         int a = A, b = B, nodes = 0;
         for (int j = 0; j < K; ++j) {
           ElFields fa{field(a, 0), field(a, 1), field(a, 2), field(a, 3), field(a, 4)};
-#define FOMO_ELC_CASE(NN)                                                                     \
-  case NN:                                                                                    \
-    k_el_vel<NN><<<grd, blk, 0, cs>>>(g, c, dtx, dtz, h, fa, m, field(b, 0), field(b, 1));    \
-    k_el_str<NN><<<grd, blk, 0, cs>>>(g, c, dtx, dtz, h, fa, field(b, 0), field(b, 1), m,     \
-                                      field(b, 2), field(b, 3), field(b, 4));                 \
+#define FOMO_ELC_CASE(NN, SPV)                                                                  \
+  case NN:                                                                                      \
+    k_el_vel<NN, SPV><<<grd, blk, 0, cs>>>(g, c, dtx, dtz, h, fa, m, field(b, 0), field(b, 1)); \
+    k_el_str<NN, SPV><<<grd, blk, 0, cs>>>(g, c, dtx, dtz, h, fa, field(b, 0), field(b, 1), m,  \
+                                           field(b, 2), field(b, 3), field(b, 4));              \
     break;
-          switch (P.N) { FOMO_ELC_CASE(1) FOMO_ELC_CASE(2) FOMO_ELC_CASE(3) FOMO_ELC_CASE(4) FOMO_ELC_CASE(5) }
+#define FOMO_ELC_SWITCH(SPV)                                                                 \
+  switch (P.N) {                                                                             \
+    FOMO_ELC_CASE(1, SPV) FOMO_ELC_CASE(2, SPV) FOMO_ELC_CASE(3, SPV) FOMO_ELC_CASE(4, SPV) \
+    FOMO_ELC_CASE(5, SPV)                                                                    \
+  }
+          if (P.sponge) {
+            FOMO_ELC_SWITCH(true)
+          } else {
+            FOMO_ELC_SWITCH(false)
+          }
+#undef FOMO_ELC_SWITCH
 #undef FOMO_ELC_CASE
           k_inject_record_at<<<P.ns, 256, 0, cs>>>(d_it, j, P.nt, P.plane, P.n_src, d_src, d_wav,
                                                    field(b, 2), field(b, 3), P.n_rec, d_rec,
@@ -552,14 +579,24 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
       } else if (ce == cudaSuccess) {
         int a = A, b = B, nodes = 0;
         for (int j = 0; j < K; ++j) {
-#define FOMO_ACC_CASE(NN)                                                                         \
-  case NN:                                                                                        \
-    k_ac_vel<NN><<<grd, blk, 0, cs>>>(g, c, dtx, dtz, h, field(a, 2), field(a, 0), field(a, 1),  \
-                                      bx, bz, field(b, 0), field(b, 1));                          \
-    k_ac_prs<NN><<<grd, blk, 0, cs>>>(g, c, dtx, dtz, h, field(a, 2), field(b, 0), field(b, 1),  \
-                                      kap, field(b, 2));                                          \
+#define FOMO_ACC_CASE(NN, SPV)                                                                 \
+  case NN:                                                                                     \
+    k_ac_vel<NN, SPV><<<grd, blk, 0, cs>>>(g, c, dtx, dtz, h, field(a, 2), field(a, 0),        \
+                                           field(a, 1), bx, bz, field(b, 0), field(b, 1));     \
+    k_ac_prs<NN, SPV><<<grd, blk, 0, cs>>>(g, c, dtx, dtz, h, field(a, 2), field(b, 0),        \
+                                           field(b, 1), kap, field(b, 2));                     \
     break;
-          switch (P.N) { FOMO_ACC_CASE(1) FOMO_ACC_CASE(2) FOMO_ACC_CASE(3) FOMO_ACC_CASE(4) FOMO_ACC_CASE(5) }
+#define FOMO_ACC_SWITCH(SPV)                                                                 \
+  switch (P.N) {                                                                             \
+    FOMO_ACC_CASE(1, SPV) FOMO_ACC_CASE(2, SPV) FOMO_ACC_CASE(3, SPV) FOMO_ACC_CASE(4, SPV) \
+    FOMO_ACC_CASE(5, SPV)                                                                    \
+  }
+          if (P.sponge) {
+            FOMO_ACC_SWITCH(true)
+          } else {
+            FOMO_ACC_SWITCH(false)
+          }
+#undef FOMO_ACC_SWITCH
 #undef FOMO_ACC_CASE
           k_inject_record_at<<<P.ns, 256, 0, cs>>>(d_it, j, P.nt, P.plane, P.n_src, d_src, d_wav,
                                                    field(b, 2), nullptr, P.n_rec, d_rec,
@@ -619,13 +656,23 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
         launches += 1;
         sweeps_per_step = 1;
       } else {
-#define FOMO_EL_CASE(NN)                                                                       \
+#define FOMO_EL_CASE(NN, SPV)                                                                  \
   case NN:                                                                                     \
-    k_el_vel<NN><<<grd, blk, 0, st>>>(g, c, dtx, dtz, h, a, m, field(B, 0), field(B, 1));      \
-    k_el_str<NN><<<grd, blk, 0, st>>>(g, c, dtx, dtz, h, a, field(B, 0), field(B, 1), m,       \
-                                      field(B, 2), field(B, 3), field(B, 4));                  \
+    k_el_vel<NN, SPV><<<grd, blk, 0, st>>>(g, c, dtx, dtz, h, a, m, field(B, 0), field(B, 1)); \
+    k_el_str<NN, SPV><<<grd, blk, 0, st>>>(g, c, dtx, dtz, h, a, field(B, 0), field(B, 1), m,  \
+                                           field(B, 2), field(B, 3), field(B, 4));             \
     break;
-        switch (P.N) { FOMO_EL_CASE(1) FOMO_EL_CASE(2) FOMO_EL_CASE(3) FOMO_EL_CASE(4) FOMO_EL_CASE(5) }
+#define FOMO_EL_SWITCH(SPV)                                                                      \
+  switch (P.N) {                                                                                 \
+    FOMO_EL_CASE(1, SPV) FOMO_EL_CASE(2, SPV) FOMO_EL_CASE(3, SPV) FOMO_EL_CASE(4, SPV)         \
+    FOMO_EL_CASE(5, SPV)                                                                         \
+  }
+        if (P.sponge) {
+          FOMO_EL_SWITCH(true)
+        } else {
+          FOMO_EL_SWITCH(false)
+        }
+#undef FOMO_EL_SWITCH
 #undef FOMO_EL_CASE
         launches += 2;
         sweeps_per_step = 2;
@@ -647,14 +694,24 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
       const float* bx = d_mat;
       const float* bz = d_mat + P.plane;
       const float* kap = d_mat + 2 * P.plane;
-#define FOMO_AC_CASE(NN)                                                                          \
-  case NN:                                                                                        \
-    k_ac_vel<NN><<<grd, blk, 0, st>>>(g, c, dtx, dtz, h, p0, vx0, vz0, bx, bz, field(B, 0),      \
-                                      field(B, 1));                                               \
-    k_ac_prs<NN><<<grd, blk, 0, st>>>(g, c, dtx, dtz, h, p0, field(B, 0), field(B, 1), kap,      \
-                                      field(B, 2));                                               \
+#define FOMO_AC_CASE(NN, SPV)                                                                  \
+  case NN:                                                                                     \
+    k_ac_vel<NN, SPV><<<grd, blk, 0, st>>>(g, c, dtx, dtz, h, p0, vx0, vz0, bx, bz,            \
+                                           field(B, 0), field(B, 1));                          \
+    k_ac_prs<NN, SPV><<<grd, blk, 0, st>>>(g, c, dtx, dtz, h, p0, field(B, 0), field(B, 1),    \
+                                           kap, field(B, 2));                                  \
     break;
-      switch (P.N) { FOMO_AC_CASE(1) FOMO_AC_CASE(2) FOMO_AC_CASE(3) FOMO_AC_CASE(4) FOMO_AC_CASE(5) }
+#define FOMO_AC_SWITCH(SPV)                                                                      \
+  switch (P.N) {                                                                                 \
+    FOMO_AC_CASE(1, SPV) FOMO_AC_CASE(2, SPV) FOMO_AC_CASE(3, SPV) FOMO_AC_CASE(4, SPV)         \
+    FOMO_AC_CASE(5, SPV)                                                                         \
+  }
+      if (P.sponge) {
+        FOMO_AC_SWITCH(true)
+      } else {
+        FOMO_AC_SWITCH(false)
+      }
+#undef FOMO_AC_SWITCH
 #undef FOMO_AC_CASE
       sweeps_per_step = 2;
       FOMO_CU(ctx, prof_mark(it, 1));

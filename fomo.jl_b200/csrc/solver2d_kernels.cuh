@@ -42,6 +42,16 @@ struct ElMat {
   int pack_pitch = 0;  // column pairs per pack row
 };
 
+// Cerjan sponge (boundary/sponge.jl:31-83), fused into the sweep that produces
+// the field: the updated value times damp[d], d = the cell's distance in cells
+// to the nearest edge of the padded grid, for d < nbc.  In sponge mode HabcDev
+// carries the user's nbc and the damping table (wtab[d], d < nbc).
+__device__ __forceinline__ float sponge_damp(const Geo2& g, const HabcDev& h, int x, int z,
+                                             float u) {
+  const int d = min(min(x, g.nx - 1 - x), min(z, g.nz - 1 - z));
+  return d < h.nbc ? __fmul_rn(u, __ldg(h.wtab + d)) : u;
+}
+
 template <int N>
 __device__ __forceinline__ void el_vel_at(const Geo2& g, const Coef& c, float dtx, float dtz,
                                           const ElFields& a, const ElMat& m, int x, int z,
@@ -61,7 +71,8 @@ __device__ __forceinline__ void el_vel_at(const Geo2& g, const Coef& c, float dt
   uz = vz;
 }
 
-template <int N>
+// SP: the sponge boundary instead of the fused HABC.
+template <int N, bool SP = false>
 __global__ void __launch_bounds__(256) k_el_vel(Geo2 g, Coef c, float dtx, float dtz, HabcDev h,
                                                 ElFields a, ElMat m, float* __restrict__ vx1,
                                                 float* __restrict__ vz1) {
@@ -74,7 +85,10 @@ __global__ void __launch_bounds__(256) k_el_vel(Geo2 g, Coef c, float dtx, float
   el_vel_at<N>(g, c, dtx, dtz, a, m, x, z, ux, uz);
   long long p = (long long)z * g.ld + x;
   int sx, sz, dist;
-  if (frame2(g, x, z, sx, sz, dist)) {
+  if constexpr (SP) {
+    ux = sponge_damp(g, h, x, z, ux);
+    uz = sponge_damp(g, h, x, z, uz);
+  } else if (frame2(g, x, z, sx, sz, dist)) {
     float wx = habc_weight(h, 0, dist), wz = habc_weight(h, 1, dist);
     float fox = __ldg(a.vx + p), foz = __ldg(a.vz + p);
     if (sx != 0 && sz != 0) {
@@ -122,7 +136,7 @@ __device__ __forceinline__ void el_str_at(const Geo2& g, const Coef& c, float dt
   }
 }
 
-template <int N>
+template <int N, bool SP = false>
 __global__ void __launch_bounds__(256) k_el_str(Geo2 g, Coef c, float dtx, float dtz, HabcDev h,
                                                 ElFields a, const float* __restrict__ vx1,
                                                 const float* __restrict__ vz1, ElMat m,
@@ -139,7 +153,11 @@ __global__ void __launch_bounds__(256) k_el_str(Geo2 g, Coef c, float dtx, float
   el_str_at<N>(g, c, dtx, dtz, vx, vz, a, m, x, z, sxx, szz, sxz);
   long long p = (long long)z * g.ld + x;
   int sx, sz, dist;
-  if (frame2(g, x, z, sx, sz, dist)) {
+  if constexpr (SP) {
+    sxx = sponge_damp(g, h, x, z, sxx);
+    szz = sponge_damp(g, h, x, z, szz);
+    sxz = sponge_damp(g, h, x, z, sxz);
+  } else if (frame2(g, x, z, sx, sz, dist)) {
     float w = habc_weight(h, 2, dist);
     float o1 = __ldg(a.txx + p), o2 = __ldg(a.tzz + p), o3 = __ldg(a.txz + p);
     if (sx != 0 && sz != 0) {
@@ -226,7 +244,7 @@ __device__ __forceinline__ void ac_vel_cell(const Geo2& g, const Coef& c, float 
   }
 }
 
-template <int N>
+template <int N, bool SP = false>
 __global__ void __launch_bounds__(256) k_ac_vel(Geo2 g, Coef c, float dtx, float dtz, HabcDev h,
                                                 const float* __restrict__ p0,
                                                 const float* __restrict__ vx0,
@@ -240,7 +258,13 @@ __global__ void __launch_bounds__(256) k_ac_vel(Geo2 g, Coef c, float dtx, float
   const long long so = (long long)blockIdx.z * g.plane;
   p0 += so; vx0 += so; vz0 += so;
   float ux, uz;
-  ac_vel_cell<N>(g, c, dtx, dtz, h, p0, vx0, vz0, bx, bz, x, z, ux, uz);
+  if constexpr (SP) {
+    ac_vel_at<N>(g, c, dtx, dtz, p0, vx0, vz0, bx, bz, x, z, ux, uz);
+    ux = sponge_damp(g, h, x, z, ux);
+    uz = sponge_damp(g, h, x, z, uz);
+  } else {
+    ac_vel_cell<N>(g, c, dtx, dtz, h, p0, vx0, vz0, bx, bz, x, z, ux, uz);
+  }
   long long p = (long long)z * g.ld + x;
   vx1[so + p] = ux;
   vz1[so + p] = uz;
@@ -290,7 +314,7 @@ __device__ __forceinline__ float ac_prs_cell(const Geo2& g, const Coef& c, float
   return u;
 }
 
-template <int N>
+template <int N, bool SP = false>
 __global__ void __launch_bounds__(256) k_ac_prs(Geo2 g, Coef c, float dtx, float dtz, HabcDev h,
                                                 const float* __restrict__ p0,
                                                 const float* __restrict__ vx1,
@@ -301,7 +325,12 @@ __global__ void __launch_bounds__(256) k_ac_prs(Geo2 g, Coef c, float dtx, float
   int z = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= g.nx || z >= g.nz) return;
   const long long so = (long long)blockIdx.z * g.plane;
-  const float u = ac_prs_cell<N>(g, c, dtx, dtz, h, p0 + so, vx1 + so, vz1 + so, kappa, x, z);
+  float u;
+  if constexpr (SP)
+    u = sponge_damp(g, h, x, z,
+                    ac_prs_at<N>(g, c, dtx, dtz, vx1 + so, vz1 + so, p0 + so, kappa, x, z));
+  else
+    u = ac_prs_cell<N>(g, c, dtx, dtz, h, p0 + so, vx1 + so, vz1 + so, kappa, x, z);
   p1[so + (long long)z * g.ld + x] = u;
 }
 

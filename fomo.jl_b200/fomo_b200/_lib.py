@@ -23,6 +23,7 @@ FOMO_EUNSUPPORTED = -5
 FOMO_F_DEVICE_PTRS = 1
 FOMO_F_PROFILE = 2
 FOMO_F_STEP_LAUNCH = 4
+FOMO_F_SPONGE = 8
 FOMO_FP32, FOMO_FP16, FOMO_BF16 = 0, 1, 2
 FOMO_KERNEL_AUTO, FOMO_KERNEL_TWO_PHASE, FOMO_KERNEL_SINGLE_SWEEP = 0, 1, 2
 
@@ -71,7 +72,8 @@ class Shot2D(C.Structure):
 
 class Opts(C.Structure):
     _fields_ = [("flags", C.c_uint32), ("precision", C.c_int32), ("kernel", C.c_int32),
-                ("check_every", C.c_int32), ("final_state", C.c_void_p)]
+                ("check_every", C.c_int32), ("final_state", C.c_void_p),
+                ("sponge_factor", C.c_float)]
 
 
 class Stats(C.Structure):

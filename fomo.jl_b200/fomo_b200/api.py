@@ -188,13 +188,19 @@ def _precision(p) -> int:
     return table[key]
 
 
-def _opts(kernel: int = 0, final_state: Optional[np.ndarray] = None, precision: int = 0):
+def _opts(kernel: int = 0, final_state: Optional[np.ndarray] = None, precision: int = 0,
+          sponge_factor=None):
+    """``sponge_factor`` not None selects boundary=:sponge with that Cerjan factor."""
     o = L.Opts()
     o.flags = 0
     o.precision = precision
     o.kernel = kernel
     o.check_every = 0
     o.final_state = _ptr(final_state)
+    o.sponge_factor = 0.0
+    if sponge_factor is not None:
+        o.flags |= L.FOMO_F_SPONGE
+        o.sponge_factor = float(np.float32(sponge_factor))
     return o
 
 
@@ -208,12 +214,12 @@ def _acq(sxm: np.ndarray, szm: np.ndarray, wm: np.ndarray, rx: np.ndarray, rz: n
     return L.Acq(ns, n_src, _ptr(sxm), _ptr(szm), _ptr(wm), rx.size, _ptr(rx), _ptr(rz))
 
 
-def _check_boundary(boundary):
+def _check_boundary(boundary) -> bool:
+    """acoustic2d.jl:65-66 / elastic2d.jl:63-64; True for the Cerjan sponge."""
     b = str(boundary).lstrip(":")
     if b not in ("habc", "sponge"):
         raise ArgumentError(f"boundary must be :habc or :sponge, got {boundary}")
-    if b == "sponge":
-        raise NotImplementedError("boundary=:sponge is not provided by libfomo_b200 (HABC only)")
+    return b == "sponge"
 
 
 def _snap_list(snaps: Optional[np.ndarray]) -> list:
@@ -230,8 +236,11 @@ def acoustic2d(vp, rho, dh, dt, nt, f0, *, sx: Sequence[int], sz: Sequence[int],
                v_ref=None, sponge_factor=0.015, wavelet=None, scale_source_by_dt: bool = False,
                use_cuda_graph: bool = True, verbose: bool = True, device: int = 0,
                kernel: int = 0, final_state: Optional[np.ndarray] = None) -> Acoustic2DResult:
-    """2D acoustic velocity-pressure simulation (equations/acoustic2d/acoustic2d.jl:47-192)."""
-    _check_boundary(boundary)
+    """2D acoustic velocity-pressure simulation (equations/acoustic2d/acoustic2d.jl:47-192).
+
+    ``boundary="sponge"`` runs the Cerjan layer of the user's ``nbc`` cells with
+    ``sponge_factor`` (boundary/sponge.jl); ``v_ref`` is then ignored."""
+    sponge = _check_boundary(boundary)
     vp, rho = _f32F(vp), _f32F(rho)
     nx, nz = vp.shape
     dh, dt, f0 = np.float32(dh), np.float32(dt), np.float32(f0)
@@ -254,7 +263,7 @@ def acoustic2d(vp, rho, dh, dt, nt, f0, *, sx: Sequence[int], sz: Sequence[int],
     ctx = L.context(device)
     g = _grid(nx, nz, dh, dt, nt, nbc, fd_order, v_ref)
     acq = _acq(sxv.reshape(-1, 1, order="F"), szv.reshape(-1, 1, order="F"), wm, rxv, rzv)
-    o = _opts(kernel, final_state)
+    o = _opts(kernel, final_state, sponge_factor=sponge_factor if sponge else None)
     ctx.check(L.lib().fomo_acoustic2d(ctx.handle, C.byref(g), _ptr(vp), _ptr(rho), C.byref(acq),
                                       int(snap_interval), _ptr(seis[0]), _ptr(seis[1]),
                                       _ptr(seis[2]), _ptr(snaps), C.byref(o), C.byref(st)))
@@ -268,8 +277,10 @@ def elastic2d(vp, vs, rho, dh, dt, nt, f0, *, sx: Sequence[int], sz: Sequence[in
               use_cuda_graph: bool = True, verbose: bool = True, device: int = 0,
               kernel: int = 0, final_state: Optional[np.ndarray] = None,
               precision="fp32") -> Elastic2DResult:
-    """2D elastic velocity-stress simulation (equations/elastic2d/elastic2d.jl:45-163)."""
-    _check_boundary(boundary)
+    """2D elastic velocity-stress simulation (equations/elastic2d/elastic2d.jl:45-163).
+
+    ``boundary="sponge"`` as in :func:`acoustic2d` (FP32 storage only)."""
+    sponge = _check_boundary(boundary)
     vp, vs, rho = _f32F(vp), _f32F(vs), _f32F(rho)
     nx, nz = vp.shape
     dh, dt, f0 = np.float32(dh), np.float32(dt), np.float32(f0)
@@ -293,7 +304,8 @@ def elastic2d(vp, vs, rho, dh, dt, nt, f0, *, sx: Sequence[int], sz: Sequence[in
     ctx = L.context(device)
     g = _grid(nx, nz, dh, dt, nt, nbc, fd_order, v_ref)
     acq = _acq(sxv.reshape(-1, 1, order="F"), szv.reshape(-1, 1, order="F"), wm, rxv, rzv)
-    o = _opts(kernel, final_state, _precision(precision))
+    o = _opts(kernel, final_state, _precision(precision),
+              sponge_factor=sponge_factor if sponge else None)
     ctx.check(L.lib().fomo_elastic2d(ctx.handle, C.byref(g), _ptr(vp), _ptr(vs), _ptr(rho),
                                      C.byref(acq), int(snap_interval), _ptr(seis[0]),
                                      _ptr(seis[1]), _ptr(snaps), C.byref(o), C.byref(st)))

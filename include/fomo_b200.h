@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define FOMO_ABI_VERSION 1
+#define FOMO_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define FOMO_API __attribute__((visibility("default")))
@@ -55,6 +55,9 @@ extern "C" {
 #define FOMO_F_PROFILE 2u     /* time the sweep kernels of a window of steps  */
 #define FOMO_F_STEP_LAUNCH 4u /* launch every time step from the host (no      */
                               /* replayed CUDA-graph chunks; same results)      */
+#define FOMO_F_SPONGE 8u      /* boundary = :sponge: Cerjan layer of the user's  */
+                              /* nbc cells (boundary/sponge.jl) instead of HABC;  */
+                              /* acoustic2d and elastic2d (+ batch), FP32 only    */
 
 /* fomo_opts.precision: storage format of wavefields and material arrays */
 #define FOMO_FP32 0
@@ -99,6 +102,7 @@ typedef struct fomo_opts {
   int32_t kernel;       /* FOMO_KERNEL_*                                        */
   int32_t check_every;  /* NaN/Inf sentinel every K steps, 0 = off              */
   float* final_state;   /* optional HOST buffer: padded end-of-run wavefields   */
+  float sponge_factor;  /* FOMO_F_SPONGE: Cerjan factor (reference default 0.015) */
 } fomo_opts;
 
 typedef struct fomo_stats {

@@ -429,6 +429,38 @@ void acoustic_prs(const G2& g, int M, const Coef<T>& c, T dtx, T dtz, const T* k
   }
 }
 
+// Cerjan sponge (boundary/sponge.jl:31-48): with d the distance in cells from a
+// padded-grid cell to the nearest edge, damp(d) = exp(-r^2), r = factor * (nbc - d),
+// for d < nbc (the user's nbc, not pad); damp = 1 elsewhere.  r and r^2 round to
+// FP32 as in the reference; exp is taken in double and rounded once to FP32.
+// The FP64 oracle uses the same FP32 table (the reference stores it as Float32).
+std::vector<float> sponge_table(int nbc, float factor) {
+  std::vector<float> t((size_t)std::max(nbc, 0));
+  for (int d = 0; d < nbc; ++d) {
+    const float r = factor * (float)(nbc - d);
+    const float rr = r * r;
+    t[(size_t)d] = (float)std::exp(-(double)rr);
+  }
+  return t;
+}
+
+// apply_sponge! (boundary/sponge.jl:56-83): field *= damp over the whole padded grid.
+template <class T>
+void apply_sponge(const G2& g, const std::vector<float>& damp, T* f) {
+  const int nbc = (int)damp.size();
+#pragma omp parallel for schedule(static)
+  for (int j = 0; j < g.nz; ++j) {
+    const int dz = std::min(j, g.nz - 1 - j);
+    for (int i = 0; i < g.nx; ++i) {
+      const int d = std::min(std::min(i, g.nx - 1 - i), dz);
+      if (d < nbc) {
+        const size_t q = (size_t)i + (size_t)g.nx * (size_t)j;
+        f[q] = f[q] * (T)damp[(size_t)d];
+      }
+    }
+  }
+}
+
 // Snapshot of the interior (unpadded) part of a padded field.
 template <class T, class O>
 void snap_interior(const G2& g, int pad, const T* f, O* out) {
@@ -442,7 +474,8 @@ int run_elastic2d(int nx, int nz, int ns, const float* vp, const float* vs, cons
                   float dh, float dt, int nt, int nbc, int fd_order, float v_ref, int n_src,
                   const int32_t* sx, const int32_t* sz, const float* wavelet, int n_rec,
                   const int32_t* rx, const int32_t* rz, T* seis_vx, T* seis_vz, int snap_interval,
-                  T* snaps, T* final_fields, StoreSpec ss = StoreSpec()) {
+                  T* snaps, T* final_fields, StoreSpec ss = StoreSpec(),
+                  float sponge_factor = -1.0f) {
   int N = order_to_N(fd_order);
   if (N < 0) return -2;
   int M = N, pad = nbc + M;
@@ -474,6 +507,9 @@ int run_elastic2d(int nx, int nz, int ns, const float* vp, const float* vs, cons
     for (long q = 0; q < (long)f.size(); ++q)
       if (!zone_f32 || !in_zone((size_t)q)) f[q] = round_store(f[q], sfmt);
   };
+  const bool sponge = sponge_factor >= 0.0f;  // boundary = :sponge (elastic2d.jl:83-87)
+  if (sponge && sk != kStoreF32) return -2;
+  const std::vector<float> damp = sponge ? sponge_table(nbc, sponge_factor) : std::vector<float>();
   Habc<T> h = init_habc<T>(pad, v_ref, dt, dh);
   std::vector<FramePt> fr = frame_points(g, h.nbc);
   Coef<T> c = coef<T>(fd_order);
@@ -487,23 +523,33 @@ int run_elastic2d(int nx, int nz, int ns, const float* vp, const float* vs, cons
     for (auto* v : {&st.vx, &st.vz, &st.txx, &st.tzz, &st.txz, &st.o1, &st.o2, &st.o3})
       v->assign(ncell, T(0));
     for (int it = 1; it <= nt; ++it) {
-      st.o1 = st.vx;
-      st.o2 = st.vz;
-      elastic_vel(g, M, c, dtx, dtz, bx.data(), bz.data(), st);
-      habc_det(g, h, fr, 0, st.vx.data(), st.o1.data(), scr);
-      habc_det(g, h, fr, 1, st.vz.data(), st.o2.data(), scr);
-      round_all(st.vx);  // stored v'' (the stress update reads the stored values)
-      round_all(st.vz);
-      st.o1 = st.txx;
-      st.o2 = st.tzz;
-      st.o3 = st.txz;
-      elastic_str(g, M, c, dtx, dtz, lam.data(), lam2mu.data(), mutxz.data(), st);
-      habc_det(g, h, fr, 2, st.txx.data(), st.o1.data(), scr);
-      habc_det(g, h, fr, 2, st.tzz.data(), st.o2.data(), scr);
-      habc_det(g, h, fr, 2, st.txz.data(), st.o3.data(), scr);
-      round_all(st.txx);
-      round_all(st.tzz);
-      round_all(st.txz);
+      if (sponge) {  // legacy loop, elastic2d.jl:180-195
+        elastic_vel(g, M, c, dtx, dtz, bx.data(), bz.data(), st);
+        apply_sponge(g, damp, st.vx.data());
+        apply_sponge(g, damp, st.vz.data());
+        elastic_str(g, M, c, dtx, dtz, lam.data(), lam2mu.data(), mutxz.data(), st);
+        apply_sponge(g, damp, st.txx.data());
+        apply_sponge(g, damp, st.tzz.data());
+        apply_sponge(g, damp, st.txz.data());
+      } else {
+        st.o1 = st.vx;
+        st.o2 = st.vz;
+        elastic_vel(g, M, c, dtx, dtz, bx.data(), bz.data(), st);
+        habc_det(g, h, fr, 0, st.vx.data(), st.o1.data(), scr);
+        habc_det(g, h, fr, 1, st.vz.data(), st.o2.data(), scr);
+        round_all(st.vx);  // stored v'' (the stress update reads the stored values)
+        round_all(st.vz);
+        st.o1 = st.txx;
+        st.o2 = st.tzz;
+        st.o3 = st.txz;
+        elastic_str(g, M, c, dtx, dtz, lam.data(), lam2mu.data(), mutxz.data(), st);
+        habc_det(g, h, fr, 2, st.txx.data(), st.o1.data(), scr);
+        habc_det(g, h, fr, 2, st.tzz.data(), st.o2.data(), scr);
+        habc_det(g, h, fr, 2, st.txz.data(), st.o3.data(), scr);
+        round_all(st.txx);
+        round_all(st.tzz);
+        round_all(st.txz);
+      }
       for (int q = 0; q < n_src; ++q) {  // batch_acq.jl:58-71, sequential in source order
         size_t p = g.at(sx[(size_t)s * n_src + q] + pad, sz[(size_t)s * n_src + q] + pad);
         T w = (T)wavelet[(size_t)q + (size_t)n_src * (it - 1)] * st_;
@@ -540,7 +586,8 @@ int run_acoustic2d(int nx, int nz, int ns, const float* vp, const float* rho, fl
                    int nt, int nbc, int fd_order, float v_ref, int n_src, const int32_t* sx,
                    const int32_t* sz, const float* wavelet, int n_rec, const int32_t* rx,
                    const int32_t* rz, T* seis_p, T* seis_vx, T* seis_vz, int snap_interval,
-                   T* snaps, T* final_fields, int zone_nbc_override) {
+                   T* snaps, T* final_fields, int zone_nbc_override,
+                   float sponge_factor = -1.0f) {
   int N = order_to_N(fd_order);
   if (N < 0) return -2;
   int M = N, pad = nbc + M;
@@ -554,6 +601,8 @@ int run_acoustic2d(int nx, int nz, int ns, const float* vp, const float* rho, fl
   // zone_nbc_override > 0 restates the pre-v0.2 zone (= nbc) used by the
   // calibration in test/verify_patch.jl:9-11; 0 keeps the production zone pad-1.
   if (zone_nbc_override > 0) h.nbc = zone_nbc_override;
+  const bool sponge = sponge_factor >= 0.0f;  // boundary = :sponge (acoustic2d.jl:84-87)
+  const std::vector<float> damp = sponge ? sponge_table(nbc, sponge_factor) : std::vector<float>();
   std::vector<FramePt> fr = frame_points(g, h.nbc);
   Coef<T> c = coef<T>(fd_order);
   T dtx = (T)dt / (T)dh, dtz = dtx;
@@ -564,14 +613,22 @@ int run_acoustic2d(int nx, int nz, int ns, const float* vp, const float* rho, fl
     AcousticState<T> st;
     for (auto* v : {&st.vx, &st.vz, &st.p, &st.o1, &st.o2, &st.o3}) v->assign(ncell, T(0));
     for (int it = 1; it <= nt; ++it) {
-      st.o1 = st.vx;
-      st.o2 = st.vz;
-      acoustic_vel(g, M, c, dtx, dtz, bx.data(), bz.data(), st);
-      habc_det(g, h, fr, 0, st.vx.data(), st.o1.data(), scr);
-      habc_det(g, h, fr, 1, st.vz.data(), st.o2.data(), scr);
-      st.o3 = st.p;
-      acoustic_prs(g, M, c, dtx, dtz, kappa.data(), st);
-      habc_det(g, h, fr, 2, st.p.data(), st.o3.data(), scr);
+      if (sponge) {  // legacy loop, acoustic2d.jl:213-227
+        acoustic_vel(g, M, c, dtx, dtz, bx.data(), bz.data(), st);
+        apply_sponge(g, damp, st.vx.data());
+        apply_sponge(g, damp, st.vz.data());
+        acoustic_prs(g, M, c, dtx, dtz, kappa.data(), st);
+        apply_sponge(g, damp, st.p.data());
+      } else {
+        st.o1 = st.vx;
+        st.o2 = st.vz;
+        acoustic_vel(g, M, c, dtx, dtz, bx.data(), bz.data(), st);
+        habc_det(g, h, fr, 0, st.vx.data(), st.o1.data(), scr);
+        habc_det(g, h, fr, 1, st.vz.data(), st.o2.data(), scr);
+        st.o3 = st.p;
+        acoustic_prs(g, M, c, dtx, dtz, kappa.data(), st);
+        habc_det(g, h, fr, 2, st.p.data(), st.o3.data(), scr);
+      }
       for (int q = 0; q < n_src; ++q) {  // inject_source.jl:4-24
         size_t p = g.at(sx[(size_t)s * n_src + q] + pad, sz[(size_t)s * n_src + q] + pad);
         st.p[p] += (T)wavelet[(size_t)q + (size_t)n_src * (it - 1)];
@@ -1185,6 +1242,53 @@ int oracle_acoustic2d(int prec, int nx, int nz, int ns, const float* vp, const f
                              wavelet, n_rec, rx, rz, (double*)seis_p, (double*)seis_vx,
                              (double*)seis_vz, snap_interval, (double*)snaps,
                              (double*)final_fields, zone_nbc_override));
+}
+
+// boundary = :sponge with Cerjan factor sponge_factor (>= 0): the legacy loops
+// acoustic2d.jl:213-227 and elastic2d.jl:180-195.
+int oracle_acoustic2d_sponge(int prec, float sponge_factor, int nx, int nz, int ns,
+                             const float* vp, const float* rho, float dh, float dt, int nt,
+                             int nbc, int fd_order, int n_src, const int32_t* sx,
+                             const int32_t* sz, const float* wavelet, int n_rec, const int32_t* rx,
+                             const int32_t* rz, void* seis_p, void* seis_vx, void* seis_vz,
+                             int snap_interval, void* snaps, void* final_fields) {
+  if (!(sponge_factor >= 0.0f)) return -2;
+  return ORACLE_PREC_DISPATCH(
+      prec,
+      run_acoustic2d<float>(nx, nz, ns, vp, rho, dh, dt, nt, nbc, fd_order, 1.0f, n_src, sx, sz,
+                            wavelet, n_rec, rx, rz, (float*)seis_p, (float*)seis_vx,
+                            (float*)seis_vz, snap_interval, (float*)snaps, (float*)final_fields,
+                            0, sponge_factor),
+      run_acoustic2d<double>(nx, nz, ns, vp, rho, dh, dt, nt, nbc, fd_order, 1.0f, n_src, sx, sz,
+                             wavelet, n_rec, rx, rz, (double*)seis_p, (double*)seis_vx,
+                             (double*)seis_vz, snap_interval, (double*)snaps,
+                             (double*)final_fields, 0, sponge_factor));
+}
+
+int oracle_elastic2d_sponge(int prec, float sponge_factor, int nx, int nz, int ns,
+                            const float* vp, const float* vs, const float* rho, float dh, float dt,
+                            int nt, int nbc, int fd_order, int n_src, const int32_t* sx,
+                            const int32_t* sz, const float* wavelet, int n_rec, const int32_t* rx,
+                            const int32_t* rz, void* seis_vx, void* seis_vz, int snap_interval,
+                            void* snaps, void* final_fields) {
+  if (!(sponge_factor >= 0.0f)) return -2;
+  return ORACLE_PREC_DISPATCH(
+      prec,
+      run_elastic2d<float>(nx, nz, ns, vp, vs, rho, dh, dt, nt, nbc, fd_order, 1.0f, n_src, sx,
+                           sz, wavelet, n_rec, rx, rz, (float*)seis_vx, (float*)seis_vz,
+                           snap_interval, (float*)snaps, (float*)final_fields, StoreSpec(),
+                           sponge_factor),
+      run_elastic2d<double>(nx, nz, ns, vp, vs, rho, dh, dt, nt, nbc, fd_order, 1.0f, n_src, sx,
+                            sz, wavelet, n_rec, rx, rz, (double*)seis_vx, (double*)seis_vz,
+                            snap_interval, (double*)snaps, (double*)final_fields, StoreSpec(),
+                            sponge_factor));
+}
+
+// sponge_table for the tests (boundary/sponge.jl:31-48).
+int oracle_sponge_table(int nbc, float factor, float* out) {
+  std::vector<float> t = sponge_table(nbc, factor);
+  std::copy(t.begin(), t.end(), out);
+  return 0;
 }
 
 int oracle_scalar2d(int prec, int nx, int nz, const float* vp, float dh, float dt, int nt,

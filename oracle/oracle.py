@@ -56,6 +56,18 @@ def lib():
                                         C.c_float, C.c_float, C.c_int, C.c_int, C.c_int, C.c_float,
                                         C.c_int, _i32p, _i32p, _f32p, C.c_int, _i32p, _i32p,
                                         vp, vp, vp, C.c_int, vp, vp, C.c_int]
+        L.oracle_acoustic2d_sponge.restype = C.c_int
+        L.oracle_acoustic2d_sponge.argtypes = [C.c_int, C.c_float, C.c_int, C.c_int, C.c_int,
+                                               _f32p, _f32p, C.c_float, C.c_float, C.c_int,
+                                               C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f32p,
+                                               C.c_int, _i32p, _i32p, vp, vp, vp, C.c_int, vp, vp]
+        L.oracle_elastic2d_sponge.restype = C.c_int
+        L.oracle_elastic2d_sponge.argtypes = [C.c_int, C.c_float, C.c_int, C.c_int, C.c_int,
+                                              _f32p, _f32p, _f32p, C.c_float, C.c_float, C.c_int,
+                                              C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f32p,
+                                              C.c_int, _i32p, _i32p, vp, vp, C.c_int, vp, vp]
+        L.oracle_sponge_table.restype = C.c_int
+        L.oracle_sponge_table.argtypes = [C.c_int, C.c_float, vp]
         L.oracle_scalar2d.restype = C.c_int
         L.oracle_scalar2d.argtypes = [C.c_int, C.c_int, C.c_int, _f32p, C.c_float, C.c_float,
                                       C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, _i32p, _i32p,
@@ -133,13 +145,14 @@ def round_store(x, store: str) -> np.ndarray:
 
 def elastic2d(vp, vs, rho, dh, dt, nt, *, sx, sz, rx, rz, wavelet, nbc=50, fd_order=8,
               v_ref=None, snap_interval=0, prec=32, n_shots=1, final=False, store=None,
-              sv=1.0, st=1.0, fp32_band=0):
+              sv=1.0, st=1.0, fp32_band=0, sponge_factor=None):
     """Elastic velocity-stress run.  ``sx``/``sz``: (n_src, n_shots).  ``wavelet``: (n_src, nt).
 
     ``store`` ("fp16"/"bf16") emulates FP32 arithmetic on wavefields stored
     in that format under power-of-two scales ``sv`` (velocity) and ``st``
     (stress); cells closer than ``fp32_band`` to an edge keep FP32 storage;
-    results are returned unscaled.
+    results are returned unscaled.  ``sponge_factor`` (not None) selects
+    boundary=:sponge, the Cerjan layer of boundary/sponge.jl, instead of HABC.
     """
     vp, vs, rho = _f32(vp), _f32(vs), _f32(rho)
     nx, nz = vp.shape
@@ -157,7 +170,14 @@ def elastic2d(vp, vs, rho, dh, dt, nt, *, sx, sz, rx, rz, wavelet, nbc=50, fd_or
     nxp, nzp = nx + 2 * (nbc + M), nz + 2 * (nbc + M)
     fin = np.zeros((nxp, nzp, 5, ns), dtype=T, order="F") if final else None
     vr = default_v_ref(vp) if v_ref is None else float(v_ref)
-    if store is not None:
+    if sponge_factor is not None:
+        if store is not None:
+            raise ValueError("the sponge boundary runs FP32 storage only")
+        rc = lib().oracle_elastic2d_sponge(prec, float(sponge_factor), nx, nz, ns, vp, vs, rho, dh,
+                                           dt, nt, nbc, fd_order, n_src, sxm, szm, w, nrec, rx,
+                                           rz, _ptr(svx), _ptr(svz), snap_interval, _ptr(snaps),
+                                           _ptr(fin))
+    elif store is not None:
         if prec != 32:
             raise ValueError("storage emulation runs FP32 arithmetic")
         rc = lib().oracle_elastic2d_store(STORE[store], sv, st, int(fp32_band), nx, nz, ns, vp, vs, rho, dh, dt,
@@ -174,7 +194,9 @@ def elastic2d(vp, vs, rho, dh, dt, nt, *, sx, sz, rx, rz, wavelet, nbc=50, fd_or
 
 
 def acoustic2d(vp, rho, dh, dt, nt, *, sx, sz, rx, rz, wavelet, nbc=50, fd_order=8, v_ref=None,
-               snap_interval=0, prec=32, n_shots=1, final=False, zone_nbc=0):
+               snap_interval=0, prec=32, n_shots=1, final=False, zone_nbc=0, sponge_factor=None):
+    """Acoustic velocity-pressure run; ``sponge_factor`` (not None) selects the
+    Cerjan sponge boundary (boundary/sponge.jl) instead of HABC."""
     vp, rho = _f32(vp), _f32(rho)
     nx, nz = vp.shape
     sxm, szm = _src_matrix(sx, n_shots), _src_matrix(sz, n_shots)
@@ -191,9 +213,16 @@ def acoustic2d(vp, rho, dh, dt, nt, *, sx, sz, rx, rz, wavelet, nbc=50, fd_order
     nxp, nzp = nx + 2 * (nbc + M), nz + 2 * (nbc + M)
     fin = np.zeros((nxp, nzp, 3, ns), dtype=T, order="F") if final else None
     vr = default_v_ref(vp) if v_ref is None else float(v_ref)
-    rc = lib().oracle_acoustic2d(prec, nx, nz, ns, vp, rho, dh, dt, nt, nbc, fd_order, vr, n_src,
-                                 sxm, szm, w, nrec, rx, rz, _ptr(sp), _ptr(svx), _ptr(svz),
-                                 snap_interval, _ptr(snaps), _ptr(fin), int(zone_nbc))
+    if sponge_factor is not None:
+        rc = lib().oracle_acoustic2d_sponge(prec, float(sponge_factor), nx, nz, ns, vp, rho, dh,
+                                            dt, nt, nbc, fd_order, n_src, sxm, szm, w, nrec, rx,
+                                            rz, _ptr(sp), _ptr(svx), _ptr(svz), snap_interval,
+                                            _ptr(snaps), _ptr(fin))
+    else:
+        rc = lib().oracle_acoustic2d(prec, nx, nz, ns, vp, rho, dh, dt, nt, nbc, fd_order, vr,
+                                     n_src, sxm, szm, w, nrec, rx, rz, _ptr(sp), _ptr(svx),
+                                     _ptr(svz), snap_interval, _ptr(snaps), _ptr(fin),
+                                     int(zone_nbc))
     if rc != 0:
         raise RuntimeError(f"oracle_acoustic2d failed: {rc}")
     return dict(seis_p=sp, seis_vx=svx, seis_vz=svz, snaps=snaps, final=fin)
@@ -298,6 +327,13 @@ def habc_apply(f, f_old, pad, v_ref, dt, dh, kind):
     nxp, nzp = f.shape
     lib().oracle_habc_apply_f32(nxp, nzp, pad, v_ref, dt, dh, kind, _ptr(f), _ptr(fo))
     return f
+
+
+def sponge_table(nbc, factor):
+    """Cerjan damping factors damp[d], d = 0 .. nbc-1 cells from the padded edge."""
+    out = np.zeros(max(int(nbc), 0), np.float32)
+    lib().oracle_sponge_table(int(nbc), float(factor), _ptr(out))
+    return out
 
 
 def ricker(f0, dt, nt):

@@ -77,3 +77,39 @@ def test_create_without_device_fails_cleanly(fomo):
     h = C.c_void_p()
     assert _lib.lib().fomo_create(C.byref(h), 0) == _lib.FOMO_ECUDA
     assert not h.value
+
+
+_STRUCTS = [("Grid2D", "fomo_grid2d"), ("Acq", "fomo_acq"), ("Grid3D", "fomo_grid3d"),
+            ("Acq3D", "fomo_acq3d"), ("Shot2D", "fomo_shot2d"), ("Opts", "fomo_opts"),
+            ("Stats", "fomo_stats")]
+
+
+def test_ctypes_struct_layouts_match_header(fomo, tmp_path):
+    """Every ctypes mirror has the size and field offsets of its C struct."""
+    import shutil
+    import subprocess
+
+    from fomo_b200 import _lib as L
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    inc = Path(__file__).resolve().parents[1] / "include"
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "fomo_b200.h"',
+             "int main(void) {"]
+    want = []
+    for py, c in _STRUCTS:
+        cls = getattr(L, py)
+        lines.append(f'  printf("%zu\\n", sizeof({c}));')
+        want.append(C.sizeof(cls))
+        for name, _ in cls._fields_:
+            lines.append(f'  printf("%zu\\n", offsetof({c}, {name}));')
+            want.append(getattr(cls, name).offset)
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", str(inc), "-o", str(exe), str(src)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True,
+                                          text=True).stdout.split()]
+    assert got == want

@@ -40,12 +40,23 @@ def test_wavelet_length_and_keywords(fomo):
         fomo.acoustic2d(vp, rho, 10.0, 1e-3, 50, 15.0, wavelet=np.zeros(49), **kw)
     with pytest.raises(fomo.ArgumentError):
         fomo.acoustic2d(vp, rho, 10.0, 1e-3, 50, 15.0, boundary="pml", **kw)
-    with pytest.raises(NotImplementedError):
-        fomo.acoustic2d(vp, rho, 10.0, 1e-3, 50, 15.0, boundary=":sponge", **kw)
     with pytest.raises(fomo.ArgumentError):
         fomo.scalar2d(vp, 10.0, 1e-3, 50, 15.0, source_scale=":foo", **kw)
     with pytest.raises(fomo.ArgumentError):
         fomo.acoustic2d_batch(vp, rho, 10.0, 1e-3, 50, 15.0, sx=[[5, 6]], sz=[[3]], rx=[4], rz=[3])
+
+
+def test_sponge_boundary_options(fomo):
+    """boundary=:sponge sets FOMO_F_SPONGE and the Cerjan factor in fomo_opts."""
+    from fomo_b200 import _lib as L
+    from fomo_b200.api import _check_boundary, _opts
+
+    assert _check_boundary(":sponge") and _check_boundary("sponge")
+    assert not _check_boundary(":habc")
+    o = _opts(sponge_factor=0.02)
+    assert o.flags & L.FOMO_F_SPONGE and o.sponge_factor == np.float32(0.02)
+    o = _opts()
+    assert not o.flags & L.FOMO_F_SPONGE
 
 
 def test_dispersion_warning(fomo):

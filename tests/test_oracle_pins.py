@@ -4,8 +4,10 @@ The reference (Julia, not runnable here) ships no golden vectors, so these
 checks restate its test properties and numbers:
   * HABC absorption residual vs a large-domain reference: 1.245e-2 with the
     production zone pad-1 and 1.336e-2 with the old zone nbc, CPU float64
-    calibration (test/verify_patch.jl:5-12, :76-92)
-  * exact mirror symmetry under causal shielding (verify_patch.jl:59-73)
+    calibration (test/verify_patch.jl:5-12, :76-92), and 2.87e-2 with the
+    Cerjan sponge of the same layer count (verify_patch.jl:11)
+  * exact mirror symmetry under causal shielding, HABC and sponge
+    (verify_patch.jl:59-73)
   * multi-source linearity (verify_patch.jl:97-104)
   * the two-pass Higdon CPU reference (verify_det_graph.jl:59-94)
   * the scalar same-scheme CPU transcription (verify_scalar.jl:33-86) and the
@@ -27,7 +29,7 @@ def _calib():
 
 
 # ---------------------------------------------------------------------------
-def _habc_residual(O, prec, zone_nbc=0):
+def _habc_residual(O, prec, zone_nbc=0, sponge_factor=None):
     from fomo_b200.synthetic import edge_extend, symmetric_model
 
     nxr, nzr, ntr, L = 301, 201, 1500, 270
@@ -36,7 +38,7 @@ def _habc_residual(O, prec, zone_nbc=0):
     rx = np.arange(1, nxr + 1)
     kw = dict(wavelet=w, nbc=20, fd_order=4, prec=prec)
     h = O.acoustic2d(vp, rho, 10.0, 1e-3, ntr, sx=[151], sz=[41], rx=rx, rz=np.full(nxr, 41),
-                     zone_nbc=zone_nbc, **kw)
+                     zone_nbc=zone_nbc, sponge_factor=sponge_factor, **kw)
     ref = O.acoustic2d(edge_extend(vp, L), edge_extend(rho, L), 10.0, 1e-3, ntr, sx=[151 + L],
                        sz=[41 + L], rx=rx + L, rz=np.full(nxr, 41 + L), **kw)
     return rel_l2(h["seis_p"], ref["seis_p"])
@@ -55,6 +57,15 @@ def test_habc_absorption_fp32_within_reference_bound(oracle):
     r = _habc_residual(oracle, 32)
     assert r < c["test_bound"]
     assert abs(r - c["zone_pad_minus_1"]) / c["zone_pad_minus_1"] < 5e-3, r
+
+
+def test_sponge_absorption_matches_reference_calibration(oracle):
+    """The small-domain run with boundary=:sponge (factor 0.015, nbc 20) against
+    the large-domain reference: 2.87e-2 in the reference's calibration."""
+    c = _calib()["habc_absorption"]["sponge_same_layers"]
+    for prec in (64, 32):
+        r = _habc_residual(oracle, prec, sponge_factor=0.015)
+        assert abs(r - c) / c < 2e-3, (prec, r)
 
 
 # ---------------------------------------------------------------------------
@@ -76,12 +87,14 @@ def _rel_asym_vx(d):
     return float(np.linalg.norm(e + e[::-1]) / np.linalg.norm(e))
 
 
-def test_mirror_symmetry_under_causal_shielding(oracle):
+@pytest.mark.parametrize("sponge_factor", [None, 0.015], ids=["habc", "sponge"])
+def test_mirror_symmetry_under_causal_shielding(oracle, sponge_factor):
     vp, vs, rho, rx, rz = _shielded_setup()
     assert np.array_equal(vp, vp[::-1]) and np.array_equal(rho, rho[::-1])
     nts = 1200
     w = oracle.ricker(10.0, 1e-3, nts).reshape(1, -1)
-    kw = dict(sx=[301], sz=[41], rx=rx, rz=rz, wavelet=w, nbc=30, fd_order=4)
+    kw = dict(sx=[301], sz=[41], rx=rx, rz=rz, wavelet=w, nbc=30, fd_order=4,
+              sponge_factor=sponge_factor)
     a = oracle.acoustic2d(vp, rho, 10.0, 1e-3, nts, **kw)
     assert _rel_sym(a["seis_p"][:, :, 0]) < 1e-5
     assert _rel_sym(a["seis_vz"][:, :, 0]) < 1e-5
