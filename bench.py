@@ -17,6 +17,7 @@ Secondary workloads (one JSON line each, same keys; not the default line):
     --workload uneven         64 acoustic shots on grids of uneven size (graph run)
     --workload elastic3d      elastic3d 400x400x300, nbc 40, order 8 (nt from --nt)
     --workload readme         steps/s on the grids of Fomo's published throughput table
+    --workload sponge         Fomo's HABC-vs-sponge benchmark (acoustic and elastic 401x401)
 """
 from __future__ import annotations
 
@@ -501,6 +502,70 @@ def readme_grids(args):
                               "device": "B200", "dtype": "f32"}), flush=True)
 
 
+# Fomo's HABC-vs-sponge benchmark (example/benchmark/habc_vs_sponge*.jl and
+# output/report*.txt, RTX 3060): wall-clock of the whole call in seconds
+# (including warm-up and JIT there), and the late-time interior energy.
+SPONGE_BENCH = {
+    "acoustic2d": dict(nt=1500, snap=30, ref_s={"habc": 9.285, "sponge": 0.504},
+                       ref_energy={"habc": 3.540e-07, "sponge": 9.363e-06}),
+    "elastic2d": dict(nt=2500, snap=50, ref_s={"habc": 11.581, "sponge": 1.108},
+                      ref_energy={"habc": 1.470e-08, "sponge": 2.069e-06}),
+}
+
+
+def sponge_bench(args):
+    """401x401 homogeneous model (vp 2500, vs 1500, rho 2000), dh 10 m, dt 1 ms,
+    15 Hz Ricker at the centre, receivers every 2nd x at mid-depth, nbc 50,
+    order 8, snapshots every `snap` steps; the same call with boundary=:habc and
+    boundary=:sponge.  `wall_s`: the public call end to end (host model in,
+    seismograms and snapshots out), median of --steps after --warmup calls;
+    `kernel_s`: the library's CUDA-event time of the time loop.  Energy: mean over
+    the last quarter of the snapshots of sum(f^2) less a 50-cell margin,
+    normalised to its peak (habc_vs_sponge.jl:98-127)."""
+    import time
+    import warnings
+
+    import fomo_b200 as F
+
+    warnings.simplefilter("ignore")
+    n = 401
+    vp = np.full((n, n), 2500.0, np.float32, order="F")
+    vs = np.full((n, n), 1500.0, np.float32, order="F")
+    rho = np.full((n, n), 2000.0, np.float32, order="F")
+    rx = np.arange(1, n + 1, 2)
+    for eq, c in SPONGE_BENCH.items():
+        kw = dict(sx=[n // 2], sz=[n // 2], rx=rx, rz=np.full(rx.size, n // 2), nbc=50,
+                  fd_order=8, snap_interval=c["snap"])
+        out = {}
+        for bnd in ("habc", "sponge"):
+            def run():
+                t0 = time.perf_counter()
+                if eq == "acoustic2d":
+                    r = F.acoustic2d(vp, rho, 10.0, 1e-3, c["nt"], 15.0, boundary=bnd, **kw)
+                else:
+                    r = F.elastic2d(vp, vs, rho, 10.0, 1e-3, c["nt"], 15.0, boundary=bnd, **kw)
+                return time.perf_counter() - t0, r
+
+            for _ in range(max(1, args.warmup)):
+                run()
+            runs = [run() for _ in range(max(1, args.steps))]
+            snaps = np.stack(runs[-1][1].snaps, axis=2)[50:-50, 50:-50].astype(np.float64)
+            e = (snaps ** 2).sum(axis=(0, 1))
+            e /= e.max()
+            late = float(e[3 * e.size // 4 - 1:].mean())
+            out[bnd] = {"wall_s": float(np.median([t for t, _ in runs])),
+                        "kernel_s": float(np.median([r.stats.kernel_time_s for _, r in runs])),
+                        "late_energy": late}
+        print(json.dumps({"workload": "reference HABC-vs-sponge benchmark", "equation": eq,
+                          "grid": [n, n], "nt": c["nt"], "snap_interval": c["snap"],
+                          "habc": out["habc"], "sponge": out["sponge"],
+                          "late_energy_ratio": out["sponge"]["late_energy"]
+                          / out["habc"]["late_energy"],
+                          "reference_rtx3060_wall_s": c["ref_s"],
+                          "reference_late_energy": c["ref_energy"],
+                          "device": "B200", "dtype": "f32"}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -513,9 +578,16 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", choices=["elastic-batch", "elastic-fp16", "uneven", "elastic3d",
-                                           "readme"],
+                                           "readme", "sponge"],
                     default="elastic-batch")
     args = ap.parse_args()
+    if args.workload == "sponge":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference's HABC-vs-sponge "
+                              "benchmark is compared against its published RTX 3060 report"}))
+            return
+        sponge_bench(args)
+        return
     if args.workload == "readme":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference's README grids "

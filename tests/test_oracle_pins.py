@@ -6,6 +6,8 @@ checks restate its test properties and numbers:
     production zone pad-1 and 1.336e-2 with the old zone nbc, CPU float64
     calibration (test/verify_patch.jl:5-12, :76-92), and 2.87e-2 with the
     Cerjan sponge of the same layer count (verify_patch.jl:11)
+  * the late-time interior energy of the sponge run in the reference's
+    HABC-vs-sponge benchmark, 9.363e-06 (example/benchmark/output/report.txt:12-15)
   * exact mirror symmetry under causal shielding, HABC and sponge
     (verify_patch.jl:59-73)
   * multi-source linearity (verify_patch.jl:97-104)
@@ -66,6 +68,25 @@ def test_sponge_absorption_matches_reference_calibration(oracle):
     for prec in (64, 32):
         r = _habc_residual(oracle, prec, sponge_factor=0.015)
         assert abs(r - c) / c < 2e-3, (prec, r)
+
+
+def test_sponge_late_energy_matches_reference_benchmark(oracle):
+    """example/benchmark/habc_vs_sponge.jl: 401x401 homogeneous acoustic run
+    with the sponge; late-time interior energy normalised to its peak."""
+    c = _calib()["sponge_energy"]
+    n, nt = 401, 1500
+    vp = np.full((n, n), 2500.0, np.float32)
+    rho = np.full((n, n), 2000.0, np.float32)
+    rx = np.arange(1, n + 1, 2)
+    r = oracle.acoustic2d(vp, rho, 10.0, 1e-3, nt, sx=[n // 2], sz=[n // 2], rx=rx,
+                          rz=np.full(rx.size, n // 2), wavelet=oracle.ricker(15.0, 1e-3, nt)[None],
+                          nbc=50, fd_order=8, snap_interval=30, sponge_factor=0.015)
+    s = r["snaps"][50:-50, 50:-50, :, 0].astype(np.float64)
+    e = (s ** 2).sum(axis=(0, 1))
+    e /= e.max()
+    k = e.size
+    late = e[3 * k // 4 - 1:].mean()  # Julia (3k÷4):k
+    assert abs(late - c["late_energy_sponge"]) / c["late_energy_sponge"] < 1e-3, late
 
 
 # ---------------------------------------------------------------------------
