@@ -17,6 +17,7 @@ struct fomo_ctx {
   int device = 0;
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr;  // snapshot copies that overlap the time loop
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   void* ws = nullptr;  // device workspace, grown on demand and reused
   size_t ws_bytes = 0;

@@ -473,6 +473,25 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
       }
     }
   } exec_guard{chunk_exec, st};
+  // Snapshot streaming: with host outputs, the frames of replayed chunk k are
+  // copied to the caller's buffer on the copy stream once chunk k has run (an
+  // event per chunk), while later chunks compute.  Only the frames of the
+  // step-by-step remainder are copied after the time loop.
+  struct ChunkEvents {
+    std::vector<cudaEvent_t> ev;
+    ~ChunkEvents() {
+      for (auto e : ev) cudaEventDestroy(e);
+    }
+  } chunk_ev;
+  int streamed_chunks = 0, frames_per_chunk = 0;
+  auto replay = [&](int nchunk) -> cudaError_t {
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; e == cudaSuccess && k < nchunk; ++k) {
+      e = cudaGraphLaunch(chunk_exec, st);
+      if (e == cudaSuccess && k < (int)chunk_ev.ev.size()) e = cudaEventRecord(chunk_ev.ev[k], st);
+    }
+    return e;
+  };
   {
     const bool scalar = P.phys == kScalar;
     const bool elastic = P.phys == kElastic;
@@ -491,6 +510,11 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
     }
     const int nchunk = K > 0 ? P.nt / K : 0;
     if (nchunk >= 2) {
+      if (si && !P.dev && outs.snaps) {
+        chunk_ev.ev.assign(nchunk, nullptr);
+        for (auto& e : chunk_ev.ev) FOMO_CU(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        frames_per_chunk = K / si;
+      }
       int* d_it = ws_ptr<int>(ctx, o_it);
       FOMO_CU(ctx, cudaMemsetAsync(d_it, 0, sizeof(int), st));
       const cudaStream_t cs = ctx->own_stream;  // the caller's may be uncapturable
@@ -525,10 +549,11 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
         ce = cudaStreamEndCapture(cs, &graph);
         if (ce == cudaSuccess) ce = cudaGraphInstantiate(&chunk_exec, graph, 0);
         if (graph) cudaGraphDestroy(graph);
-        for (int k = 0; ce == cudaSuccess && k < nchunk; ++k) ce = cudaGraphLaunch(chunk_exec, st);
+        if (ce == cudaSuccess) ce = replay(nchunk);
         if (ce == cudaSuccess) {
           launches += nchunk * nodes;
           it_first = nchunk * K + 1;
+          if (frames_per_chunk) streamed_chunks = nchunk;
         }
       } else if (ce == cudaSuccess && elastic) {
         const ElMat& m = emat;
@@ -571,10 +596,11 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
         ce = cudaStreamEndCapture(cs, &graph);
         if (ce == cudaSuccess) ce = cudaGraphInstantiate(&chunk_exec, graph, 0);
         if (graph) cudaGraphDestroy(graph);
-        for (int k = 0; ce == cudaSuccess && k < nchunk; ++k) ce = cudaGraphLaunch(chunk_exec, st);
+        if (ce == cudaSuccess) ce = replay(nchunk);
         if (ce == cudaSuccess) {
           launches += nchunk * nodes;
           it_first = nchunk * K + 1;
+          if (frames_per_chunk) streamed_chunks = nchunk;
         }
       } else if (ce == cudaSuccess) {
         int a = A, b = B, nodes = 0;
@@ -616,16 +642,28 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
         ce = cudaStreamEndCapture(cs, &graph);
         if (ce == cudaSuccess) ce = cudaGraphInstantiate(&chunk_exec, graph, 0);
         if (graph) cudaGraphDestroy(graph);
-        for (int k = 0; ce == cudaSuccess && k < nchunk; ++k) ce = cudaGraphLaunch(chunk_exec, st);
+        if (ce == cudaSuccess) ce = replay(nchunk);
         if (ce == cudaSuccess) {
           launches += nchunk * nodes;
           it_first = nchunk * K + 1;
+          if (frames_per_chunk) streamed_chunks = nchunk;
         }
       }
       if (ce != cudaSuccess)
         return fail(ctx, FOMO_ECUDA, std::string("replayed step chunk: ") + cudaGetErrorString(ce));
     }
   }
+  // Step-by-step runs with host snapshots copy frame k-1 once frame k is written:
+  // the host waits on that pageable copy while the GPU still holds snap_interval
+  // queued steps.  (Replayed chunks stream their frames after the loop instead.)
+  const bool lag_stream = !P.dev && d_snap && outs.snaps && P.snap_interval > 0 &&
+                          streamed_chunks == 0;
+  ChunkEvents frame_ev;
+  if (lag_stream) {
+    frame_ev.ev.assign(2, nullptr);
+    for (auto& e : frame_ev.ev) FOMO_CU(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  long long lag_done = 0;  // frames [0, lag_done) copied during the loop
   for (int it = it_first; it <= P.nt; ++it) {
     FOMO_CU(ctx, prof_mark(it, 0));
     if (P.phys == kElastic) {
@@ -764,6 +802,17 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
                                      sizeof(float) * P.ld, sizeof(float) * P.nx, P.nz,
                                      cudaMemcpyDeviceToDevice, st));
     }
+    if (lag_stream && it % P.snap_interval == 0) {
+      const int k = it / P.snap_interval - 1;
+      FOMO_CU(ctx, cudaEventRecord(frame_ev.ev[k & 1], st));
+      if (k >= 1) {
+        FOMO_CU(ctx, cudaStreamWaitEvent(ctx->copy_stream, frame_ev.ev[(k - 1) & 1], 0));
+        FOMO_CU(ctx, cudaMemcpyAsync(outs.snaps + (long long)(k - 1) * nint,
+                                     d_snap + (long long)(k - 1) * nint, sizeof(float) * nint,
+                                     cudaMemcpyDeviceToHost, ctx->copy_stream));
+        lag_done = k;
+      }
+    }
     if (P.phys == kScalar) {
       int t = A;
       A = B;
@@ -777,12 +826,25 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
 
   // ---- results ----
   if (!P.dev) {
+    // frames of the replayed chunks first: each waits only for its own chunk (a
+    // copy into pageable memory returns when done, so these overlap the chunks
+    // that follow; a copy on st would wait for the whole loop)
+    const long long streamed =
+        streamed_chunks ? (long long)streamed_chunks * frames_per_chunk : lag_done;
+    for (int k = 0; k < streamed_chunks; ++k) {
+      FOMO_CU(ctx, cudaStreamWaitEvent(ctx->copy_stream, chunk_ev.ev[k], 0));
+      const long long f0 = (long long)k * frames_per_chunk;
+      FOMO_CU(ctx, cudaMemcpyAsync(outs.snaps + f0 * nint, d_snap + f0 * nint,
+                                   sizeof(float) * frames_per_chunk * nint,
+                                   cudaMemcpyDeviceToHost, ctx->copy_stream));
+    }
     for (int k = 0; k < outs.nseis; ++k)
       if (outs.seis[k] && seis_n)
         FOMO_CU(ctx, cudaMemcpyAsync(outs.seis[k], d_seis[k], sizeof(float) * seis_n,
                                      cudaMemcpyDeviceToHost, st));
-    if (d_snap && P.nsnap)
-      FOMO_CU(ctx, cudaMemcpyAsync(outs.snaps, d_snap, sizeof(float) * P.nsnap * nint,
+    if (d_snap && P.nsnap > streamed)
+      FOMO_CU(ctx, cudaMemcpyAsync(outs.snaps + streamed * nint, d_snap + streamed * nint,
+                                   sizeof(float) * (P.nsnap - streamed) * nint,
                                    cudaMemcpyDeviceToHost, st));
   }
   if (opts && opts->final_state) {
@@ -808,6 +870,7 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
       }
   }
   FOMO_CU(ctx, cudaStreamSynchronize(st));
+  if (streamed_chunks || lag_done) FOMO_CU(ctx, cudaStreamSynchronize(ctx->copy_stream));
   if (kernel == FOMO_KERNEL_SINGLE_SWEEP) {
     int hflag = 0;
     FOMO_CU(ctx, cudaMemcpy(&hflag, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost));

@@ -66,6 +66,22 @@ def test_acoustic2d_chunks_equal_step_launches(fomo, step_launch):
     assert la == lb + 8
 
 
+def test_acoustic2d_streamed_snapshots_with_remainder(fomo, step_launch):
+    """Snapshots every 40 steps, 290 steps: three replayed 80-step chunks whose six
+    frames are copied out while later chunks run, and a 50-step remainder holding
+    the seventh frame."""
+    vp, rho = _model()
+    kw = dict(sx=[45], sz=[10], rx=np.arange(1, 91, 4), rz=np.full(23, 8), nbc=10, fd_order=8,
+              snap_interval=40)
+    a = fomo.acoustic2d(vp, rho, 10.0, 1e-3, 290, 15.0, **kw)
+    b = step_launch(fomo.acoustic2d, vp, rho, 10.0, 1e-3, 290, 15.0, **kw)
+    assert len(a.snaps) == len(b.snaps) == 7
+    for x, y in zip(a.snaps, b.snaps):
+        assert np.array_equal(x, y)
+    assert np.array_equal(a.seis_p, b.seis_p)
+    assert all(np.abs(x).max() > 0 for x in a.snaps)
+
+
 def test_acoustic2d_batch_chunks_equal_step_launches(fomo, step_launch):
     """Two shots, no snapshots, 200 steps: three 64-step chunks and 8 single steps."""
     vp, rho = _model()
