@@ -1,7 +1,7 @@
 """fomo_b200 -- Fomo.jl's time-stepping solvers on B200 (sm_100a) via libfomo_b200.so.
 
 Python mirror of the reference's public API (acoustic2d, elastic2d, scalar2d,
-the _batch variants, acoustic3d and elastic3d) over the C ABI in include/fomo_b200.h.  The CUDA
+the _batch variants, acoustic3d, elastic3d and coupled2d) over the C ABI in include/fomo_b200.h.  The CUDA
 library is the only compute path; there is no CPU fallback.
 """
 from ._lib import FomoError, context, lib  # noqa: F401
@@ -11,6 +11,8 @@ from .api import (  # noqa: F401
     acoustic3d,
     acoustic2d_batch,
     acoustic2d_uneven,
+    coupled2d,
+    debug_coupled_medium,
     debug_medium2d,
     elastic2d,
     elastic2d_batch,

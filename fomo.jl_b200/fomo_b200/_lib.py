@@ -35,6 +35,7 @@ EXPORTS = (
     "fomo_scalar2d_noalloc", "fomo_acoustic3d", "fomo_elastic3d", "fomo_acoustic2d_uneven",
     "fomo_corr_param_count", "fomo_corr_features", "fomo_corr_target", "fomo_corr_forward",
     "fomo_corr_gradients", "fomo_corr_adam", "fomo_scalar2d_snapshots", "fomo_scalar2d_corrected",
+    "fomo_coupled2d", "fomo_debug_coupled_medium",
 )
 
 
@@ -122,6 +123,10 @@ def lib() -> C.CDLL:
             L.fomo_elastic2d_batch.argtypes = [vp, g, vp, vp, vp, a, vp, vp, o, s]
             L.fomo_scalar2d.argtypes = [vp, g, vp, a, vp, o, s]
             L.fomo_debug_medium2d.argtypes = [vp, i32, i32, i32, i32, f32, f32, vp, vp, vp, vp]
+            L.fomo_coupled2d.argtypes = [vp, g, vp, vp, f32, C.c_double, a, i32, vp, vp, vp, vp,
+                                         o, s]
+            L.fomo_debug_coupled_medium.argtypes = [vp, i32, i32, i32, i32, f32, C.c_double, vp,
+                                                    vp, vp]
             L.fomo_scalar2d_noalloc.argtypes = [g, vp, a, vp, vp, C.c_char_p, i32]
             L.fomo_scalar2d_noalloc.restype = C.c_int
             L.fomo_acoustic2d_uneven.argtypes = [vp, f32, f32, i32, i32, i32, i32,

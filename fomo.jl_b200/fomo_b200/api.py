@@ -114,6 +114,15 @@ class Elastic2DBatchResult(NamedTuple):
     stats: BatchStats
 
 
+class Coupled2DResult(NamedTuple):
+    """coupled2d's NamedTuple (coupled2d.jl:165-170)."""
+    seis_P: np.ndarray
+    seis_S: np.ndarray
+    snaps_P: list
+    snaps_S: list
+    stats: Stats
+
+
 class Scalar2DResult(NamedTuple):
     seis_u: np.ndarray
     stats: Stats
@@ -621,4 +630,61 @@ def debug_medium2d(kind: str, vp, vs, rho, pad: int, dt=1.0, dh=1.0, device: int
     ctx.check(L.lib().fomo_debug_medium2d(ctx.handle, k, nx, nz, pad, float(np.float32(dt)),
                                           float(np.float32(dh)), _ptr(vp), _ptr(vs), _ptr(rho),
                                           _ptr(out)))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# coupled2d: coupled P-S potentials (equations/coupled2d/coupled2d.jl:53-171)
+# ---------------------------------------------------------------------------
+def coupled2d(vp, vs, dh, dt, nt, f0, *, sx: Sequence[int], sz: Sequence[int], rx, rz,
+              nbc: int = 50, fd_order: int = 8, snap_interval: int = 0, v_ref_p=None,
+              v_ref_s=None, smooth_sigma: float = 3.0, wavelet=None, verbose: bool = True,
+              device: int = 0) -> Coupled2DResult:
+    """2D coupled P-S potential simulation (constant density).  ``smooth_sigma``
+    smooths alpha = vp^2, beta = vs^2 (grid points) before their derivatives."""
+    vp, vs = _f32F(vp), _f32F(vs)
+    nx, nz = vp.shape
+    if vs.shape != vp.shape:
+        raise ArgumentError("vp and vs sizes differ")
+    dh, dt, f0 = np.float32(dh), np.float32(dt), np.float32(f0)
+    _check_geometry(nx, nz, sx, sz, rx, rz)
+    vmin_disp = _min_pos(vs) if np.any(vs > 0) else _min_pos(vp)  # coupled2d.jl:75-76
+    _check_numerics(vp.max(), vmin_disp, dh, dt, f0, fd_order, centered=True)
+    v_ref_p = _min_pos(vp) if v_ref_p is None else np.float32(v_ref_p)
+    v_ref_s = _min_pos(vs) if v_ref_s is None else np.float32(v_ref_s)
+    w = _wavelet_row(wavelet, f0, dt, nt)
+    sxv, szv = _i32F(sx).ravel(), _i32F(sz).ravel()
+    if sxv.size != szv.size:
+        raise ArgumentError("sx and sz lengths differ")
+    wm = np.asfortranarray(np.repeat(w[None, :], sxv.size, axis=0))
+    rxv, rzv = _i32F(rx).ravel(), _i32F(rz).ravel()
+    nrec = rxv.size
+    seis = [np.zeros((nrec, nt), dtype=np.float32, order="F") for _ in range(2)]
+    nsnap = nt // snap_interval if snap_interval > 0 else 0
+    snaps = [np.zeros((nx, nz, nsnap), dtype=np.float32, order="F") if nsnap else None
+             for _ in range(2)]
+    st = L.Stats()
+    ctx = L.context(device)
+    g = _grid(nx, nz, dh, dt, nt, nbc, fd_order, v_ref_p)
+    acq = _acq(sxv.reshape(-1, 1, order="F"), szv.reshape(-1, 1, order="F"), wm, rxv, rzv)
+    o = _opts()
+    ctx.check(L.lib().fomo_coupled2d(ctx.handle, C.byref(g), _ptr(vp), _ptr(vs), float(v_ref_s),
+                                     float(smooth_sigma), C.byref(acq), int(snap_interval),
+                                     _ptr(seis[0]), _ptr(seis[1]), _ptr(snaps[0]),
+                                     _ptr(snaps[1]), C.byref(o), C.byref(st)))
+    _remember(st)
+    return Coupled2DResult(seis[0], seis[1], _snap_list(snaps[0]), _snap_list(snaps[1]),
+                           Stats(st.kernel_time_s))
+
+
+def debug_coupled_medium(vp, vs, dh, nbc, fd_order, smooth_sigma=3.0, device: int = 0):
+    """coupled2d's device-prepared medium, (nx + 2 pad, nz + 2 pad, 8)."""
+    vp, vs = _f32F(vp), _f32F(vs)
+    nx, nz = vp.shape
+    pad = nbc + fd_order // 2
+    out = np.zeros((nx + 2 * pad, nz + 2 * pad, 8), np.float32, order="F")
+    ctx = L.context(device)
+    ctx.check(L.lib().fomo_debug_coupled_medium(ctx.handle, nx, nz, int(nbc), int(fd_order),
+                                                float(dh), float(smooth_sigma), _ptr(vp),
+                                                _ptr(vs), _ptr(out)))
     return out

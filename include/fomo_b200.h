@@ -319,7 +319,29 @@ FOMO_API int fomo_scalar2d_corrected(fomo_ctx* ctx, const fomo_grid2d* g, const 
 FOMO_API int fomo_scalar2d_noalloc(const fomo_grid2d* g, const float* vp, const fomo_acq* acq,
                                    float* seis_u, void* stream, char* err, int32_t err_len);
 
+/* ---- coupled P-S potentials -------------------------------------------- */
+/* coupled2d (equations/coupled2d/coupled2d.jl:53-171): constant-density coupled
+ * P and S potentials on a regular grid with centered differences.  g->v_ref is
+ * v_ref_p and v_ref_s the S field's HABC velocity (<= 0: minimum of the
+ * positive vp, resp. vs).  smooth_sigma: Gaussian smoothing in grid points of
+ * alpha = vp^2 and beta = vs^2 before their derivatives (<= 0: none; radius
+ * ceil(3 sigma) <= 1024).  The wavelet (n_src, nt) is added to P.  Host arrays
+ * only; FP32; HABC only (the reference's racy HABC in deterministic form).
+ * seis_P, seis_S: (n_rec, nt); snaps_P, snaps_S: (nx, nz, nt / snap_interval)
+ * or NULL.  acq->n_shots must be 1. */
+FOMO_API int fomo_coupled2d(fomo_ctx* ctx, const fomo_grid2d* g, const float* vp,
+                            const float* vs, float v_ref_s, double smooth_sigma,
+                            const fomo_acq* acq, int32_t snap_interval, float* seis_P,
+                            float* seis_S, float* snaps_P, float* snaps_S,
+                            const fomo_opts* opts, fomo_stats* stats);
+
 /* ---- diagnostics -------------------------------------------------------- */
+/* coupled2d's device medium (coupled2d/medium.jl:46-107) downloaded to `out`,
+ * (nx + 2 pad, nz + 2 pad, 8) column-major with pad = nbc + fd_order / 2:
+ * alpha, beta, d alpha/dx, d alpha/dz, d beta/dx, d beta/dz, lap alpha, lap beta. */
+FOMO_API int fomo_debug_coupled_medium(fomo_ctx* ctx, int32_t nx, int32_t nz, int32_t nbc,
+                                       int32_t fd_order, float dh, double smooth_sigma,
+                                       const float* vp, const float* vs, float* out);
 /* Device-side medium preparation, downloaded to `out` (padded, column-major):
  * kind 0 elastic -> bx,bz,lam,lam2mu,mu_txz; 1 acoustic -> bx,bz,kappa;
  * 2 scalar -> c2.  Mirrors utils/pad_array.jl and equations/<eq>/medium.jl. */

@@ -1119,6 +1119,249 @@ int run_elastic3d(int nx, int ny, int nz, const float* vp, const float* vs, cons
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// coupled2d: coupled P-S potentials (equations/coupled2d/*, constant density).
+// ---------------------------------------------------------------------------
+// utils/FD_centered.jl:15-21 -- centered first-derivative coefficients.
+const float kD1[6][5] = {
+    {0, 0, 0, 0, 0},
+    {(float)0.5, 0, 0, 0, 0},
+    {(float)(2.0 / 3.0), (float)(-1.0 / 12.0), 0, 0, 0},
+    {(float)(3.0 / 4.0), (float)(-3.0 / 20.0), (float)(1.0 / 60.0), 0, 0},
+    {(float)(4.0 / 5.0), (float)(-1.0 / 5.0), (float)(4.0 / 105.0), (float)(-1.0 / 280.0), 0},
+    {(float)(5.0 / 6.0), (float)(-5.0 / 21.0), (float)(5.0 / 84.0), (float)(-5.0 / 504.0),
+     (float)(1.0 / 1260.0)},
+};
+
+// coupled2d/medium.jl:121-126 -- taps exp(-0.5 (k/sigma)^2), k = -r..r, r = ceil(3 sigma),
+// rounded to T and divided by their sum (summed in T from k = -r).
+template <class T>
+std::vector<T> gaussian_taps(double sigma) {
+  const int r = (int)std::ceil(3.0 * sigma);
+  std::vector<T> k((size_t)(2 * r + 1));
+  for (int q = -r; q <= r; ++q) {
+    const double x = (double)q / sigma;
+    k[(size_t)(q + r)] = (T)std::exp(-0.5 * (x * x));
+  }
+  T s = T(0);
+  for (T v : k) s = s + v;
+  for (T& v : k) v = v / s;
+  return k;
+}
+
+// coupled2d/medium.jl:118-151 -- separable smoothing, x pass then z pass, clamped
+// indices; each tap is one multiply and one add (the reference's CPU loop).
+template <class T>
+std::vector<T> gaussian_smooth(const G2& g, const std::vector<T>& f, const std::vector<T>& taps) {
+  const int r = (int)(taps.size() - 1) / 2;
+  std::vector<T> tmp(g.n()), out(g.n());
+#pragma omp parallel for schedule(static)
+  for (int j = 1; j <= g.nz; ++j)
+    for (int i = 1; i <= g.nx; ++i) {
+      T v = T(0);
+      for (int q = -r; q <= r; ++q) {
+        const int ii = std::min(std::max(i + q, 1), g.nx);
+        v = v + taps[(size_t)(q + r)] * f[g.at(ii, j)];
+      }
+      tmp[g.at(i, j)] = v;
+    }
+#pragma omp parallel for schedule(static)
+  for (int j = 1; j <= g.nz; ++j)
+    for (int i = 1; i <= g.nx; ++i) {
+      T v = T(0);
+      for (int q = -r; q <= r; ++q) {
+        const int jj = std::min(std::max(j + q, 1), g.nz);
+        v = v + taps[(size_t)(q + r)] * tmp[g.at(i, jj)];
+      }
+      out[g.at(i, j)] = v;
+    }
+  return out;
+}
+
+// coupled2d/medium.jl:157-193 -- gradients (x: M < i <= nx-M, every j; z: the
+// transpose) and the Laplacian (both ranges) of the smoothed field; 0 elsewhere.
+template <class T>
+void coupled_derivs(const G2& g, int N, T h, const std::vector<T>& f, T* dx, T* dz, T* lap) {
+  const int M = N;
+  const T ih2 = T(1) / (h * h);
+  const T c0 = (T)kD2C0[N];
+  for (size_t q = 0; q < g.n(); ++q) dx[q] = dz[q] = lap[q] = T(0);
+#pragma omp parallel for schedule(static)
+  for (int j = 1; j <= g.nz; ++j)
+    for (int i = 1; i <= g.nx; ++i) {
+      const size_t p = g.at(i, j);
+      if (i > M && i <= g.nx - M) {
+        T v = T(0);
+        for (int l = 1; l <= N; ++l) v = v + (T)kD1[N][l - 1] * (f[p + l] - f[p - l]);
+        dx[p] = v / h;
+      }
+      if (j > M && j <= g.nz - M) {
+        T v = T(0);
+        for (int l = 1; l <= N; ++l)
+          v = v + (T)kD1[N][l - 1] * (f[p + (size_t)l * g.nx] - f[p - (size_t)l * g.nx]);
+        dz[p] = v / h;
+      }
+      if (i > M && i <= g.nx - M && j > M && j <= g.nz - M) {
+        T a = c0 * f[p], b = c0 * f[p];
+        for (int l = 1; l <= N; ++l) {
+          a = a + (T)kD2[N][l - 1] * (f[p + l] + f[p - l]);
+          b = b + (T)kD2[N][l - 1] * (f[p + (size_t)l * g.nx] + f[p - (size_t)l * g.nx]);
+        }
+        lap[p] = (a + b) * ih2;
+      }
+    }
+}
+
+// The eight planes of CoupledMedium (medium.jl:46-107): alpha, beta (unsmoothed
+// vp^2, vs^2), then d alpha/dx, d alpha/dz, d beta/dx, d beta/dz, lap alpha,
+// lap beta of the smoothed fields (smooth_sigma <= 0: no smoothing).
+template <class T>
+std::vector<T> coupled_medium(const G2& g, int N, const float* vp, const float* vs, int nx,
+                              int nz, int pad, float dh, double sigma) {
+  const size_t n = g.n();
+  std::vector<T> m(8 * n);
+  std::vector<T> vpp = pad_array<T>(vp, nx, nz, pad), vsp = pad_array<T>(vs, nx, nz, pad);
+  std::vector<T> a(n), b(n);
+  for (size_t q = 0; q < n; ++q) {
+    a[q] = vpp[q] * vpp[q];
+    b[q] = vsp[q] * vsp[q];
+  }
+  std::vector<T> as = a, bs = b;
+  if (sigma > 0) {
+    const std::vector<T> taps = gaussian_taps<T>(sigma);
+    as = gaussian_smooth(g, a, taps);
+    bs = gaussian_smooth(g, b, taps);
+  }
+  std::copy(a.begin(), a.end(), m.begin());
+  std::copy(b.begin(), b.end(), m.begin() + n);
+  const T h = (T)dh;
+  coupled_derivs(g, N, h, as, m.data() + 2 * n, m.data() + 3 * n, m.data() + 6 * n);
+  coupled_derivs(g, N, h, bs, m.data() + 4 * n, m.data() + 5 * n, m.data() + 7 * n);
+  return m;
+}
+
+template <class T>
+struct CoupledState {
+  std::vector<T> P, S, dP, dS, o1, o2;
+};
+
+// update_fields.jl:27-108, "velocity" half step on M < i, j <= n - M.  The
+// operation order (one fma per stencil term, the right-hand sides as written
+// below) is this implementation's canonical FP32 sequence; the GPU kernel
+// repeats it.
+template <class T>
+void coupled_vel(const G2& g, int N, const T* m, T dt, T ih, T ih2, CoupledState<T>& s) {
+  const int M = N;
+  const size_t n = g.n(), nx = g.nx;
+  const T c0 = (T)kD2C0[N];
+#pragma omp parallel for schedule(static)
+  for (int j = M + 1; j <= g.nz - M; ++j)
+    for (int i = M + 1; i <= g.nx - M; ++i) {
+      const size_t p = g.at(i, j);
+      const T* P = s.P.data();
+      const T* S = s.S.data();
+      T dPx = 0, dPz = 0, dSx = 0, dSz = 0;
+      T lPx = c0 * P[p], lPz = c0 * P[p], lSx = c0 * S[p], lSz = c0 * S[p];
+      for (int l = 1; l <= N; ++l) {
+        const T c1 = (T)kD1[N][l - 1], c2 = (T)kD2[N][l - 1];
+        const size_t lz = (size_t)l * nx;
+        dPx = fmaT(c1, P[p + l] - P[p - l], dPx);
+        dPz = fmaT(c1, P[p + lz] - P[p - lz], dPz);
+        lPx = fmaT(c2, P[p + l] + P[p - l], lPx);
+        lPz = fmaT(c2, P[p + lz] + P[p - lz], lPz);
+        dSx = fmaT(c1, S[p + l] - S[p - l], dSx);
+        dSz = fmaT(c1, S[p + lz] - S[p - lz], dSz);
+        lSx = fmaT(c2, S[p + l] + S[p - l], lSx);
+        lSz = fmaT(c2, S[p + lz] + S[p - lz], lSz);
+      }
+      dPx = dPx * ih;
+      dPz = dPz * ih;
+      dSx = dSx * ih;
+      dSz = dSz * ih;
+      const T lapP = (lPx + lPz) * ih2, lapS = (lSx + lSz) * ih2;
+      const T a = m[p], b = m[n + p], ax = m[2 * n + p], az = m[3 * n + p], bx = m[4 * n + p],
+              bz = m[5 * n + p], la = m[6 * n + p], lb = m[7 * n + p];
+      const T Pc = P[p];
+      T rP = Pc * la;
+      rP = fmaT(T(2), fmaT(ax, dPx, az * dPz), rP);
+      rP = fmaT(T(-2) * Pc, lb, rP);
+      rP = fmaT(T(2), fmaT(bx, dSz, -(bz * dSx)), rP);
+      rP = fmaT(a, lapP, rP);
+      T rS = T(2) * fmaT(bx, dSx, bz * dSz);
+      rS = fmaT(T(2), fmaT(bz, dPx, -(bx * dPz)), rS);
+      rS = fmaT(b, lapS, rS);
+      s.dP[p] = fmaT(dt, rP, s.dP[p]);
+      s.dS[p] = fmaT(dt, rS, s.dS[p]);
+    }
+}
+
+// update_fields.jl:120-141, "position" half step.
+template <class T>
+void coupled_pos(const G2& g, int M, T dt, CoupledState<T>& s) {
+#pragma omp parallel for schedule(static)
+  for (int j = M + 1; j <= g.nz - M; ++j)
+    for (int i = M + 1; i <= g.nx - M; ++i) {
+      const size_t p = g.at(i, j);
+      s.P[p] = fmaT(dt, s.dP[p], s.P[p]);
+      s.S[p] = fmaT(dt, s.dS[p], s.S[p]);
+    }
+}
+
+// coupled2d.jl:53-171 and the loop :192-260.  The loop's racy full-grid HABC
+// (boundary/habc/kernels.jl:122-190) is applied in the deterministic two-pass
+// form (pre-correction neighbours), with weights w_vx for dP/dt, dS/dt and
+// w_tau for P, S, and the Higdon coefficients of v_ref_p (P fields) and
+// v_ref_s (S fields).
+template <class T>
+int run_coupled2d(int nx, int nz, const float* vp, const float* vs, float dh, float dt, int nt,
+                  int nbc, int fd_order, float v_ref_p, float v_ref_s, double sigma, int n_src,
+                  const int32_t* sx, const int32_t* sz, const float* wavelet, int n_rec,
+                  const int32_t* rx, const int32_t* rz, T* seis_P, T* seis_S, int snap_interval,
+                  T* snaps_P, T* snaps_S, T* medium_out) {
+  const int N = order_to_N(fd_order);
+  if (N < 0) return -2;
+  const int M = N, pad = nbc + M;
+  if (pad < 2) return -2;
+  G2 g{nx + 2 * pad, nz + 2 * pad};
+  const std::vector<T> med = coupled_medium<T>(g, N, vp, vs, nx, nz, pad, dh, sigma);
+  if (medium_out) std::copy(med.begin(), med.end(), medium_out);
+  Habc<T> hp = init_habc<T>(pad, v_ref_p, dt, dh), hs = init_habc<T>(pad, v_ref_s, dt, dh);
+  std::vector<FramePt> fr = frame_points(g, hp.nbc);
+  const T tdt = (T)dt, ih = T(1) / (T)dh, ih2 = ih * ih;
+  const size_t ncell = g.n(), nint = (size_t)nx * nz;
+  CoupledState<T> st;
+  for (auto* v : {&st.P, &st.S, &st.dP, &st.dS, &st.o1, &st.o2}) v->assign(ncell, T(0));
+  std::vector<T> scr;
+  for (int it = 1; it <= nt; ++it) {
+    st.o1 = st.dP;
+    st.o2 = st.dS;
+    coupled_vel(g, N, med.data(), tdt, ih, ih2, st);
+    habc_det(g, hp, fr, 0, st.dP.data(), st.o1.data(), scr);
+    habc_det(g, hs, fr, 0, st.dS.data(), st.o2.data(), scr);
+    st.o1 = st.P;
+    st.o2 = st.S;
+    coupled_pos(g, M, tdt, st);
+    habc_det(g, hp, fr, 2, st.P.data(), st.o1.data(), scr);
+    habc_det(g, hs, fr, 2, st.S.data(), st.o2.data(), scr);
+    for (int q = 0; q < n_src; ++q) {  // inject_source!(P): coupled2d.jl:239-243
+      size_t p = g.at(sx[q] + pad, sz[q] + pad);
+      st.P[p] += (T)wavelet[(size_t)q + (size_t)n_src * (it - 1)];
+    }
+    for (int r = 0; r < n_rec; ++r) {  // coupled2d.jl:245-250
+      size_t p = g.at(rx[r] + pad, rz[r] + pad);
+      size_t o = (size_t)r + (size_t)n_rec * (it - 1);
+      if (seis_P) seis_P[o] = st.P[p];
+      if (seis_S) seis_S[o] = st.S[p];
+    }
+    if (snap_interval > 0 && it % snap_interval == 0) {  // coupled2d.jl:252-258
+      const int k = it / snap_interval - 1;
+      if (snaps_P) snap_interior(g, pad, st.P.data(), snaps_P + nint * (size_t)k);
+      if (snaps_S) snap_interior(g, pad, st.S.data(), snaps_S + nint * (size_t)k);
+    }
+  }
+  return 0;
+}
+
 extern "C" {
 
 int oracle_version(void) { return 1; }
@@ -1282,6 +1525,24 @@ int oracle_elastic2d_sponge(int prec, float sponge_factor, int nx, int nz, int n
                             sz, wavelet, n_rec, rx, rz, (double*)seis_vx, (double*)seis_vz,
                             snap_interval, (double*)snaps, (double*)final_fields, StoreSpec(),
                             sponge_factor));
+}
+
+int oracle_coupled2d(int prec, int nx, int nz, const float* vp, const float* vs, float dh,
+                     float dt, int nt, int nbc, int fd_order, float v_ref_p, float v_ref_s,
+                     double smooth_sigma, int n_src, const int32_t* sx, const int32_t* sz,
+                     const float* wavelet, int n_rec, const int32_t* rx, const int32_t* rz,
+                     void* seis_P, void* seis_S, int snap_interval, void* snaps_P, void* snaps_S,
+                     void* medium_out) {
+  return ORACLE_PREC_DISPATCH(
+      prec,
+      run_coupled2d<float>(nx, nz, vp, vs, dh, dt, nt, nbc, fd_order, v_ref_p, v_ref_s,
+                           smooth_sigma, n_src, sx, sz, wavelet, n_rec, rx, rz, (float*)seis_P,
+                           (float*)seis_S, snap_interval, (float*)snaps_P, (float*)snaps_S,
+                           (float*)medium_out),
+      run_coupled2d<double>(nx, nz, vp, vs, dh, dt, nt, nbc, fd_order, v_ref_p, v_ref_s,
+                            smooth_sigma, n_src, sx, sz, wavelet, n_rec, rx, rz, (double*)seis_P,
+                            (double*)seis_S, snap_interval, (double*)snaps_P, (double*)snaps_S,
+                            (double*)medium_out));
 }
 
 // sponge_table for the tests (boundary/sponge.jl:31-48).

@@ -68,6 +68,11 @@ def lib():
                                               C.c_int, _i32p, _i32p, vp, vp, C.c_int, vp, vp]
         L.oracle_sponge_table.restype = C.c_int
         L.oracle_sponge_table.argtypes = [C.c_int, C.c_float, vp]
+        L.oracle_coupled2d.restype = C.c_int
+        L.oracle_coupled2d.argtypes = [C.c_int, C.c_int, C.c_int, _f32p, _f32p, C.c_float,
+                                       C.c_float, C.c_int, C.c_int, C.c_int, C.c_float,
+                                       C.c_float, C.c_double, C.c_int, _i32p, _i32p, _f32p,
+                                       C.c_int, _i32p, _i32p, vp, vp, C.c_int, vp, vp, vp]
         L.oracle_scalar2d.restype = C.c_int
         L.oracle_scalar2d.argtypes = [C.c_int, C.c_int, C.c_int, _f32p, C.c_float, C.c_float,
                                       C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, _i32p, _i32p,
@@ -327,6 +332,37 @@ def habc_apply(f, f_old, pad, v_ref, dt, dh, kind):
     nxp, nzp = f.shape
     lib().oracle_habc_apply_f32(nxp, nzp, pad, v_ref, dt, dh, kind, _ptr(f), _ptr(fo))
     return f
+
+
+def coupled2d(vp, vs, dh, dt, nt, *, sx, sz, rx, rz, wavelet, nbc=50, fd_order=8,
+              v_ref_p=None, v_ref_s=None, smooth_sigma=3.0, snap_interval=0, prec=32,
+              medium=False):
+    """Coupled P-S potential run (equations/coupled2d).  ``wavelet``: (n_src, nt).
+    ``medium=True`` also returns the eight prepared medium planes (nxp, nzp, 8)."""
+    vp, vs = _f32(vp), _f32(vs)
+    nx, nz = vp.shape
+    sxv, szv = _i32(np.ravel(sx)), _i32(np.ravel(sz))
+    n_src = sxv.size
+    w = _f32(wavelet).reshape(n_src, nt, order="F")
+    rx, rz = _i32(rx), _i32(rz)
+    nrec = rx.size
+    T = _dt(prec)
+    sP = np.zeros((nrec, nt), dtype=T, order="F")
+    sS = np.zeros_like(sP)
+    nsnap = nt // snap_interval if snap_interval > 0 else 0
+    snP = np.zeros((nx, nz, nsnap), dtype=T, order="F") if nsnap else None
+    snS = np.zeros_like(snP) if nsnap else None
+    M = fd_order // 2
+    nxp, nzp = nx + 2 * (nbc + M), nz + 2 * (nbc + M)
+    med = np.zeros((nxp, nzp, 8), dtype=T, order="F") if medium else None
+    vrp = default_v_ref(vp) if v_ref_p is None else float(v_ref_p)
+    vrs = default_v_ref(vs) if v_ref_s is None else float(v_ref_s)
+    rc = lib().oracle_coupled2d(prec, nx, nz, vp, vs, dh, dt, nt, nbc, fd_order, vrp, vrs,
+                                float(smooth_sigma), n_src, sxv, szv, w, nrec, rx, rz, _ptr(sP),
+                                _ptr(sS), snap_interval, _ptr(snP), _ptr(snS), _ptr(med))
+    if rc != 0:
+        raise RuntimeError(f"oracle_coupled2d failed: {rc}")
+    return dict(seis_P=sP, seis_S=sS, snaps_P=snP, snaps_S=snS, medium=med)
 
 
 def sponge_table(nbc, factor):
