@@ -18,6 +18,7 @@ Secondary workloads (one JSON line each, same keys; not the default line):
     --workload elastic3d      elastic3d 400x400x300, nbc 40, order 8 (nt from --nt)
     --workload readme         steps/s on the grids of Fomo's published throughput table
     --workload sponge         Fomo's HABC-vs-sponge benchmark (acoustic and elastic 401x401)
+    --workload coupled        coupled2d on the grids of Fomo's two coupled2d demos
 """
 from __future__ import annotations
 
@@ -566,6 +567,64 @@ def sponge_bench(args):
                           "device": "B200", "dtype": "f32"}), flush=True)
 
 
+def _coupled_demo_models():
+    """The models of example/coupled2d_simple_demo.jl (400x300, two layers) and
+    example/coupled2d_demo.jl (601x601, three thin scatterers)."""
+    vp1 = np.full((400, 300), 2500.0, np.float32, order="F")
+    vs1 = np.full((400, 300), 1200.0, np.float32, order="F")
+    vp1[:, 149:] = 3500.0
+    vs1[:, 149:] = 1800.0
+    vp2 = np.full((601, 601), 3000.0, np.float32, order="F")
+    vs2 = np.full((601, 601), 1500.0, np.float32, order="F")
+    vp2[:, 149:152] = 3300.0
+    vs2[:, 299:302] = 1650.0
+    vp2[:, 449:452] = 3300.0
+    vs2[:, 449:452] = 1650.0
+    return [
+        dict(name="coupled2d_simple_demo", vp=vp1, vs=vs1, dh=10.0, dt=1e-3, nt=2000, sz=10,
+             snap=50),
+        dict(name="coupled2d_demo", vp=vp2, vs=vs2, dh=5.0, dt=5e-4, nt=4000, sz=5, snap=100),
+    ]
+
+
+def coupled_bench(args):
+    """coupled2d on the two demo setups: 15 Hz Ricker at (nx/2, sz), receivers
+    every 2nd x at depth sz, nbc 100, order 8, snapshots of P and S.  `wall_s`:
+    the public call end to end, median of --steps after --warmup calls;
+    `loop_s`: the library's CUDA-event time of the time loop; `alg_gbs`: the
+    algorithmic bytes of the two update kernels (80 B per padded cell and step)
+    over the loop time."""
+    import time
+    import warnings
+
+    import fomo_b200 as F
+
+    warnings.simplefilter("ignore")
+    peak, pkind = _peaks()
+    for c in _coupled_demo_models():
+        nx, nz = c["vp"].shape
+        rx = np.arange(1, nx + 1, 2)
+        kw = dict(sx=[nx // 2], sz=[c["sz"]], rx=rx, rz=np.full(rx.size, c["sz"]), nbc=100,
+                  fd_order=8, snap_interval=c["snap"])
+
+        def run():
+            t0 = time.perf_counter()
+            r = F.coupled2d(c["vp"], c["vs"], c["dh"], c["dt"], c["nt"], 15.0, **kw)
+            return time.perf_counter() - t0, r, F.api.last_stats.alg_bytes
+
+        for _ in range(max(1, args.warmup)):
+            run()
+        runs = [run() for _ in range(max(1, args.steps))]
+        wall = float(np.median([t for t, _, _ in runs]))
+        loop = float(np.median([r.stats.kernel_time_s for _, r, _ in runs]))
+        gbs = runs[-1][2] / loop / 1e9
+        print(json.dumps({"workload": "coupled2d demo", "demo": c["name"], "grid": [nx, nz],
+                          "nt": c["nt"], "snap_interval": c["snap"], "wall_s": wall,
+                          "loop_s": loop, "steps_per_s": c["nt"] / loop, "alg_gbs": gbs,
+                          "hbm_frac": gbs / peak, "peak_gbs": peak, "peak_kind": pkind,
+                          "device": "B200", "dtype": "f32"}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -578,9 +637,16 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", choices=["elastic-batch", "elastic-fp16", "uneven", "elastic3d",
-                                           "readme", "sponge"],
+                                           "readme", "sponge", "coupled"],
                     default="elastic-batch")
     args = ap.parse_args()
+    if args.workload == "coupled":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference publishes no "
+                              "coupled2d timing"}))
+            return
+        coupled_bench(args)
+        return
     if args.workload == "sponge":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference's HABC-vs-sponge "

@@ -439,6 +439,7 @@ int fomo_coupled2d(fomo_ctx* ctx, const fomo_grid2d* gp, const float* vp, const 
   const size_t o_wav = ar.take<float>(std::max<long long>((long long)acq->n_src * nt, 1));
   const size_t o_seis = ar.take<float>(std::max<long long>(2 * seis_n, 1));
   const size_t o_snap = ar.take<float>(std::max<long long>(2LL * nsnap * nint, 1));
+  const size_t o_it = ar.take<int>(1);  // device step index of replayed chunks
   if ((rc = ensure_workspace(ctx, ar.off))) return rc;
   float* d_model = ws_ptr<float>(ctx, o_model);
   float* d_med = ws_ptr<float>(ctx, o_med);
@@ -488,17 +489,87 @@ int fomo_coupled2d(fomo_ctx* ctx, const fomo_grid2d* gp, const float* vp, const 
   dim3 blk(32, 8), grd(cdiv(g.nx, 32), cdiv(g.nz, 8));
   int launches = 0;
   int A = 0, B = 1;
-  FOMO_CU(ctx, cudaEventRecord(ctx->ev0, st));
-  for (int it = 1; it <= nt; ++it) {
+  // one step's two updates on stream `s`, set a -> set b
+  auto updates = [&](cudaStream_t s, int a, int b) {
 #define FOMO_CPV_CASE(NN)                                                                    \
   case NN:                                                                                   \
-    k_cp_vel<NN><<<grd, blk, 0, st>>>(g, c, dt, ih, ih2, hp, hs, m, field(A, 0), field(A, 1), \
-                                      field(A, 2), field(A, 3), field(B, 2), field(B, 3));   \
+    k_cp_vel<NN><<<grd, blk, 0, s>>>(g, c, dt, ih, ih2, hp, hs, m, field(a, 0), field(a, 1),  \
+                                     field(a, 2), field(a, 3), field(b, 2), field(b, 3));    \
     break;
     switch (N) { FOMO_CPV_CASE(1) FOMO_CPV_CASE(2) FOMO_CPV_CASE(3) FOMO_CPV_CASE(4) FOMO_CPV_CASE(5) }
 #undef FOMO_CPV_CASE
-    k_cp_pos<<<grd, blk, 0, st>>>(g, dt, hp, hs, field(A, 0), field(A, 1), field(B, 2),
-                                  field(B, 3), field(B, 0), field(B, 1));
+    k_cp_pos<<<grd, blk, 0, s>>>(g, dt, hp, hs, field(a, 0), field(a, 1), field(b, 2),
+                                 field(b, 3), field(b, 0), field(b, 1));
+  };
+  FOMO_CU(ctx, cudaEventRecord(ctx->ev0, st));
+  // Replayed chunks of K steps (K even: the ping-pong sets return to their
+  // start; a multiple of snap_interval <= 256), captured once with a device
+  // step index, as the acoustic solver does; the rest launch step by step
+  // (FOMO_F_STEP_LAUNCH: every step), with identical results.
+  int it_first = 1;
+  cudaGraphExec_t exec = nullptr;
+  struct ExecGuard {
+    cudaGraphExec_t& e;
+    cudaStream_t s;
+    ~ExecGuard() {
+      if (e) {
+        cudaStreamSynchronize(s);
+        cudaGraphExecDestroy(e);
+      }
+    }
+  } exec_guard{exec, st};
+  {
+    const int si = nsnap ? snap_interval : 0;
+    int K = 0;
+    if (!(opts && (opts->flags & FOMO_F_STEP_LAUNCH))) {
+      if (si == 0) {
+        K = 64;
+      } else if (si <= 256) {
+        K = si * std::max(1, (64 + si / 2) / si);
+        if (K % 2) K *= 2;
+      }
+    }
+    const int nchunk = K > 0 ? nt / K : 0;
+    if (nchunk >= 2) {
+      int* d_it = ws_ptr<int>(ctx, o_it);
+      FOMO_CU(ctx, cudaMemsetAsync(d_it, 0, sizeof(int), st));
+      const cudaStream_t cs = ctx->own_stream;  // the caller's stream may be uncapturable
+      cudaGraph_t graph = nullptr;
+      cudaError_t ce = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+      int nodes = 0;
+      if (ce == cudaSuccess) {
+        int a = A, b = B;
+        for (int j = 0; j < K; ++j) {
+          updates(cs, a, b);
+          k_inject_record_at<<<1, 256, 0, cs>>>(d_it, j, nt, pl, acq->n_src, d_src, d_wav,
+                                                field(b, 0), nullptr, acq->n_rec, d_rec,
+                                                field(b, 0), field(b, 1), nullptr, d_seis,
+                                                d_seis + seis_n, nullptr);
+          nodes += 3;
+          if (si && (j + 1) % si == 0) {
+            for (int f = 0; f < 2; ++f)
+              k_snap_at<<<dim3(cdiv(nx, 128), nz), 128, 0, cs>>>(
+                  d_it, j, si, field(b, f) + pad + (long long)pad * g.ld, g.ld, nx, nz,
+                  d_snap + (long long)f * nsnap * nint);
+            nodes += 2;
+          }
+          std::swap(a, b);
+        }
+        k_step_add<<<1, 1, 0, cs>>>(d_it, K);
+        ++nodes;
+        ce = cudaStreamEndCapture(cs, &graph);
+      }
+      if (ce == cudaSuccess) ce = cudaGraphInstantiate(&exec, graph, 0);
+      if (graph) cudaGraphDestroy(graph);
+      for (int k = 0; ce == cudaSuccess && k < nchunk; ++k) ce = cudaGraphLaunch(exec, st);
+      if (ce != cudaSuccess)
+        return fail(ctx, FOMO_ECUDA, std::string("replayed step chunk: ") + cudaGetErrorString(ce));
+      launches += nchunk * nodes;
+      it_first = nchunk * K + 1;
+    }
+  }
+  for (int it = it_first; it <= nt; ++it) {
+    updates(st, A, B);
     k_inject_record<<<1, 256, 0, st>>>(it, nt, pl, acq->n_src, d_src, d_wav, field(B, 0), nullptr,
                                        acq->n_rec, d_rec, field(B, 0), field(B, 1), nullptr,
                                        d_seis, d_seis + seis_n, nullptr);

@@ -52,7 +52,9 @@ def test_coupled2d_bitwise_vs_oracle(fomo, oracle, fd_order):
     assert rel_l2(r.seis_P, o64["seis_P"]) < 1e-5
     assert rel_l2(r.seis_S, o64["seis_S"]) < 1e-5
     assert np.abs(r.seis_S).max() > 0
-    assert fomo.api.last_stats.gpu_launches == 3 * nt
+    # two 150-step replayed chunks: 3 launches a step, 2 snapshot kernels per
+    # frame and the step-index advance
+    assert fomo.api.last_stats.gpu_launches == 2 * (3 * 150 + 2 * 2 + 1)
 
 
 def test_coupled2d_keywords(fomo, oracle):
@@ -78,3 +80,29 @@ def test_homogeneous_s_stays_zero(fomo):
                        rz=[30, 30, 30], nbc=10, fd_order=8)
     assert np.abs(r.seis_P).max() > 0
     assert not np.any(r.seis_S)
+
+
+def test_coupled2d_chunks_equal_step_launches(fomo, monkeypatch):
+    """Snapshots every 40 steps, 290 steps: three replayed 80-step chunks and a
+    50-step remainder launched step by step (FOMO_F_STEP_LAUNCH: all steps)."""
+    from fomo_b200 import _lib as L
+
+    vp, vs = _model(60, 44, seed=2)
+    kw = dict(sx=[30], sz=[12], rx=np.arange(1, 61, 3), rz=np.full(20, 8), nbc=10, fd_order=8,
+              snap_interval=40)
+    a = fomo.coupled2d(vp, vs, 10.0, 1e-3, 290, 15.0, **kw)
+    orig = fomo.api._opts
+
+    def opts(*oa, **okw):
+        o = orig(*oa, **okw)
+        o.flags |= L.FOMO_F_STEP_LAUNCH
+        return o
+
+    monkeypatch.setattr(fomo.api, "_opts", opts)
+    b = fomo.coupled2d(vp, vs, 10.0, 1e-3, 290, 15.0, **kw)
+    assert fomo.api.last_stats.gpu_launches == 3 * 290
+    assert np.array_equal(a.seis_P, b.seis_P)
+    assert np.array_equal(a.seis_S, b.seis_S)
+    assert len(a.snaps_P) == 7
+    for x, y in zip(a.snaps_P + a.snaps_S, b.snaps_P + b.snaps_S):
+        assert np.array_equal(x, y)
