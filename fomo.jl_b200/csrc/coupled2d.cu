@@ -12,14 +12,16 @@
 //   k_cp_vel: dP/dt, dS/dt += dt * RHS(P, S, medium), then the Higdon boundary
 //             with weights w_vx and the coefficients of v_ref_p (dP/dt) and
 //             v_ref_s (dS/dt);
-//   k_cp_pos: P, S += dt * dP/dt, dS/dt, then the boundary with weights w_tau;
-//   injection into P, recording of P and S.
+//   k_cp_pos: P, S += dt * dP/dt, dS/dt, then the boundary with weights w_tau,
+//             then, on source and receiver cells, injection into P and
+//             recording of P and S.
 // The reference applies its racy full-grid HABC kernel (boundary/habc/
 // kernels.jl:122-190) here; these kernels fuse the same formula in the
 // deterministic two-pass form (a frame cell reads its neighbour's
 // pre-correction value, recomputed from A), as the other 2D solvers do.
 #include <algorithm>
 #include <cmath>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -201,7 +203,7 @@ __device__ __forceinline__ void cp_vel_at(const Geo2& g, const CCoef& c, float d
 }
 
 template <int N>
-__global__ void __launch_bounds__(256) k_cp_vel(Geo2 g, CCoef c, float dt, float ih, float ih2,
+__global__ void __launch_bounds__(256, 6) k_cp_vel(Geo2 g, CCoef c, float dt, float ih, float ih2,
                                                 HabcDev hp, HabcDev hs, CpMat m,
                                                 const float* __restrict__ P,
                                                 const float* __restrict__ S,
@@ -253,12 +255,34 @@ __device__ __forceinline__ void cp_pos_at(const Geo2& g, float dt, const float* 
   uS = __fmaf_rn(dt, __ldg(dS1 + p), uS);
 }
 
+// Source and receiver cells, for the injection into P and the recording of P
+// and S that k_cp_pos does for the cells it owns (coupled2d.jl:239-250): a tag
+// plane (-1, or an entry per distinct cell) and per entry the source indices q
+// (ascending: coincident sources add in source order) then the receivers r.
+struct CpTags {
+  const int* tag;   // pitched like the fields
+  const int4* ent;  // sources list[x, y), receivers list[z, w)
+  const int* list;
+  const float* wav;  // (n_src, nt)
+  int n_src, n_rec;
+  float* seisP;
+  float* seisS;
+  const int* it0;  // steps completed before this launch's chunk
+};
+
+__global__ void k_cp_tags(int* __restrict__ tag, const int* __restrict__ lin, int n) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n) tag[lin[e]] = e;
+}
+
+// j: the step's index within its chunk (step it = *it0 + j + 1).
 __global__ void __launch_bounds__(256) k_cp_pos(Geo2 g, float dt, HabcDev hp, HabcDev hs,
                                                 const float* __restrict__ P0,
                                                 const float* __restrict__ S0,
                                                 const float* __restrict__ dP1,
                                                 const float* __restrict__ dS1,
-                                                float* __restrict__ P1, float* __restrict__ S1) {
+                                                float* __restrict__ P1, float* __restrict__ S1,
+                                                CpTags t, int j) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x, z = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= g.nx || z >= g.nz) return;
   float uP, uS;
@@ -284,6 +308,18 @@ __global__ void __launch_bounds__(256) k_cp_pos(Geo2 g, float dt, HabcDev hp, Ha
       cp_pos_at(g, dt, P0, S0, dP1, dS1, xn, zn, nP, nS);
       uP = higdon_edge(w, uP, higdon_side(hp, nP, foP, __ldg(P0 + pn)));
       uS = higdon_edge(w, uS, higdon_side(hs, nS, foS, __ldg(S0 + pn)));
+    }
+  }
+  const int e = __ldg(t.tag + p);
+  if (e >= 0) {  // injection, then recording (the reference's launch order)
+    const long long k = (long long)(*t.it0 + j);  // it - 1
+    const int4 E = t.ent[e];
+    for (int i = E.x; i < E.y; ++i)
+      uP = __fadd_rn(uP, __ldg(t.wav + t.list[i] + (long long)t.n_src * k));
+    for (int i = E.z; i < E.w; ++i) {
+      const long long o = t.list[i] + (long long)t.n_rec * k;
+      t.seisP[o] = uP;
+      t.seisS[o] = uS;
     }
   }
   P1[p] = uP;
@@ -417,11 +453,36 @@ int fomo_coupled2d(fomo_ctx* ctx, const fomo_grid2d* gp, const float* vp, const 
   if (!std::isfinite(vrp) || !std::isfinite(vrs))
     return fail(ctx, FOMO_EARG, "vp and vs need a positive value for v_ref_p, v_ref_s");
   HabcHost hhp = make_habc(pad, vrp, gp->dt, gp->dh), hhs = make_habc(pad, vrs, gp->dt, gp->dh);
-  std::vector<int32_t> src_lin(acq->n_src), rec_lin(acq->n_rec);
-  for (int k = 0; k < acq->n_src; ++k)
-    src_lin[k] = (acq->sx[k] - 1 + pad) + g.ld * (acq->sz[k] - 1 + pad);
-  for (int k = 0; k < acq->n_rec; ++k)
-    rec_lin[k] = (acq->rx[k] - 1 + pad) + g.ld * (acq->rz[k] - 1 + pad);
+  // tagged cells: one entry per distinct source or receiver cell
+  std::vector<int32_t> ent_lin;
+  std::vector<std::vector<int32_t>> ent_src, ent_rec;
+  {
+    std::map<int32_t, int> at;
+    auto entry = [&](int32_t lin) {
+      auto it = at.find(lin);
+      if (it != at.end()) return it->second;
+      const int e = (int)ent_lin.size();
+      at[lin] = e;
+      ent_lin.push_back(lin);
+      ent_src.emplace_back();
+      ent_rec.emplace_back();
+      return e;
+    };
+    for (int k = 0; k < acq->n_src; ++k)
+      ent_src[entry((acq->sx[k] - 1 + pad) + g.ld * (acq->sz[k] - 1 + pad))].push_back(k);
+    for (int k = 0; k < acq->n_rec; ++k)
+      ent_rec[entry((acq->rx[k] - 1 + pad) + g.ld * (acq->rz[k] - 1 + pad))].push_back(k);
+  }
+  const int n_ent = (int)ent_lin.size();
+  std::vector<int4> ents(n_ent);
+  std::vector<int32_t> elist;
+  for (int e = 0; e < n_ent; ++e) {
+    ents[e].x = (int)elist.size();
+    elist.insert(elist.end(), ent_src[e].begin(), ent_src[e].end());
+    ents[e].y = ents[e].z = (int)elist.size();
+    elist.insert(elist.end(), ent_rec[e].begin(), ent_rec[e].end());
+    ents[e].w = (int)elist.size();
+  }
   const int nsnap = snap_interval > 0 ? nt / snap_interval : 0;
   const long long seis_n = (long long)acq->n_rec * nt;
 
@@ -434,8 +495,10 @@ int fomo_coupled2d(fomo_ctx* ctx, const fomo_grid2d* gp, const float* vp, const 
   const size_t o_state = ar.take<float>(8 * pl);
   const size_t o_taps = ar.take<float>(std::max<size_t>(G.taps.size(), 1));
   const size_t o_w = ar.take<float>(hhp.wtab.size());
-  const size_t o_src = ar.take<int32_t>(std::max(acq->n_src, 1));
-  const size_t o_rec = ar.take<int32_t>(std::max(acq->n_rec, 1));
+  const size_t o_tag = ar.take<int32_t>(pl);
+  const size_t o_ent = ar.take<int4>(std::max(n_ent, 1));
+  const size_t o_elin = ar.take<int32_t>(std::max(n_ent, 1));
+  const size_t o_list = ar.take<int32_t>(std::max<size_t>(elist.size(), 1));
   const size_t o_wav = ar.take<float>(std::max<long long>((long long)acq->n_src * nt, 1));
   const size_t o_seis = ar.take<float>(std::max<long long>(2 * seis_n, 1));
   const size_t o_snap = ar.take<float>(std::max<long long>(2LL * nsnap * nint, 1));
@@ -446,8 +509,10 @@ int fomo_coupled2d(fomo_ctx* ctx, const fomo_grid2d* gp, const float* vp, const 
   float* d_state = ws_ptr<float>(ctx, o_state);
   float* d_taps = ws_ptr<float>(ctx, o_taps);
   float* d_w = ws_ptr<float>(ctx, o_w);
-  int32_t* d_src = ws_ptr<int32_t>(ctx, o_src);
-  int32_t* d_rec = ws_ptr<int32_t>(ctx, o_rec);
+  int32_t* d_tag = ws_ptr<int32_t>(ctx, o_tag);
+  int4* d_ent = ws_ptr<int4>(ctx, o_ent);
+  int32_t* d_elin = ws_ptr<int32_t>(ctx, o_elin);
+  int32_t* d_list = ws_ptr<int32_t>(ctx, o_list);
   float* d_wav = ws_ptr<float>(ctx, o_wav);
   float* d_seis = ws_ptr<float>(ctx, o_seis);
   float* d_snap = ws_ptr<float>(ctx, o_snap);
@@ -458,15 +523,18 @@ int fomo_coupled2d(fomo_ctx* ctx, const fomo_grid2d* gp, const float* vp, const 
                                  cudaMemcpyHostToDevice, st));
   FOMO_CU(ctx, cudaMemcpyAsync(d_w, hhp.wtab.data(), sizeof(float) * hhp.wtab.size(),
                                cudaMemcpyHostToDevice, st));
-  if (acq->n_src) {
-    FOMO_CU(ctx, cudaMemcpyAsync(d_src, src_lin.data(), sizeof(int32_t) * acq->n_src,
-                                 cudaMemcpyHostToDevice, st));
+  if (acq->n_src)
     FOMO_CU(ctx, cudaMemcpyAsync(d_wav, acq->wavelet, sizeof(float) * acq->n_src * nt,
                                  cudaMemcpyHostToDevice, st));
-  }
-  if (acq->n_rec)
-    FOMO_CU(ctx, cudaMemcpyAsync(d_rec, rec_lin.data(), sizeof(int32_t) * acq->n_rec,
+  FOMO_CU(ctx, cudaMemsetAsync(d_tag, 0xFF, sizeof(int32_t) * pl, st));  // -1
+  if (n_ent) {
+    FOMO_CU(ctx, cudaMemcpyAsync(d_ent, ents.data(), sizeof(int4) * n_ent, cudaMemcpyHostToDevice, st));
+    FOMO_CU(ctx, cudaMemcpyAsync(d_elin, ent_lin.data(), sizeof(int32_t) * n_ent,
                                  cudaMemcpyHostToDevice, st));
+    FOMO_CU(ctx, cudaMemcpyAsync(d_list, elist.data(), sizeof(int32_t) * elist.size(),
+                                 cudaMemcpyHostToDevice, st));
+    k_cp_tags<<<cdiv(n_ent, 256), 256, 0, st>>>(d_tag, d_elin, n_ent);
+  }
   if ((rc = build_medium(ctx, st, g, nx, nz, pad, N, gp->dh, smooth_sigma, d_model,
                          d_model + nint, d_med, ws_ptr<float>(ctx, o_tmp), d_taps, G.taps)))
     return rc;
@@ -490,7 +558,11 @@ int fomo_coupled2d(fomo_ctx* ctx, const fomo_grid2d* gp, const float* vp, const 
   int launches = 0;
   int A = 0, B = 1;
   // one step's two updates on stream `s`, set a -> set b
-  auto updates = [&](cudaStream_t s, int a, int b) {
+  int* d_it = ws_ptr<int>(ctx, o_it);
+  FOMO_CU(ctx, cudaMemsetAsync(d_it, 0, sizeof(int), st));
+  const CpTags tg{d_tag, d_ent, d_list, d_wav, acq->n_src, acq->n_rec, d_seis, d_seis + seis_n,
+                  d_it};
+  auto updates = [&](cudaStream_t s, int a, int b, int j) {
 #define FOMO_CPV_CASE(NN)                                                                    \
   case NN:                                                                                   \
     k_cp_vel<NN><<<grd, blk, 0, s>>>(g, c, dt, ih, ih2, hp, hs, m, field(a, 0), field(a, 1),  \
@@ -499,7 +571,7 @@ int fomo_coupled2d(fomo_ctx* ctx, const fomo_grid2d* gp, const float* vp, const 
     switch (N) { FOMO_CPV_CASE(1) FOMO_CPV_CASE(2) FOMO_CPV_CASE(3) FOMO_CPV_CASE(4) FOMO_CPV_CASE(5) }
 #undef FOMO_CPV_CASE
     k_cp_pos<<<grd, blk, 0, s>>>(g, dt, hp, hs, field(a, 0), field(a, 1), field(b, 2),
-                                 field(b, 3), field(b, 0), field(b, 1));
+                                 field(b, 3), field(b, 0), field(b, 1), tg, j);
   };
   FOMO_CU(ctx, cudaEventRecord(ctx->ev0, st));
   // Replayed chunks of K steps (K even: the ping-pong sets return to their
@@ -531,8 +603,6 @@ int fomo_coupled2d(fomo_ctx* ctx, const fomo_grid2d* gp, const float* vp, const 
     }
     const int nchunk = K > 0 ? nt / K : 0;
     if (nchunk >= 2) {
-      int* d_it = ws_ptr<int>(ctx, o_it);
-      FOMO_CU(ctx, cudaMemsetAsync(d_it, 0, sizeof(int), st));
       const cudaStream_t cs = ctx->own_stream;  // the caller's stream may be uncapturable
       cudaGraph_t graph = nullptr;
       cudaError_t ce = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
@@ -540,12 +610,8 @@ int fomo_coupled2d(fomo_ctx* ctx, const fomo_grid2d* gp, const float* vp, const 
       if (ce == cudaSuccess) {
         int a = A, b = B;
         for (int j = 0; j < K; ++j) {
-          updates(cs, a, b);
-          k_inject_record_at<<<1, 256, 0, cs>>>(d_it, j, nt, pl, acq->n_src, d_src, d_wav,
-                                                field(b, 0), nullptr, acq->n_rec, d_rec,
-                                                field(b, 0), field(b, 1), nullptr, d_seis,
-                                                d_seis + seis_n, nullptr);
-          nodes += 3;
+          updates(cs, a, b, j);
+          nodes += 2;
           if (si && (j + 1) % si == 0) {
             for (int f = 0; f < 2; ++f)
               k_snap_at<<<dim3(cdiv(nx, 128), nz), 128, 0, cs>>>(
@@ -569,11 +635,8 @@ int fomo_coupled2d(fomo_ctx* ctx, const fomo_grid2d* gp, const float* vp, const 
     }
   }
   for (int it = it_first; it <= nt; ++it) {
-    updates(st, A, B);
-    k_inject_record<<<1, 256, 0, st>>>(it, nt, pl, acq->n_src, d_src, d_wav, field(B, 0), nullptr,
-                                       acq->n_rec, d_rec, field(B, 0), field(B, 1), nullptr,
-                                       d_seis, d_seis + seis_n, nullptr);
-    launches += 3;
+    updates(st, A, B, it - it_first);  // *d_it = it_first - 1 after the chunks
+    launches += 2;
     if (nsnap && it % snap_interval == 0) {  // coupled2d.jl:252-258
       const long long k = it / snap_interval - 1;
       for (int f = 0; f < 2; ++f)

@@ -52,9 +52,9 @@ def test_coupled2d_bitwise_vs_oracle(fomo, oracle, fd_order):
     assert rel_l2(r.seis_P, o64["seis_P"]) < 1e-5
     assert rel_l2(r.seis_S, o64["seis_S"]) < 1e-5
     assert np.abs(r.seis_S).max() > 0
-    # two 150-step replayed chunks: 3 launches a step, 2 snapshot kernels per
+    # two 150-step replayed chunks: 2 launches a step, 2 snapshot kernels per
     # frame and the step-index advance
-    assert fomo.api.last_stats.gpu_launches == 2 * (3 * 150 + 2 * 2 + 1)
+    assert fomo.api.last_stats.gpu_launches == 2 * (2 * 150 + 2 * 2 + 1)
 
 
 def test_coupled2d_keywords(fomo, oracle):
@@ -62,11 +62,13 @@ def test_coupled2d_keywords(fomo, oracle):
     vp, vs = _model(50, 40, seed=9)
     nt = 200
     w = (fomo.ricker_wavelet(12.0, 1e-3, nt) * 2.0).astype(np.float32)
-    kw = dict(sx=[25, 30], sz=[10, 12], rx=np.arange(1, 51, 2), rz=np.full(25, 6), nbc=10,
-              fd_order=6)
+    # two coincident sources (added in source order) and receivers on a source cell
+    rx = np.concatenate([np.arange(1, 51, 2), [25, 25]])
+    rz = np.concatenate([np.full(25, 6), [10, 10]])
+    kw = dict(sx=[25, 30, 25], sz=[10, 12, 10], rx=rx, rz=rz, nbc=10, fd_order=6)
     r = fomo.coupled2d(vp, vs, 10.0, 1e-3, nt, 12.0, v_ref_p=2000.0, v_ref_s=900.0,
                        smooth_sigma=1.0, wavelet=w, **kw)
-    o = oracle.coupled2d(vp, vs, 10.0, 1e-3, nt, wavelet=np.repeat(w[None], 2, axis=0),
+    o = oracle.coupled2d(vp, vs, 10.0, 1e-3, nt, wavelet=np.repeat(w[None], 3, axis=0),
                          v_ref_p=2000.0, v_ref_s=900.0, smooth_sigma=1.0, **kw)
     assert np.array_equal(r.seis_P, o["seis_P"])
     assert np.array_equal(r.seis_S, o["seis_S"])
@@ -100,7 +102,7 @@ def test_coupled2d_chunks_equal_step_launches(fomo, monkeypatch):
 
     monkeypatch.setattr(fomo.api, "_opts", opts)
     b = fomo.coupled2d(vp, vs, 10.0, 1e-3, 290, 15.0, **kw)
-    assert fomo.api.last_stats.gpu_launches == 3 * 290
+    assert fomo.api.last_stats.gpu_launches == 2 * 290
     assert np.array_equal(a.seis_P, b.seis_P)
     assert np.array_equal(a.seis_S, b.seis_S)
     assert len(a.snaps_P) == 7
