@@ -21,7 +21,6 @@
 // pre-correction value, recomputed from A), as the other 2D solvers do.
 #include <algorithm>
 #include <cmath>
-#include <map>
 #include <string>
 #include <vector>
 
@@ -255,26 +254,6 @@ __device__ __forceinline__ void cp_pos_at(const Geo2& g, float dt, const float* 
   uS = __fmaf_rn(dt, __ldg(dS1 + p), uS);
 }
 
-// Source and receiver cells, for the injection into P and the recording of P
-// and S that k_cp_pos does for the cells it owns (coupled2d.jl:239-250): a tag
-// plane (-1, or an entry per distinct cell) and per entry the source indices q
-// (ascending: coincident sources add in source order) then the receivers r.
-struct CpTags {
-  const int* tag;   // pitched like the fields
-  const int4* ent;  // sources list[x, y), receivers list[z, w)
-  const int* list;
-  const float* wav;  // (n_src, nt)
-  int n_src, n_rec;
-  float* seisP;
-  float* seisS;
-  const int* it0;  // steps completed before this launch's chunk
-};
-
-__global__ void k_cp_tags(int* __restrict__ tag, const int* __restrict__ lin, int n) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e < n) tag[lin[e]] = e;
-}
-
 // j: the step's index within its chunk (step it = *it0 + j + 1).
 __global__ void __launch_bounds__(256) k_cp_pos(Geo2 g, float dt, HabcDev hp, HabcDev hs,
                                                 const float* __restrict__ P0,
@@ -282,7 +261,7 @@ __global__ void __launch_bounds__(256) k_cp_pos(Geo2 g, float dt, HabcDev hp, Ha
                                                 const float* __restrict__ dP1,
                                                 const float* __restrict__ dS1,
                                                 float* __restrict__ P1, float* __restrict__ S1,
-                                                CpTags t, int j) {
+                                                CellTags t, int j) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x, z = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= g.nx || z >= g.nz) return;
   float uP, uS;
@@ -311,16 +290,11 @@ __global__ void __launch_bounds__(256) k_cp_pos(Geo2 g, float dt, HabcDev hp, Ha
     }
   }
   const int e = __ldg(t.tag + p);
-  if (e >= 0) {  // injection, then recording (the reference's launch order)
+  if (e >= 0) {  // injection into P, then recording of P and S (coupled2d.jl:239-250)
     const long long k = (long long)(*t.it0 + j);  // it - 1
     const int4 E = t.ent[e];
-    for (int i = E.x; i < E.y; ++i)
-      uP = __fadd_rn(uP, __ldg(t.wav + t.list[i] + (long long)t.n_src * k));
-    for (int i = E.z; i < E.w; ++i) {
-      const long long o = t.list[i] + (long long)t.n_rec * k;
-      t.seisP[o] = uP;
-      t.seisS[o] = uS;
-    }
+    uP = tag_inject(t, E, k, uP);
+    tag_record(t, E, k, uP, uS, 0.0f);
   }
   P1[p] = uP;
   S1[p] = uS;
@@ -454,35 +428,13 @@ int fomo_coupled2d(fomo_ctx* ctx, const fomo_grid2d* gp, const float* vp, const 
     return fail(ctx, FOMO_EARG, "vp and vs need a positive value for v_ref_p, v_ref_s");
   HabcHost hhp = make_habc(pad, vrp, gp->dt, gp->dh), hhs = make_habc(pad, vrs, gp->dt, gp->dh);
   // tagged cells: one entry per distinct source or receiver cell
-  std::vector<int32_t> ent_lin;
-  std::vector<std::vector<int32_t>> ent_src, ent_rec;
-  {
-    std::map<int32_t, int> at;
-    auto entry = [&](int32_t lin) {
-      auto it = at.find(lin);
-      if (it != at.end()) return it->second;
-      const int e = (int)ent_lin.size();
-      at[lin] = e;
-      ent_lin.push_back(lin);
-      ent_src.emplace_back();
-      ent_rec.emplace_back();
-      return e;
-    };
-    for (int k = 0; k < acq->n_src; ++k)
-      ent_src[entry((acq->sx[k] - 1 + pad) + g.ld * (acq->sz[k] - 1 + pad))].push_back(k);
-    for (int k = 0; k < acq->n_rec; ++k)
-      ent_rec[entry((acq->rx[k] - 1 + pad) + g.ld * (acq->rz[k] - 1 + pad))].push_back(k);
-  }
-  const int n_ent = (int)ent_lin.size();
-  std::vector<int4> ents(n_ent);
-  std::vector<int32_t> elist;
-  for (int e = 0; e < n_ent; ++e) {
-    ents[e].x = (int)elist.size();
-    elist.insert(elist.end(), ent_src[e].begin(), ent_src[e].end());
-    ents[e].y = ents[e].z = (int)elist.size();
-    elist.insert(elist.end(), ent_rec[e].begin(), ent_rec[e].end());
-    ents[e].w = (int)elist.size();
-  }
+  std::vector<int32_t> src_lin(acq->n_src), rec_lin(acq->n_rec);
+  for (int k = 0; k < acq->n_src; ++k)
+    src_lin[k] = (acq->sx[k] - 1 + pad) + g.ld * (acq->sz[k] - 1 + pad);
+  for (int k = 0; k < acq->n_rec; ++k)
+    rec_lin[k] = (acq->rx[k] - 1 + pad) + g.ld * (acq->rz[k] - 1 + pad);
+  const CellTagHost tags = make_cell_tags(src_lin.data(), acq->n_src, rec_lin.data(), acq->n_rec);
+  const int n_ent = (int)tags.lin.size();
   const int nsnap = snap_interval > 0 ? nt / snap_interval : 0;
   const long long seis_n = (long long)acq->n_rec * nt;
 
@@ -498,7 +450,7 @@ int fomo_coupled2d(fomo_ctx* ctx, const fomo_grid2d* gp, const float* vp, const 
   const size_t o_tag = ar.take<int32_t>(pl);
   const size_t o_ent = ar.take<int4>(std::max(n_ent, 1));
   const size_t o_elin = ar.take<int32_t>(std::max(n_ent, 1));
-  const size_t o_list = ar.take<int32_t>(std::max<size_t>(elist.size(), 1));
+  const size_t o_list = ar.take<int32_t>(std::max<size_t>(tags.list.size(), 1));
   const size_t o_wav = ar.take<float>(std::max<long long>((long long)acq->n_src * nt, 1));
   const size_t o_seis = ar.take<float>(std::max<long long>(2 * seis_n, 1));
   const size_t o_snap = ar.take<float>(std::max<long long>(2LL * nsnap * nint, 1));
@@ -528,12 +480,13 @@ int fomo_coupled2d(fomo_ctx* ctx, const fomo_grid2d* gp, const float* vp, const 
                                  cudaMemcpyHostToDevice, st));
   FOMO_CU(ctx, cudaMemsetAsync(d_tag, 0xFF, sizeof(int32_t) * pl, st));  // -1
   if (n_ent) {
-    FOMO_CU(ctx, cudaMemcpyAsync(d_ent, ents.data(), sizeof(int4) * n_ent, cudaMemcpyHostToDevice, st));
-    FOMO_CU(ctx, cudaMemcpyAsync(d_elin, ent_lin.data(), sizeof(int32_t) * n_ent,
+    FOMO_CU(ctx, cudaMemcpyAsync(d_ent, tags.ent.data(), sizeof(int4) * n_ent,
                                  cudaMemcpyHostToDevice, st));
-    FOMO_CU(ctx, cudaMemcpyAsync(d_list, elist.data(), sizeof(int32_t) * elist.size(),
+    FOMO_CU(ctx, cudaMemcpyAsync(d_elin, tags.lin.data(), sizeof(int32_t) * n_ent,
                                  cudaMemcpyHostToDevice, st));
-    k_cp_tags<<<cdiv(n_ent, 256), 256, 0, st>>>(d_tag, d_elin, n_ent);
+    FOMO_CU(ctx, cudaMemcpyAsync(d_list, tags.list.data(), sizeof(int32_t) * tags.list.size(),
+                                 cudaMemcpyHostToDevice, st));
+    k_set_tags<<<cdiv(n_ent, 256), 256, 0, st>>>(d_tag, d_elin, n_ent);
   }
   if ((rc = build_medium(ctx, st, g, nx, nz, pad, N, gp->dh, smooth_sigma, d_model,
                          d_model + nint, d_med, ws_ptr<float>(ctx, o_tmp), d_taps, G.taps)))
@@ -560,8 +513,16 @@ int fomo_coupled2d(fomo_ctx* ctx, const fomo_grid2d* gp, const float* vp, const 
   // one step's two updates on stream `s`, set a -> set b
   int* d_it = ws_ptr<int>(ctx, o_it);
   FOMO_CU(ctx, cudaMemsetAsync(d_it, 0, sizeof(int), st));
-  const CpTags tg{d_tag, d_ent, d_list, d_wav, acq->n_src, acq->n_rec, d_seis, d_seis + seis_n,
-                  d_it};
+  CellTags tg;
+  tg.tag = d_tag;
+  tg.ent = d_ent;
+  tg.list = d_list;
+  tg.wav = d_wav;
+  tg.n_src = acq->n_src;
+  tg.n_rec = acq->n_rec;
+  tg.s0 = d_seis;
+  tg.s1 = d_seis + seis_n;
+  tg.it0 = d_it;
   auto updates = [&](cudaStream_t s, int a, int b, int j) {
 #define FOMO_CPV_CASE(NN)                                                                    \
   case NN:                                                                                   \

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
 #include <string>
 #include <vector>
 
@@ -155,6 +156,42 @@ __device__ __forceinline__ float dp(const float* __restrict__ f, long long p, lo
   for (int l = 1; l <= N; ++l)
     acc = __fmaf_rn(c.a[l - 1], __fsub_rn(__ldg(f + p + l * s), __ldg(f + p - (l - 1) * s)), acc);
   return acc;
+}
+
+// Host side of the cell tags (CellTags, solver2d_kernels.cuh): one entry per
+// distinct source or receiver cell (linear pitched index), listing the source
+// indices (ascending) then the receiver indices at that cell.
+struct CellTagHost {
+  std::vector<int32_t> lin;  // entry -> cell
+  std::vector<int4> ent;     // sources list[x, y), receivers list[z, w)
+  std::vector<int32_t> list;
+};
+inline CellTagHost make_cell_tags(const int32_t* src_lin, int n_src, const int32_t* rec_lin,
+                                  int n_rec) {
+  CellTagHost t;
+  std::map<int32_t, int> at;
+  std::vector<std::vector<int32_t>> srcs, recs;
+  auto entry = [&](int32_t lin) {
+    auto it = at.find(lin);
+    if (it != at.end()) return it->second;
+    const int e = (int)t.lin.size();
+    at[lin] = e;
+    t.lin.push_back(lin);
+    srcs.emplace_back();
+    recs.emplace_back();
+    return e;
+  };
+  for (int k = 0; k < n_src; ++k) srcs[entry(src_lin[k])].push_back(k);
+  for (int k = 0; k < n_rec; ++k) recs[entry(rec_lin[k])].push_back(k);
+  t.ent.resize(t.lin.size());
+  for (size_t e = 0; e < t.lin.size(); ++e) {
+    t.ent[e].x = (int)t.list.size();
+    t.list.insert(t.list.end(), srcs[e].begin(), srcs[e].end());
+    t.ent[e].y = t.ent[e].z = (int)t.list.size();
+    t.list.insert(t.list.end(), recs[e].begin(), recs[e].end());
+    t.ent[e].w = (int)t.list.size();
+  }
+  return t;
 }
 
 // Host helpers

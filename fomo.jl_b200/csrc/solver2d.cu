@@ -10,6 +10,7 @@
 #include <mutex>
 #include <string>
 #include <tuple>
+#include <type_traits>
 
 #include "solver2d_kernels.cuh"
 #include "mixed2d.cuh"
@@ -333,6 +334,17 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
   size_t o_snap = (!P.dev && outs.snaps && P.nsnap) ? ar.take<float>(P.nsnap * nint) : 0;
   size_t o_bounds = ar.take<long long>(kMaxGrid + 1);
   size_t o_it = ar.take<int>(1);  // device step index of replayed chunks
+  // Single-shot two-phase runs inject and record inside the step's last update
+  // kernel, on tagged cells (CellTags), instead of a separate launch.
+  const bool tagged = P.ns == 1 && !P.fp16 && kernel == FOMO_KERNEL_TWO_PHASE &&
+                      (P.phys == kAcoustic || P.phys == kElastic) && !hook;
+  CellTagHost tags;
+  if (tagged) tags = make_cell_tags(src_lin.data(), P.n_src, rec_lin.data(), P.n_rec);
+  const int n_ent = (int)tags.lin.size();
+  size_t o_tag = tagged ? ar.take<int32_t>(P.plane) : 0;
+  size_t o_ent = tagged ? ar.take<int4>(std::max(n_ent, 1)) : 0;
+  size_t o_elin = tagged ? ar.take<int32_t>(std::max(n_ent, 1)) : 0;
+  size_t o_list = tagged ? ar.take<int32_t>(std::max<size_t>(tags.list.size(), 1)) : 0;
   const bool sweep = kernel == FOMO_KERNEL_SINGLE_SWEEP;
   size_t o_pack = sweep ? ar.take<float>(sweep_pack_floats(P.nxp, P.nzp)) : 0;
   if ((rc = ensure_workspace(ctx, ar.off))) return rc;
@@ -398,6 +410,33 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
     for (int k = 0; k < outs.nseis; ++k)
       if (d_seis[k]) FOMO_CU(ctx, cudaMemsetAsync(d_seis[k], 0, sizeof(float) * seis_n, st));
 
+  int* d_it = ws_ptr<int>(ctx, o_it);
+  FOMO_CU(ctx, cudaMemsetAsync(d_it, 0, sizeof(int), st));
+  CellTags tg;
+  if (tagged) {
+    int32_t* d_tag = ws_ptr<int32_t>(ctx, o_tag);
+    FOMO_CU(ctx, cudaMemsetAsync(d_tag, 0xFF, sizeof(int32_t) * P.plane, st));  // -1
+    if (n_ent) {
+      FOMO_CU(ctx, cudaMemcpyAsync(ws_ptr<int4>(ctx, o_ent), tags.ent.data(), sizeof(int4) * n_ent,
+                                   cudaMemcpyHostToDevice, st));
+      FOMO_CU(ctx, cudaMemcpyAsync(ws_ptr<int32_t>(ctx, o_elin), tags.lin.data(),
+                                   sizeof(int32_t) * n_ent, cudaMemcpyHostToDevice, st));
+      FOMO_CU(ctx, cudaMemcpyAsync(ws_ptr<int32_t>(ctx, o_list), tags.list.data(),
+                                   sizeof(int32_t) * tags.list.size(), cudaMemcpyHostToDevice, st));
+      k_set_tags<<<cdiv(n_ent, 256), 256, 0, st>>>(d_tag, ws_ptr<int32_t>(ctx, o_elin), n_ent);
+    }
+    tg.tag = d_tag;
+    tg.ent = ws_ptr<int4>(ctx, o_ent);
+    tg.list = ws_ptr<int32_t>(ctx, o_list);
+    tg.wav = d_wav;
+    tg.n_src = P.n_src;
+    tg.n_rec = P.n_rec;
+    tg.s0 = d_seis[0];
+    tg.s1 = d_seis[1];
+    tg.s2 = d_seis[2];
+    tg.it0 = d_it;
+  }
+
   Geo2 g{P.nxp, P.nzp, P.ld, P.M, hh.nbc, P.plane};
   Coef c;
   for (int l = 0; l < 5; ++l) c.a[l] = kFD[P.N][l];
@@ -453,6 +492,58 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
     if (int hr = hook->begin(ctx, st, P, d_wav)) return hr;
   FOMO_CU(ctx, cudaEventRecord(ctx->ev0, st));
   int A = 0, B = 1, C2 = 2;  // scalar: A = u^{n-1}, B = u^n, C2 = u^{n+1}
+  // One two-phase step, set a -> set b, on stream s (j: the step's index in its
+  // chunk, for the tagged kernels), with the sponge and tag variants chosen here.
+  auto el_two_phase = [&](cudaStream_t s, int a, int b, int j) {
+    const ElFields fa{field(a, 0), field(a, 1), field(a, 2), field(a, 3), field(a, 4)};
+    auto go = [&](auto spc, auto tgc) {
+      constexpr bool SPV = decltype(spc)::value, TGV = decltype(tgc)::value;
+      switch (P.N) {
+#define FOMO_EL2_CASE(NN)                                                                        \
+  case NN:                                                                                       \
+    k_el_vel<NN, SPV><<<grd, blk, 0, s>>>(g, c, dtx, dtz, h, fa, emat, field(b, 0), field(b, 1)); \
+    k_el_str<NN, SPV, TGV><<<grd, blk, 0, s>>>(g, c, dtx, dtz, h, fa, field(b, 0), field(b, 1),   \
+                                               emat, field(b, 2), field(b, 3), field(b, 4), tg,  \
+                                               j);                                               \
+    break;
+        FOMO_EL2_CASE(1) FOMO_EL2_CASE(2) FOMO_EL2_CASE(3) FOMO_EL2_CASE(4) FOMO_EL2_CASE(5)
+#undef FOMO_EL2_CASE
+      }
+    };
+    if (P.sponge) {
+      if (tagged) go(std::true_type{}, std::true_type{});
+      else go(std::true_type{}, std::false_type{});
+    } else {
+      if (tagged) go(std::false_type{}, std::true_type{});
+      else go(std::false_type{}, std::false_type{});
+    }
+  };
+  auto ac_two_phase = [&](cudaStream_t s, int a, int b, int j) {
+    const float* bx = d_mat;
+    const float* bz = d_mat + P.plane;
+    const float* kap = d_mat + 2 * P.plane;
+    auto go = [&](auto spc, auto tgc) {
+      constexpr bool SPV = decltype(spc)::value, TGV = decltype(tgc)::value;
+      switch (P.N) {
+#define FOMO_AC2_CASE(NN)                                                                        \
+  case NN:                                                                                       \
+    k_ac_vel<NN, SPV><<<grd, blk, 0, s>>>(g, c, dtx, dtz, h, field(a, 2), field(a, 0),           \
+                                          field(a, 1), bx, bz, field(b, 0), field(b, 1));        \
+    k_ac_prs<NN, SPV, TGV><<<grd, blk, 0, s>>>(g, c, dtx, dtz, h, field(a, 2), field(b, 0),      \
+                                               field(b, 1), kap, field(b, 2), tg, j);            \
+    break;
+        FOMO_AC2_CASE(1) FOMO_AC2_CASE(2) FOMO_AC2_CASE(3) FOMO_AC2_CASE(4) FOMO_AC2_CASE(5)
+#undef FOMO_AC2_CASE
+      }
+    };
+    if (P.sponge) {
+      if (tagged) go(std::true_type{}, std::true_type{});
+      else go(std::true_type{}, std::false_type{});
+    } else {
+      if (tagged) go(std::false_type{}, std::true_type{});
+      else go(std::false_type{}, std::false_type{});
+    }
+  };
   // Acoustic, scalar and two-phase elastic runs on small grids are bound by
   // launch latency.  A chunk of K steps (the updates, inject/record; the interior snapshot where
   // the step is a multiple of snap_interval; the advance of a device step
@@ -515,8 +606,6 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
         for (auto& e : chunk_ev.ev) FOMO_CU(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         frames_per_chunk = K / si;
       }
-      int* d_it = ws_ptr<int>(ctx, o_it);
-      FOMO_CU(ctx, cudaMemsetAsync(d_it, 0, sizeof(int), st));
       const cudaStream_t cs = ctx->own_stream;  // the caller's may be uncapturable
       const float* bx = d_mat;
       const float* bz = d_mat + P.plane;
@@ -556,33 +645,17 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
           if (frames_per_chunk) streamed_chunks = nchunk;
         }
       } else if (ce == cudaSuccess && elastic) {
-        const ElMat& m = emat;
         int a = A, b = B, nodes = 0;
         for (int j = 0; j < K; ++j) {
-          ElFields fa{field(a, 0), field(a, 1), field(a, 2), field(a, 3), field(a, 4)};
-#define FOMO_ELC_CASE(NN, SPV)                                                                  \
-  case NN:                                                                                      \
-    k_el_vel<NN, SPV><<<grd, blk, 0, cs>>>(g, c, dtx, dtz, h, fa, m, field(b, 0), field(b, 1)); \
-    k_el_str<NN, SPV><<<grd, blk, 0, cs>>>(g, c, dtx, dtz, h, fa, field(b, 0), field(b, 1), m,  \
-                                           field(b, 2), field(b, 3), field(b, 4));              \
-    break;
-#define FOMO_ELC_SWITCH(SPV)                                                                 \
-  switch (P.N) {                                                                             \
-    FOMO_ELC_CASE(1, SPV) FOMO_ELC_CASE(2, SPV) FOMO_ELC_CASE(3, SPV) FOMO_ELC_CASE(4, SPV) \
-    FOMO_ELC_CASE(5, SPV)                                                                    \
-  }
-          if (P.sponge) {
-            FOMO_ELC_SWITCH(true)
-          } else {
-            FOMO_ELC_SWITCH(false)
+          el_two_phase(cs, a, b, j);
+          nodes += 2;
+          if (!tagged) {
+            k_inject_record_at<<<P.ns, 256, 0, cs>>>(d_it, j, P.nt, P.plane, P.n_src, d_src, d_wav,
+                                                     field(b, 2), field(b, 3), P.n_rec, d_rec,
+                                                     field(b, 0), field(b, 1), nullptr, d_seis[0],
+                                                     d_seis[1], nullptr);
+            ++nodes;
           }
-#undef FOMO_ELC_SWITCH
-#undef FOMO_ELC_CASE
-          k_inject_record_at<<<P.ns, 256, 0, cs>>>(d_it, j, P.nt, P.plane, P.n_src, d_src, d_wav,
-                                                   field(b, 2), field(b, 3), P.n_rec, d_rec,
-                                                   field(b, 0), field(b, 1), nullptr, d_seis[0],
-                                                   d_seis[1], nullptr);
-          nodes += 3;
           if (si && (j + 1) % si == 0) {
             k_snap_at<<<dim3(cdiv(P.nx, 128), P.nz), 128, 0, cs>>>(
                 d_it, j, si, field(b, 1) + P.pad + (long long)P.pad * P.ld, P.ld, P.nx, P.nz,
@@ -605,30 +678,15 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
       } else if (ce == cudaSuccess) {
         int a = A, b = B, nodes = 0;
         for (int j = 0; j < K; ++j) {
-#define FOMO_ACC_CASE(NN, SPV)                                                                 \
-  case NN:                                                                                     \
-    k_ac_vel<NN, SPV><<<grd, blk, 0, cs>>>(g, c, dtx, dtz, h, field(a, 2), field(a, 0),        \
-                                           field(a, 1), bx, bz, field(b, 0), field(b, 1));     \
-    k_ac_prs<NN, SPV><<<grd, blk, 0, cs>>>(g, c, dtx, dtz, h, field(a, 2), field(b, 0),        \
-                                           field(b, 1), kap, field(b, 2));                     \
-    break;
-#define FOMO_ACC_SWITCH(SPV)                                                                 \
-  switch (P.N) {                                                                             \
-    FOMO_ACC_CASE(1, SPV) FOMO_ACC_CASE(2, SPV) FOMO_ACC_CASE(3, SPV) FOMO_ACC_CASE(4, SPV) \
-    FOMO_ACC_CASE(5, SPV)                                                                    \
-  }
-          if (P.sponge) {
-            FOMO_ACC_SWITCH(true)
-          } else {
-            FOMO_ACC_SWITCH(false)
+          ac_two_phase(cs, a, b, j);
+          nodes += 2;
+          if (!tagged) {
+            k_inject_record_at<<<P.ns, 256, 0, cs>>>(d_it, j, P.nt, P.plane, P.n_src, d_src, d_wav,
+                                                     field(b, 2), nullptr, P.n_rec, d_rec,
+                                                     field(b, 2), field(b, 0), field(b, 1),
+                                                     d_seis[0], d_seis[1], d_seis[2]);
+            ++nodes;
           }
-#undef FOMO_ACC_SWITCH
-#undef FOMO_ACC_CASE
-          k_inject_record_at<<<P.ns, 256, 0, cs>>>(d_it, j, P.nt, P.plane, P.n_src, d_src, d_wav,
-                                                   field(b, 2), nullptr, P.n_rec, d_rec,
-                                                   field(b, 2), field(b, 0), field(b, 1),
-                                                   d_seis[0], d_seis[1], d_seis[2]);
-          nodes += 3;
           if (si && (j + 1) % si == 0) {
             k_snap_at<<<dim3(cdiv(P.nx, 128), P.nz), 128, 0, cs>>>(
                 d_it, j, si, field(b, 2) + P.pad + (long long)P.pad * P.ld, P.ld, P.nx, P.nz,
@@ -694,24 +752,7 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
         launches += 1;
         sweeps_per_step = 1;
       } else {
-#define FOMO_EL_CASE(NN, SPV)                                                                  \
-  case NN:                                                                                     \
-    k_el_vel<NN, SPV><<<grd, blk, 0, st>>>(g, c, dtx, dtz, h, a, m, field(B, 0), field(B, 1)); \
-    k_el_str<NN, SPV><<<grd, blk, 0, st>>>(g, c, dtx, dtz, h, a, field(B, 0), field(B, 1), m,  \
-                                           field(B, 2), field(B, 3), field(B, 4));             \
-    break;
-#define FOMO_EL_SWITCH(SPV)                                                                      \
-  switch (P.N) {                                                                                 \
-    FOMO_EL_CASE(1, SPV) FOMO_EL_CASE(2, SPV) FOMO_EL_CASE(3, SPV) FOMO_EL_CASE(4, SPV)         \
-    FOMO_EL_CASE(5, SPV)                                                                         \
-  }
-        if (P.sponge) {
-          FOMO_EL_SWITCH(true)
-        } else {
-          FOMO_EL_SWITCH(false)
-        }
-#undef FOMO_EL_SWITCH
-#undef FOMO_EL_CASE
+        el_two_phase(st, A, B, it - it_first);  // *d_it = it_first - 1 after the chunks
         launches += 2;
         sweeps_per_step = 2;
       }
@@ -720,43 +761,22 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
         k_elh_inject_record<<<P.ns, 256, 0, st>>>(it, P.nt, g, P.n_src, d_src, d_wav, hfield(B, 2),
                                                   hfield(B, 3), P.n_rec, d_rec, hfield(B, 0),
                                                   hfield(B, 1), d_seis[0], d_seis[1]);
-      else
+      else if (!tagged)
         k_inject_record<<<P.ns, 256, 0, st>>>(it, P.nt, P.plane, P.n_src, d_src, d_wav, field(B, 2),
                                               field(B, 3), P.n_rec, d_rec, field(B, 0), field(B, 1),
                                               nullptr, d_seis[0], d_seis[1], nullptr);
-      launches += 1;
+      if (!tagged) launches += 1;
     } else if (P.phys == kAcoustic) {
-      const float* p0 = field(A, 2);
-      const float* vx0 = field(A, 0);
-      const float* vz0 = field(A, 1);
-      const float* bx = d_mat;
-      const float* bz = d_mat + P.plane;
-      const float* kap = d_mat + 2 * P.plane;
-#define FOMO_AC_CASE(NN, SPV)                                                                  \
-  case NN:                                                                                     \
-    k_ac_vel<NN, SPV><<<grd, blk, 0, st>>>(g, c, dtx, dtz, h, p0, vx0, vz0, bx, bz,            \
-                                           field(B, 0), field(B, 1));                          \
-    k_ac_prs<NN, SPV><<<grd, blk, 0, st>>>(g, c, dtx, dtz, h, p0, field(B, 0), field(B, 1),    \
-                                           kap, field(B, 2));                                  \
-    break;
-#define FOMO_AC_SWITCH(SPV)                                                                      \
-  switch (P.N) {                                                                                 \
-    FOMO_AC_CASE(1, SPV) FOMO_AC_CASE(2, SPV) FOMO_AC_CASE(3, SPV) FOMO_AC_CASE(4, SPV)         \
-    FOMO_AC_CASE(5, SPV)                                                                         \
-  }
-      if (P.sponge) {
-        FOMO_AC_SWITCH(true)
-      } else {
-        FOMO_AC_SWITCH(false)
-      }
-#undef FOMO_AC_SWITCH
-#undef FOMO_AC_CASE
+      ac_two_phase(st, A, B, it - it_first);  // *d_it = it_first - 1 after the chunks
       sweeps_per_step = 2;
       FOMO_CU(ctx, prof_mark(it, 1));
-      k_inject_record<<<P.ns, 256, 0, st>>>(it, P.nt, P.plane, P.n_src, d_src, d_wav, field(B, 2),
-                                            nullptr, P.n_rec, d_rec, field(B, 2), field(B, 0),
-                                            field(B, 1), d_seis[0], d_seis[1], d_seis[2]);
-      launches += 3;
+      launches += 2;
+      if (!tagged) {
+        k_inject_record<<<P.ns, 256, 0, st>>>(it, P.nt, P.plane, P.n_src, d_src, d_wav, field(B, 2),
+                                              nullptr, P.n_rec, d_rec, field(B, 2), field(B, 0),
+                                              field(B, 1), d_seis[0], d_seis[1], d_seis[2]);
+        launches += 1;
+      }
     } else {
       D2Coef dc;
       dc.two_c0 = 2.0f * kD2C0[P.N];

@@ -42,6 +42,43 @@ struct ElMat {
   int pack_pitch = 0;  // column pairs per pack row
 };
 
+// Source and receiver cells of a single-shot run, handled inside the step's
+// last update kernel by the threads that own them: injection (sources in source
+// order, as k_inject_record adds them), then recording.
+struct CellTags {
+  const int* tag = nullptr;   // pitched like the fields: -1, or an entry per distinct cell
+  const int4* ent = nullptr;  // per entry: sources list[x, y), receivers list[z, w)
+  const int* list = nullptr;
+  const float* wav = nullptr;  // (n_src, nt)
+  int n_src = 0, n_rec = 0;
+  float* s0 = nullptr;  // seismograms (null: not recorded)
+  float* s1 = nullptr;
+  float* s2 = nullptr;
+  const int* it0 = nullptr;  // steps completed before this launch's chunk
+};
+
+static __global__ void k_set_tags(int* __restrict__ tag, const int* __restrict__ lin, int n) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n) tag[lin[e]] = e;
+}
+
+// u plus the wavelets of the entry's sources at 0-based step k, in source order.
+__device__ __forceinline__ float tag_inject(const CellTags& t, const int4& E, long long k,
+                                            float u) {
+  for (int i = E.x; i < E.y; ++i)
+    u = __fadd_rn(u, __ldg(t.wav + t.list[i] + (long long)t.n_src * k));
+  return u;
+}
+__device__ __forceinline__ void tag_record(const CellTags& t, const int4& E, long long k,
+                                           float r0, float r1, float r2) {
+  for (int i = E.z; i < E.w; ++i) {
+    const long long o = t.list[i] + (long long)t.n_rec * k;
+    if (t.s0) t.s0[o] = r0;
+    if (t.s1) t.s1[o] = r1;
+    if (t.s2) t.s2[o] = r2;
+  }
+}
+
 // Cerjan sponge (boundary/sponge.jl:31-83), fused into the sweep that produces
 // the field: the updated value times damp[d], d = the cell's distance in cells
 // to the nearest edge of the padded grid, for d < nbc.  In sponge mode HabcDev
@@ -136,12 +173,15 @@ __device__ __forceinline__ void el_str_at(const Geo2& g, const Coef& c, float dt
   }
 }
 
-template <int N, bool SP = false>
+// TG: single shot; inject into txx, tzz and record vx, vz on tagged cells
+// (step *t.it0 + j + 1).
+template <int N, bool SP = false, bool TG = false>
 __global__ void __launch_bounds__(256) k_el_str(Geo2 g, Coef c, float dtx, float dtz, HabcDev h,
                                                 ElFields a, const float* __restrict__ vx1,
                                                 const float* __restrict__ vz1, ElMat m,
                                                 float* __restrict__ txx1, float* __restrict__ tzz1,
-                                                float* __restrict__ txz1) {
+                                                float* __restrict__ txz1,
+                                                CellTags t = CellTags{}, int j = 0) {
   int x = blockIdx.x * blockDim.x + threadIdx.x;
   int z = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= g.nx || z >= g.nz) return;
@@ -179,6 +219,16 @@ __global__ void __launch_bounds__(256) k_el_str(Geo2 g, Coef c, float dtx, float
       sxx = higdon_edge(w, sxx, higdon_side(h, n1, o1, __ldg(a.txx + pn)));
       szz = higdon_edge(w, szz, higdon_side(h, n2, o2, __ldg(a.tzz + pn)));
       sxz = higdon_edge(w, sxz, higdon_side(h, n3, o3, __ldg(a.txz + pn)));
+    }
+  }
+  if constexpr (TG) {
+    const int e = __ldg(t.tag + p);
+    if (e >= 0) {
+      const long long k = (long long)(*t.it0 + j);
+      const int4 E = t.ent[e];
+      sxx = tag_inject(t, E, k, sxx);
+      szz = tag_inject(t, E, k, szz);
+      tag_record(t, E, k, __ldg(vx + p), __ldg(vz + p), 0.0f);
     }
   }
   txx1[so + p] = sxx;
@@ -314,13 +364,15 @@ __device__ __forceinline__ float ac_prs_cell(const Geo2& g, const Coef& c, float
   return u;
 }
 
-template <int N, bool SP = false>
+// TG: single shot; inject into p and record p, vx, vz on tagged cells.
+template <int N, bool SP = false, bool TG = false>
 __global__ void __launch_bounds__(256) k_ac_prs(Geo2 g, Coef c, float dtx, float dtz, HabcDev h,
                                                 const float* __restrict__ p0,
                                                 const float* __restrict__ vx1,
                                                 const float* __restrict__ vz1,
                                                 const float* __restrict__ kappa,
-                                                float* __restrict__ p1) {
+                                                float* __restrict__ p1,
+                                                CellTags t = CellTags{}, int j = 0) {
   int x = blockIdx.x * blockDim.x + threadIdx.x;
   int z = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= g.nx || z >= g.nz) return;
@@ -331,6 +383,16 @@ __global__ void __launch_bounds__(256) k_ac_prs(Geo2 g, Coef c, float dtx, float
                     ac_prs_at<N>(g, c, dtx, dtz, vx1 + so, vz1 + so, p0 + so, kappa, x, z));
   else
     u = ac_prs_cell<N>(g, c, dtx, dtz, h, p0 + so, vx1 + so, vz1 + so, kappa, x, z);
+  if constexpr (TG) {
+    const long long p = (long long)z * g.ld + x;
+    const int e = __ldg(t.tag + p);
+    if (e >= 0) {
+      const long long k = (long long)(*t.it0 + j);
+      const int4 E = t.ent[e];
+      u = tag_inject(t, E, k, u);
+      tag_record(t, E, k, u, __ldg(vx1 + p), __ldg(vz1 + p));
+    }
+  }
   p1[so + (long long)z * g.ld + x] = u;
 }
 
