@@ -334,10 +334,15 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
   size_t o_snap = (!P.dev && outs.snaps && P.nsnap) ? ar.take<float>(P.nsnap * nint) : 0;
   size_t o_bounds = ar.take<long long>(kMaxGrid + 1);
   size_t o_it = ar.take<int>(1);  // device step index of replayed chunks
-  // Single-shot two-phase runs inject and record inside the step's last update
-  // kernel, on tagged cells (CellTags), instead of a separate launch.
-  const bool tagged = P.ns == 1 && !P.fp16 && kernel == FOMO_KERNEL_TWO_PHASE &&
-                      (P.phys == kAcoustic || P.phys == kElastic) && !hook;
+  // Single-shot two-phase runs on grids up to 2 M cells, which are bound by
+  // launch latency, inject and record inside the step's last update kernel on
+  // tagged cells (CellTags) instead of a separate launch.  Larger grids keep the
+  // separate kernel: a step costs tens of microseconds there, and the tag code
+  // raises the acoustic pressure kernel from 40 to 54 registers (6 -> 4 blocks
+  // per SM).
+  const bool tagged = P.ns == 1 && !P.fp16 && !hook &&
+                      (long long)P.nxp * P.nzp <= 2000000LL &&
+                      (P.phys == kScalar || kernel == FOMO_KERNEL_TWO_PHASE);
   CellTagHost tags;
   if (tagged) tags = make_cell_tags(src_lin.data(), P.n_src, rec_lin.data(), P.n_rec);
   const int n_ent = (int)tags.lin.size();
@@ -518,6 +523,23 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
       else go(std::false_type{}, std::false_type{});
     }
   };
+  // One scalar leapfrog step u^{n+1} (set n) from u^n (set b) and u^{n-1} (set a).
+  auto sc_step = [&](cudaStream_t s, int a, int b, int n, int j, const D2Coef& dc) {
+    auto go = [&](auto tgc) {
+      constexpr bool TGV = decltype(tgc)::value;
+      switch (P.N) {
+#define FOMO_SC2_CASE(NN)                                                                     \
+  case NN:                                                                                    \
+    k_sc_step<NN, TGV><<<grd, blk, 0, s>>>(g, dc, h, field(b, 0), field(a, 0), d_mat,          \
+                                           field(n, 0), tg, j);                               \
+    break;
+        FOMO_SC2_CASE(1) FOMO_SC2_CASE(2) FOMO_SC2_CASE(3) FOMO_SC2_CASE(4) FOMO_SC2_CASE(5)
+#undef FOMO_SC2_CASE
+      }
+    };
+    if (tagged) go(std::true_type{});
+    else go(std::false_type{});
+  };
   auto ac_two_phase = [&](cudaStream_t s, int a, int b, int j) {
     const float* bx = d_mat;
     const float* bz = d_mat + P.plane;
@@ -618,16 +640,15 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
         for (int l = 0; l < 5; ++l) dc.d[l] = kD2[P.N][l];
         int a = A, b = B, n = C2, nodes = 0;
         for (int j = 0; j < K; ++j) {
-#define FOMO_SCC_CASE(NN)                                                                 \
-  case NN:                                                                                \
-    k_sc_step<NN><<<grd, blk, 0, cs>>>(g, dc, h, field(b, 0), field(a, 0), d_mat, field(n, 0)); \
-    break;
-          switch (P.N) { FOMO_SCC_CASE(1) FOMO_SCC_CASE(2) FOMO_SCC_CASE(3) FOMO_SCC_CASE(4) FOMO_SCC_CASE(5) }
-#undef FOMO_SCC_CASE
-          k_inject_record_at<<<1, 256, 0, cs>>>(d_it, j, P.nt, P.plane, P.n_src, d_src, d_wav,
-                                                field(n, 0), nullptr, P.n_rec, d_rec, field(n, 0),
-                                                nullptr, nullptr, d_seis[0], nullptr, nullptr);
-          nodes += 2;
+          sc_step(cs, a, b, n, j, dc);
+          ++nodes;
+          if (!tagged) {
+            k_inject_record_at<<<1, 256, 0, cs>>>(d_it, j, P.nt, P.plane, P.n_src, d_src, d_wav,
+                                                  field(n, 0), nullptr, P.n_rec, d_rec,
+                                                  field(n, 0), nullptr, nullptr, d_seis[0],
+                                                  nullptr, nullptr);
+            ++nodes;
+          }
           const int t = a;
           a = b;
           b = n;
@@ -781,12 +802,7 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
       D2Coef dc;
       dc.two_c0 = 2.0f * kD2C0[P.N];
       for (int l = 0; l < 5; ++l) dc.d[l] = kD2[P.N][l];
-#define FOMO_SC_CASE(NN)                                                                      \
-  case NN:                                                                                    \
-    k_sc_step<NN><<<grd, blk, 0, st>>>(g, dc, h, field(B, 0), field(A, 0), d_mat, field(C2, 0)); \
-    break;
-      switch (P.N) { FOMO_SC_CASE(1) FOMO_SC_CASE(2) FOMO_SC_CASE(3) FOMO_SC_CASE(4) FOMO_SC_CASE(5) }
-#undef FOMO_SC_CASE
+      sc_step(st, A, B, C2, it - it_first, dc);  // *d_it = it_first - 1 after the chunks
       sweeps_per_step = 1;
       FOMO_CU(ctx, prof_mark(it, 1));
       if (hook && hook->corrects()) {
@@ -800,11 +816,13 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
                                            P.n_rec, d_rec, field(C2, 0), nullptr, nullptr,
                                            d_seis[0], nullptr, nullptr);
         launches += 3 + hook->launches_per_step();
-      } else {
+      } else if (!tagged) {
         k_inject_record<<<1, 256, 0, st>>>(it, P.nt, P.plane, P.n_src, d_src, d_wav, field(C2, 0),
                                            nullptr, P.n_rec, d_rec, field(C2, 0), nullptr, nullptr,
                                            d_seis[0], nullptr, nullptr);
         launches += 2;
+      } else {
+        launches += 1;
       }
       if (hook)
         if (int hr = hook->after_step(ctx, st, it, field(C2, 0), P)) return hr;

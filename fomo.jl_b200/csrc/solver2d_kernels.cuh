@@ -424,12 +424,14 @@ __device__ __forceinline__ float sc_at(const Geo2& g, const D2Coef& c, const flo
   return __fmaf_rn(__ldg(c2 + p), lap, __fsub_rn(__fmul_rn(2.0f, uc), __ldg(u0 + p)));
 }
 
-template <int N>
+// TG: inject into u and record it on tagged cells (step *t.it0 + j + 1).
+template <int N, bool TG = false>
 __global__ void __launch_bounds__(256) k_sc_step(Geo2 g, D2Coef c, HabcDev h,
                                                  const float* __restrict__ u1,
                                                  const float* __restrict__ u0,
                                                  const float* __restrict__ c2,
-                                                 float* __restrict__ u2) {
+                                                 float* __restrict__ u2,
+                                                 CellTags t = CellTags{}, int j = 0) {
   int x = blockIdx.x * blockDim.x + threadIdx.x;
   int z = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= g.nx || z >= g.nz) return;
@@ -450,6 +452,15 @@ __global__ void __launch_bounds__(256) k_sc_step(Geo2 g, D2Coef c, HabcDev h,
       long long pn = (long long)zn * g.ld + xn;
       float a = sc_at<N>(g, c, u1, u0, c2, xn, zn);
       u = higdon_edge(w, u, higdon_side(h, a, fo, __ldg(u1 + pn)));
+    }
+  }
+  if constexpr (TG) {
+    const int e = __ldg(t.tag + p);
+    if (e >= 0) {
+      const long long k = (long long)(*t.it0 + j);
+      const int4 E = t.ent[e];
+      u = tag_inject(t, E, k, u);
+      tag_record(t, E, k, u, 0.0f, 0.0f);
     }
   }
   u2[p] = u;

@@ -176,3 +176,9 @@ def test_single_shot_tagged_cells_vs_oracle(fomo, oracle, step_launch, launch):
     oe = oracle.elastic2d(vp, vs, rho, 5.0, 5e-4, nt, wavelet=np.repeat(we[None], 3, axis=0), **kw)
     assert np.array_equal(e.seis_vx, oe["seis_vx"][:, :, 0])
     assert np.array_equal(e.seis_vz, oe["seis_vz"][:, :, 0])
+    kws = {k: v for k, v in kw.items() if k != "snap_interval"}
+    u = run(fomo.scalar2d, vp, 5.0, 5e-4, nt, 20.0, source_scale="none", **kws)
+    ou = oracle.scalar2d(vp, 5.0, 5e-4, nt, wavelet=np.repeat(we[None], 3, axis=0), **kws)
+    su = ou["seis_u"] if ou["seis_u"].ndim == 2 else ou["seis_u"][:, :, 0]
+    assert np.array_equal(u.seis_u, su)
+    assert np.abs(u.seis_u).max() > 0
