@@ -743,6 +743,29 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
     for (auto& e : frame_ev.ev) FOMO_CU(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   }
   long long lag_done = 0;  // frames [0, lag_done) copied during the loop
+  // Seismograms of step-by-step runs (the large-batch single sweep) are copied
+  // the same way, in blocks of kSeisBlock steps, one block behind: each block is
+  // one strided copy per component ((n_rec, steps) per shot, pitch n_rec * nt).
+  constexpr int kSeisBlock = 128;
+  const bool seis_stream = !P.dev && seis_n > 0 && it_first == 1 && P.nt >= 2 * kSeisBlock;
+  ChunkEvents seis_ev;
+  if (seis_stream) {
+    seis_ev.ev.assign(2, nullptr);
+    for (auto& e : seis_ev.ev) FOMO_CU(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  long long seis_done = 0;  // time steps [0, seis_done) of every seismogram copied
+  auto copy_seis = [&](long long t0, long long t1, cudaStream_t s) -> cudaError_t {
+    const size_t pitch = sizeof(float) * (size_t)P.n_rec * P.nt;
+    for (int k = 0; k < outs.nseis; ++k) {
+      if (!outs.seis[k]) continue;
+      cudaError_t e = cudaMemcpy2DAsync(outs.seis[k] + (long long)P.n_rec * t0, pitch,
+                                        d_seis[k] + (long long)P.n_rec * t0, pitch,
+                                        sizeof(float) * (size_t)P.n_rec * (t1 - t0), P.ns,
+                                        cudaMemcpyDeviceToHost, s);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  };
   for (int it = it_first; it <= P.nt; ++it) {
     FOMO_CU(ctx, prof_mark(it, 0));
     if (P.phys == kElastic) {
@@ -840,6 +863,16 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
                                      sizeof(float) * P.ld, sizeof(float) * P.nx, P.nz,
                                      cudaMemcpyDeviceToDevice, st));
     }
+    if (seis_stream && it % kSeisBlock == 0) {
+      const int b = it / kSeisBlock - 1;  // steps [b, b + 1) * kSeisBlock are enqueued
+      FOMO_CU(ctx, cudaEventRecord(seis_ev.ev[b & 1], st));
+      if (b >= 1) {
+        FOMO_CU(ctx, cudaStreamWaitEvent(ctx->copy_stream, seis_ev.ev[(b - 1) & 1], 0));
+        FOMO_CU(ctx, copy_seis((long long)(b - 1) * kSeisBlock, (long long)b * kSeisBlock,
+                               ctx->copy_stream));
+        seis_done = (long long)b * kSeisBlock;
+      }
+    }
     if (lag_stream && it % P.snap_interval == 0) {
       const int k = it / P.snap_interval - 1;
       FOMO_CU(ctx, cudaEventRecord(frame_ev.ev[k & 1], st));
@@ -876,10 +909,14 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
                                    sizeof(float) * frames_per_chunk * nint,
                                    cudaMemcpyDeviceToHost, ctx->copy_stream));
     }
-    for (int k = 0; k < outs.nseis; ++k)
-      if (outs.seis[k] && seis_n)
-        FOMO_CU(ctx, cudaMemcpyAsync(outs.seis[k], d_seis[k], sizeof(float) * seis_n,
-                                     cudaMemcpyDeviceToHost, st));
+    if (seis_n && seis_done == 0) {
+      for (int k = 0; k < outs.nseis; ++k)
+        if (outs.seis[k])
+          FOMO_CU(ctx, cudaMemcpyAsync(outs.seis[k], d_seis[k], sizeof(float) * seis_n,
+                                       cudaMemcpyDeviceToHost, st));
+    } else if (seis_n) {
+      FOMO_CU(ctx, copy_seis(seis_done, P.nt, st));
+    }
     if (d_snap && P.nsnap > streamed)
       FOMO_CU(ctx, cudaMemcpyAsync(outs.snaps + streamed * nint, d_snap + streamed * nint,
                                    sizeof(float) * (P.nsnap - streamed) * nint,
@@ -908,7 +945,8 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
       }
   }
   FOMO_CU(ctx, cudaStreamSynchronize(st));
-  if (streamed_chunks || lag_done) FOMO_CU(ctx, cudaStreamSynchronize(ctx->copy_stream));
+  if (streamed_chunks || lag_done || seis_done)
+    FOMO_CU(ctx, cudaStreamSynchronize(ctx->copy_stream));
   if (kernel == FOMO_KERNEL_SINGLE_SWEEP) {
     int hflag = 0;
     FOMO_CU(ctx, cudaMemcpy(&hflag, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost));

@@ -182,3 +182,23 @@ def test_single_shot_tagged_cells_vs_oracle(fomo, oracle, step_launch, launch):
     su = ou["seis_u"] if ou["seis_u"].ndim == 2 else ou["seis_u"][:, :, 0]
     assert np.array_equal(u.seis_u, su)
     assert np.abs(u.seis_u).max() > 0
+
+
+@pytest.mark.parametrize("kernel", [1, 2])
+def test_streamed_seismograms_vs_oracle(fomo, oracle, kernel):
+    """Step-by-step runs copy the seismograms in 128-step blocks while the loop
+    runs (two shots: one strided copy per block and component); 400 steps give
+    three streamed blocks and a 16-step remainder."""
+    from fomo_b200.synthetic import layered_elastic
+
+    vp, vs, rho = layered_elastic(60, 40, n_layers=3, seed=12)
+    nt = 400
+    rx = np.arange(1, 61, 4)
+    rz = np.full(rx.size, 5)
+    kw = dict(sx=[15, 45], sz=[5, 8], rx=rx, rz=rz, nbc=8, fd_order=8)
+    r = fomo.elastic2d_batch(vp, vs, rho, 5.0, 5e-4, nt, 20.0, kernel=kernel, **kw)
+    w = fomo.ricker_wavelet(20.0, 5e-4, nt)
+    o = oracle.elastic2d(vp, vs, rho, 5.0, 5e-4, nt, wavelet=w[None], n_shots=2, **kw)
+    assert np.array_equal(r.seis_vx, o["seis_vx"])
+    assert np.array_equal(r.seis_vz, o["seis_vz"])
+    assert np.abs(r.seis_vz[:, -1, :]).max() > 0
