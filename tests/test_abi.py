@@ -65,6 +65,10 @@ def test_bad_arguments_return_codes_without_a_device(fomo):
     assert L.fomo_last_error(None) == b"null context"
     # solver entry points reject a NULL context instead of crashing
     assert L.fomo_elastic2d_batch(None, None, None, None, None, None, None, None, None, None) != 0
+    assert L.fomo_coupled2d(None, None, None, None, 0.0, 3.0, None, 0, None, None, None, None,
+                            None, None) == _lib.FOMO_EARG
+    assert L.fomo_debug_coupled_medium(None, 4, 4, 2, 8, 10.0, 3.0, None, None,
+                                       None) == _lib.FOMO_EARG
 
 
 def test_create_without_device_fails_cleanly(fomo):
