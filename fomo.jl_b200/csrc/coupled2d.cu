@@ -540,6 +540,16 @@ int fomo_coupled2d(fomo_ctx* ctx, const fomo_grid2d* gp, const float* vp, const 
   // step index, as the acoustic solver does; the rest launch step by step
   // (FOMO_F_STEP_LAUNCH: every step), with identical results.
   int it_first = 1;
+  // Snapshot frames of replayed chunk k are copied to the caller once chunk k
+  // has run (an event per chunk, the context's copy stream), while later chunks
+  // compute; copies into pageable memory return when done.
+  struct Events {
+    std::vector<cudaEvent_t> ev;
+    ~Events() {
+      for (auto e : ev) cudaEventDestroy(e);
+    }
+  } chunk_ev;
+  int streamed_chunks = 0, frames_per_chunk = 0;
   cudaGraphExec_t exec = nullptr;
   struct ExecGuard {
     cudaGraphExec_t& e;
@@ -588,7 +598,17 @@ int fomo_coupled2d(fomo_ctx* ctx, const fomo_grid2d* gp, const float* vp, const 
       }
       if (ce == cudaSuccess) ce = cudaGraphInstantiate(&exec, graph, 0);
       if (graph) cudaGraphDestroy(graph);
-      for (int k = 0; ce == cudaSuccess && k < nchunk; ++k) ce = cudaGraphLaunch(exec, st);
+      if (ce == cudaSuccess && si && (snaps_P || snaps_S)) {
+        chunk_ev.ev.assign(nchunk, nullptr);
+        for (auto& e : chunk_ev.ev)
+          if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+        frames_per_chunk = K / si;
+      }
+      for (int k = 0; ce == cudaSuccess && k < nchunk; ++k) {
+        ce = cudaGraphLaunch(exec, st);
+        if (ce == cudaSuccess && frames_per_chunk) ce = cudaEventRecord(chunk_ev.ev[k], st);
+      }
+      if (ce == cudaSuccess && frames_per_chunk) streamed_chunks = nchunk;
       if (ce != cudaSuccess)
         return fail(ctx, FOMO_ECUDA, std::string("replayed step chunk: ") + cudaGetErrorString(ce));
       launches += nchunk * nodes;
@@ -610,6 +630,18 @@ int fomo_coupled2d(fomo_ctx* ctx, const fomo_grid2d* gp, const float* vp, const 
     std::swap(A, B);
   }
   FOMO_CU(ctx, cudaEventRecord(ctx->ev1, st));
+  float* const snaps_out[2] = {snaps_P, snaps_S};
+  for (int k = 0; k < streamed_chunks; ++k) {
+    FOMO_CU(ctx, cudaStreamWaitEvent(ctx->copy_stream, chunk_ev.ev[k], 0));
+    const long long f0 = (long long)k * frames_per_chunk;
+    for (int f = 0; f < 2; ++f)
+      if (snaps_out[f])
+        FOMO_CU(ctx, cudaMemcpyAsync(snaps_out[f] + f0 * nint,
+                                     d_snap + ((long long)f * nsnap + f0) * nint,
+                                     sizeof(float) * frames_per_chunk * nint,
+                                     cudaMemcpyDeviceToHost, ctx->copy_stream));
+  }
+  const long long streamed = (long long)streamed_chunks * frames_per_chunk;
   if (seis_n) {
     if (seis_P)
       FOMO_CU(ctx, cudaMemcpyAsync(seis_P, d_seis, sizeof(float) * seis_n, cudaMemcpyDeviceToHost, st));
@@ -617,15 +649,15 @@ int fomo_coupled2d(fomo_ctx* ctx, const fomo_grid2d* gp, const float* vp, const 
       FOMO_CU(ctx, cudaMemcpyAsync(seis_S, d_seis + seis_n, sizeof(float) * seis_n,
                                    cudaMemcpyDeviceToHost, st));
   }
-  if (nsnap) {
-    if (snaps_P)
-      FOMO_CU(ctx, cudaMemcpyAsync(snaps_P, d_snap, sizeof(float) * nsnap * nint,
-                                   cudaMemcpyDeviceToHost, st));
-    if (snaps_S)
-      FOMO_CU(ctx, cudaMemcpyAsync(snaps_S, d_snap + nsnap * nint, sizeof(float) * nsnap * nint,
-                                   cudaMemcpyDeviceToHost, st));
-  }
+  if (nsnap > streamed)
+    for (int f = 0; f < 2; ++f)
+      if (snaps_out[f])
+        FOMO_CU(ctx, cudaMemcpyAsync(snaps_out[f] + streamed * nint,
+                                     d_snap + ((long long)f * nsnap + streamed) * nint,
+                                     sizeof(float) * (nsnap - streamed) * nint,
+                                     cudaMemcpyDeviceToHost, st));
   FOMO_CU(ctx, cudaStreamSynchronize(st));
+  if (streamed_chunks) FOMO_CU(ctx, cudaStreamSynchronize(ctx->copy_stream));
   float ms = 0.0f;
   FOMO_CU(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
   if (stats) {
