@@ -557,14 +557,49 @@ def sponge_bench(args):
             out[bnd] = {"wall_s": float(np.median([t for t, _ in runs])),
                         "kernel_s": float(np.median([r.stats.kernel_time_s for _, r in runs])),
                         "late_energy": late}
-        print(json.dumps({"workload": "reference HABC-vs-sponge benchmark", "equation": eq,
-                          "grid": [n, n], "nt": c["nt"], "snap_interval": c["snap"],
-                          "habc": out["habc"], "sponge": out["sponge"],
-                          "late_energy_ratio": out["sponge"]["late_energy"]
-                          / out["habc"]["late_energy"],
-                          "reference_rtx3060_wall_s": c["ref_s"],
-                          "reference_late_energy": c["ref_energy"],
-                          "device": "B200", "dtype": "f32"}), flush=True)
+        line = {"workload": "reference HABC-vs-sponge benchmark", "equation": eq,
+                "grid": [n, n], "nt": c["nt"], "snap_interval": c["snap"],
+                "habc": out["habc"], "sponge": out["sponge"],
+                "late_energy_ratio": out["sponge"]["late_energy"] / out["habc"]["late_energy"],
+                "reference_rtx3060_wall_s": c["ref_s"],
+                "reference_late_energy": c["ref_energy"], "device": "B200", "dtype": "f32"}
+        if not args.no_cpu:
+            from oracle import oracle as O
+
+            w = np.asarray(F.ricker_wavelet(15.0, 1e-3, c["nt"]))
+            okw = {k: v for k, v in kw.items() if k != "snap_interval"}
+
+            def orun(m):
+                if eq == "acoustic2d":
+                    O.acoustic2d(vp, rho, 10.0, 1e-3, m, wavelet=w[None, :m], sponge_factor=0.015,
+                                 **okw)
+                else:
+                    O.elastic2d(vp, vs, rho, 10.0, 1e-3, m, wavelet=w[None, :m],
+                                sponge_factor=0.015, **okw)
+
+            rate, m, cores = _oracle_steps_per_s(orun, c["nt"])
+            line["cpu_baseline"] = {"value": c["nt"] / rate, "unit": "s (sponge run)",
+                                    "cores": cores, "kind": "port",
+                                    "sample": f"{m} of {c['nt']} steps scaled linearly; FP32 "
+                                    "C++/OpenMP oracle with the sponge"}
+        print(json.dumps(line), flush=True)
+
+
+def _oracle_steps_per_s(run, nt, target_s=4.0):
+    """Steps/s of an oracle run on all host threads, timed on a bounded sample:
+    run(n) runs n time steps; n is sized from a 2-step probe to about target_s."""
+    import time
+
+    from oracle import oracle as O
+
+    O.build()
+    t0 = time.perf_counter()
+    run(2)
+    t = time.perf_counter() - t0
+    n = int(max(2, min(nt, round(2 * target_s / max(t, 1e-6)))))
+    t0 = time.perf_counter()
+    run(n)
+    return n / (time.perf_counter() - t0), n, O.max_threads()
 
 
 def _coupled_demo_models():
@@ -618,11 +653,24 @@ def coupled_bench(args):
         wall = float(np.median([t for t, _, _ in runs]))
         loop = float(np.median([r.stats.kernel_time_s for _, r, _ in runs]))
         gbs = runs[-1][2] / loop / 1e9
-        print(json.dumps({"workload": "coupled2d demo", "demo": c["name"], "grid": [nx, nz],
-                          "nt": c["nt"], "snap_interval": c["snap"], "wall_s": wall,
-                          "loop_s": loop, "steps_per_s": c["nt"] / loop, "alg_gbs": gbs,
-                          "hbm_frac": gbs / peak, "peak_gbs": peak, "peak_kind": pkind,
-                          "device": "B200", "dtype": "f32"}), flush=True)
+        line = {"workload": "coupled2d demo", "demo": c["name"], "grid": [nx, nz],
+                "nt": c["nt"], "snap_interval": c["snap"], "wall_s": wall,
+                "loop_s": loop, "steps_per_s": c["nt"] / loop, "alg_gbs": gbs,
+                "hbm_frac": gbs / peak, "peak_gbs": peak, "peak_kind": pkind,
+                "device": "B200", "dtype": "f32"}
+        if not args.no_cpu:
+            from oracle import oracle as O
+
+            w = np.asarray(F.ricker_wavelet(15.0, c["dt"], c["nt"]))
+
+            def orun(n):
+                O.coupled2d(c["vp"], c["vs"], c["dh"], c["dt"], n, wavelet=w[None, :n], **kw)
+
+            rate, n, cores = _oracle_steps_per_s(orun, c["nt"])
+            line["cpu_baseline"] = {"value": rate, "unit": "steps/s", "cores": cores,
+                                    "kind": "port", "sample": f"{n} of {c['nt']} steps; FP32 "
+                                    "C++/OpenMP oracle (run_coupled2d)"}
+        print(json.dumps(line), flush=True)
 
 
 def main():
