@@ -32,7 +32,7 @@ def test_coupled_medium_bitwise(fomo, oracle, fd_order, sigma):
         assert np.array_equal(got[:, :, k], want[:, :, k]), k
 
 
-@pytest.mark.parametrize("fd_order", [4, 8, 10])
+@pytest.mark.parametrize("fd_order", [2, 4, 6, 8, 10])
 def test_coupled2d_bitwise_vs_oracle(fomo, oracle, fd_order):
     vp, vs = _model()
     nt, nbc = 300, 12

@@ -183,3 +183,18 @@ def test_sponge_unsupported_combinations(fomo):
     with pytest.raises(L.FomoError) as e:
         fomo.elastic2d(vp, vs, rho, 5.0, 5e-4, 20, 20.0, sponge_factor=-1.0, **kw)
     assert e.value.code == L.FOMO_EARG
+
+
+def test_sponge_with_no_layers_is_the_plain_update(fomo, oracle):
+    """nbc = 0: no damped cells (reference: d < nbc never holds), so the sponge
+    run is the bare update with a fixed outer ring; bit-exact to the oracle."""
+    from fomo_b200.synthetic import two_layer
+
+    vp, rho = _vacuum_top(*two_layer(50, 40))
+    nt = 120
+    w = fomo.ricker_wavelet(15.0, 1e-3, nt)
+    kw = dict(sx=[25], sz=[10], rx=np.arange(1, 51, 4), rz=np.full(13, 6), nbc=0, fd_order=8)
+    r = fomo.acoustic2d(vp, rho, 10.0, 1e-3, nt, 15.0, boundary="sponge", **kw)
+    o = oracle.acoustic2d(vp, rho, 10.0, 1e-3, nt, wavelet=w[None], sponge_factor=FACTOR, **kw)
+    assert np.array_equal(r.seis_p, o["seis_p"][:, :, 0])
+    assert np.abs(r.seis_p).max() > 0
