@@ -121,3 +121,17 @@ def test_uneven_batch_validation(fomo):
         fomo.acoustic2d_uneven([vp1, vp2 * 3], [rho1, rho2], 10.0, 1e-3, 50, 15.0, **kw)
     with pytest.raises(ValueError):
         fomo.acoustic2d_uneven([vp1, vp2], [rho1, rho2], 10.0, 1e-3, 50, 15.0, fd_order=7, **kw)
+
+
+def test_coupled2d_validation(fomo):
+    """coupled2d.jl:71-77: geometry and the centered CFL bound are checked on the
+    host; the shapes of vp and vs must agree."""
+    vp = np.full((40, 30), 3000.0, np.float32)
+    vs = np.full((40, 30), 1700.0, np.float32)
+    kw = dict(sx=[5], sz=[3], rx=[4], rz=[3])
+    with pytest.raises(fomo.ArgumentError):
+        fomo.coupled2d(vp, vs[:, :20], 10.0, 1e-3, 50, 15.0, **kw)
+    with pytest.raises(fomo.ArgumentError):
+        fomo.coupled2d(vp, vs, 10.0, 9e-3, 50, 15.0, **kw)
+    with pytest.raises(fomo.ArgumentError):
+        fomo.coupled2d(vp, vs, 10.0, 1e-3, 50, 15.0, sx=[41], sz=[3], rx=[4], rz=[3])
