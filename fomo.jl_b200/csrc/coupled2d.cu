@@ -293,8 +293,8 @@ __global__ void __launch_bounds__(256) k_cp_pos(Geo2 g, float dt, HabcDev hp, Ha
   if (e >= 0) {  // injection into P, then recording of P and S (coupled2d.jl:239-250)
     const long long k = (long long)(*t.it0 + j);  // it - 1
     const int4 E = t.ent[e];
-    uP = tag_inject(t, E, k, uP);
-    tag_record(t, E, k, uP, uS, 0.0f);
+    uP = tag_inject(t, E, k, 0, uP);
+    tag_record(t, E, k, 0, uP, uS, 0.0f);
   }
   P1[p] = uP;
   S1[p] = uS;
@@ -520,6 +520,7 @@ int fomo_coupled2d(fomo_ctx* ctx, const fomo_grid2d* gp, const float* vp, const 
   tg.wav = d_wav;
   tg.n_src = acq->n_src;
   tg.n_rec = acq->n_rec;
+  tg.nt = nt;
   tg.s0 = d_seis;
   tg.s1 = d_seis + seis_n;
   tg.it0 = d_it;

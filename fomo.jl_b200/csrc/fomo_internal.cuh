@@ -159,8 +159,9 @@ __device__ __forceinline__ float dp(const float* __restrict__ f, long long p, lo
 }
 
 // Host side of the cell tags (CellTags, solver2d_kernels.cuh): one entry per
-// distinct source or receiver cell (linear pitched index), listing the source
-// indices (ascending) then the receiver indices at that cell.
+// distinct source or receiver cell (linear pitched index within a shot's
+// plane), listing the source indices s * n_src + q (ascending) then the
+// receiver indices at that cell.  src_lin holds all shots' sources.
 struct CellTagHost {
   std::vector<int32_t> lin;  // entry -> cell
   std::vector<int4> ent;     // sources list[x, y), receivers list[z, w)

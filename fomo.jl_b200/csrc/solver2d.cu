@@ -334,17 +334,16 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
   size_t o_snap = (!P.dev && outs.snaps && P.nsnap) ? ar.take<float>(P.nsnap * nint) : 0;
   size_t o_bounds = ar.take<long long>(kMaxGrid + 1);
   size_t o_it = ar.take<int>(1);  // device step index of replayed chunks
-  // Single-shot two-phase runs on grids up to 2 M cells, which are bound by
-  // launch latency, inject and record inside the step's last update kernel on
-  // tagged cells (CellTags) instead of a separate launch.  Larger grids keep the
+  // Two-phase runs of up to 2 M shot-cells, which are bound by launch latency,
+  // inject and record inside the step's last update kernel on tagged cells
+  // (CellTags) instead of a separate launch.  Larger grids keep the
   // separate kernel: a step costs tens of microseconds there, and the tag code
   // raises the acoustic pressure kernel from 40 to 54 registers (6 -> 4 blocks
   // per SM).
-  const bool tagged = P.ns == 1 && !P.fp16 && !hook &&
-                      (long long)P.nxp * P.nzp <= 2000000LL &&
+  const bool tagged = !P.fp16 && !hook && (long long)P.nxp * P.nzp * P.ns <= 2000000LL &&
                       (P.phys == kScalar || kernel == FOMO_KERNEL_TWO_PHASE);
   CellTagHost tags;
-  if (tagged) tags = make_cell_tags(src_lin.data(), P.n_src, rec_lin.data(), P.n_rec);
+  if (tagged) tags = make_cell_tags(src_lin.data(), (int)nsrc_all, rec_lin.data(), P.n_rec);
   const int n_ent = (int)tags.lin.size();
   size_t o_tag = tagged ? ar.take<int32_t>(P.plane) : 0;
   size_t o_ent = tagged ? ar.take<int4>(std::max(n_ent, 1)) : 0;
@@ -436,6 +435,7 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
     tg.wav = d_wav;
     tg.n_src = P.n_src;
     tg.n_rec = P.n_rec;
+    tg.nt = P.nt;
     tg.s0 = d_seis[0];
     tg.s1 = d_seis[1];
     tg.s2 = d_seis[2];

@@ -42,16 +42,18 @@ struct ElMat {
   int pack_pitch = 0;  // column pairs per pack row
 };
 
-// Source and receiver cells of a single-shot run, handled inside the step's
-// last update kernel by the threads that own them: injection (sources in source
-// order, as k_inject_record adds them), then recording.
+// Source and receiver cells of a run, handled inside the step's last update
+// kernel by the threads that own them: injection (each shot's sources in source
+// order, as k_inject_record adds them), then recording.  One plane serves every
+// shot of a batch: receivers are shared, and a source entry holds the index
+// s * n_src + q of source q of shot s, which only shot s's threads apply.
 struct CellTags {
   const int* tag = nullptr;   // pitched like the fields: -1, or an entry per distinct cell
   const int4* ent = nullptr;  // per entry: sources list[x, y), receivers list[z, w)
   const int* list = nullptr;
-  const float* wav = nullptr;  // (n_src, nt)
-  int n_src = 0, n_rec = 0;
-  float* s0 = nullptr;  // seismograms (null: not recorded)
+  const float* wav = nullptr;  // (n_src, nt), shared by the shots
+  int n_src = 0, n_rec = 0, nt = 0;
+  float* s0 = nullptr;  // seismograms (n_rec, nt, n_shots) (null: not recorded)
   float* s1 = nullptr;
   float* s2 = nullptr;
   const int* it0 = nullptr;  // steps completed before this launch's chunk
@@ -62,17 +64,22 @@ static __global__ void k_set_tags(int* __restrict__ tag, const int* __restrict__
   if (e < n) tag[lin[e]] = e;
 }
 
-// u plus the wavelets of the entry's sources at 0-based step k, in source order.
+// u plus the wavelets of shot `shot`'s sources in the entry at 0-based step k,
+// in source order.
 __device__ __forceinline__ float tag_inject(const CellTags& t, const int4& E, long long k,
-                                            float u) {
-  for (int i = E.x; i < E.y; ++i)
-    u = __fadd_rn(u, __ldg(t.wav + t.list[i] + (long long)t.n_src * k));
+                                            int shot, float u) {
+  for (int i = E.x; i < E.y; ++i) {
+    const int e = t.list[i];
+    const int s = e / t.n_src;  // an entry with sources implies n_src > 0
+    if (s == shot) u = __fadd_rn(u, __ldg(t.wav + (e - s * t.n_src) + (long long)t.n_src * k));
+  }
   return u;
 }
 __device__ __forceinline__ void tag_record(const CellTags& t, const int4& E, long long k,
-                                           float r0, float r1, float r2) {
+                                           int shot, float r0, float r1, float r2) {
+  const long long base = (long long)t.n_rec * (k + (long long)t.nt * shot);
   for (int i = E.z; i < E.w; ++i) {
-    const long long o = t.list[i] + (long long)t.n_rec * k;
+    const long long o = t.list[i] + base;
     if (t.s0) t.s0[o] = r0;
     if (t.s1) t.s1[o] = r1;
     if (t.s2) t.s2[o] = r2;
@@ -173,8 +180,7 @@ __device__ __forceinline__ void el_str_at(const Geo2& g, const Coef& c, float dt
   }
 }
 
-// TG: single shot; inject into txx, tzz and record vx, vz on tagged cells
-// (step *t.it0 + j + 1).
+// TG: inject into txx, tzz and record vx, vz on tagged cells (step *t.it0 + j + 1).
 template <int N, bool SP = false, bool TG = false>
 __global__ void __launch_bounds__(256) k_el_str(Geo2 g, Coef c, float dtx, float dtz, HabcDev h,
                                                 ElFields a, const float* __restrict__ vx1,
@@ -226,9 +232,9 @@ __global__ void __launch_bounds__(256) k_el_str(Geo2 g, Coef c, float dtx, float
     if (e >= 0) {
       const long long k = (long long)(*t.it0 + j);
       const int4 E = t.ent[e];
-      sxx = tag_inject(t, E, k, sxx);
-      szz = tag_inject(t, E, k, szz);
-      tag_record(t, E, k, __ldg(vx + p), __ldg(vz + p), 0.0f);
+      sxx = tag_inject(t, E, k, blockIdx.z, sxx);
+      szz = tag_inject(t, E, k, blockIdx.z, szz);
+      tag_record(t, E, k, blockIdx.z, __ldg(vx + p), __ldg(vz + p), 0.0f);
     }
   }
   txx1[so + p] = sxx;
@@ -364,7 +370,7 @@ __device__ __forceinline__ float ac_prs_cell(const Geo2& g, const Coef& c, float
   return u;
 }
 
-// TG: single shot; inject into p and record p, vx, vz on tagged cells.
+// TG: inject into p and record p, vx, vz on tagged cells.
 template <int N, bool SP = false, bool TG = false>
 __global__ void __launch_bounds__(256) k_ac_prs(Geo2 g, Coef c, float dtx, float dtz, HabcDev h,
                                                 const float* __restrict__ p0,
@@ -389,8 +395,8 @@ __global__ void __launch_bounds__(256) k_ac_prs(Geo2 g, Coef c, float dtx, float
     if (e >= 0) {
       const long long k = (long long)(*t.it0 + j);
       const int4 E = t.ent[e];
-      u = tag_inject(t, E, k, u);
-      tag_record(t, E, k, u, __ldg(vx1 + p), __ldg(vz1 + p));
+      u = tag_inject(t, E, k, blockIdx.z, u);
+      tag_record(t, E, k, blockIdx.z, u, __ldg(vx1 + so + p), __ldg(vz1 + so + p));
     }
   }
   p1[so + (long long)z * g.ld + x] = u;
@@ -459,8 +465,8 @@ __global__ void __launch_bounds__(256) k_sc_step(Geo2 g, D2Coef c, HabcDev h,
     if (e >= 0) {
       const long long k = (long long)(*t.it0 + j);
       const int4 E = t.ent[e];
-      u = tag_inject(t, E, k, u);
-      tag_record(t, E, k, u, 0.0f, 0.0f);
+      u = tag_inject(t, E, k, 0, u);
+      tag_record(t, E, k, 0, u, 0.0f, 0.0f);
     }
   }
   u2[p] = u;

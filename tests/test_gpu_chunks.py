@@ -202,3 +202,34 @@ def test_streamed_seismograms_vs_oracle(fomo, oracle, kernel):
     assert np.array_equal(r.seis_vx, o["seis_vx"])
     assert np.array_equal(r.seis_vz, o["seis_vz"])
     assert np.abs(r.seis_vz[:, -1, :]).max() > 0
+
+
+@pytest.mark.parametrize("launch", ["chunks", "steps"])
+def test_batch_tagged_cells_vs_oracle(fomo, oracle, step_launch, launch):
+    """Batches inject and record on one shared tag plane: shot 0 has two
+    coincident sources, shot 1 a source on the same cell, and a receiver sits
+    there; each shot applies only its own sources."""
+    from fomo_b200.synthetic import layered_elastic
+
+    run = (lambda f, *a, **k: f(*a, **k)) if launch == "chunks" else step_launch
+    vp, rho = _model()
+    nt = 160
+    rx = np.concatenate([np.arange(1, 91, 9), [20]])
+    rz = np.concatenate([np.full(10, 8), [10]])
+    kw = dict(sx=[[20, 20], [20, 60]], sz=[[10, 10], [10, 25]], rx=rx, rz=rz, nbc=10,
+              fd_order=8)
+    w = fomo.ricker_wavelet(15.0, 1e-3, nt)
+    a = run(fomo.acoustic2d_batch, vp, rho, 10.0, 1e-3, nt, 15.0, **kw)
+    okw = dict(kw, sx=np.array(kw["sx"]).T, sz=np.array(kw["sz"]).T)
+    o = oracle.acoustic2d(vp, rho, 10.0, 1e-3, nt, wavelet=np.repeat(w[None], 2, axis=0),
+                          n_shots=2, **okw)
+    for x, y in ((a.seis_p, o["seis_p"]), (a.seis_vx, o["seis_vx"]), (a.seis_vz, o["seis_vz"])):
+        assert np.array_equal(x, y)
+    assert not np.array_equal(a.seis_p[:, :, 0], a.seis_p[:, :, 1])
+    vp, vs, rho = layered_elastic(90, 60, n_layers=3, seed=8)
+    we = fomo.ricker_wavelet(20.0, 5e-4, nt)
+    e = run(fomo.elastic2d_batch, vp, vs, rho, 5.0, 5e-4, nt, 20.0, kernel=1, **kw)
+    oe = oracle.elastic2d(vp, vs, rho, 5.0, 5e-4, nt, wavelet=np.repeat(we[None], 2, axis=0),
+                          n_shots=2, **okw)
+    assert np.array_equal(e.seis_vx, oe["seis_vx"])
+    assert np.array_equal(e.seis_vz, oe["seis_vz"])
