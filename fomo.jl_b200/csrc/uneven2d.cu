@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(256) k_uac_vel(const UShot* __restrict__ shots
                                                  float dtz, const float* __restrict__ wtab,
                                                  int nbc, int wstride, int set) {
   const int tile = blockIdx.x;
-  const UShot& sh = shots[tile_shot[tile]];
+  const UShot sh = shots[tile_shot[tile]];
   const int lt = tile - sh.tile0;
   const int tz = lt / sh.tiles_x, tx = lt - tz * sh.tiles_x;
   const int x = tx * blockDim.x + threadIdx.x, z = tz * blockDim.y + threadIdx.y;
@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(256) k_uac_prs(const UShot* __restrict__ shots
                                                  float dtz, const float* __restrict__ wtab,
                                                  int nbc, int wstride, int set) {
   const int tile = blockIdx.x;
-  const UShot& sh = shots[tile_shot[tile]];
+  const UShot sh = shots[tile_shot[tile]];
   const int lt = tile - sh.tile0;
   const int tz = lt / sh.tiles_x, tx = lt - tz * sh.tiles_x;
   const int x = tx * blockDim.x + threadIdx.x, z = tz * blockDim.y + threadIdx.y;
