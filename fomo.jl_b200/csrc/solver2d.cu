@@ -549,10 +549,17 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
       switch (P.N) {
 #define FOMO_AC2_CASE(NN)                                                                        \
   case NN:                                                                                       \
-    k_ac_vel<NN, SPV><<<grd, blk, 0, s>>>(g, c, dtx, dtz, h, field(a, 2), field(a, 0),           \
-                                          field(a, 1), bx, bz, field(b, 0), field(b, 1));        \
-    k_ac_prs<NN, SPV, TGV><<<grd, blk, 0, s>>>(g, c, dtx, dtz, h, field(a, 2), field(b, 0),      \
-                                               field(b, 1), kap, field(b, 2), tg, j);            \
+    if constexpr (TGV) {                                                                         \
+      k_ac_vel<NN, SPV><<<grd, blk, 0, s>>>(g, c, dtx, dtz, h, field(a, 2), field(a, 0),         \
+                                            field(a, 1), bx, bz, field(b, 0), field(b, 1));      \
+      k_ac_prs<NN, SPV, true><<<grd, blk, 0, s>>>(g, c, dtx, dtz, h, field(a, 2), field(b, 0),   \
+                                                  field(b, 1), kap, field(b, 2), tg, j);         \
+    } else {                                                                                     \
+      k_ac_vel8<NN, SPV><<<grd, blk, 0, s>>>(g, c, dtx, dtz, h, field(a, 2), field(a, 0),        \
+                                             field(a, 1), bx, bz, field(b, 0), field(b, 1));     \
+      k_ac_prs8<NN, SPV><<<grd, blk, 0, s>>>(g, c, dtx, dtz, h, field(a, 2), field(b, 0),        \
+                                             field(b, 1), kap, field(b, 2), tg, j);              \
+    }                                                                                            \
     break;
         FOMO_AC2_CASE(1) FOMO_AC2_CASE(2) FOMO_AC2_CASE(3) FOMO_AC2_CASE(4) FOMO_AC2_CASE(5)
 #undef FOMO_AC2_CASE

@@ -300,14 +300,17 @@ __device__ __forceinline__ void ac_vel_cell(const Geo2& g, const Coef& c, float 
   }
 }
 
-template <int N, bool SP = false>
-__global__ void __launch_bounds__(256) k_ac_vel(Geo2 g, Coef c, float dtx, float dtz, HabcDev h,
-                                                const float* __restrict__ p0,
-                                                const float* __restrict__ vx0,
-                                                const float* __restrict__ vz0,
-                                                const float* __restrict__ bx,
-                                                const float* __restrict__ bz,
-                                                float* __restrict__ vx1, float* __restrict__ vz1) {
+// The acoustic velocity update comes in two occupancy forms with one body:
+// k_ac_vel (no register bound; 40 registers, 6 blocks per SM) for the small,
+// latency-bound tagged runs, and k_ac_vel8 (8 blocks per SM, 32 registers) for
+// large grids.  The results are the same.
+#define FOMO_AC_VEL_PARAMS                                                                 \
+  Geo2 g, Coef c, float dtx, float dtz, HabcDev h, const float* __restrict__ p0,           \
+      const float* __restrict__ vx0, const float* __restrict__ vz0,                        \
+      const float* __restrict__ bx, const float* __restrict__ bz, float* __restrict__ vx1, \
+      float* __restrict__ vz1
+template <int N, bool SP>
+__device__ __forceinline__ void ac_vel_body(FOMO_AC_VEL_PARAMS) {
   int x = blockIdx.x * blockDim.x + threadIdx.x;
   int z = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= g.nx || z >= g.nz) return;
@@ -325,6 +328,15 @@ __global__ void __launch_bounds__(256) k_ac_vel(Geo2 g, Coef c, float dtx, float
   vx1[so + p] = ux;
   vz1[so + p] = uz;
 }
+template <int N, bool SP = false>
+__global__ void __launch_bounds__(256) k_ac_vel(FOMO_AC_VEL_PARAMS) {
+  ac_vel_body<N, SP>(g, c, dtx, dtz, h, p0, vx0, vz0, bx, bz, vx1, vz1);
+}
+template <int N, bool SP = false>
+__global__ void __launch_bounds__(256, 8) k_ac_vel8(FOMO_AC_VEL_PARAMS) {
+  ac_vel_body<N, SP>(g, c, dtx, dtz, h, p0, vx0, vz0, bx, bz, vx1, vz1);
+}
+#undef FOMO_AC_VEL_PARAMS
 
 template <int N>
 __device__ __forceinline__ float ac_prs_at(const Geo2& g, const Coef& c, float dtx, float dtz,
@@ -370,15 +382,15 @@ __device__ __forceinline__ float ac_prs_cell(const Geo2& g, const Coef& c, float
   return u;
 }
 
-// TG: inject into p and record p, vx, vz on tagged cells.
-template <int N, bool SP = false, bool TG = false>
-__global__ void __launch_bounds__(256) k_ac_prs(Geo2 g, Coef c, float dtx, float dtz, HabcDev h,
-                                                const float* __restrict__ p0,
-                                                const float* __restrict__ vx1,
-                                                const float* __restrict__ vz1,
-                                                const float* __restrict__ kappa,
-                                                float* __restrict__ p1,
-                                                CellTags t = CellTags{}, int j = 0) {
+// TG: inject into p and record p, vx, vz on tagged cells.  k_ac_prs (no register
+// bound) serves the small tagged runs, k_ac_prs8 (8 blocks per SM) large grids,
+// as for the velocity update.
+#define FOMO_AC_PRS_PARAMS                                                                  \
+  Geo2 g, Coef c, float dtx, float dtz, HabcDev h, const float* __restrict__ p0,            \
+      const float* __restrict__ vx1, const float* __restrict__ vz1,                         \
+      const float* __restrict__ kappa, float* __restrict__ p1, CellTags t, int j
+template <int N, bool SP, bool TG>
+__device__ __forceinline__ void ac_prs_body(FOMO_AC_PRS_PARAMS) {
   int x = blockIdx.x * blockDim.x + threadIdx.x;
   int z = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= g.nx || z >= g.nz) return;
@@ -401,6 +413,15 @@ __global__ void __launch_bounds__(256) k_ac_prs(Geo2 g, Coef c, float dtx, float
   }
   p1[so + (long long)z * g.ld + x] = u;
 }
+template <int N, bool SP = false, bool TG = false>
+__global__ void __launch_bounds__(256) k_ac_prs(FOMO_AC_PRS_PARAMS) {
+  ac_prs_body<N, SP, TG>(g, c, dtx, dtz, h, p0, vx1, vz1, kappa, p1, t, j);
+}
+template <int N, bool SP = false>
+__global__ void __launch_bounds__(256, 8) k_ac_prs8(FOMO_AC_PRS_PARAMS) {
+  ac_prs_body<N, SP, false>(g, c, dtx, dtz, h, p0, vx1, vz1, kappa, p1, t, j);
+}
+#undef FOMO_AC_PRS_PARAMS
 
 // ---------------------------------------------------------------------------
 // scalar2d leapfrog (scalar2d/scalar2d.jl:29-84): u2 = update(u1, u0), then
@@ -430,9 +451,10 @@ __device__ __forceinline__ float sc_at(const Geo2& g, const D2Coef& c, const flo
   return __fmaf_rn(__ldg(c2 + p), lap, __fsub_rn(__fmul_rn(2.0f, uc), __ldg(u0 + p)));
 }
 
-// TG: inject into u and record it on tagged cells (step *t.it0 + j + 1).
+// TG: inject into u and record it on tagged cells (step *t.it0 + j + 1).  Tagged
+// (small, latency-bound) runs take 6 blocks per SM, untagged (large) ones 8.
 template <int N, bool TG = false>
-__global__ void __launch_bounds__(256) k_sc_step(Geo2 g, D2Coef c, HabcDev h,
+__global__ void __launch_bounds__(256, TG ? 6 : 8) k_sc_step(Geo2 g, D2Coef c, HabcDev h,
                                                  const float* __restrict__ u1,
                                                  const float* __restrict__ u0,
                                                  const float* __restrict__ c2,

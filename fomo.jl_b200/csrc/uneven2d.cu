@@ -40,7 +40,7 @@ struct UShot {
 };
 
 template <int N>
-__global__ void __launch_bounds__(256) k_uac_vel(const UShot* __restrict__ shots,
+__global__ void __launch_bounds__(256, 8) k_uac_vel(const UShot* __restrict__ shots,
                                                  const int* __restrict__ tile_shot,
                                                  float* __restrict__ state,
                                                  const float* __restrict__ mat, Coef c, float dtx,
