@@ -201,8 +201,13 @@ int tune_sweep(fomo_ctx* ctx, cudaStream_t st, SweepPlan& sp, int N, const Geo2&
     FOMO_CU(ctx, cudaEventElapsedTime(&ms, e0, e1));
     return FOMO_OK;
   };
+  // Candidates: the warp-specialized sweeps and, for FP32 batches with the
+  // pair pack built, the shot-pair sweeps (the older families measured slower
+  // on every problem; FOMO_SWEEP_CONFIG still selects them).
+  const bool pairs_ok = !h16 && m.ppack != nullptr && ns >= 2;
   for (int v = 0; v < sweep_num_variants(); ++v) {
     if (sweep_variant_h16(v) != h16) continue;
+    if (sweep_variant_pair(v) ? !pairs_ok : !sweep_variant_ws(v)) continue;
     int txs[4];
     int ntx = sweep_tx_candidates(v, N, g.nx, txs, 4);
     for (int k = 0; k < ntx; ++k) {
@@ -318,12 +323,20 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
   const int nfield = P.phys == kElastic ? 5 : (P.phys == kAcoustic ? 3 : 1);
   const int nsets = P.phys == kScalar ? 3 : 2;
   const long long seis_n = (long long)P.n_rec * P.nt * P.ns;
+  // Shots allocated per field: single-sweep FP32 elastic runs may take the
+  // shot-pair sweep, whose pair-interleaved fields hold an even number of shots
+  // (an odd batch carries one all-zero shot).
+  const bool sweep = kernel == FOMO_KERNEL_SINGLE_SWEEP;
+  const bool pair_ok = sweep && !P.fp16 && P.phys == kElastic;
+  const int nsa = pair_ok ? P.ns + (P.ns & 1) : P.ns;
   Arena ar;
   size_t o_model = P.dev ? 0 : ar.take<float>(3 * nint);
   size_t o_mat = ar.take<float>(nmat * P.plane);
-  size_t o_state = ar.take<float>((long long)nsets * nfield * P.ns * P.plane);
+  size_t o_state = ar.take<float>((long long)nsets * nfield * nsa * P.plane);
   size_t o_state16 = P.fp16 ? ar.take<__half>((long long)nsets * nfield * P.ns * P.plane) : 0;
-  size_t o_unpack = (P.fp16 && opts && opts->final_state) ? ar.take<float>(P.nxp * (long long)P.nzp) : 0;
+  size_t o_unpack = ((P.fp16 || pair_ok) && opts && opts->final_state)
+                        ? ar.take<float>(P.nxp * (long long)P.nzp)
+                        : 0;
   const std::vector<float> damp = P.sponge ? sponge_table(P.nbc, P.sponge_factor) : std::vector<float>();
   if (P.sponge) hh.wtab = damp.empty() ? std::vector<float>(1, 1.0f) : damp;
   size_t o_w = ar.take<float>(hh.wtab.size());
@@ -349,8 +362,8 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
   size_t o_ent = tagged ? ar.take<int4>(std::max(n_ent, 1)) : 0;
   size_t o_elin = tagged ? ar.take<int32_t>(std::max(n_ent, 1)) : 0;
   size_t o_list = tagged ? ar.take<int32_t>(std::max<size_t>(tags.list.size(), 1)) : 0;
-  const bool sweep = kernel == FOMO_KERNEL_SINGLE_SWEEP;
   size_t o_pack = sweep ? ar.take<float>(sweep_pack_floats(P.nxp, P.nzp)) : 0;
+  size_t o_ppack = pair_ok ? ar.take<float>(pair_pack_floats(P.nxp, P.nzp)) : 0;
   if ((rc = ensure_workspace(ctx, ar.off))) return rc;
 
   const float* d_vp = vp;
@@ -403,7 +416,7 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
                                P.nz, P.pad, P.ld, dtdh, d_vp, d_vs, d_rho, d_mat, d_mat + P.plane,
                                d_mat + 2 * P.plane, d_mat + 3 * P.plane, d_mat + 4 * P.plane));
   // ---- zero state (reset!, batch.jl:30-35) ----
-  FOMO_CU(ctx, cudaMemsetAsync(d_state, 0, sizeof(float) * nsets * nfield * P.ns * P.plane, st));
+  FOMO_CU(ctx, cudaMemsetAsync(d_state, 0, sizeof(float) * nsets * nfield * nsa * P.plane, st));
   if (P.fp16) {
     FOMO_CU(ctx, cudaMemsetAsync(d_state16, 0, sizeof(__half) * nsets * nfield * P.ns * P.plane, st));
     // fold the storage scales into the materials (powers of two: exact)
@@ -447,7 +460,7 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
   for (int l = 0; l < 5; ++l) c.a[l] = kFD[P.N][l];
   HabcDev h{hh.q, hh.qt, hh.qxt, P.sponge ? P.nbc : hh.nbc, hh.wstride, d_w};
   const float dtx = dtdh, dtz = dtdh;
-  auto field = [&](int set, int f) { return d_state + ((long long)set * nfield + f) * P.ns * P.plane; };
+  auto field = [&](int set, int f) { return d_state + ((long long)set * nfield + f) * nsa * P.plane; };
   auto hfield = [&](int set, int f) {
     return HField{field(set, f), d_state16 + ((long long)set * nfield + f) * P.ns * P.plane};
   };
@@ -456,6 +469,12 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
   SweepPlan sp;
   if (sweep) {
     FOMO_CU(ctx, build_sweep_pack(st, g, emat, ws_ptr<float>(ctx, o_pack)));
+    if (pair_ok) {
+      PairPack pp;
+      FOMO_CU(ctx, build_pair_pack(st, g, emat, ws_ptr<float>(ctx, o_ppack), pp));
+      emat.ppack = ws_ptr<float>(ctx, o_ppack);
+      emat.ppack_pitch = pp.pitch;
+    }
     float* sets[2][5] = {{field(0, 2), field(0, 3), field(0, 4), field(0, 0), field(0, 1)},
                          {field(1, 2), field(1, 3), field(1, 4), field(1, 0), field(1, 1)}};
     __half* sets16[10];
@@ -473,12 +492,14 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
                     P.fp16 ? &o16 : nullptr);
     if (rc) return rc;
     // the tuning launches ran on the zero state; restore it
-    FOMO_CU(ctx, cudaMemsetAsync(d_state, 0, sizeof(float) * nsets * nfield * P.ns * P.plane, st));
+    FOMO_CU(ctx, cudaMemsetAsync(d_state, 0, sizeof(float) * nsets * nfield * nsa * P.plane, st));
     if (P.fp16)
       FOMO_CU(ctx, cudaMemsetAsync(d_state16, 0, sizeof(__half) * nsets * nfield * P.ns * P.plane,
                                    st));
   }
   FOMO_CU(ctx, cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), st));
+  // the shot-pair sweep's fields are pair-interleaved (sweep2d.cuh)
+  const bool pairs = sweep && sp.family == 5;
 
   dim3 blk(32, 8), grd(cdiv(P.nxp, 32), cdiv(P.nzp, 8), P.ns);
   int launches = 0;
@@ -812,6 +833,10 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
         k_elh_inject_record<<<P.ns, 256, 0, st>>>(it, P.nt, g, P.n_src, d_src, d_wav, hfield(B, 2),
                                                   hfield(B, 3), P.n_rec, d_rec, hfield(B, 0),
                                                   hfield(B, 1), d_seis[0], d_seis[1]);
+      else if (pairs)
+        FOMO_CU(ctx, launch_inject_record_pair(st, it, P.nt, P.ns, P.plane, P.n_src, d_src, d_wav,
+                                               field(B, 2), field(B, 3), P.n_rec, d_rec,
+                                               field(B, 0), field(B, 1), d_seis[0], d_seis[1]));
       else if (!tagged)
         k_inject_record<<<P.ns, 256, 0, st>>>(it, P.nt, P.plane, P.n_src, d_src, d_wav, field(B, 2),
                                               field(B, 3), P.n_rec, d_rec, field(B, 0), field(B, 1),
@@ -863,6 +888,10 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
       const int k = it / P.snap_interval - 1;
       k_elh_unpack<<<dim3(cdiv(P.nx, 128), P.nz), 128, 0, st>>>(
           g, hfield(B, 1), 0, P.pad, P.pad, P.nx, P.nz, kFp16Sv, d_snap + (long long)k * nint);
+    } else if (pairs && d_snap && P.snap_interval > 0 && it % P.snap_interval == 0) {
+      const int k = it / P.snap_interval - 1;  // vz of shot 0, interior
+      FOMO_CU(ctx, launch_pair_unpack(st, field(B, 1), P.plane, P.ld, P.pad, P.pad, P.nx, P.nz, 0,
+                                      d_snap + (long long)k * nint));
     } else if (d_snap && P.snap_interval > 0 && it % P.snap_interval == 0) {
       int k = it / P.snap_interval - 1;
       const float* src = (P.phys == kAcoustic ? field(B, 2) : field(B, 1)) + P.pad + (long long)P.pad * P.ld;
@@ -939,6 +968,15 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
           k_elh_unpack<<<dim3(cdiv(P.nxp, 128), P.nzp), 128, 0, st>>>(
               g, hfield(A, f), (long long)s * P.plane, 0, 0, P.nxp, P.nzp,
               f < 2 ? kFp16Sv : kFp16St, tmp);
+          FOMO_CU(ctx, cudaMemcpyAsync(opts->final_state + ((long long)s * nfield + f) * hp, tmp,
+                                       sizeof(float) * hp, cudaMemcpyDeviceToHost, st));
+          FOMO_CU(ctx, cudaStreamSynchronize(st));  // tmp is reused by the next field
+          continue;
+        }
+        if (pairs) {
+          float* tmp = ws_ptr<float>(ctx, o_unpack);
+          FOMO_CU(ctx, launch_pair_unpack(st, field(A, f), P.plane, P.ld, 0, 0, P.nxp, P.nzp, s,
+                                          tmp));
           FOMO_CU(ctx, cudaMemcpyAsync(opts->final_state + ((long long)s * nfield + f) * hp, tmp,
                                        sizeof(float) * hp, cudaMemcpyDeviceToHost, st));
           FOMO_CU(ctx, cudaStreamSynchronize(st));  // tmp is reused by the next field

@@ -40,6 +40,9 @@ struct ElMat {
   // single sweep (layout in sweep2d.cuh); null where that kernel is not used.
   const float* pack = nullptr;
   int pack_pitch = 0;  // column pairs per pack row
+  // Duplicated-value pack of the shot-pair sweep (PairPack in sweep2d.cuh).
+  const float* ppack = nullptr;
+  int ppack_pitch = 0;
 };
 
 // Source and receiver cells of a run, handled inside the step's last update

@@ -2754,7 +2754,16 @@ int pick_kernel_2d(int phys, int N, int nxp, int nzp, int ns) {
 
 bool sweep2d_supported(int phys, int N) { return phys == 1 && N >= 1 && N <= 5 && encoder(); }
 
-int sweep_num_variants() { return kNumVariants + kNumX2 + kNumRW + kNumRL + kNumWS; }
+constexpr int kWSBase = kNumVariants + kNumX2 + kNumRW + kNumRL;
+constexpr int kPairBase = kWSBase + kNumWS;  // the shot-pair variants (sweep2d_pair.cu)
+
+int sweep_num_variants() { return kPairBase + pair_num_variants(); }
+
+bool sweep_variant_ws(int variant) { return variant >= kWSBase && variant < kPairBase; }
+
+bool sweep_variant_pair(int variant) {
+  return variant >= kPairBase && variant < kPairBase + pair_num_variants();
+}
 
 int sweep_pack_pitch(int nx) { return ((nx + 2 * 128 + kPackColPad) / 2 + 16) & ~15; }
 
@@ -2778,7 +2787,7 @@ cudaError_t build_sweep_pack(cudaStream_t st, const Geo2& g, ElMat& m, float* ds
 // ping-pong sets).  variant selects (threads, rows per chunk, prefetch depth);
 // TX is the strip width (multiple of 4).
 bool sweep_variant_h16(int variant) {
-  const int v = variant - kNumVariants - kNumX2 - kNumRW - kNumRL;
+  const int v = variant - kWSBase;
   return v >= 0 && v < kNumWS && kWSH16[v];
 }
 
@@ -2788,13 +2797,23 @@ cudaError_t make_sweep_plan(SweepPlan& sp, int N, int variant, int TX, int per_s
   auto enc = encoder();
   if (!enc) return cudaErrorNotSupported;
   if (variant < 0 || variant >= sweep_num_variants() || per_sm < 1) return cudaErrorInvalidValue;
-  const bool ws = variant >= kNumVariants + kNumX2 + kNumRW + kNumRL;
+  const bool pr = sweep_variant_pair(variant);
+  const bool ws = !pr && variant >= kWSBase;
   const bool rl = !ws && variant >= kNumVariants + kNumX2 + kNumRW;
   const bool rw = !ws && !rl && variant >= kNumVariants + kNumX2;
   const bool x2 = variant >= kNumVariants;  // the 2-row TMA-box families
   int W = 0, R = 2;
   sp.h16 = false;
-  if (ws) {
+  // a shot-pair plan walks (pair, strip) items; gm.ns holds the pair count
+  const int items_ns = pr ? (ns + 1) / 2 : ns;
+  if (pr) {
+    const int v = variant - kPairBase;
+    if (sets16 || TX < 8 || TX > pair_txmax(N, v) || (TX & 1)) 
+      return cudaErrorInvalidValue;
+    W = pair_box_width(N, v);
+    sp.family = 5;
+    sp.P = 1;
+  } else if (ws) {
     const int v = variant - kNumVariants - kNumX2 - kNumRW - kNumRL;
     if (kWSH16[v]) {
       // binary16 rows: every TMA x coordinate (strip * TX - 8 - 8, strip * TX - 8)
@@ -2843,8 +2862,9 @@ cudaError_t make_sweep_plan(SweepPlan& sp, int N, int variant, int TX, int per_s
   sp.gm.TX = TX;
   sp.gm.W = W;
   sp.gm.nstrip = (g.nx + TX - 1) / TX;
-  sp.gm.ns = ns;
-  sp.smem = ws   ? ws_smem_for(N, variant - kNumVariants - kNumX2 - kNumRW - kNumRL, g.nbc + 3)
+  sp.gm.ns = items_ns;
+  sp.smem = pr   ? pair_smem(N, variant - kPairBase, g.nbc + 3)
+             : ws   ? ws_smem_for(N, variant - kNumVariants - kNumX2 - kNumRW - kNumRL, g.nbc + 3)
              : rl ? rl_smem_for(N, variant - kNumVariants - kNumX2 - kNumRW, g.nbc + 3)
              : rw ? rw_smem_for(N, variant - kNumVariants - kNumX2, g.nbc + 3)
              : x2 ? x2_smem_for(N, variant - kNumVariants, g.nbc + 3)
@@ -2855,7 +2875,7 @@ cudaError_t make_sweep_plan(SweepPlan& sp, int N, int variant, int TX, int per_s
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   sp.per_sm = std::min(per_sm, bps);
-  const long long rows = (long long)sp.gm.nstrip * ns * g.nz;
+  const long long rows = (long long)sp.gm.nstrip * items_ns * g.nz;
   sp.grid = (int)std::max(1LL, std::min({(long long)sp.per_sm * nsm, rows, (long long)kMaxGrid}));
   sp.frame_weight = frame_weight;
   // Cost-balanced split of the flattened (strip, shot, row) space.  A row costs
@@ -2942,6 +2962,22 @@ cudaError_t make_sweep_plan(SweepPlan& sp, int N, int variant, int TX, int per_s
     if (e != cudaSuccess) return e;
     sp.d_bounds = d_bounds;
   }
+  if (pr) {
+    // pair-interleaved fields: one 8-byte element {shot 2p, shot 2p+1} per cell
+    for (int s = 0; s < 2; ++s)
+      for (int f = 0; f < 5; ++f) {
+        cuuint64_t dims[3] = {(cuuint64_t)g.nx, (cuuint64_t)g.nz, (cuuint64_t)items_ns};
+        cuuint64_t strides[2] = {(cuuint64_t)g.ld * 8, (cuuint64_t)g.plane * 8};
+        cuuint32_t box[3] = {(cuuint32_t)W, 2, 1};
+        cuuint32_t es[3] = {1, 1, 1};
+        CUresult r = enc(&sp.tm[s][f], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, sets[s][f], dims,
+                         strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+      }
+    return cudaSuccess;
+  }
   for (int s = 0; s < 2; ++s)
     for (int f = 0; f < (x2 ? 5 : 3); ++f) {
       cuuint64_t dims[3] = {(cuuint64_t)g.nx, (cuuint64_t)g.nz, (cuuint64_t)ns};
@@ -2965,6 +3001,15 @@ cudaError_t make_sweep_plan(SweepPlan& sp, int N, int variant, int TX, int per_s
 
 int sweep_tx_candidates(int variant, int N, int nx, int* out, int max_out) {
   int n = 0;
+  if (sweep_variant_pair(variant)) {
+    // the widest strip, and the narrowest (even) strip with the same strip count
+    const int tmax = pair_txmax(N, variant - kPairBase);
+    if (tmax >= 8 && n < max_out) out[n++] = tmax;
+    const int ns = (nx + tmax - 1) / tmax;
+    const int tbal = (((nx + ns - 1) / ns) + 1) & ~1;
+    if (tbal >= 8 && tbal < tmax && n < max_out) out[n++] = tbal;
+    return n;
+  }
   if (variant >= kNumVariants) {
     // the widest strip, and the narrowest strip with the same strip count
     const int v = variant - kNumVariants - kNumX2 - kNumRW;
@@ -3057,6 +3102,7 @@ int occ_ws(const SweepPlan& sp) {
 }
 
 int sweep_blocks_per_sm(const SweepPlan& sp) {
+  if (sp.family == 5) return pair_blocks_per_sm(sp.N, sp.variant - kPairBase, sp.smem);
   if (sp.family == 4) {
 #define FOMO_OCC_WS(V, NN, NV, PP, MB, SP, HH) \
   case V: return occ_ws<NN, NV, PP, MB, SP, HH>(sp);
@@ -3123,6 +3169,21 @@ cudaError_t launch_sweep_elastic(cudaStream_t st, const SweepPlan& sp, int set, 
                                  float dtx, float dtz, const HabcDev& h, const ElFields& a,
                                  const ElMat& m, const ElOut& o, int* err, const ElOut16* o16) {
   if (sp.h16 != (o16 != nullptr)) return cudaErrorInvalidValue;
+  if (sp.family == 5) {
+    const PairPack mp{reinterpret_cast<const float4*>(m.ppack),
+                      reinterpret_cast<const float4*>(m.ppack) +
+                          (long long)(sp.gm.nz + 2 * kPairRowPad) * m.ppack_pitch,
+                      reinterpret_cast<const float2*>(m.ppack +
+                                                      8LL * (sp.gm.nz + 2 * kPairRowPad) *
+                                                          m.ppack_pitch),
+                      m.ppack_pitch};
+    const PairOut po{reinterpret_cast<float2*>(o.vx), reinterpret_cast<float2*>(o.vz),
+                     reinterpret_cast<float2*>(o.txx), reinterpret_cast<float2*>(o.tzz),
+                     reinterpret_cast<float2*>(o.txz)};
+    if (!m.ppack) return cudaErrorInvalidValue;
+    return launch_pair_elastic(st, sp, sp.variant - kPairBase, set,
+                               make_pair_coef(c, dtx, dtz, h), h, mp, po, err);
+  }
   if (sp.family == 4) {
     switch (sp.N) {
       case 1: return launch_ws_n<1>(st, sp, set, c, dtx, dtz, h, m, o, o16, err);

@@ -59,7 +59,8 @@ struct ElOut16 {
 struct SweepPlan {
   int N = 0, variant = 0;
   int family = 0;            // 0: column-per-thread, 1: pair-blocked, 2: register-window,
-                             // 3: lean register-window, 4: warp-specialized
+                             // 3: lean register-window, 4: warp-specialized,
+                             // 5: shot pairs (packed FP32, pair-interleaved fields)
   int P = 0;                 // pair-blocked: prefetch depth (row pairs)
   int per_sm = 1, grid = 1;  // persistent CTAs per SM, grid size
   float frame_weight = 1.0f; // extra cost of a frame cell in the row-range split
@@ -70,6 +71,63 @@ struct SweepPlan {
   bool h16 = false;      // binary16 storage form (tm16 maps the binary16 arrays)
   CUtensorMap tm16[2][5];
 };
+
+// ---- shot-pair sweep (sweep2d_pair.cu) -------------------------------------
+// Fields of a shot-pair run are pair-interleaved: element (x, z) of pair p is
+// the float2 {shot 2p, shot 2p+1} at (p * plane + z * ld + x) float2 units;
+// an odd batch carries one all-zero shot.  The materials come from a pack of
+// duplicated values (both lanes of a float2 equal), kPairRowPad zero rows
+// above and below the grid and kPairColPad zero columns left of it:
+//   v : float4 {bx, bx, bz, bz}   l : float4 {lam, lam, l2m, l2m}   mu: float2 {mut, mut}
+// element (z, x) of each region at (z + kPairRowPad) * pitch + x + kPairColPad.
+constexpr int kPairRowPad = 32;
+constexpr int kPairColPad = 16;
+struct PairPack {
+  const float4* v;
+  const float4* l;
+  const float2* mu;
+  int pitch;  // cells per pack row
+};
+struct PairOut {
+  float2* vx;
+  float2* vz;
+  float2* txx;
+  float2* tzz;
+  float2* txz;
+};
+// Stencil and Higdon constants, duplicated into both lanes.
+struct PairCoef {
+  float2 a[5];
+  float2 dtx, dtz;
+  float2 nq, nqt, nqxt;  // -q, -qt, -qxt
+};
+int pair_num_variants();
+int pair_threads(int v);
+int pair_txmax(int N, int v);       // widest strip of a variant (even)
+int pair_box_width(int N, int v);   // TMA box width in float2 elements
+size_t pair_smem(int N, int v, int wstride);
+int pair_blocks_per_sm(int N, int v, size_t smem);
+int pair_pack_pitch(int nx);
+size_t pair_pack_floats(int nx, int nz);
+cudaError_t build_pair_pack(cudaStream_t st, const Geo2& g, const ElMat& m, float* dst,
+                            PairPack& out);
+PairCoef make_pair_coef(const Coef& c, float dtx, float dtz, const HabcDev& h);
+cudaError_t launch_pair_elastic(cudaStream_t st, const SweepPlan& sp, int v, int set,
+                                const PairCoef& k, const HabcDev& h, const PairPack& mp,
+                                const PairOut& o, int* err);
+// Injection then recording of one step on pair-layout txx/tzz and vx/vz
+// (k_inject_record's order and semantics), one block per shot.
+cudaError_t launch_inject_record_pair(cudaStream_t st, int it, int nt, int ns, long long plane,
+                                      int n_src, const int* src_lin, const float* wav, float* txx,
+                                      float* tzz, int n_rec, const int* rec_lin, const float* vx,
+                                      const float* vz, float* s0, float* s1);
+// Columns [x0, x0 + nx) of rows [z0, z0 + nz) of shot `shot` of a pair-layout
+// field into out (unpitched).
+cudaError_t launch_pair_unpack(cudaStream_t st, const float* f, long long plane, int ld, int x0,
+                               int z0, int nx, int nz, int shot, float* out);
+// Is a sweep variant (the plan numbering) a shot-pair / warp-specialized variant?
+bool sweep_variant_pair(int variant);
+bool sweep_variant_ws(int variant);
 
 // Kernel family for a problem (FOMO_KERNEL_TWO_PHASE / _SINGLE_SWEEP).
 int pick_kernel_2d(int phys, int N, int nxp, int nzp, int ns);

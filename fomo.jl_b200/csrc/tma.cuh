@@ -1,0 +1,63 @@
+// tma.cuh -- shared-memory mbarrier and TMA (cp.async.bulk.tensor) primitives
+// for sm_100a kernels, and the bounded mbarrier wait every kernel here uses.
+#pragma once
+#include <cuda.h>
+#include <stdint.h>
+
+namespace fomo {
+namespace tma {
+
+__device__ __forceinline__ uint32_t saddr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(saddr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: gives up after 2^22 polls (about a second) and records the
+// failure in *err; the caller stops waiting on later phases as well.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err) {
+  for (int spin = 0; spin < (1 << 22); ++spin)
+    if (mbar_try_wait(bar, parity)) return true;
+  atomicOr(err, 1);
+  return false;
+}
+// Orders this thread's earlier generic-proxy shared-memory accesses before
+// the async-proxy (TMA) writes it issues next.
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// One tiled 3D box of the tensor map into shared memory (no multicast),
+// completing on `bar` by byte count.
+__device__ __forceinline__ void load_3d(void* dst, const CUtensorMap* map, int x, int y, int z,
+                                        uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(saddr(dst)),
+      "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(saddr(bar))
+      : "memory");
+}
+// Named barrier over `nthreads` threads of the CTA.
+__device__ __forceinline__ void bar_sync(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+}  // namespace tma
+}  // namespace fomo

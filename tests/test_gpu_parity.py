@@ -20,7 +20,9 @@ SWEEP_CONFIGS = ["0,112,3", "1,144,1", "2,80,2", "2,20,4", "3,112,2", "0,64,1",
                  "7,224,2", "8,196,2", "8,40,2", "7,8,1",
                  "9,224,2", "10,176,2", "11,112,4", "12,100,4", "11,8,1", "9,40,1",
                  "12,60,3", "13,224,2", "14,112,4", "15,100,3", "16,112,3", "14,8,1",
-                 "13,40,1", "16,20,2"]  # variant,TX,CTAs per SM
+                 "13,40,1", "16,20,2",
+                 "19,112,2", "19,100,1", "20,80,2", "21,40,4", "19,8,1", "21,20,2",
+                 "20,10,3"]  # variant,TX,CTAs per SM (19-21: shot-pair sweeps)
 
 
 @pytest.fixture
@@ -143,6 +145,34 @@ def test_elastic_single_sweep_configs_bitwise(fomo, oracle, sweep_config, cfg, f
     o = oracle.elastic2d(vp, vs, rho, 5.0, 5e-4, nt, sx=sx.T, sz=sz.T, rx=rx, rz=rz,
                          wavelet=w.reshape(1, -1), nbc=nbc, fd_order=fd_order, n_shots=2,
                          final=True)
+    assert np.array_equal(r.seis_vx, o["seis_vx"])
+    assert np.array_equal(r.seis_vz, o["seis_vz"])
+    assert np.array_equal(fin, o["final"])
+
+
+@pytest.mark.parametrize("cfg", ["19,112,2", "21,40,2"])
+def test_shot_pair_sweep_odd_batch_bitwise(fomo, oracle, sweep_config, cfg):
+    """The shot-pair sweep on an odd batch (the last pair carries an all-zero
+    shot) with coincident sources and a receiver on a source cell equals the
+    oracle bit for bit, final wavefields included."""
+    from fomo_b200.synthetic import layered_elastic
+
+    sweep_config(cfg)
+    vp, vs, rho = layered_elastic(97, 64, n_layers=5, seed=21)
+    vp, vs, rho = _vacuum_top(vp, vs, rho)
+    nt, nbc, fd_order = 150, 10, 8
+    rx = np.array([1, 30, 48, 48, 97])
+    rz = np.array([1, 7, 7, 64, 64])
+    sx = np.array([[48, 48], [10, 11], [90, 30]])  # (n_shots, n_src)
+    sz = np.array([[7, 7], [3, 60], [5, 5]])
+    M = fd_order // 2
+    fin = np.zeros((97 + 2 * (nbc + M), 64 + 2 * (nbc + M), 5, 3), np.float32, order="F")
+    r = fomo.elastic2d_batch(vp, vs, rho, 5.0, 5e-4, nt, 20.0, sx=sx, sz=sz, rx=rx, rz=rz,
+                             nbc=nbc, fd_order=fd_order, kernel=2, final_state=fin)
+    w = fomo.ricker_wavelet(20.0, 5e-4, nt)
+    o = oracle.elastic2d(vp, vs, rho, 5.0, 5e-4, nt, sx=sx.T, sz=sz.T, rx=rx, rz=rz,
+                         wavelet=np.repeat(w.reshape(1, -1), 2, axis=0), nbc=nbc,
+                         fd_order=fd_order, n_shots=3, final=True)
     assert np.array_equal(r.seis_vx, o["seis_vx"])
     assert np.array_equal(r.seis_vz, o["seis_vz"])
     assert np.array_equal(fin, o["final"])
