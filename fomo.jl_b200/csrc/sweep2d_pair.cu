@@ -69,6 +69,14 @@ __device__ __forceinline__ float2 ph_corner(const float4& wt, float2 fc, float2 
   return p_fma(lo2(wt), fc, p_mul(p_mul(hi2(wt), make_float2(0.5f, 0.5f)), p_add(sx, sz)));
 }
 
+// The value as the result of an (empty) asm statement: the compiler keeps a
+// duplicated constant pair in registers instead of rebuilding it from the
+// constant bank before every packed instruction that reads it.
+__device__ __forceinline__ float2 pinned(float2 v) {
+  asm volatile("" : "+f"(v.x), "+f"(v.y));
+  return v;
+}
+
 // (a + d) mod n for a in [0, n), 0 <= d < n
 __device__ __forceinline__ int ring(int a, int d, int n) {
   const int t = a + d;
@@ -104,10 +112,18 @@ template <int N, int NV, int P, int MINB>
 __global__ void __launch_bounds__(2 * NV, MINB)
     k_el_pair(const __grid_constant__ CUtensorMap tm_xx, const __grid_constant__ CUtensorMap tm_zz,
               const __grid_constant__ CUtensorMap tm_xz, const __grid_constant__ CUtensorMap tm_vx,
-              const __grid_constant__ CUtensorMap tm_vz, SweepGeom gm, PairCoef k, HabcDev h,
+              const __grid_constant__ CUtensorMap tm_vz, SweepGeom gm, PairCoef kp, HabcDev h,
               PairPack mp, PairOut o, const long long* __restrict__ bounds,
               int* __restrict__ err) {
   using S = PairShape<N, NV, P>;
+  PairCoef k;
+#pragma unroll
+  for (int l = 0; l < 5; ++l) k.a[l] = pinned(kp.a[l]);
+  k.dtx = pinned(kp.dtx);
+  k.dtz = pinned(kp.dtz);
+  k.nq = pinned(kp.nq);
+  k.nqt = pinned(kp.nqt);
+  k.nqxt = pinned(kp.nqxt);
   constexpr int NT = 2 * NV;
   constexpr int W = S::W, M = N, TN = S::TN, HV = S::HV;
   constexpr int NZ = S::NZ, NO = S::NO, LVV = S::LVV;
@@ -504,22 +520,32 @@ __global__ void __launch_bounds__(2 * NV, MINB)
 
 namespace {
 
-// (threads per role, prefetch depth, CTAs per SM the register budget targets)
-#define FOMO_PAIR_VARIANTS(X, NN) X(0, NN, 128, 1, 2) X(1, NN, 96, 1, 2) X(2, NN, 64, 1, 4)
-constexpr int kPairNV[] = {128, 96, 64};
+// Pair variants: (form 0; threads per role; TMA prefetch depth in row pairs;
+// CTAs per SM the register budget targets).  Deeper prefetch keeps more HBM
+// reads in flight per SM; narrower CTAs keep two or three of them resident.
+#define FOMO_PAIR_VARIANTS(X, NN)                                                         \
+  X(0, NN, 0, 128, 1, 2) X(1, NN, 0, 96, 2, 2) X(2, NN, 0, 96, 3, 2) X(3, NN, 0, 64, 3, 3) \
+  X(4, NN, 0, 128, 3, 1)
+constexpr int kPairNV[] = {128, 96, 96, 64, 128};
 constexpr int kNumPair = sizeof(kPairNV) / sizeof(kPairNV[0]);
 constexpr int kMaxDynSmemPair = 227 * 1024;
 
-template <int N, int NV, int P>
+template <int N, int F, int NV, int P>
 size_t pair_smem_bytes(int wstride) {
+  static_assert(F == 0, "one kernel form");
   using S = PairShape<N, NV, P>;
   return (size_t)S::O_WT * 8 + (size_t)3 * wstride * 16 + sizeof(uint64_t) * S::NO;
 }
 
-template <int N, int NV, int P, int MINB>
+template <int N, int F, int NV, int P, int MINB>
+auto pair_kernel() {
+  return k_el_pair<N, NV, P, MINB>;
+}
+
+template <int N, int F, int NV, int P, int MINB>
 cudaError_t launch_p(cudaStream_t st, const SweepPlan& sp, int set, const PairCoef& k,
                      const HabcDev& h, const PairPack& mp, const PairOut& o, int* err) {
-  auto kern = k_el_pair<N, NV, P, MINB>;
+  auto kern = pair_kernel<N, F, NV, P, MINB>();
   static std::atomic<int> attr_set{0};
   if (!attr_set.load(std::memory_order_acquire)) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -534,10 +560,10 @@ cudaError_t launch_p(cudaStream_t st, const SweepPlan& sp, int set, const PairCo
   return cudaGetLastError();
 }
 
-template <int N, int NV, int P, int MINB>
+template <int N, int F, int NV, int P, int MINB>
 int occ_p(size_t smem) {
   int nb = 0;
-  auto kern = k_el_pair<N, NV, P, MINB>;
+  auto kern = pair_kernel<N, F, NV, P, MINB>();
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemPair);
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, 2 * NV, smem) != cudaSuccess) {
     cudaGetLastError();
@@ -624,8 +650,8 @@ int pair_box_width(int N, int v) {
 }
 
 size_t pair_smem(int N, int v, int wstride) {
-#define FOMO_SMEM_P(V, NN, NV, PP, MB) \
-  case V: return pair_smem_bytes<NN, NV, PP>(wstride);
+#define FOMO_SMEM_P(V, NN, FF, NV, PP, MB) \
+  case V: return pair_smem_bytes<NN, FF, NV, PP>(wstride);
 #define FOMO_SMEM_PN(NN)                             \
   case NN:                                           \
     switch (v) { FOMO_PAIR_VARIANTS(FOMO_SMEM_P, NN) } \
@@ -637,8 +663,8 @@ size_t pair_smem(int N, int v, int wstride) {
 }
 
 int pair_blocks_per_sm(int N, int v, size_t smem) {
-#define FOMO_OCC_P(V, NN, NV, PP, MB) \
-  case V: return occ_p<NN, NV, PP, MB>(smem);
+#define FOMO_OCC_P(V, NN, FF, NV, PP, MB) \
+  case V: return occ_p<NN, FF, NV, PP, MB>(smem);
 #define FOMO_OCC_PN(NN)                             \
   case NN:                                          \
     switch (v) { FOMO_PAIR_VARIANTS(FOMO_OCC_P, NN) } \
@@ -683,8 +709,8 @@ cudaError_t launch_pair_elastic(cudaStream_t st, const SweepPlan& sp, int v, int
                                 const PairCoef& k, const HabcDev& h, const PairPack& mp,
                                 const PairOut& o, int* err) {
   if (!mp.v || mp.pitch < 1 || h.wstride <= sp.gm.nbc) return cudaErrorInvalidValue;
-#define FOMO_LAUNCH_P(V, NN, NV, PP, MB) \
-  case V: return launch_p<NN, NV, PP, MB>(st, sp, set, k, h, mp, o, err);
+#define FOMO_LAUNCH_P(V, NN, FF, NV, PP, MB) \
+  case V: return launch_p<NN, FF, NV, PP, MB>(st, sp, set, k, h, mp, o, err);
 #define FOMO_LAUNCH_PN(NN)                              \
   case NN:                                              \
     switch (v) { FOMO_PAIR_VARIANTS(FOMO_LAUNCH_P, NN) } \

@@ -22,7 +22,8 @@ SWEEP_CONFIGS = ["0,112,3", "1,144,1", "2,80,2", "2,20,4", "3,112,2", "0,64,1",
                  "12,60,3", "13,224,2", "14,112,4", "15,100,3", "16,112,3", "14,8,1",
                  "13,40,1", "16,20,2",
                  "19,112,2", "19,100,1", "20,80,2", "21,40,4", "19,8,1", "21,20,2",
-                 "20,10,3"]  # variant,TX,CTAs per SM (19-21: shot-pair sweeps)
+                 "20,10,3", "22,48,3", "22,8,2", "23,112,1",
+                 "23,60,1"]  # variant,TX,CTAs per SM (19-23: shot-pair sweeps)
 
 
 @pytest.fixture
@@ -150,7 +151,7 @@ def test_elastic_single_sweep_configs_bitwise(fomo, oracle, sweep_config, cfg, f
     assert np.array_equal(fin, o["final"])
 
 
-@pytest.mark.parametrize("cfg", ["19,112,2", "21,40,2"])
+@pytest.mark.parametrize("cfg", ["19,112,2", "21,40,2", "22,48,3", "20,8,1"])
 def test_shot_pair_sweep_odd_batch_bitwise(fomo, oracle, sweep_config, cfg):
     """The shot-pair sweep on an odd batch (the last pair carries an all-zero
     shot) with coincident sources and a receiver on a source cell equals the
