@@ -171,6 +171,37 @@ def cpu_baseline(cfg, target_s=12.0, threads=None):
     return nt_s, cores, run
 
 
+def l2_vs_fp64(cfg, seis_vx, seis_vz, shot, nt_s, threads=None):
+    """Error statement of the timed run: its seismograms of one shot (numpy
+    (n_rec, nt) arrays) over the first nt_s steps against the FP64 oracle of
+    the same scheme, plus whether they equal the FP32 oracle bit for bit.
+    Sample k of a seismogram depends only on steps 1..k, so the first nt_s
+    samples of the full run are those of an nt_s-step run."""
+    from oracle import oracle as O
+
+    O.build()
+    if threads:
+        O.set_threads(threads)
+    w = np.asarray(__import__("fomo_b200").ricker_wavelet(cfg["f0"], cfg["dt"], nt_s))
+    kw = dict(sx=[[int(cfg["sx"][shot])]], sz=[[int(cfg["sz"][shot])]], rx=cfg["rx"], rz=cfg["rz"],
+              wavelet=w.reshape(1, -1), nbc=cfg["nbc"], fd_order=cfg["fd_order"])
+    t0 = time.perf_counter()
+    o64 = O.elastic2d(cfg["vp"], cfg["vs"], cfg["rho"], cfg["dh"], cfg["dt"], nt_s, prec=64, **kw)
+    o32 = O.elastic2d(cfg["vp"], cfg["vs"], cfg["rho"], cfg["dh"], cfg["dt"], nt_s, **kw)
+    t = time.perf_counter() - t0
+
+    def rel(a, b):
+        a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+        return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+    gx, gz = seis_vx[:, :nt_s], seis_vz[:, :nt_s]
+    return {"vx": rel(gx, o64["seis_vx"][:, :, 0]), "vz": rel(gz, o64["seis_vz"][:, :, 0]),
+            "bitwise_vs_fp32_oracle": bool(np.array_equal(gx, o32["seis_vx"][:, :, 0]) and
+                                           np.array_equal(gz, o32["seis_vz"][:, :, 0])),
+            "shot": int(shot), "nt_sampled": int(nt_s), "tolerance": 1e-5,
+            "oracle": f"C++ restatement of the scheme in FP64 and FP32 ({t:.1f} s on the host)"}
+
+
 def reference_arm(args, cfg):
     world, rank, _ = _dist()
     if rank != 0:
@@ -341,6 +372,11 @@ def ours(args, cfg):
         "finite": finite,
     }
     if rank == 0 and world == 1 and not os.environ.get("FOMO_BENCH_NO_CPU"):
+        # the middle shot of the timed run over its first 800 steps vs the FP64 oracle
+        mid = ns // 2
+        sv = d_svx[mid].T.contiguous().cpu().numpy()  # (n_rec, nt)
+        szv = d_svz[mid].T.contiguous().cpu().numpy()
+        line["l2_vs_fp64"] = l2_vs_fp64(cfg, sv, szv, mid, min(nt, 800))
         nt_s, cores, run = cpu_baseline(cfg)
         t = run(nt_s)
         cv = ns / (t * nt / nt_s)

@@ -19,12 +19,17 @@
 //    (other streams, other host threads) race and corrupt each other.
 //  * The array keeps the previous call's contents; each call clears the
 //    wavefields and the error word before it starts.
-//  * The first call on a device looks up the array's device address
-//    (cudaGetSymbolAddress) with that device current.  Make that first call
-//    before any stream capture begins.
+//  * Every call looks up the array's device address (cudaGetSymbolAddress,
+//    which allocates nothing) on the current device and context, so a device
+//    reset or a different current context never leaves it a stale address.
+//  * The call is synchronous: it returns once the run has finished on its
+//    stream and the results are in the caller's buffers.
+//  * Like the other C entry points it makes none of the reference's argument
+//    checks on the time step (the centered CFL bound of utils/checks.jl:61-70)
+//    or on dispersion: an unstable dt runs and its result grows without bound.
+//    The caller (or a binding such as the Python mirror) makes those checks.
 #include <algorithm>
 #include <cstdio>
-#include <mutex>
 
 #include "solver2d_kernels.cuh"
 
@@ -37,33 +42,23 @@ constexpr size_t kNoallocBytes = size_t(32) << 20;
 // code this name is only a handle for cudaGetSymbolAddress, never an address.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-unsigned char* g_scratch_dev[kMaxDevices];  // device address of the array, per device
-
 void set_err(char* err, int len, const char* msg) {
   if (err && len > 0) std::snprintf(err, (size_t)len, "%s", msg);
 }
 
-// Once per device, with that device current.
-int scratch_address(int dev, unsigned char** out, char* err, int len) {
-  if (dev < 0 || dev >= kMaxDevices) {
-    set_err(err, len, "device ordinal beyond the no-alloc table");
-    return FOMO_EUNSUPPORTED;
+// The array's device address in the current device's current context.  Looked
+// up on every call (no cache), so it always belongs to the context the call
+// launches in.
+int scratch_address(unsigned char** out, char* err, int len) {
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p) {
+    char b[256];
+    std::snprintf(b, sizeof b, "cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+    set_err(err, len, b);
+    return FOMO_ECUDA;
   }
-  std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_scratch_dev[dev]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) {
-      char b[256];
-      std::snprintf(b, sizeof b, "cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
-      set_err(err, len, b);
-      return FOMO_ECUDA;
-    }
-    g_scratch_dev[dev] = static_cast<unsigned char*>(p);
-  }
-  *out = g_scratch_dev[dev];
+  *out = static_cast<unsigned char*>(p);
   return FOMO_OK;
 }
 
@@ -71,7 +66,7 @@ inline size_t up256(size_t b) { return (b + 255) & ~size_t(255); }
 
 // Padded linear source/receiver indices with the range check of
 // utils/checks.jl:8-13 (a bad index sets *flag and is never used), and the
-// HABC weight table of boundary/habc/habc.jl:158-162 by distance-to-edge.
+// HABC weight table of boundary/habc/habc.jl:17-44 by distance-to-edge.
 __global__ void k_noalloc_prep(int nx, int nz, int pad, int nxp, int n_src,
                                const int32_t* __restrict__ sx, const int32_t* __restrict__ sz,
                                int n_rec, const int32_t* __restrict__ rx,
@@ -173,7 +168,7 @@ extern "C" int fomo_scalar2d_noalloc(const fomo_grid2d* g, const float* vp, cons
     return FOMO_ECUDA;
   }
   unsigned char* base = nullptr;
-  int rc = scratch_address(dev, &base, err, err_len);
+  int rc = scratch_address(&base, err, err_len);
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
   float* u = reinterpret_cast<float*>(base + o_u);
@@ -183,7 +178,7 @@ extern "C" int fomo_scalar2d_noalloc(const fomo_grid2d* g, const float* vp, cons
   int32_t* rec_lin = reinterpret_cast<int32_t*>(base + o_rec);
   int* flag = reinterpret_cast<int*>(base + o_flag);
 
-  // HABC coefficients (habc.jl:148-156), float32 as the reference computes them
+  // HABC coefficients (boundary/habc/habc.jl:17-44), float32 as the reference computes them
   const float r = (g->v_ref * g->dt) / g->dh;
   const float b = 0.45f, beta = 1.0f, br = beta + r, den = br * (1.0f - b);
   HabcDev h{(b * br - r) / den, (b * br - beta) / den, b / (b - 1.0f), pad - 1, wstride, wtab};

@@ -13,7 +13,7 @@ namespace fomo {
 
 // ---------------------------------------------------------------------------
 // elastic2d velocity / stress updates (elastic2d/fused_kernels.jl:21-124,
-// batch.jl:278-378).  Materials are shared by all shots; fields carry the
+// batch.jl:38-154).  Materials are shared by all shots; fields carry the
 // shot offset already.
 // ---------------------------------------------------------------------------
 struct ElFields {
@@ -89,7 +89,7 @@ __device__ __forceinline__ void tag_record(const CellTags& t, const int4& E, lon
   }
 }
 
-// Cerjan sponge (boundary/sponge.jl:31-83), fused into the sweep that produces
+// Cerjan sponge (boundary/sponge.jl:30-78), fused into the sweep that produces
 // the field: the updated value times damp[d], d = the cell's distance in cells
 // to the nearest edge of the padded grid, for d < nbc.  In sponge mode HabcDev
 // carries the user's nbc and the damping table (wtab[d], d < nbc).

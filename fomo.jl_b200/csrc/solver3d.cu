@@ -3,7 +3,7 @@
 // One step = velocity update (all cells, A -> B) + two-pass HABC on the
 // velocity frame + stress/pressure update (A,B -> B) + two-pass HABC on the
 // stress frame + inject/record.  The reference's 3D Higdon kernel
-// (boundary/habc/kernels_3d.jl:172-244) updates in place and races between
+// (boundary/habc/kernels_3d.jl:117-193) updates in place and races between
 // neighbouring frame cells; here pass 1 evaluates every frame cell from the
 // read-only pre-correction field into a frame-indexed scratch and pass 2
 // writes it back, so results are deterministic (the same two-pass form as the
@@ -568,7 +568,7 @@ struct FieldOut3 {
 };
 
 // Pass 1: the Higdon value of every frame cell of NF fields into scratch --
-// kernels_3d.jl:186-240 evaluated from read-only inputs: the mean of the
+// kernels_3d.jl:151-193 evaluated from read-only inputs: the mean of the
 // active directions' side terms, blended with the weight ramp.  The cell's
 // sides, distance and neighbour offsets are shared by its fields.
 template <int NF>

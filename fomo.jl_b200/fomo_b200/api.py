@@ -69,12 +69,24 @@ def get_centered_d2(order: int):
 
 
 def ricker_wavelet(f0, dt, nt) -> np.ndarray:
-    """Ricker wavelet (utils/ricker_wavelet.jl:6-12), evaluated in float64, returned as float32."""
-    f0 = float(np.float32(f0))
-    t = np.arange(int(nt), dtype=np.float64) * float(np.float32(dt))
-    tau = t - 1.5 / f0
-    a = (np.pi * f0 * tau) ** 2
-    return ((1.0 - 2.0 * a) * np.exp(-a)).astype(np.float32)
+    """Ricker wavelet (utils/ricker_wavelet.jl:6-12) in the reference's Float32 arithmetic.
+
+    With f0 and dt Float32, as the public functions pass them, the reference
+    evaluates: t = (0:nt-1) .* dt (a Float32 range: each element is the exact
+    product rounded once), t0 = 1f0/f0, tau = t - 1.5f0*t0, x = Float32(pi)*f0*tau
+    and (1 - 2x^2) * exp(-x^2), every operation rounded to Float32.  The
+    exponential is the platform's single-precision exp (numpy's), which may
+    differ from Julia's Float32 exp by an ulp on some samples.
+    """
+    f0 = np.float32(f0)
+    dt = np.float32(dt)
+    t = (np.arange(int(nt), dtype=np.float64) * np.float64(dt)).astype(np.float32)
+    t0 = np.float32(1.0) / f0
+    tau = t - np.float32(1.5) * t0
+    x = (np.float32(np.pi) * f0) * tau
+    a = x * x
+    with np.errstate(under="ignore"):
+        return ((np.float32(1.0) - np.float32(2.0) * a) * np.exp(-a)).astype(np.float32)
 
 
 class Stats(NamedTuple):
@@ -592,7 +604,7 @@ def acoustic3d(vp, rho, dh, dt, nt, f0, *, sx, sy, sz, rx, ry, rz, nbc: int = 50
                fd_order: int = 8, snap_interval: int = 0, snap_plane="xz", snap_index: int = 0,
                v_ref=None, wavelet=None, device: int = 0,
                final_state: Optional[np.ndarray] = None):
-    """3D acoustic simulation (equations/acoustic3d/acoustic3d.jl:37-188).
+    """3D acoustic simulation (equations/acoustic3d/acoustic3d.jl:37-185).
 
     Returns ``(seis_vx, seis_vy, seis_vz, snaps)``; snapshots hold p on the
     chosen plane.  The HABC is the reference's 3D Higdon formula evaluated in
@@ -606,7 +618,7 @@ def elastic3d(vp, vs, rho, dh, dt, nt, f0, *, sx, sy, sz, rx, ry, rz, nbc: int =
               fd_order: int = 8, snap_interval: int = 0, snap_plane="xz", snap_index: int = 0,
               v_ref=None, wavelet=None, device: int = 0,
               final_state: Optional[np.ndarray] = None, kernel: int = 0):
-    """3D elastic simulation (equations/elastic3d/elastic3d.jl:37-165).
+    """3D elastic simulation (equations/elastic3d/elastic3d.jl:37-162).
 
     Returns ``(seis_vx, seis_vy, seis_vz, snaps)``; sources inject into txx,
     tyy and tzz; snapshots hold vz.  ``kernel``: 0 or 3 = z-marching updates,

@@ -219,8 +219,8 @@ typedef struct fomo_acq3d {
   const int32_t* rz;
 } fomo_acq3d;
 
-/* acoustic3d (equations/acoustic3d/acoustic3d.jl:37-188) and elastic3d
- * (equations/elastic3d/elastic3d.jl:37-165).  Seismograms (n_rec, nt) of vx,
+/* acoustic3d (equations/acoustic3d/acoustic3d.jl:37-185) and elastic3d
+ * (equations/elastic3d/elastic3d.jl:37-162).  Seismograms (n_rec, nt) of vx,
  * vy, vz.  Snapshots every snap_interval steps of p (acoustic) or vz (elastic)
  * on the plane snap_plane (0 :xz at y = snap_index, 1 :xy at z, 2 :yz at x;
  * snap_index 1-based, 0 selects ny/2 as the reference does), laid out
@@ -313,9 +313,12 @@ FOMO_API int fomo_scalar2d_corrected(fomo_ctx* ctx, const fomo_grid2d* g, const 
  * and returns after the stream has finished the run.  Problems whose working
  * set exceeds the array return FOMO_EARG.  All calls share the array (it keeps
  * the previous call's contents; the wavefields are cleared at each start), so
- * calls that overlap on the GPU race.  The first call on a device looks up the
- * array's address and should come before any stream capture.  `err` (may be
- * NULL) receives a message of at most err_len bytes. */
+ * calls that overlap on the GPU race.  Each call looks up the array's address
+ * in the current device and context (this allocates nothing), and returns only
+ * once the run has finished (synchronous).  As with the other entry points,
+ * the reference's time-step checks (centered CFL, utils/checks.jl:61-70) and
+ * dispersion warning are the caller's: an unstable dt is not rejected here.
+ * `err` (may be NULL) receives a message of at most err_len bytes. */
 FOMO_API int fomo_scalar2d_noalloc(const fomo_grid2d* g, const float* vp, const fomo_acq* acq,
                                    float* seis_u, void* stream, char* err, int32_t err_len);
 

@@ -329,7 +329,7 @@ Coef<T> coef(int fd_order) {
 
 // ---------------------------------------------------------------------------
 // elastic2d: elastic2d/fused_kernels.jl:21-124 + loop order :200-240
-// (batch: elastic2d/batch.jl:278-423, bit-identical per shot by construction)
+// (batch: elastic2d/batch.jl:38-183, bit-identical per shot by construction)
 // ---------------------------------------------------------------------------
 template <class T>
 struct ElasticState {
@@ -444,7 +444,7 @@ std::vector<float> sponge_table(int nbc, float factor) {
   return t;
 }
 
-// apply_sponge! (boundary/sponge.jl:56-83): field *= damp over the whole padded grid.
+// apply_sponge! (boundary/sponge.jl:55-78): field *= damp over the whole padded grid.
 template <class T>
 void apply_sponge(const G2& g, const std::vector<float>& damp, T* f) {
   const int nbc = (int)damp.size();
@@ -723,7 +723,7 @@ int run_scalar2d(int nx, int nz, const float* vp, float dh, float dt, int nt, in
 
 // ===========================================================================
 // 3D: pad_array_3d.jl:8-89, elastic3d/medium.jl:31-123, acoustic3d/medium.jl:33-63,
-// habc_3d.jl:23-55, kernels_3d.jl:172-244 (Higdon averaged over the active
+// habc_3d.jl:23-55, kernels_3d.jl:117-193 (Higdon averaged over the active
 // directions, evaluated two-pass from read-only inputs), update kernels of
 // elastic3d/update_*.jl and acoustic3d/update_*.jl, loops elastic3d.jl:122-162
 // and acoustic3d.jl:134-185.
@@ -1034,7 +1034,7 @@ int run_elastic3d(int nx, int ny, int nz, const float* vp, const float* vs, cons
         for (int i = M + 1; i <= g.nx - M; ++i) {
           size_t q = g.at(i, j, k);
           T a1 = 0, a2 = 0, a3 = 0, b1 = 0, b2 = 0, b3 = 0, c1 = 0, c2 = 0, c3 = 0;
-          for (int l = 1; l <= N; ++l) {  // elastic3d/update_velocity.jl:211-237
+          for (int l = 1; l <= N; ++l) {  // elastic3d/update_velocity.jl:49-75
             T a = c.a[l - 1];
             a1 = fmaT(a, txx[q + (l - 1)] - txx[q - l], a1);          // dtxxdx
             a2 = fmaT(a, txy[q + l * Y] - txy[q - (l - 1) * Y], a2);  // dtxydy
@@ -1062,7 +1062,7 @@ int run_elastic3d(int nx, int ny, int nz, const float* vp, const float* vs, cons
         for (int i = M + 1; i <= g.nx - M; ++i) {
           size_t q = g.at(i, j, k);
           T dxx = 0, dyy = 0, dzz = 0, dxy = 0, dyx = 0, dxz = 0, dzx = 0, dyz = 0, dzy = 0;
-          for (int l = 1; l <= N; ++l) {  // elastic3d/update_stress.jl:316-339
+          for (int l = 1; l <= N; ++l) {  // elastic3d/update_stress.jl:51-80
             T a = c.a[l - 1];
             dxx = fmaT(a, vx[q + l] - vx[q - (l - 1)], dxx);
             dyy = fmaT(a, vy[q + l * Y] - vy[q - (l - 1) * Y], dyy);

@@ -373,11 +373,21 @@ def sponge_table(nbc, factor):
 
 
 def ricker(f0, dt, nt):
-    """Ricker wavelet (utils/ricker_wavelet.jl:6-12), evaluated in float64 and rounded to float32."""
-    t = np.arange(nt, dtype=np.float64) * float(np.float32(dt))
-    tau = t - 1.5 / float(np.float32(f0))
-    a = (np.pi * float(np.float32(f0)) * tau) ** 2
-    return ((1.0 - 2.0 * a) * np.exp(-a)).astype(np.float32)
+    """Ricker wavelet (utils/ricker_wavelet.jl:6-12) with Float32 f0, dt: the
+    range t = (0:nt-1) .* dt rounds each exact product once; t0 = 1f0/f0,
+    tau = t .- 1.5f0*t0, x = (pi*f0) .* tau with pi taken as Float32, and
+    (1 - 2 x^2) * exp(-x^2) are Float32 operations (exp: the platform's)."""
+    f32 = np.float32
+    f0, dt = f32(f0), f32(dt)
+    t = np.array([f32(k * float(dt)) for k in range(int(nt))], dtype=np.float32)
+    t0 = f32(f32(1.0) / f0)
+    tau = (t - f32(f32(1.5) * t0)).astype(np.float32)
+    pf = f32(f32(np.pi) * f0)
+    x = (pf * tau).astype(np.float32)
+    sq = (x * x).astype(np.float32)
+    with np.errstate(under="ignore"):
+        e = np.exp(-sq).astype(np.float32)
+    return ((f32(1.0) - f32(2.0) * sq) * e).astype(np.float32)
 
 
 if __name__ == "__main__":  # pragma: no cover

@@ -74,6 +74,30 @@ def test_ricker_matches_oracle(fomo, oracle):
     assert abs(float(w.max()) - 1.0) < 1e-6 and np.argmax(w) == 150  # peak at 1.5/f0
 
 
+@pytest.mark.parametrize("f0,dt,nt", [(15.0, 1e-3, 700), (20.0, 5e-4, 3000), (25.0, 5e-4, 2000),
+                                      (12.0, 8e-4, 2500)])
+def test_ricker_is_float32_arithmetic_within_float64_bound(fomo, f0, dt, nt):
+    """utils/ricker_wavelet.jl:6-12 computes in Float32 (t0 = 1f0/f0, 1.5f0*t0,
+    Float32 exp).  The mirror follows those steps: it sits within the rounding
+    bound of a float64 evaluation of the same formula (absolute 2e-6 on a unit
+    peak: tau cancels near the peak, where t ~ 1.5/f0 is resolved to a Float32
+    ulp), and is not the float64 result rounded once."""
+    w = fomo.ricker_wavelet(f0, dt, nt)
+    assert w.dtype == np.float32 and w.shape == (nt,)
+    f, d = float(np.float32(f0)), float(np.float32(dt))
+    t = np.arange(nt, dtype=np.float64) * d
+    x = np.pi * f * (t - 1.5 / f)
+    w64 = (1.0 - 2.0 * x * x) * np.exp(-x * x)
+    assert float(np.abs(w.astype(np.float64) - w64).max()) < 2e-6
+    # the first samples are 1 - 2x^2 times exp(-x^2) with x ~ -1.5 pi: Float32 steps
+    f32 = np.float32
+    t1 = f32(f32(1.0) * np.float32(dt))
+    x1 = f32(f32(np.float32(np.pi) * np.float32(f0)) *
+             f32(t1 - f32(f32(1.5) * f32(f32(1.0) / np.float32(f0)))))
+    a1 = f32(x1 * x1)
+    assert w[1] == f32(f32(f32(1.0) - f32(2.0) * a1) * np.exp(-a1))
+
+
 def test_scalar_source_scaling(fomo):
     from fomo_b200.api import scalar_wavelet_matrix
 

@@ -1,7 +1,7 @@
 """Pin the 3D CPU oracle against an independent vectorised restatement.
 
 The reference has no 3D test or golden vector, and its 3D Higdon kernel
-(boundary/habc/kernels_3d.jl:172-244) updates in place and races, so there is
+(boundary/habc/kernels_3d.jl:117-193) updates in place and races, so there is
 no output of it to pin against.  The oracle's C++ loops are therefore checked
 here, in float64, against a second restatement written directly from the
 reference's formulas with whole-array numpy slicing:
@@ -10,7 +10,7 @@ reference's formulas with whole-array numpy slicing:
   * the staggered updates (acoustic3d/update_velocity.jl:16-53,
     update_pressure.jl:16-50; elastic3d/update_velocity.jl:17-84,
     update_stress.jl:21-94),
-  * the 3D Higdon average over active directions (kernels_3d.jl:186-240)
+  * the 3D Higdon average over active directions (kernels_3d.jl:151-193)
     evaluated from read-only inputs, with the weight offsets of habc_3d.jl:40-43,
   * inject-then-record order and plane snapshots (acoustic3d.jl:134-185).
 Agreement is to 1e-12 relative (the two differ only in fma contraction).

@@ -178,7 +178,7 @@ def test_det_habc_matches_reference_cpu_two_pass(oracle):
     fo = rng.standard_normal((nxp, nzp)).astype(np.float32)
     nbc, qs, wt = oracle.habc_coeffs(pad, 3000.0, 1e-3, 10.0)
     assert nbc == pad - 1
-    # w_tau as init_habc builds it (habc.jl:158-162), from the distance table
+    # w_tau as init_habc builds it (habc.jl:17-44), from the distance table
     ii, jj = np.meshgrid(np.arange(1, nxp + 1), np.arange(1, nzp + 1), indexing="ij")
     dist = np.minimum(np.minimum(ii - 1, nxp - ii), np.minimum(jj - 1, nzp - jj))
     w = np.clip((dist - 0.75) / (pad - 1), 0.0, 1.0).astype(np.float32)
