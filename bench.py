@@ -371,6 +371,36 @@ def ours(args, cfg):
         "clocks": clocks,
         "finite": finite,
     }
+    if rank == 0 and world == 1 and not os.environ.get("FOMO_BENCH_NO_REPLICA"):
+        # the same batch through the CUDA C++ replica of Fomo's CUDA.jl step
+        # (FOMO_KERNEL_REPLICA), timed on a bounded number of steps and scaled
+        nt_r = min(nt, 300)
+        r_vx = torch.empty((ns, nt_r, nrec), dtype=torch.float32, device=dev)
+        r_vz = torch.empty_like(r_vx)
+
+        def rep_run():
+            return D.elastic2d_batch(d_vp, d_vs, d_rho, dh=cfg["dh"], dt=cfg["dt"], nt=nt_r,
+                                     nbc=cfg["nbc"], fd_order=cfg["fd_order"], v_ref=v_ref,
+                                     sx=d_sx, sz=d_sz, wavelet=d_w[:nt_r], rx=d_rx, rz=d_rz,
+                                     seis_vx=r_vx, seis_vz=r_vz, kernel=4, device=local)
+
+        rep_run()
+        torch.cuda.synchronize()
+        e4, e5 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e4.record(stream)
+        for _ in range(2):
+            rep_run()
+        e5.record(stream)
+        torch.cuda.synchronize()
+        rep_ms_step = e4.elapsed_time(e5) / 2 / nt_r  # per time step of the batch
+        ours_ms_step = ms / nt
+        same = bool(torch.equal(r_vx, d_svx[:, :nt_r]) and torch.equal(r_vz, d_svz[:, :nt_r]))
+        line["replica"] = {
+            "label": "replica of Fomo's CUDA.jl elastic2d_batch step, not Fomo itself",
+            "value": ns / (rep_ms_step * 1e-3 * nt), "unit": "shots/s",
+            "ms_per_time_step": rep_ms_step, "ours_ms_per_time_step": ours_ms_step,
+            "ratio": rep_ms_step / ours_ms_step, "nt_sampled": nt_r,
+            "launches_per_time_step": 8, "seismograms_equal_ours": same}
     if rank == 0 and world == 1 and not os.environ.get("FOMO_BENCH_NO_CPU"):
         # the middle shot of the timed run over its first 800 steps vs the FP64 oracle
         mid = ns // 2

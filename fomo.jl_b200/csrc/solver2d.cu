@@ -14,6 +14,7 @@
 
 #include "solver2d_kernels.cuh"
 #include "mixed2d.cuh"
+#include "replica2d.cuh"
 #include "sweep2d.cuh"
 
 namespace fomo {
@@ -313,6 +314,11 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
   HabcHost hh = make_habc(P.pad, P.v_ref, P.dt, P.dh);
 
   int kernel = P.kernel;
+  // the replica of the reference's CUDA.jl step exists for elastic HABC FP32 runs
+  const bool replica = kernel == FOMO_KERNEL_REPLICA;
+  if (replica && (P.phys != kElastic || P.fp16 || P.sponge || hook))
+    return fail(ctx, FOMO_EARG,
+                "FOMO_KERNEL_REPLICA replicates the elastic2d HABC FP32 step only");
   if (P.sponge) kernel = FOMO_KERNEL_TWO_PHASE;
   if (kernel == FOMO_KERNEL_AUTO) kernel = pick_kernel_2d((int)P.phys, P.N, P.nxp, P.nzp, P.ns);
   if (kernel == FOMO_KERNEL_SINGLE_SWEEP && !sweep2d_supported((int)P.phys, P.N))
@@ -364,6 +370,11 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
   size_t o_list = tagged ? ar.take<int32_t>(std::max<size_t>(tags.list.size(), 1)) : 0;
   size_t o_pack = sweep ? ar.take<float>(sweep_pack_floats(P.nxp, P.nzp)) : 0;
   size_t o_ppack = pair_ok ? ar.take<float>(pair_pack_floats(P.nxp, P.nzp)) : 0;
+  // replica: strip backups of the five fields, three weight planes, frame scratch
+  const long long rep_total = replica ? replica_frame_total(P.nxp, P.nzp, hh.nbc) : 0;
+  size_t o_rep = replica ? ar.take<float>((long long)5 * P.ns * P.plane) : 0;
+  size_t o_repw = replica ? ar.take<float>(3 * P.plane) : 0;
+  size_t o_repscr = replica ? ar.take<float>(std::max(1LL, 3 * rep_total * P.ns)) : 0;
   if ((rc = ensure_workspace(ctx, ar.off))) return rc;
 
   const float* d_vp = vp;
@@ -500,6 +511,21 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
   FOMO_CU(ctx, cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), st));
   // the shot-pair sweep's fields are pair-interleaved (sweep2d.cuh)
   const bool pairs = sweep && sp.family == 5;
+  // the replica updates set 0 in place, with backups and scratch of its own
+  RepFields rw{};
+  float *rep_wv = nullptr, *rep_wz = nullptr, *rep_wt = nullptr, *rep_scr = nullptr;
+  if (replica) {
+    float* ro = ws_ptr<float>(ctx, o_rep);
+    const long long fs = (long long)P.ns * P.plane;
+    rw = RepFields{field(0, 0), field(0, 1), field(0, 2), field(0, 3), field(0, 4),
+                   ro,          ro + fs,     ro + 2 * fs, ro + 3 * fs, ro + 4 * fs};
+    FOMO_CU(ctx, cudaMemsetAsync(ro, 0, sizeof(float) * 5 * fs, st));
+    rep_wv = ws_ptr<float>(ctx, o_repw);
+    rep_wz = rep_wv + P.plane;
+    rep_wt = rep_wz + P.plane;
+    rep_scr = ws_ptr<float>(ctx, o_repscr);
+    FOMO_CU(ctx, replica_setup(st, g, h, rep_wv, rep_wz, rep_wt));
+  }
 
   dim3 blk(32, 8), grd(cdiv(P.nxp, 32), cdiv(P.nzp, 8), P.ns);
   int launches = 0;
@@ -796,7 +822,15 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
   };
   for (int it = it_first; it <= P.nt; ++it) {
     FOMO_CU(ctx, prof_mark(it, 0));
-    if (P.phys == kElastic) {
+    if (P.phys == kElastic && replica) {
+      FOMO_CU(ctx, replica_step(st, P.N, g, c, dtx, dtz, h, rw, emat, rep_wv, rep_wz, rep_wt,
+                                rep_scr, P.ns, it, P.nt, P.n_src, d_src, d_wav, P.n_rec, d_rec,
+                                d_seis[0], d_seis[1]));
+      const int rl = 2 + (rep_total > 0 ? 4 : 0) + (P.n_src > 0) + (P.n_rec > 0);
+      launches += rl;
+      sweeps_per_step = rl;
+      FOMO_CU(ctx, prof_mark(it, 1));
+    } else if (P.phys == kElastic) {
       ElFields a{field(A, 0), field(A, 1), field(A, 2), field(A, 3), field(A, 4)};
       const ElMat& m = emat;
       if (P.fp16 && kernel == FOMO_KERNEL_SINGLE_SWEEP) {
@@ -894,7 +928,8 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
                                       d_snap + (long long)k * nint));
     } else if (d_snap && P.snap_interval > 0 && it % P.snap_interval == 0) {
       int k = it / P.snap_interval - 1;
-      const float* src = (P.phys == kAcoustic ? field(B, 2) : field(B, 1)) + P.pad + (long long)P.pad * P.ld;
+      const float* src = (P.phys == kAcoustic ? field(B, 2) : field(replica ? A : B, 1)) + P.pad +
+                         (long long)P.pad * P.ld;
       FOMO_CU(ctx, cudaMemcpy2DAsync(d_snap + (long long)k * nint, sizeof(float) * P.nx, src,
                                      sizeof(float) * P.ld, sizeof(float) * P.nx, P.nz,
                                      cudaMemcpyDeviceToDevice, st));
@@ -926,7 +961,7 @@ int run2d(fomo_ctx* ctx, Plan2& P, const float* vp, const float* vs, const float
       B = C2;
       C2 = t;
     } else {
-      std::swap(A, B);
+      if (!replica) std::swap(A, B);  // the replica updates in place
     }
   }
   FOMO_CU(ctx, cudaEventRecord(ctx->ev1, st));

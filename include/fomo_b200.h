@@ -71,6 +71,10 @@ extern "C" {
 #define FOMO_KERNEL_ZMARCH 3       /* 3D: z-marching velocity and stress updates;  */
                                    /* TWO_PHASE = per-cell updates; AUTO = z-marching */
                                    /* velocity + per-cell stress (stats: AUTO)        */
+#define FOMO_KERNEL_REPLICA 4      /* elastic2d(_batch): a CUDA C++ replica of the    */
+                                   /* reference's CUDA.jl step (batch.jl:157-183:     */
+                                   /* 8 launches, strip backups, frame scratch), a    */
+                                   /* measurement baseline; AUTO never picks it       */
 
 typedef struct fomo_ctx fomo_ctx;
 

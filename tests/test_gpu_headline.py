@@ -42,11 +42,12 @@ def headline(oracle):
 
 
 # None: the autotuner's pick; then the shot-pair sweep and the one-shot
-# warp-specialized sweep pinned (variant, strip width, CTAs per SM)
-@pytest.mark.parametrize("cfg_pin", [None, "19,112,2", "14,112,4"])
+# warp-specialized sweep pinned (variant, strip width, CTAs per SM); "replica":
+# the CUDA C++ replica of the reference's CUDA.jl step (FOMO_KERNEL_REPLICA)
+@pytest.mark.parametrize("cfg_pin", [None, "19,112,2", "14,112,4", "replica"])
 def test_headline_geometry_bitwise_and_fp64_error(fomo, headline, monkeypatch, cfg_pin):
     cfg, sx, sz, o32, o64 = headline
-    if cfg_pin:
+    if cfg_pin and cfg_pin != "replica":
         monkeypatch.setenv("FOMO_SWEEP_CONFIG", cfg_pin)
     else:
         monkeypatch.delenv("FOMO_SWEEP_CONFIG", raising=False)
@@ -54,7 +55,8 @@ def test_headline_geometry_bitwise_and_fp64_error(fomo, headline, monkeypatch, c
         warnings.simplefilter("ignore")  # the layout is below 4 points per wavelength by design
         r = fomo.elastic2d_batch(cfg["vp"], cfg["vs"], cfg["rho"], cfg["dh"], cfg["dt"], NT,
                                  cfg["f0"], sx=sx, sz=sz, rx=cfg["rx"], rz=cfg["rz"],
-                                 nbc=cfg["nbc"], fd_order=cfg["fd_order"], kernel=2)
+                                 nbc=cfg["nbc"], fd_order=cfg["fd_order"],
+                                 kernel=4 if cfg_pin == "replica" else 2)
     assert np.isfinite(r.seis_vz).all() and np.abs(r.seis_vz).max() > 0.0
     assert np.array_equal(r.seis_vx, o32["seis_vx"])
     assert np.array_equal(r.seis_vz, o32["seis_vz"])
