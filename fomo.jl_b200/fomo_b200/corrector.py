@@ -87,23 +87,25 @@ class Kernels:
         self.ctx.use_torch_stream(self.torch.cuda.current_stream(self.dev))
 
     def features(self, u, u_prev, c2, ld, u_off, c2_off, scale, n, h, w, src=None,
-                 inj_next=None, inj_prev=None):
-        """src: (n, 2) int32 window source cells (one source per window) or None."""
+                 inj_next=None, inj_prev=None, n_src=1):
+        """src: (n, n_src, 2) int32 window source cells (flattened) or None;
+        inj_next / inj_prev: (n, n_src) injected values."""
         feat = self.torch.empty((n, h, w, 16), dtype=self.torch.bfloat16, device=self.dev)
         opt = lambda t: _p(t) if t is not None else None  # noqa: E731
         self._sync_stream()
         self.ctx.check(L.lib().fomo_corr_features(
             self.ctx.handle, n, h, w, u, u_prev, c2, ld, _p(u_off), 0, _p(c2_off), 0, opt(scale),
-            1 if src is not None else 0, opt(src), opt(inj_next), opt(inj_prev), _p(feat)))
+            n_src if src is not None else 0, opt(src), opt(inj_next), opt(inj_prev), _p(feat)))
         return feat
 
-    def target(self, fd_order, u, u_prev, u_next, c2, ld, u_off, c2_off, scale, src, inj, n, h, w):
+    def target(self, fd_order, u, u_prev, u_next, c2, ld, u_off, c2_off, scale, src, inj, n, h, w,
+               src_r=SRC_RADIUS):
         tgt = self.torch.empty((n, h, w), dtype=self.torch.float32, device=self.dev)
         mask = self.torch.empty_like(tgt)
         self._sync_stream()
         self.ctx.check(L.lib().fomo_corr_target(
             self.ctx.handle, n, h, w, fd_order, u, u_prev, u_next, c2, ld, _p(u_off), 0,
-            _p(c2_off), 0, _p(scale), _p(src), _p(inj), SRC_RADIUS, _p(tgt), _p(mask)))
+            _p(c2_off), 0, _p(scale), _p(src), _p(inj), int(src_r), _p(tgt), _p(mask)))
         return tgt, mask
 
     def forward(self, feat, params):
@@ -133,8 +135,29 @@ class Kernels:
 # ---------------------------------------------------------------------------
 # solver entry points
 # ---------------------------------------------------------------------------
+def smooth_source(xc, zc, sigma, radius):
+    """A spatially smooth source on one grid: the cells (1-based) of the square
+    of half-width `radius` around (xc, zc) and their weights exp(-r^2 / (2 sigma^2)),
+    r and sigma in cells of that grid.  sigma = 0 is the point source (xc, zc).
+
+    The weights sample one physical source density, so two grids sampling the
+    same physical square (the fine one with twice the cells per side and sigma,
+    radius in its own cells) inject the same source: each cell adds
+    v^2 dt^2 * weight * wavelet, the scalar update's discretisation of a
+    distributed source term, with no area factor."""
+    if sigma <= 0:
+        return [int(xc)], [int(zc)], np.ones(1, np.float32)
+    sx, sz, wt = [], [], []
+    for dz in range(-radius, radius + 1):
+        for dx in range(-radius, radius + 1):
+            sx.append(int(xc + dx))
+            sz.append(int(zc + dz))
+            wt.append(np.exp(-(dx * dx + dz * dz) / (2.0 * sigma * sigma)))
+    return sx, sz, np.asarray(wt, np.float32)
+
+
 def _scalar_inputs(vp, dh, dt, nt, f0, sx, sz, rx, rz, fd_order, wavelet, source_scale,
-                   wavelet_factor):
+                   wavelet_factor, weights=None):
     vp = _f32F(vp)
     nx, nz = vp.shape
     dh, dt, f0 = np.float32(dh), np.float32(dt), np.float32(f0)
@@ -145,17 +168,20 @@ def _scalar_inputs(vp, dh, dt, nt, f0, sx, sz, rx, rz, fd_order, wavelet, source
         w = (w * np.float32(wavelet_factor)).astype(np.float32)
     sxv, szv = _i32F(sx).ravel(), _i32F(sz).ravel()
     wm = scalar_wavelet_matrix(w, vp, dt, sxv, szv, str(source_scale).lstrip(":"))
+    if weights is not None:
+        wm = np.asfortranarray((wm * np.asarray(weights, np.float32)[:, None]).astype(np.float32))
     return vp, dh, dt, sxv, szv, wm, _i32F(rx).ravel(), _i32F(rz).ravel()
 
 
 def scalar2d_corrected(vp, dh, dt, nt, f0, *, params, sx, sz, rx, rz, nbc: int = 50,
                        fd_order: int = 8, v_ref=None, wavelet=None, source_scale="v2dt2",
-                       wavelet_factor: float = 1.0, device: int = 0):
+                       wavelet_factor: float = 1.0, weights=None, device: int = 0):
     """scalar2d (equations/scalar2d/scalar2d.jl:104-189) with the learned
-    correction after every step.  Returns (seis_u, kernel_time_s)."""
+    correction after every step.  weights: per-source factors of the wavelet
+    (a smooth source, ``smooth_source``).  Returns (seis_u, kernel_time_s)."""
     vp, dh, dt, sxv, szv, wm, rxv, rzv = _scalar_inputs(vp, dh, dt, nt, f0, sx, sz, rx, rz,
                                                         fd_order, wavelet, source_scale,
-                                                        wavelet_factor)
+                                                        wavelet_factor, weights)
     p = np.ascontiguousarray(params, dtype=np.float32)
     if p.size != param_count():
         raise ArgumentError(f"corrector needs {param_count()} parameters, got {p.size}")
@@ -171,8 +197,25 @@ def scalar2d_corrected(vp, dh, dt, nt, f0, *, params, sx, sz, rx, rz, nbc: int =
     return seis, st.kernel_time_s
 
 
+def scalar2d_sources(vp, dh, dt, nt, f0, *, sx, sz, weights, rx, rz, nbc=50, fd_order=8,
+                     wavelet=None, device=0):
+    """Plain scalar2d with a per-source factor on the wavelet (a smooth source);
+    returns (seis_u, kernel_time_s)."""
+    vp, dh, dt, sxv, szv, wm, rxv, rzv = _scalar_inputs(vp, dh, dt, nt, f0, sx, sz, rx, rz,
+                                                        fd_order, wavelet, "v2dt2", 1.0, weights)
+    seis = np.zeros((rxv.size, nt), dtype=np.float32, order="F")
+    st = L.Stats()
+    ctx = L.context(device)
+    g = _grid(vp.shape[0], vp.shape[1], dh, dt, nt, nbc, fd_order, _min_pos(vp))
+    acq = L.Acq(1, sxv.size, _ptr(sxv), _ptr(szv), _ptr(wm), rxv.size, _ptr(rxv), _ptr(rzv))
+    o = L.Opts()
+    ctx.check(L.lib().fomo_scalar2d(ctx.handle, C.byref(g), _ptr(vp), C.byref(acq), _ptr(seis),
+                                    C.byref(o), C.byref(st)))
+    return seis, st.kernel_time_s
+
+
 def fine_snapshots(vp, dh, dt, nt, f0, *, sx, sz, nbc=50, fd_order=8, stride=2, device=0,
-                   rx=None, rz=None):
+                   rx=None, rz=None, weights=None):
     """Fine scalar2d run whose interior wavefield is kept every `stride` steps
     on every `stride`-th node: a torch tensor (nt // stride, ceil(nz/stride),
     ceil(nx/stride)); entry k is the field after step (k+1)*stride."""
@@ -181,7 +224,7 @@ def fine_snapshots(vp, dh, dt, nt, f0, *, sx, sz, nbc=50, fd_order=8, stride=2, 
     rx = [1] if rx is None else rx
     rz = [1] if rz is None else rz
     vp, dh, dt, sxv, szv, wm, rxv, rzv = _scalar_inputs(vp, dh, dt, nt, f0, sx, sz, rx, rz,
-                                                        fd_order, None, "v2dt2", 1.0)
+                                                        fd_order, None, "v2dt2", 1.0, weights)
     nx, nz = vp.shape
     mx, mz = -(-nx // stride), -(-nz // stride)
     count = (nt - stride) // stride + 1
@@ -219,10 +262,14 @@ class Pairs(NamedTuple):
 
 
 def make_pairs(K: Kernels, snaps, c2, src_xz, w_coarse, n_pairs, fd_order, rng,
-               patch=PATCH) -> Pairs:
+               patch=PATCH, src_r=SRC_RADIUS) -> Pairs:
     """n_pairs training windows from one fine run's coarse-sampled snapshots.
-    src_xz: 0-based coarse source cell (x, z); w_coarse: the coarse run's
-    injected values per step (already source-scaled)."""
+    src_xz: 0-based coarse source cells [(x, z), ...] (the first is the centre);
+    w_coarse: the coarse run's injected values (n_src, nt) (already source-scaled);
+    src_r: half-width of the square around the centre left out of the targets."""
+    src_xz = [tuple(v) for v in np.atleast_2d(np.asarray(src_xz))]
+    w_coarse = np.atleast_2d(np.asarray(w_coarse, np.float32))
+    n_src = len(src_xz)
     torch = K.torch
     count, mz, mx = snaps.shape
     plane = mz * mx
@@ -248,18 +295,22 @@ def make_pairs(K: Kernels, snaps, c2, src_xz, w_coarse, n_pairs, fd_order, rng,
         c_off.append(z0 * mx + x0)
         win = snaps[c, z0:z0 + patch, x0:x0 + patch].abs().max().item()
         scale.append(1.0 / win if win > 0 else 0.0)
-        src.append((src_xz[0] - x0, src_xz[1] - z0))
-        inj.append(float(w_coarse[c + 1]))  # injected during step it = c + 2 (index it - 1)
-        injp.append(float(w_coarse[c]))      # and during the previous step
+        src.append([(sx_ - x0, sz_ - z0) for sx_, sz_ in src_xz])
+        inj.append(w_coarse[:, c + 1])  # injected during step it = c + 2 (index it - 1)
+        injp.append(w_coarse[:, c])     # and during the previous step
     t = lambda a, dt: torch.tensor(np.asarray(a), dtype=dt, device=K.dev)  # noqa: E731
     u_off, c_off = t(u_off, torch.int64), t(c_off, torch.int64)
     scale, inj, injp = t(scale, torch.float32), t(inj, torch.float32), t(injp, torch.float32)
-    src = t(np.asarray(src, dtype=np.int32).ravel(), torch.int32)
+    src_all = np.asarray(src, dtype=np.int32)  # (n, n_src, 2)
+    src = t(src_all.ravel(), torch.int32)
+    centre = t(src_all[:, 0, :].ravel(), torch.int32)
+    inj_c = inj[:, 0].contiguous()
+    inj, injp = inj.ravel().contiguous(), injp.ravel().contiguous()
     base = _p(snaps)
     feat = K.features(base, base - 4 * plane, _p(c2t), mx, u_off, c_off, scale, n_pairs, patch,
-                      patch, src=src, inj_next=inj, inj_prev=injp)
+                      patch, src=src, inj_next=inj, inj_prev=injp, n_src=n_src)
     tgt, mask = K.target(fd_order, base, base - 4 * plane, base + 4 * plane, _p(c2t), mx, u_off,
-                         c_off, scale, src, inj, n_pairs, patch, patch)
+                         c_off, scale, centre, inj_c, n_pairs, patch, patch, src_r=src_r)
     torch.cuda.synchronize(K.dev)
     return Pairs(feat, tgt, mask)
 
@@ -324,23 +375,29 @@ def one_step_error(K: Kernels, pairs: Pairs, params) -> float:
 class Workload(NamedTuple):
     vp_fine: list
     vp_coarse: list
-    src: list        # coarse (sx, sz), 1-based
+    src: list        # coarse (sx, sz), 1-based: the source centre
     rx: np.ndarray   # coarse receivers, 1-based
     rz: np.ndarray
+    src_sigma: float = 0.0  # Gaussian width in coarse cells (0: point source)
+    src_radius: int = 0     # half-width of the source square in coarse cells
 
 
 def workload(n_shots, nxc, nzc, seed, corr=(100.0, 400.0), vmin=1500.0, vmax=4500.0,
-             dh_fine=5.0):
+             dh_fine=5.0, src_sigma=0.0):
     """Learned-coarse workload: per shot a 2D Gaussian random field on the fine
     grid (2 nxc - 1) x (2 nzc - 1) (correlation length ~ U(corr), clipped to
     vmin..vmax), its coarse model on every 2nd node, a source at a random x
     at coarse depth 10 (or nzc // 4 on small grids), receivers every 2nd
-    coarse x at depth 10 (or nzc // 4)."""
+    coarse x at depth 10 (or nzc // 4).  src_sigma > 0 (coarse cells) makes
+    the source a smooth Gaussian patch of half-width ceil(2.5 src_sigma),
+    sampled identically by both grids (``smooth_source``)."""
     from .synthetic import grf2d
 
     rng = np.random.default_rng(seed)
     nxf, nzf = 2 * nxc - 1, 2 * nzc - 1
+    radius = int(np.ceil(2.5 * src_sigma)) if src_sigma > 0 else 0
     depth = min(10, max(4, nzc // 4))
+    depth = max(depth, radius + 1)
     vf, vc, src = [], [], []
     for s in range(n_shots):
         cl = float(rng.uniform(*corr))
@@ -348,9 +405,26 @@ def workload(n_shots, nxc, nzc, seed, corr=(100.0, 400.0), vmin=1500.0, vmax=450
                   seed * 1000 + s, vmin, vmax)
         vf.append(v)
         vc.append(np.asfortranarray(v[::2, ::2]))
-        src.append((int(rng.integers(nxc // 8 + 1, nxc - nxc // 8)), depth))
+        src.append((int(rng.integers(max(nxc // 8, radius) + 1, nxc - max(nxc // 8, radius))),
+                    depth))
     rx = np.arange(2, nxc, 2)
-    return Workload(vf, vc, src, rx, np.full(rx.size, depth))
+    return Workload(vf, vc, src, rx, np.full(rx.size, depth), float(src_sigma), radius)
+
+
+def _sources(w: Workload, s: int, fine: bool):
+    """Source cells (1-based) and weights of shot s on the coarse or fine grid."""
+    xc, zc = w.src[s]
+    if fine:
+        return smooth_source(2 * xc - 1, 2 * zc - 1, 2.0 * w.src_sigma, 2 * w.src_radius)
+    return smooth_source(xc, zc, w.src_sigma, w.src_radius)
+
+
+def _wavelet_factor(w: Workload) -> float:
+    """Coarse raw wavelet / fine raw wavelet for the same physical source: a
+    point source is a one-cell density 1/dh^2, so its coarse value is
+    (dh_f / dh_c)^2 = 1/4 of the fine one; a smooth source samples the same
+    density on both grids (factor 1)."""
+    return 1.0 if w.src_sigma > 0 else 0.25
 
 
 def pairs_from_fine(K, w: Workload, shots, *, dh_c, dt_c, nt_c, f0, nbc_c, fd_order, n_pairs,
@@ -360,13 +434,17 @@ def pairs_from_fine(K, w: Workload, shots, *, dh_c, dt_c, nt_c, f0, nbc_c, fd_or
     parts = []
     per = max(1, n_pairs // len(shots))
     for s in shots:
-        sxc, szc = w.src[s]
-        snaps = fine_snapshots(w.vp_fine[s], dh_c / 2, dt_c / 2, 2 * nt_c, f0, sx=[2 * sxc - 1],
-                               sz=[2 * szc - 1], nbc=2 * nbc_c, fd_order=fd_order)
+        fsx, fsz, fwt = _sources(w, s, fine=True)
+        csx, csz, cwt = _sources(w, s, fine=False)
+        snaps = fine_snapshots(w.vp_fine[s], dh_c / 2, dt_c / 2, 2 * nt_c, f0, sx=fsx, sz=fsz,
+                               nbc=2 * nbc_c, fd_order=fd_order, weights=fwt)
         c2 = coarse_c2(w.vp_coarse[s], dh_c, dt_c, nbc_c, fd_order)
-        wc = ricker_wavelet(f0, dt_c, nt_c) * np.float32(0.25)
-        wm = scalar_wavelet_matrix(wc, w.vp_coarse[s], np.float32(dt_c), [sxc], [szc], "v2dt2")[0]
-        parts.append(make_pairs(K, snaps, c2, (sxc - 1, szc - 1), wm, per, fd_order, rng))
+        wc = ricker_wavelet(f0, dt_c, nt_c) * np.float32(_wavelet_factor(w))
+        wm = scalar_wavelet_matrix(wc, w.vp_coarse[s], np.float32(dt_c), csx, csz, "v2dt2")
+        wm = (wm * cwt[:, None]).astype(np.float32)
+        cells = [(x - 1, z - 1) for x, z in zip(csx, csz)]
+        parts.append(make_pairs(K, snaps, c2, cells, wm, per, fd_order, rng,
+                                src_r=w.src_radius + SRC_RADIUS))
         del snaps
     return Pairs(torch.cat([p.feat for p in parts]), torch.cat([p.target for p in parts]),
                  torch.cat([p.mask for p in parts]))
@@ -376,23 +454,22 @@ def evaluate(w: Workload, shots, params, *, dh_c, dt_c, nt_c, f0, nbc_c, fd_orde
     """Seismogram relative L2 against the fine run at matching physical
     receivers, for the plain coarse run and the corrected one, per shot; plus
     the coarse kernel times.  Returns a list of dicts."""
-    from .api import scalar2d
-
     out = []
-    wc = ricker_wavelet(f0, dt_c, nt_c) * np.float32(0.25)
+    wc = ricker_wavelet(f0, dt_c, nt_c) * np.float32(_wavelet_factor(w))
     for s in shots:
-        sxc, szc = w.src[s]
-        fine = scalar2d(w.vp_fine[s], dh_c / 2, dt_c / 2, 2 * nt_c, f0, sx=[2 * sxc - 1],
-                        sz=[2 * szc - 1], rx=2 * w.rx - 1, rz=2 * w.rz - 1, nbc=2 * nbc_c,
-                        fd_order=fd_order)
-        ref = fine.seis_u[:, 1::2]
-        plain = scalar2d(w.vp_coarse[s], dh_c, dt_c, nt_c, f0, sx=[sxc], sz=[szc], rx=w.rx,
-                         rz=w.rz, nbc=nbc_c, fd_order=fd_order, wavelet=wc)
-        corr, t_corr = scalar2d_corrected(w.vp_coarse[s], dh_c, dt_c, nt_c, f0, params=params,
-                                          sx=[sxc], sz=[szc], rx=w.rx, rz=w.rz, nbc=nbc_c,
+        fsx, fsz, fwt = _sources(w, s, fine=True)
+        csx, csz, cwt = _sources(w, s, fine=False)
+        fine, t_fine = scalar2d_sources(w.vp_fine[s], dh_c / 2, dt_c / 2, 2 * nt_c, f0, sx=fsx,
+                                        sz=fsz, weights=fwt, rx=2 * w.rx - 1, rz=2 * w.rz - 1,
+                                        nbc=2 * nbc_c, fd_order=fd_order)
+        ref = fine[:, 1::2]
+        plain, t_plain = scalar2d_sources(w.vp_coarse[s], dh_c, dt_c, nt_c, f0, sx=csx, sz=csz,
+                                          weights=cwt, rx=w.rx, rz=w.rz, nbc=nbc_c,
                                           fd_order=fd_order, wavelet=wc)
+        corr, t_corr = scalar2d_corrected(w.vp_coarse[s], dh_c, dt_c, nt_c, f0, params=params,
+                                          sx=csx, sz=csz, rx=w.rx, rz=w.rz, nbc=nbc_c,
+                                          fd_order=fd_order, wavelet=wc, weights=cwt)
         e = lambda a: float(np.linalg.norm(a - ref) / np.linalg.norm(ref))  # noqa: E731
-        out.append(dict(shot=s, err_plain=e(plain.seis_u), err_corrected=e(corr),
-                        t_fine=fine.stats.kernel_time_s, t_plain=plain.stats.kernel_time_s,
-                        t_corrected=t_corr))
+        out.append(dict(shot=s, err_plain=e(plain), err_corrected=e(corr), t_fine=t_fine,
+                        t_plain=t_plain, t_corrected=t_corr))
     return out

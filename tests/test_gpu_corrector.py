@@ -136,11 +136,17 @@ def test_zero_corrector_equals_plain_scalar2d(fomo):
     assert np.array_equal(zero, plain)
 
 
-def test_trained_corrector_gain(fomo):
-    """Ablation: the corrector trained on solver-generated pairs of two shots
-    cuts the held-out one-step error of the coarse step (1.0 = no corrector)
-    and keeps the corrected run stable; the seismogram errors of both runs
-    against the fine run are recorded."""
+@pytest.mark.parametrize("src_sigma", [0.0, 1.0])
+def test_trained_corrector_one_step_gain(fomo, src_sigma):
+    """Ablation of the learned part on solver-generated pairs (two training shots,
+    a held-out shot): training cuts the held-out ONE-STEP error of the coarse
+    step to under half (1.0 = no corrector), and the corrected run stays stable
+    and within 5 % of the plain coarse run's seismogram error.  That is what
+    the corrector achieves: it does NOT lower the seismogram error against the
+    fine run (measured 7.20 % plain, 7.27 % corrected with the smooth source;
+    16.61 % / 16.65 % with the point source), so no gain is asserted.  The
+    smooth source (a Gaussian patch both grids sample, src_sigma in coarse
+    cells) is what halves the plain coarse error."""
     import warnings
 
     from fomo_b200 import corrector as CR
@@ -149,7 +155,7 @@ def test_trained_corrector_gain(fomo):
     K = CR.Kernels(0)
     rng = np.random.default_rng(0)
     cfg = dict(dh_c=10.0, dt_c=1e-3, nt_c=300, f0=25.0, nbc_c=20, fd_order=8)
-    w = CR.workload(3, 96, 64, seed=7)
+    w = CR.workload(3, 96, 64, seed=7, src_sigma=src_sigma)
     train = CR.pairs_from_fine(K, w, [0, 1], n_pairs=1024, rng=rng, **cfg)
     held = CR.pairs_from_fine(K, w, [2], n_pairs=256, rng=rng, **cfg)
     params, losses = CR.train(K, train, CR.init_params(0), epochs=20, lr=1e-2)
@@ -161,4 +167,7 @@ def test_trained_corrector_gain(fomo):
     r = CR.evaluate(w, [2], params, **cfg)[0]
     print(f"one-step error {trained:.3f}; seismogram error plain {r['err_plain']:.4f} "
           f"corrected {r['err_corrected']:.4f}")
-    assert np.isfinite(r["err_corrected"]) and r["err_corrected"] < 2 * r["err_plain"]
+    assert np.isfinite(r["err_corrected"])
+    assert abs(r["err_corrected"] - r["err_plain"]) < 0.05 * r["err_plain"]
+    if src_sigma > 0:
+        assert r["err_plain"] < 0.1  # the smooth source halves the point source's 16.6 %
