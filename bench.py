@@ -492,10 +492,11 @@ def secondary(args):
     torch.cuda.synchronize()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     kt, cells, algb, launches = [], 0.0, 0.0, 0
+    res = None
     with ClockSampler(local) as clk:
         ev[0].record(stream)
         for _ in range(args.steps):
-            _, t, cells, algb, nl = run()
+            res, t, cells, algb, nl = run()
             kt.append(t)
             launches += int(nl)
         ev[1].record(stream)
@@ -518,8 +519,68 @@ def secondary(args):
                          "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
                          "kernel": "whole time loop (library CUDA events)"},
             "gpu_launches": launches, "clocks": clk.summary()}
+    if rank == 0 and not os.environ.get("FOMO_BENCH_NO_CPU"):
+        nt_run = c["nt"] if args.workload != "elastic3d" else nt
+        line["l2_vs_fp64"] = secondary_l2(args.workload, c, res, nt_run)
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def secondary_l2(workload, c, r, nt):
+    """Error statement of a secondary line against the FP64 oracle of the same
+    scheme: elastic-fp16 -- the middle shot's seismograms over the first
+    min(nt, 1000) steps; uneven -- the smallest shot over its whole run (and
+    whether it equals the FP32 oracle bit for bit); elastic3d -- a reduced grid
+    (64x64x48 interior, the same dh, dt, order, nbc and model statistics, 150
+    steps), since the oracle cannot run the full volume in a bench."""
+    from oracle import oracle as O
+
+    import fomo_b200 as F
+
+    O.build()
+    t0 = time.perf_counter()
+    if workload == "elastic-fp16":
+        mid = c["sx"].size // 2
+        k = min(nt, 1000)
+        w = F.ricker_wavelet(c["f0"], c["dt"], k).reshape(1, -1)
+        o = O.elastic2d(c["vp"], c["vs"], c["rho"], c["dh"], c["dt"], k, sx=[[int(c["sx"][mid])]],
+                        sz=[[int(c["sz"][mid])]], rx=c["rx"], rz=c["rz"], wavelet=w, nbc=c["nbc"],
+                        fd_order=c["fd_order"], prec=64)
+        out = {"vx": _rel(r.seis_vx[:, :k, mid], o["seis_vx"][:, :, 0]),
+               "vz": _rel(r.seis_vz[:, :k, mid], o["seis_vz"][:, :, 0]),
+               "tolerance": 1e-2, "sample": f"shot {mid}, steps 1..{k}"}
+    elif workload == "uneven":
+        s = int(np.argmin([v.size for v in c["vps"]]))
+        w = F.ricker_wavelet(c["f0"], c["dt"], nt).reshape(1, -1)
+        kw = dict(sx=[c["sx"][s]], sz=[c["sz"][s]], rx=c["rx"][s], rz=c["rz"][s], wavelet=w,
+                  nbc=c["nbc"], fd_order=c["fd_order"])
+        o64 = O.acoustic2d(c["vps"][s], c["rhos"][s], c["dh"], c["dt"], nt, prec=64, **kw)
+        o32 = O.acoustic2d(c["vps"][s], c["rhos"][s], c["dh"], c["dt"], nt, **kw)
+        p = r.shots[s][0]
+        out = {"p": _rel(p, o64["seis_p"][:, :, 0]),
+               "bitwise_vs_fp32_oracle": bool(np.array_equal(p, o32["seis_p"][:, :, 0])),
+               "tolerance": 1e-5, "sample": f"shot {s} ({c['vps'][s].shape[0]}x"
+                                            f"{c['vps'][s].shape[1]}), all {nt} steps"}
+    else:  # elastic3d on a reduced grid of the same configuration
+        from fomo_b200.synthetic import elastic3d_config
+
+        c3 = elastic3d_config(64, 64, 48)
+        k = 150
+        w = F.ricker_wavelet(c3["f0"], c3["dt"], k)
+        kw = dict(sx=c3["sx"], sy=c3["sy"], sz=c3["sz"], rx=c3["rx"], ry=c3["ry"], rz=c3["rz"],
+                  nbc=c3["nbc"], fd_order=c3["fd_order"])
+        g = F.elastic3d(c3["vp"], c3["vs"], c3["rho"], c3["dh"], c3["dt"], k, c3["f0"], **kw)
+        o = O.elastic3d(c3["vp"], c3["vs"], c3["rho"], c3["dh"], c3["dt"], k,
+                        wavelet=w.reshape(1, -1), prec=64, **kw)
+        out = {"vz": _rel(g[2], o["seis_vz"]), "vx": _rel(g[0], o["seis_vx"]),
+               "tolerance": 1e-5, "sample": f"64x64x48 interior, {k} steps, same dh/dt/order/nbc"}
+    out["oracle"] = f"C++ restatement in FP64 ({time.perf_counter() - t0:.1f} s on the host)"
+    return out
 
 
 # Fomo's published throughput (README.md "Performance & Reproducibility", RTX 3060,
