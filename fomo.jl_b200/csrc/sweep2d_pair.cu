@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(2 * NV, MINB)
   // the same segments and iterations.
   struct Seg {
     int za, zb, pair, XV, XT, x, zv0, I, xsd, xds, cn;
-    bool xin, xfr, o_any;
+    bool xin, xfr, o_any, hbx;
     long long obase;
   };
   auto segment = [&](long long& r, Seg& g) {
@@ -192,6 +192,10 @@ __global__ void __launch_bounds__(2 * NV, MINB)
     g.xds = min(g.x, nx - 1 - g.x);
     g.cn = min(max(c + g.xsd, 0), W - 1);
     g.o_any = do_o && g.x < nx;
+    // the window reaches an x-band: only then do threads read neighbour columns'
+    // v' / s' rows (x-side Higdon), which need the shared rows and the
+    // role-local barrier (CTA-uniform per segment)
+    g.hbx = g.XV <= nbc || g.XV + NV - 1 >= nx - 1 - nbc;
     g.obase = (long long)g.pair * gm.plane + g.x;
     g.zv0 = g.za - 2 - 3 * M;  // M warm-up iterations fill the windows
     g.I = (g.zb - g.za + 4 + 4 * M + 1) / 2 + 1;
@@ -271,9 +275,11 @@ __global__ void __launch_bounds__(2 * NV, MINB)
             }
             vpc[0][rr] = ux;
             vpc[1][rr] = uz;
-            const int pr = (2 * i + rr) & 3;  // v' ring row of zv + rr
-            s_vp[pr * W + c] = ux;
-            s_vp[(4 + pr) * W + c] = uz;
+            if (g.hbx) {
+              const int pr = (2 * i + rr) & 3;  // v' ring row of zv + rr
+              s_vp[pr * W + c] = ux;
+              s_vp[(4 + pr) * W + c] = uz;
+            }
           }
         }
 #pragma unroll
@@ -281,7 +287,7 @@ __global__ void __launch_bounds__(2 * NV, MINB)
           wxz[q] = wxz[q + 2];
           wzz[q] = wzz[q + 2];
         }
-        tma::bar_sync(2, NV);  // this iteration's v' rows are in s_vp
+        if (g.hbx) tma::bar_sync(2, NV);  // this iteration's v' rows are in s_vp
         // v'' rows zv-1 (rr = 0) and zv (rr = 1); v' rows zv-2 .. zv+1 are in vpp / vpc
         if (do_v) {
 #pragma unroll
@@ -435,13 +441,15 @@ __global__ void __launch_bounds__(2 * NV, MINB)
             spc[0][rr] = sxx;
             spc[1][rr] = szz;
             spc[2][rr] = sxz;
-            const int sr = (2 * i + rr) & 3;  // s' ring row of q + rr
-            s_sp[sr * W + c] = sxx;
-            s_sp[(4 + sr) * W + c] = szz;
-            s_sp[(8 + sr) * W + c] = sxz;
+            if (g.hbx) {
+              const int sr = (2 * i + rr) & 3;  // s' ring row of q + rr
+              s_sp[sr * W + c] = sxx;
+              s_sp[(4 + sr) * W + c] = szz;
+              s_sp[(8 + sr) * W + c] = sxz;
+            }
           }
         }
-        tma::bar_sync(3, NV);  // this iteration's s' rows are in s_sp
+        if (g.hbx) tma::bar_sync(3, NV);  // this iteration's s' rows are in s_sp
         // s'' rows q-1 (rr = 0) and q (rr = 1); s' rows q-2 .. q+1 are in spp / spc
         if (g.o_any) {
 #pragma unroll
