@@ -1722,6 +1722,7 @@ __global__ void __launch_bounds__(2 * NV, MINB)
                   const __grid_constant__ CUtensorMap th_vx, const __grid_constant__ CUtensorMap th_vz,
                   SweepGeom gm, Coef c, float dtx, float dtz, HabcDev h, MatPack mp, ElOut o,
                   ElOut16 o16, const long long* __restrict__ bounds, int* __restrict__ err) {
+  static_assert(NV % 32 == 0, "each role is whole warps: named barriers count whole warps");
   // H16: binary16 storage outside the kFp16Band-wide FP32 band (th_* map the
   // binary16 arrays, o16 receives them); TMA brings the binary16 rows into
   // staging boxes (and the FP32 rows where the band reaches), each role widens

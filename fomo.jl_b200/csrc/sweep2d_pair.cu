@@ -116,6 +116,7 @@ __global__ void __launch_bounds__(2 * NV, MINB)
               PairPack mp, PairOut o, const long long* __restrict__ bounds,
               int* __restrict__ err) {
   using S = PairShape<N, NV, P>;
+  static_assert(NV % 32 == 0, "each role is whole warps: named barriers count whole warps");
   PairCoef k;
 #pragma unroll
   for (int l = 0; l < 5; ++l) k.a[l] = pinned(kp.a[l]);
