@@ -15,7 +15,8 @@ over ranks.
 Secondary workloads (one JSON line each, same keys; not the default line):
     --workload elastic-fp16   the same batch with binary16 wavefield storage
     --workload uneven         64 acoustic shots on grids of uneven size (graph run)
-    --workload elastic3d      elastic3d 400x400x300, nbc 40, order 8 (nt from --nt)
+    --workload elastic3d      elastic3d 400x400x300, nbc 40, order 8 (nt from --nt;
+                              --grid3d / --kernel3d: other sizes and kernel forms)
     --workload readme         steps/s on the grids of Fomo's published throughput table
     --workload sponge         Fomo's HABC-vs-sponge benchmark (acoustic and elastic 401x401)
     --workload coupled        coupled2d on the grids of Fomo's two coupled2d demos
@@ -454,15 +455,18 @@ def secondary(args):
     elif args.workload == "elastic3d":
         from fomo_b200.synthetic import elastic3d_config
 
-        c = elastic3d_config()
+        g3 = [int(v) for v in args.grid3d.split(",")]
+        c = elastic3d_config(*g3)
         nt = args.nt if args.nt != 3000 else 200
-        desc = (f"elastic3d: 400x400x300 (padded 488x488x388), dh 10 m, dt 0.8 ms, nt {nt} of 2500, "
-                "order 8, nbc 40, 3D GRF vp, vacuum top, 200x200 receivers")
+        pads = [v + 2 * (c["nbc"] + c["fd_order"] // 2) for v in g3]
+        desc = (f"elastic3d: {g3[0]}x{g3[1]}x{g3[2]} (padded {pads[0]}x{pads[1]}x{pads[2]}), dh 10 m, "
+                f"dt 0.8 ms, nt {nt} of 2500, order 8, nbc 40, 3D GRF vp, vacuum top, "
+                f"{c['rx'].size} receivers")
 
         def run():
             r = F.elastic3d(c["vp"], c["vs"], c["rho"], c["dh"], c["dt"], nt, c["f0"], sx=c["sx"],
                             sy=c["sy"], sz=c["sz"], rx=c["rx"], ry=c["ry"], rz=c["rz"], nbc=c["nbc"],
-                            fd_order=c["fd_order"], device=local)
+                            fd_order=c["fd_order"], device=local, kernel=args.kernel3d)
             s = F.api.last_stats
             return r, s.kernel_time_s, s.cell_updates, s.alg_bytes, s.gpu_launches
         unit, metric, per = "Gcell-updates/s", "Gcell-updates/s", None
@@ -811,6 +815,10 @@ def main():
     ap.add_argument("--nt", type=int, default=3000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--grid3d", default="400,400,300",
+                    help="elastic3d workload: interior nx,ny,nz (smaller cases for profiling)")
+    ap.add_argument("--kernel3d", type=int, default=0,
+                    help="elastic3d workload: fomo_opts.kernel (0 auto, 1 per-cell, 2 fused, 3 z-march)")
     ap.add_argument("--workload", choices=["elastic-batch", "elastic-fp16", "uneven", "elastic3d",
                                            "readme", "sponge", "coupled"],
                     default="elastic-batch")

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "fomo_internal.cuh"
+#include "sweep3d.cuh"
 
 namespace fomo {
 
@@ -47,14 +48,6 @@ __global__ void k_inject_record3(int it, int nt, int n_src, const int* __restric
 }
 
 namespace {
-
-struct Geo3 {
-  int nx, ny, nz;       // padded
-  int ld;               // x pitch
-  long long sy, sz;     // strides of y and z (ld, ld*ny)
-  long long vol;        // sz * nz
-  int M, nbc;
-};
 
 __device__ __forceinline__ bool interior3(const Geo3& g, int x, int y, int z) {
   return x >= g.M && x < g.nx - g.M && y >= g.M && y < g.ny - g.M && z >= g.M && z < g.nz - g.M;
@@ -811,6 +804,7 @@ int run3d(fomo_ctx* ctx, bool elastic, const fomo_grid3d* gp, const float* vp, c
   size_t o_mat = ar.take<float>(nmat * g.vol);
   size_t o_state = ar.take<float>(2LL * nfield * g.vol);
   size_t o_scr = ar.take<float>(std::max(1LL, nphase_max * fr.total));
+  size_t o_bnd = ar.take<char>(fused3_table_bytes(g));
   size_t o_w = ar.take<float>(wt3.size());
   size_t o_src = ar.take<int32_t>(std::max(acq->n_src, 1));
   size_t o_rec = ar.take<int32_t>(std::max(acq->n_rec, 1));
@@ -879,9 +873,15 @@ int run3d(fomo_ctx* ctx, bool elastic, const fomo_grid3d* gp, const float* vp, c
   // velocity update beats the per-cell one (1.85 vs 2.05 ms), the z-marching
   // stress update loses (2.65 vs 2.15 ms).  AUTO takes the faster of each;
   // ZMARCH and TWO_PHASE select one form for both (identical results).
+  // The fused TMA half steps (sweep3d.cu: update and Higdon boundary in one
+  // pass each) are the default wherever they run; SINGLE_SWEEP requests them.
   const int kreq = opts ? opts->kernel : FOMO_KERNEL_AUTO;
-  const bool zm_vel = elastic && kreq != FOMO_KERNEL_TWO_PHASE;
-  const bool zm_str = elastic && kreq == FOMO_KERNEL_ZMARCH;
+  const bool fused = elastic && (kreq == FOMO_KERNEL_AUTO || kreq == FOMO_KERNEL_SINGLE_SWEEP) &&
+                     fused3_supported(N);
+  if (elastic && kreq == FOMO_KERNEL_SINGLE_SWEEP && !fused)
+    return fail(ctx, FOMO_EUNSUPPORTED, "fused 3D half steps need the TMA tensor-map encoder");
+  const bool zm_vel = elastic && !fused && kreq != FOMO_KERNEL_TWO_PHASE;
+  const bool zm_str = elastic && !fused && kreq == FOMO_KERNEL_ZMARCH;
   const bool zmarch = zm_vel || zm_str;
   unsigned zgrid = 1;
   ZmPlan zp{};
@@ -897,11 +897,18 @@ int run3d(fomo_ctx* ctx, bool elastic, const fomo_grid3d* gp, const float* vp, c
     if (resident < 1) return fail(ctx, FOMO_ECUDA, "z-marching 3D kernels do not fit an SM");
     zp = make_zm_plan(g, N, resident, zgrid);
   }
+  Fused3Plan fp;
+  if (fused) {
+    FOMO_CU(ctx, fused3_make_plan(fp, g, N, d_state, d_mat, ws_ptr<char>(ctx, o_bnd), st));
+    FOMO_CU(ctx, cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), st));
+  }
   int A = 0, B = 1, launches = 0;
   FOMO_CU(ctx, cudaEventRecord(ctx->ev0, st));
   for (int it = 1; it <= nt; ++it) {
     // velocity phase
-    if (elastic) {
+    if (fused) {
+      FOMO_CU(ctx, fused3_velocity(st, fp, g, d_state, A, B, c, dtdh, h, ctx->d_flag));
+    } else if (elastic) {
       El3 a;
       El3Out o;
       for (int f = 0; f < 9; ++f) {
@@ -929,7 +936,7 @@ int run3d(fomo_ctx* ctx, bool elastic, const fomo_grid3d* gp, const float* vp, c
       switch (N) { FOMO_AC3V(1) FOMO_AC3V(2) FOMO_AC3V(3) FOMO_AC3V(4) FOMO_AC3V(5) }
 #undef FOMO_AC3V
     }
-    if (fr.total > 0) {
+    if (fr.total > 0 && !fused) {
       FieldSet3 fs;
       FieldOut3 fo;
       fs.n = 3;
@@ -942,7 +949,9 @@ int run3d(fomo_ctx* ctx, bool elastic, const fomo_grid3d* gp, const float* vp, c
       habc3_passes(st, fblocks, g, fr, h, fs, fo, d_scr);
     }
     // stress / pressure phase
-    if (elastic) {
+    if (fused) {
+      FOMO_CU(ctx, fused3_stress(st, fp, g, d_state, A, B, c, dtdh, h, ctx->d_flag));
+    } else if (elastic) {
       El3 a;
       El3Out o;
       for (int f = 0; f < 9; ++f) {
@@ -971,7 +980,7 @@ int run3d(fomo_ctx* ctx, bool elastic, const fomo_grid3d* gp, const float* vp, c
       switch (N) { FOMO_AC3P(1) FOMO_AC3P(2) FOMO_AC3P(3) FOMO_AC3P(4) FOMO_AC3P(5) }
 #undef FOMO_AC3P
     }
-    if (fr.total > 0) {
+    if (fr.total > 0 && !fused) {
       FieldSet3 fs;
       FieldOut3 fo;
       fs.n = elastic ? 6 : 1;
@@ -989,7 +998,7 @@ int run3d(fomo_ctx* ctx, bool elastic, const fomo_grid3d* gp, const float* vp, c
                                         elastic ? field(B, 5) : nullptr, acq->n_rec, d_rec,
                                         field(B, 0), field(B, 1), field(B, 2), d_seis[0],
                                         d_seis[1], d_seis[2]);
-    launches += fr.total > 0 ? 7 : 3;
+    launches += (fr.total > 0 && !fused) ? 7 : 3;
     FOMO_CU(ctx, cudaGetLastError());
     if (d_snap && snap_interval > 0 && it % snap_interval == 0) {
       // snapshot of p (acoustic) / vz (elastic) on the plane (acoustic3d.jl:177-184)
@@ -1027,6 +1036,11 @@ int run3d(fomo_ctx* ctx, bool elastic, const fomo_grid3d* gp, const float* vp, c
                                      cudaMemcpyDeviceToHost, st));
   }
   FOMO_CU(ctx, cudaStreamSynchronize(st));
+  if (fused) {
+    int hflag = 0;
+    FOMO_CU(ctx, cudaMemcpy(&hflag, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost));
+    if (hflag) return fail(ctx, FOMO_ECUDA, "fused 3D half step: a bounded TMA wait timed out");
+  }
   float ms = 0.0f;
   FOMO_CU(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
   if (stats) {
@@ -1036,7 +1050,9 @@ int run3d(fomo_ctx* ctx, bool elastic, const fomo_grid3d* gp, const float* vp, c
     stats->alg_bytes = 4.0 * (double)g.nx * g.ny * g.nz * nt * (2.0 * nfield + nmat);
     stats->n_shots = 1;
     stats->gpu_launches = launches;
-    stats->kernel = zm_str ? FOMO_KERNEL_ZMARCH : (zm_vel ? FOMO_KERNEL_AUTO : FOMO_KERNEL_TWO_PHASE);
+    stats->kernel = fused ? FOMO_KERNEL_SINGLE_SWEEP
+                          : (zm_str ? FOMO_KERNEL_ZMARCH
+                                    : (zm_vel ? FOMO_KERNEL_AUTO : FOMO_KERNEL_TWO_PHASE));
   }
   return FOMO_OK;
 }

@@ -1,0 +1,55 @@
+// sweep3d.cuh -- 3D grid geometry and the fused, TMA-staged elastic3d half
+// steps (sweep3d.cu): each launch updates one field group (velocities or
+// stresses) and applies the Higdon boundary to it in the same pass.
+#pragma once
+#include <cuda.h>
+
+#include "fomo_internal.cuh"
+
+namespace fomo {
+
+// Padded 3D grid: x fastest, then y, then z; every field is one pitched volume.
+struct Geo3 {
+  int nx, ny, nz;       // padded
+  int ld;               // x pitch
+  long long sy, sz;     // strides of y and z (ld, ld*ny)
+  long long vol;        // sz * nz
+  int M, nbc;           // half stencil; HABC zone (pad - 1)
+};
+
+// Work split of the fused half steps.  A CTA of 32 x 16 threads owns a tile of
+// 30 x 14 output columns plus a one-column ring on every side (the ring's
+// updated values feed the Higdon terms of the tile's edge cells) and marches
+// down z.  Persistent CTAs (one per SM) take segments {tile x, tile y, z0, z1}
+// from a list through a counter in device memory.
+struct Fused3Plan {
+  int N = 0;
+  int ntx = 0, nty = 0;          // tiles in x and y
+  int grid = 0;                  // persistent CTAs
+  size_t smem_v = 0, smem_s = 0; // dynamic shared memory of the two kernels
+  int4* d_segs = nullptr;        // segments in the order they are handed out
+  int nseg = 0;
+  int* d_sched = nullptr;        // [next segment, CTAs done]; zero between launches
+  // tensor maps over the two field sets (4D: x, y, z, set * 9 + field) and the
+  // materials (x, y, z, material)
+  CUtensorMap c1, c3, c6, xh, yh, xyh, xyh3, m3, m5;
+};
+
+// Whether the fused form runs for half-stencil N (TMA tensor-map encoder present).
+bool fused3_supported(int N);
+// Device bytes of the segment table for grid g.
+size_t fused3_table_bytes(const Geo3& g);
+// Builds the plan for elastic state `state` (2 sets x 9 fields of g.vol
+// floats: vx vy vz txx tyy tzz txy txz tyz) and materials `mat` (8 volumes:
+// bx by bz lam l2m mxy mxz myz); d_table: fused3_table_bytes(g) bytes of
+// device memory, 256-byte aligned.  Synchronizes `st`.
+cudaError_t fused3_make_plan(Fused3Plan& p, const Geo3& g, int N, float* state, const float* mat,
+                             void* d_table, cudaStream_t st);
+// Velocity half step: set A -> B.v (update + Higdon).  Stress half step:
+// A.tau and B.v -> B.tau (update + Higdon).  err collects bounded-wait timeouts.
+cudaError_t fused3_velocity(cudaStream_t st, const Fused3Plan& p, const Geo3& g, float* state,
+                            int A, int B, const Coef& c, float dtdh, const HabcDev& h, int* err);
+cudaError_t fused3_stress(cudaStream_t st, const Fused3Plan& p, const Geo3& g, float* state,
+                          int A, int B, const Coef& c, float dtdh, const HabcDev& h, int* err);
+
+}  // namespace fomo

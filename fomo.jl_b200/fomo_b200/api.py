@@ -621,8 +621,9 @@ def elastic3d(vp, vs, rho, dh, dt, nt, f0, *, sx, sy, sz, rx, ry, rz, nbc: int =
     """3D elastic simulation (equations/elastic3d/elastic3d.jl:37-162).
 
     Returns ``(seis_vx, seis_vy, seis_vz, snaps)``; sources inject into txx,
-    tyy and tzz; snapshots hold vz.  ``kernel``: 0 or 3 = z-marching updates,
-    1 = per-cell updates (identical results).
+    tyy and tzz; snapshots hold vz.  ``kernel``: 0 or 2 = fused TMA half steps
+    (update and Higdon boundary in one pass each), 3 = z-marching updates with
+    separate Higdon passes, 1 = per-cell updates (identical results).
     """
     return _run3d(True, vp, vs, rho, dh, dt, nt, f0, sx, sy, sz, rx, ry, rz, nbc, fd_order,
                   snap_interval, snap_plane, snap_index, v_ref, wavelet, device, final_state,

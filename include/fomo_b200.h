@@ -67,10 +67,13 @@ extern "C" {
 /* fomo_opts.kernel: time-step kernel family (0 lets the autotuner pick) */
 #define FOMO_KERNEL_AUTO 0
 #define FOMO_KERNEL_TWO_PHASE 1    /* velocity sweep + stress sweep per step      */
-#define FOMO_KERNEL_SINGLE_SWEEP 2 /* one fused sweep per step (z-marching tiles) */
-#define FOMO_KERNEL_ZMARCH 3       /* 3D: z-marching velocity and stress updates;  */
-                                   /* TWO_PHASE = per-cell updates; AUTO = z-marching */
-                                   /* velocity + per-cell stress (stats: AUTO)        */
+#define FOMO_KERNEL_SINGLE_SWEEP 2 /* one fused sweep per step (z-marching tiles); */
+                                   /* elastic3d: two TMA-staged half steps per step,  */
+                                   /* each with its Higdon boundary fused (AUTO's     */
+                                   /* pick, stats: SINGLE_SWEEP)                      */
+#define FOMO_KERNEL_ZMARCH 3       /* 3D: z-marching velocity and stress updates and  */
+                                   /* two-pass Higdon kernels; TWO_PHASE = per-cell   */
+                                   /* updates (acoustic3d: always per-cell)           */
 #define FOMO_KERNEL_REPLICA 4      /* elastic2d(_batch): a CUDA C++ replica of the    */
                                    /* reference's CUDA.jl step (batch.jl:157-183:     */
                                    /* 8 launches, strip backups, frame scratch), a    */
