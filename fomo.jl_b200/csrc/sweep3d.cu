@@ -25,6 +25,7 @@
 
 #include <algorithm>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "sweep3d.cuh"
@@ -238,8 +239,12 @@ __global__ void __launch_bounds__(kNT, 1)
       }
       issued = gk + min(R, nit);
     }
-    // z windows: planes z0-1-N .. z0+N-2 here, plane z+N from each slot
-    float wa[2 * N + 1], wb[2 * N + 1], wc[2 * N + 1];
+    // z windows (length 2N + 3): in phase p of the three-iteration cycle, plane
+    // z's window is w[p .. p + 2N] and w[p + 2N] arrives from the slot; after
+    // phase 2 the window moves down by three entries.  The updated (U) and old
+    // (O) values of the last three planes rotate by phase as well, so the
+    // cycle's three bodies carry no register moves besides the window's.
+    float wa[2 * N + 3], wb[2 * N + 3], wc[2 * N + 3];
 #pragma unroll
     for (int k = 0; k < 2 * N; ++k) {
       const int z = z0 - 1 - N + k;
@@ -247,26 +252,28 @@ __global__ void __launch_bounds__(kNT, 1)
       wb[k] = ld3(g, w1, x, y, z);
       wc[k] = ld3(g, w2, x, y, z);
     }
-    float u1[NF], u2[NF], o1[NF], o2[NF];  // updated and old values of planes z-1, z-2
+    float U[3][NF], O[3][NF];
 #pragma unroll
-    for (int f = 0; f < NF; ++f) u1[f] = u2[f] = o1[f] = o2[f] = 0.0f;
+    for (int f = 0; f < NF; ++f) U[1][f] = U[2][f] = O[1][f] = O[2][f] = 0.0f;
     const int ce = r * kCW + t + shc;  // this thread's cell in a centre box
     int qp = q;                         // slot of the previous iteration (plane z - 1)
     int qp2 = q;                        // slot of plane z - 2 (refilled after this iteration's barrier)
-    float* tcur = tring;                // tile ring planes: z, z - 1
-    float* tprev = tring + NF * kNT;
-    float* tnext = tring + 2 * NF * kNT;
-    for (int i = 0; i < nit; ++i) {
+    auto body = [&](auto P, int i) {
+      constexpr int p = decltype(P)::value, p1 = (p + 2) % 3, p2 = (p + 1) % 3;
       const int z = z0 - 1 + i;
       const float* s = slots + q * SLOT;
       if (live) {
         live = tma::mbar_wait_bounded(&bars[q], ph, err);
         if (live) ok_upto = gk + i + 1;
       }
-      wa[2 * N] = s[WIN + ce];
-      wb[2 * N] = s[WIN + S::C + ce];
-      wc[2 * N] = s[WIN + 2 * S::C + ce];
-      float o[NF], u[NF];
+      float(&wA)[2 * N + 1] = *reinterpret_cast<float(*)[2 * N + 1]>(&wa[p]);
+      float(&wB)[2 * N + 1] = *reinterpret_cast<float(*)[2 * N + 1]>(&wb[p]);
+      float(&wC)[2 * N + 1] = *reinterpret_cast<float(*)[2 * N + 1]>(&wc[p]);
+      wA[2 * N] = s[WIN + ce];
+      wB[2 * N] = s[WIN + S::C + ce];
+      wC[2 * N] = s[WIN + 2 * S::C + ce];
+      float(&o)[NF] = O[p];
+      float(&u)[NF] = U[p];
 #pragma unroll
       for (int f = 0; f < NF; ++f) u[f] = o[f] = s[OLD + f * S::C + ce];
       if (in_xy && z >= N && z < g.nz - N) {
@@ -274,10 +281,10 @@ __global__ void __launch_bounds__(kNT, 1)
           const float* pvx = s + S::S_V + (r + N) * S::XW + t + shh;
           const float* pvy = pvx + S::XY;
           const float* pvz = pvx + 2 * S::XY;
-          const float dxx = sdp<N, 1>(pvx, c), dyy = sdp<N, S::XW>(pvy, c), dzz = wdm<N>(wc, c);
+          const float dxx = sdp<N, 1>(pvx, c), dyy = sdp<N, S::XW>(pvy, c), dzz = wdm<N>(wC, c);
           const float dxy = sdm<N, S::XW>(pvx, c), dyx = sdm<N, 1>(pvy, c);
-          const float dxz = wdp<N>(wa, c), dzx = sdm<N, 1>(pvz, c);
-          const float dyz = wdp<N>(wb, c), dzy = sdm<N, S::XW>(pvz, c);
+          const float dxz = wdp<N>(wA, c), dzx = sdm<N, 1>(pvz, c);
+          const float dyz = wdp<N>(wB, c), dzy = sdm<N, S::XW>(pvz, c);
           const float lm = s[S::S_MT + ce], l2 = s[S::S_MT + S::C + ce];
           u[0] = __fmaf_rn(__fmaf_rn(lm, dzz, __fmaf_rn(lm, dyy, __fmul_rn(l2, dxx))), dtdh, o[0]);
           u[1] = __fmaf_rn(__fmaf_rn(lm, dzz, __fmaf_rn(l2, dyy, __fmul_rn(lm, dxx))), dtdh, o[1]);
@@ -291,9 +298,9 @@ __global__ void __launch_bounds__(kNT, 1)
           const float* pxy = s + S::V_XY + (r + N) * S::XW + t + shh;
           const float* pyy = s + S::V_YY + (r + N) * kCW + t + shc;
           const float* pyz = s + S::V_YZ + (r + N) * kCW + t + shc;
-          const float a1 = sdm<N, 1>(pxx, c), a2 = sdp<N, S::XW>(pxy, c), a3 = wdm<N>(wa, c);
-          const float b1 = sdp<N, 1>(pxy, c), b2 = sdm<N, kCW>(pyy, c), b3 = wdm<N>(wb, c);
-          const float c1 = sdp<N, 1>(pxz, c), c2 = sdp<N, kCW>(pyz, c), c3 = wdp<N>(wc, c);
+          const float a1 = sdm<N, 1>(pxx, c), a2 = sdp<N, S::XW>(pxy, c), a3 = wdm<N>(wA, c);
+          const float b1 = sdp<N, 1>(pxy, c), b2 = sdm<N, kCW>(pyy, c), b3 = wdm<N>(wB, c);
+          const float c1 = sdp<N, 1>(pxz, c), c2 = sdp<N, kCW>(pyz, c), c3 = wdp<N>(wC, c);
           u[0] = __fmaf_rn(__fmul_rn(s[S::V_MB + ce], dtdh), __fadd_rn(__fadd_rn(a1, a2), a3), o[0]);
           u[1] = __fmaf_rn(__fmul_rn(s[S::V_MB + S::C + ce], dtdh),
                            __fadd_rn(__fadd_rn(b1, b2), b3), o[1]);
@@ -301,6 +308,8 @@ __global__ void __launch_bounds__(kNT, 1)
                            __fadd_rn(__fadd_rn(c1, c2), c3), o[2]);
         }
       }
+      float* tcur = tring + p * NF * kNT;   // tile ring planes by phase: z, z - 1
+      const float* tprev = tring + p1 * NF * kNT;
 #pragma unroll
       for (int f = 0; f < NF; ++f) tcur[f * kNT + tid] = u[f];
       __syncthreads();  // plane z's tile is complete; plane z-2's slot is free
@@ -312,6 +321,10 @@ __global__ void __launch_bounds__(kNT, 1)
       // finish plane z - 1: Higdon(updated, old) on frame cells, the update elsewhere
       const int zq = z - 1;
       if (i >= 1 && out_ok && zq >= z0) {
+        const float(&u1)[NF] = U[p1];
+        const float(&u2)[NF] = U[p2];
+        const float(&o1)[NF] = O[p1];
+        const float(&o2)[NF] = O[p2];
         float vv[NF];
 #pragma unroll
         for (int f = 0; f < NF; ++f) vv[f] = u1[f];
@@ -338,28 +351,25 @@ __global__ void __launch_bounds__(kNT, 1)
 #pragma unroll
         for (int f = 0; f < NF; ++f) ob[f * g.vol + oi] = vv[f];
       }
-#pragma unroll
-      for (int f = 0; f < NF; ++f) {
-        u2[f] = u1[f];
-        u1[f] = u[f];
-        o2[f] = o1[f];
-        o1[f] = o[f];
-      }
-#pragma unroll
-      for (int k = 0; k < 2 * N; ++k) {
-        wa[k] = wa[k + 1];
-        wb[k] = wb[k + 1];
-        wc[k] = wc[k + 1];
-      }
-      float* tt = tnext;
-      tnext = tprev;
-      tprev = tcur;
-      tcur = tt;
       qp2 = qp;
       qp = q;
       if (++q == R) {
         q = 0;
         ph ^= 1u;
+      }
+    };
+    for (int i = 0; i < nit;) {
+      body(std::integral_constant<int, 0>{}, i);
+      if (++i >= nit) break;
+      body(std::integral_constant<int, 1>{}, i);
+      if (++i >= nit) break;
+      body(std::integral_constant<int, 2>{}, i);
+      ++i;
+#pragma unroll
+      for (int k = 0; k < 2 * N; ++k) {
+        wa[k] = wa[k + 3];
+        wb[k] = wb[k + 3];
+        wc[k] = wc[k + 3];
       }
     }
     gk += nit;
