@@ -20,9 +20,14 @@
 #include <mutex>
 #include <string>
 #include <tuple>
+#include <type_traits>
 #include <vector>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "solver2d_kernels.cuh"
+#include "tma.cuh"
 
 namespace fomo {
 namespace {
@@ -108,6 +113,439 @@ __global__ void k_uinject_record(const UShot* __restrict__ shots, float* __restr
     seis[o + blk + r] = B[k];
     seis[o + 2 * blk + r] = B[sh.plane + k];
   }
+}
+
+// ---------------------------------------------------------------------------
+// Fused single-sweep form of the step: one launch per time step covers every
+// shot.  A CTA of NTX threads owns a strip of TXO = NTX - 2N - 2 output columns
+// of one shot plus N + 1 columns on each side, one column per thread, and
+// walks down z doing both half steps in one pass:
+//   velocity at row zv: v' = update(A.v, A.p); v'' = Higdon(v', A.v) one row
+//     behind (row zv - 1), its x neighbours from a shared-memory tile ring, its
+//     z neighbours from the thread's registers;
+//   pressure at row zp = zv - N - 1: p' = update(A.p, v''), reading vx'' rows
+//     from a shared ring (x derivative) and vz'' from a register window (z
+//     derivative); p'' = Higdon(p', A.p) one row behind.
+// The edge columns of the strip only feed the neighbours' stencils and Higdon
+// terms.  Every input row comes by TMA (per-shot tensor maps, no multicast)
+// into a ring of slots guarded by mbarriers with bounded waits; a slot is
+// refilled two rows after its use (its old-value boxes serve the next row's
+// Higdon terms).  Persistent CTAs take (shot, strip, z range) segments from a
+// list in order through a counter in device memory.  The arithmetic is the
+// two-phase kernels' per-cell sequence (ac_vel_at / ac_prs_at and the Higdon
+// edge and corner blends), so results are equal bit for bit.
+// ---------------------------------------------------------------------------
+struct AcShot {
+  long long st;     // state offset: set k field f at st + (3k + f) * plane (vx, vz, p)
+  long long mat;    // material offset: bx, bz, kappa at mat + f * plane
+  long long plane;  // ld * nz
+  int nx, nz, ld, unused;
+  float q, qt, qxt, unused2;
+};
+constexpr int kAcMaps = 5;  // per shot: state x-halo row, state row, state 2 rows, material row, 2 rows
+constexpr int kAcR = 6;     // TMA slots
+constexpr int kAcVK = 8;    // vx'' ring rows
+constexpr int kAcWt = 256;  // weight-table entries per kind staged in shared memory
+
+__host__ __device__ constexpr int ac_al32(int n) { return (n + 31) & ~31; }
+
+template <int N, int NTX>
+struct AcShape {
+  static constexpr int TXO = NTX - 2 * N - 2;            // output columns per strip
+  static constexpr int XW = (NTX + 2 * N + 3 + 3) & ~3;  // p row with x halos (+3 alignment)
+  static constexpr int CW = (NTX + 3 + 3) & ~3;          // row of the strip (+3 alignment)
+  static constexpr int S_PX = 0;                          // p, row zv, x halos
+  static constexpr int S_PW = S_PX + ac_al32(XW);         // p, row zv + N (z window entry)
+  static constexpr int S_AV = S_PW + ac_al32(CW);         // vx, vz, row zv
+  static constexpr int S_MB = S_AV + ac_al32(2 * CW);     // bx, bz, row zv
+  static constexpr int S_AP = S_MB + ac_al32(2 * CW);     // p, row zp
+  static constexpr int S_KP = S_AP + ac_al32(CW);         // kappa, row zp
+  static constexpr int SLOT = S_KP + ac_al32(CW);
+  static constexpr unsigned BYTES = 4u * (XW + 7 * CW);
+  static_assert(XW <= 256 && CW <= 256, "a TMA box row holds at most 256 elements");
+  static constexpr size_t smem() {
+    return (size_t)kAcR * SLOT * 4 + (size_t)(6 + 3 + kAcVK) * NTX * 4 + 3 * kAcWt * 4 +
+           (size_t)kAcR * 8;
+  }
+};
+
+__device__ __forceinline__ void ac_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z,
+                                           uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(tma::saddr(dst)),
+      "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(tma::saddr(bar))
+      : "memory");
+}
+
+// staggered sums over shared memory (element stride 1) and register windows
+template <int N>
+__device__ __forceinline__ float ac_sdm(const float* f, const Coef& c) {
+  float acc = 0.0f;
+#pragma unroll
+  for (int l = 1; l <= N; ++l) acc = __fmaf_rn(c.a[l - 1], __fsub_rn(f[l - 1], f[-l]), acc);
+  return acc;
+}
+template <int N>
+__device__ __forceinline__ float ac_sdp(const float* f, const Coef& c) {
+  float acc = 0.0f;
+#pragma unroll
+  for (int l = 1; l <= N; ++l) acc = __fmaf_rn(c.a[l - 1], __fsub_rn(f[l], f[1 - l]), acc);
+  return acc;
+}
+template <int N>
+__device__ __forceinline__ float ac_wdm(const float (&w)[2 * N + 1], const Coef& c) {
+  float acc = 0.0f;
+#pragma unroll
+  for (int l = 1; l <= N; ++l) acc = __fmaf_rn(c.a[l - 1], __fsub_rn(w[N + l - 1], w[N - l]), acc);
+  return acc;
+}
+template <int N>
+__device__ __forceinline__ float ac_wdp(const float (&w)[2 * N + 1], const Coef& c) {
+  float acc = 0.0f;
+#pragma unroll
+  for (int l = 1; l <= N; ++l) acc = __fmaf_rn(c.a[l - 1], __fsub_rn(w[N + l], w[N - l + 1]), acc);
+  return acc;
+}
+
+// the Higdon value of one field (kernels_det.jl:22-57): edge or corner blend of
+// the side terms toward the interior-ward neighbours
+__device__ __forceinline__ float ac_higdon(const HabcDev& h, float w, int sx, int sz, float fc,
+                                           float fo, float fx, float fox, float fz, float foz) {
+  if (sx != 0 && sz != 0)
+    return higdon_corner(w, fc, higdon_side(h, fx, fo, fox), higdon_side(h, fz, fo, foz));
+  if (sx != 0) return higdon_edge(w, fc, higdon_side(h, fx, fo, fox));
+  return higdon_edge(w, fc, higdon_side(h, fz, fo, foz));
+}
+
+template <int N, int NTX>
+__global__ void __launch_bounds__(NTX, NTX <= 128 ? 4 : 2) k_uac_sweep(const AcShot* __restrict__ shots,
+                                                 const CUtensorMap* __restrict__ maps,
+                                                 const int4* __restrict__ segs, int nseg,
+                                                 int* __restrict__ sched, float* __restrict__ state,
+                                                 Coef c, float dtx, float dtz,
+                                                 const float* __restrict__ wtab, int nbc,
+                                                 int wstride, int set, int* __restrict__ err) {
+  using S = AcShape<N, NTX>;
+  static_assert(N >= 2, "the pressure front trails the velocity front by N + 1 >= 3 rows");
+  constexpr int R = kAcR, D = N + 1, VK = kAcVK;
+  static_assert(D + 1 < VK, "vx'' ring depth");
+  extern __shared__ __align__(128) float sm[];
+  float* slots = sm;
+  float* vt = sm + R * S::SLOT;  // v' tile ring [3 rows][vx, vz][NTX]
+  float* pt = vt + 6 * NTX;      // p' tile ring [3 rows][NTX]
+  float* vr = pt + 3 * NTX;      // vx'' rows [VK][NTX]
+  float* s_wt = vr + VK * NTX;   // weight ramps of vx, vz, p [3][kAcWt]
+  uint64_t* bars = reinterpret_cast<uint64_t*>(s_wt + 3 * kAcWt);
+  __shared__ int s_next;
+  const int t = threadIdx.x;
+  if (t == 0) {
+    for (int k = 0; k < R; ++k) tma::mbar_init(&bars[k], 1);
+    tma::mbar_init_fence();
+  }
+  for (int k = t; k < 3 * kAcWt; k += NTX) {
+    const int kind = k / kAcWt, d = k % kAcWt;
+    s_wt[k] = d < wstride ? __ldg(wtab + kind * wstride + d) : 1.0f;
+  }
+  auto weight = [&](int kind, int dist) {
+    return dist < kAcWt ? s_wt[kind * kAcWt + dist]
+                        : (dist < wstride ? __ldg(wtab + kind * wstride + dist) : 1.0f);
+  };
+  const bool v_lane = t >= 1 && t <= NTX - 2;           // v'' (x neighbours in the strip)
+  const bool p_lane = t >= N && t <= NTX - N - 1;       // p' (vx'' x window in the strip)
+  const bool o_lane = t >= N + 1 && t <= NTX - N - 2;   // output columns
+  int q = 0;  // TMA slot of the current iteration
+  uint32_t ph = 0;
+  long long gk = 0, ok_upto = 0, issued = 0;
+  bool live = true;
+  float* const vr_end = vr + VK * NTX;
+  for (;;) {
+    __syncthreads();  // the previous segment's readers are done with every slot and ring
+    if (t == 0) s_next = atomicAdd(&sched[0], 1);
+    __syncthreads();
+    const int sgi = s_next;
+    if (sgi >= nseg) break;
+    const int4 sg = segs[sgi];  // {shot, first output column, z0, z1}
+    const AcShot sh = shots[sg.x];
+    const CUtensorMap* mp = maps + kAcMaps * sg.x;
+    const int X0 = sg.y, z0 = sg.z, z1 = sg.w;
+    const int nx = sh.nx, nz = sh.nz, ld = sh.ld;
+    const int xl = X0 - N - 1;  // column of lane 0
+    const int x = xl + t;
+    const int bxc = xl & ~3, shc = xl - bxc;
+    const int bxh = (xl - N) & ~3, shh = xl - bxh;
+    const int zs = z0 - N - 2;            // first velocity row
+    const int nit = z1 - z0 + D + N + 3;  // velocity rows zs .. z1 + D
+    const HabcDev h{sh.q, sh.qt, sh.qxt, nbc, wstride, wtab};
+    const float* A = state + sh.st + (long long)set * 3 * sh.plane;
+    float* B = state + sh.st + (long long)(1 - set) * 3 * sh.plane;
+    const int pl = (int)sh.plane;
+    const bool x_in = x >= N && x < nx - N;
+    // x part of the frame classification (kernels_fused.jl:28-52)
+    const bool fx = x >= 1 && x <= nx - 2;
+    const int sx = x <= nbc ? 1 : (x >= nx - 1 - nbc ? -1 : 0);
+    const int xdist = min(x, nx - 1 - x);
+    const bool v_out = o_lane && x < nx;
+    const int fa = set * 3;
+    auto issue = [&](int i, int slot) {
+      float* s = slots + slot * S::SLOT;
+      uint64_t* bar = &bars[slot];
+      const int zv = zs + i, zp = zv - D;
+      tma::mbar_expect_tx(bar, S::BYTES);
+      ac_load_3d(s + S::S_PX, mp + 0, bxh, zv, fa + 2, bar);
+      ac_load_3d(s + S::S_PW, mp + 1, bxc, zv + N, fa + 2, bar);
+      ac_load_3d(s + S::S_AV, mp + 2, bxc, zv, fa + 0, bar);
+      ac_load_3d(s + S::S_MB, mp + 4, bxc, zv, 0, bar);
+      ac_load_3d(s + S::S_AP, mp + 1, bxc, zp, fa + 2, bar);
+      ac_load_3d(s + S::S_KP, mp + 3, bxc, zp, 2, bar);
+    };
+    if (t == 0 && live) {
+      tma::fence_proxy_async();
+      int sl = q;
+      for (int i = 0; i < R && i < nit; ++i) {
+        issue(i, sl);
+        sl = sl + 1 == R ? 0 : sl + 1;
+      }
+      issued = gk + min(R, nit);
+    }
+    // z windows (length 2N + 3): in phase k of the three-row cycle the window of
+    // the current row is w[k .. k + 2N]; after phase 2 it moves down three rows.
+    // wp: p rows zv - N .. zv + N (velocity); wv: vz'' rows zp - N .. zp + N.
+    float wp[2 * N + 3], wv[2 * N + 3];
+    {
+      const float* pa = A + 2 * sh.plane;
+#pragma unroll
+      for (int k = 0; k < 2 * N; ++k) {
+        const int z = zs - N + k;
+        wp[k] = (x >= 0 && x < nx && z >= 0 && z < nz) ? __ldg(pa + (long long)z * ld + x) : 0.0f;
+        wv[k] = 0.0f;
+      }
+    }
+    // v', A.v, p', A.p of the last three rows, indexed by phase
+    float VX[3], VZ[3], AX[3], AZ[3], PP[3], AP[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) VX[k] = VZ[k] = AX[k] = AZ[k] = PP[k] = AP[k] = 0.0f;
+    const int ce = t + shc;
+    const float* s = slots + q * S::SLOT;  // boxes of the current iteration
+    const float* sp = s;                    // ... and of the previous one
+    int qp = q, qp2 = q;
+    float* vrw = vr + ((zs - 1) & (VK - 1)) * NTX + t;      // vx'' row zv - 1 (written)
+    const float* vrr = vr + ((zs - D) & (VK - 1)) * NTX + t;  // vx'' row zp (read)
+    int ov = (zs - 1) * ld + x;      // output offset of row zv - 1
+    int op = (zs - D - 1) * ld + x;  // ... and of row zp - 1
+    auto body = [&](auto P, int i) {
+      constexpr int p = decltype(P)::value, p1 = (p + 2) % 3, p2 = (p + 1) % 3;
+      const int zv = zs + i, zp = zv - D;
+      if (live) {
+        live = tma::mbar_wait_bounded(&bars[q], ph, err);
+        if (live) ok_upto = gk + i + 1;
+      }
+      float(&wpw)[2 * N + 1] = *reinterpret_cast<float(*)[2 * N + 1]>(&wp[p]);
+      float(&wvw)[2 * N + 1] = *reinterpret_cast<float(*)[2 * N + 1]>(&wv[p]);
+      wpw[2 * N] = s[S::S_PW + ce];
+      // velocity update, row zv (acoustic2d/fused_kernels.jl:27-63)
+      AX[p] = VX[p] = s[S::S_AV + ce];
+      AZ[p] = VZ[p] = s[S::S_AV + S::CW + ce];
+      if (x_in && zv >= N && zv < nz - N) {
+        const float dpdx = ac_sdm<N>(s + S::S_PX + t + shh, c);
+        const float dpdz = ac_wdp<N>(wpw, c);
+        VX[p] = __fmaf_rn(__fmul_rn(s[S::S_MB + ce], dtx), dpdx, VX[p]);
+        VZ[p] = __fmaf_rn(__fmul_rn(s[S::S_MB + S::CW + ce], dtz), dpdz, VZ[p]);
+      }
+      // pressure update, row zp (fused_kernels.jl:86-114)
+      AP[p] = PP[p] = s[S::S_AP + ce];
+      if (p_lane && x_in && zp >= N && zp < nz - N) {
+        const float dvxdx = ac_sdp<N>(vrr, c);
+        const float dvzdz = ac_wdm<N>(wvw, c);
+        PP[p] = __fmaf_rn(s[S::S_KP + ce], __fmaf_rn(dvxdx, dtx, __fmul_rn(dvzdz, dtz)), PP[p]);
+      }
+      vt[p * 2 * NTX + t] = VX[p];
+      vt[p * 2 * NTX + NTX + t] = VZ[p];
+      pt[p * NTX + t] = PP[p];
+      __syncthreads();  // rows zv (v') and zp (p') are complete; the slot of i-2 is free
+      if (t == 0 && live && i >= 2 && i + R - 2 < nit) {
+        tma::fence_proxy_async();
+        issue(i + R - 2, qp2);
+        issued = gk + i + R - 1;
+      }
+      // v'' of row zv - 1 (kernels_det.jl:22-57 on the velocity frame)
+      if (i >= 1) {
+        const int zq = zv - 1;
+        float ux = VX[p1], uz = VZ[p1];
+        if (v_lane && fx && zq >= 1 && zq <= nz - 2) {
+          const int sz = zq <= nbc ? 1 : (zq >= nz - 1 - nbc ? -1 : 0);
+          if (sx | sz) {
+            const int dist = min(xdist, min(zq, nz - 1 - zq));
+            const float* vrow = vt + p1 * 2 * NTX + t;
+            const float* arow = sp + S::S_AV + ce;
+            ux = ac_higdon(h, weight(0, dist), sx, sz, ux, AX[p1], vrow[sx], arow[sx],
+                           sz > 0 ? VX[p] : VX[p2], sz > 0 ? AX[p] : AX[p2]);
+            uz = ac_higdon(h, weight(1, dist), sx, sz, uz, AZ[p1], vrow[NTX + sx],
+                           arow[S::CW + sx], sz > 0 ? VZ[p] : VZ[p2], sz > 0 ? AZ[p] : AZ[p2]);
+          }
+        }
+        *vrw = ux;
+        wvw[2 * N] = uz;
+        if (v_out && zq >= z0 && zq < z1) {
+          B[ov] = ux;
+          B[pl + ov] = uz;
+        }
+      }
+      // p'' of row zp - 1
+      if (i >= 1 && o_lane) {
+        const int zq = zp - 1;
+        float u = PP[p1];
+        if (fx && zq >= 1 && zq <= nz - 2) {
+          const int sz = zq <= nbc ? 1 : (zq >= nz - 1 - nbc ? -1 : 0);
+          if (sx | sz) {
+            const int dist = min(xdist, min(zq, nz - 1 - zq));
+            u = ac_higdon(h, weight(2, dist), sx, sz, u, AP[p1], pt[p1 * NTX + t + sx],
+                          sp[S::S_AP + ce + sx], sz > 0 ? PP[p] : PP[p2], sz > 0 ? AP[p] : AP[p2]);
+          }
+        }
+        if (x < nx && zq >= z0 && zq < z1) B[2 * pl + op] = u;
+      }
+      // advance rings, offsets and slots
+      vrw += NTX;
+      if (vrw >= vr_end) vrw -= VK * NTX;
+      vrr += NTX;
+      if (vrr >= vr_end) vrr -= VK * NTX;
+      ov += ld;
+      op += ld;
+      sp = s;
+      qp2 = qp;
+      qp = q;
+      if (++q == R) {
+        q = 0;
+        ph ^= 1u;
+        s = slots;
+      } else {
+        s += S::SLOT;
+      }
+    };
+    for (int i = 0; i < nit;) {
+      body(std::integral_constant<int, 0>{}, i);
+      if (++i >= nit) break;
+      body(std::integral_constant<int, 1>{}, i);
+      if (++i >= nit) break;
+      body(std::integral_constant<int, 2>{}, i);
+      ++i;
+#pragma unroll
+      for (int k = 0; k < 2 * N; ++k) {
+        wp[k] = wp[k + 3];
+        wv[k] = wv[k + 3];
+      }
+    }
+    gk += nit;
+  }
+  if (t == 0 && !live)
+    for (long long k = ok_upto; k < issued; ++k)
+      tma::mbar_wait_bounded(&bars[k % R], (uint32_t)((k / R) & 1), err);
+  if (t == 0) {  // the last CTA to finish rearms the counter for the next launch
+    __threadfence();
+    if (atomicAdd(&sched[1], 1) == (int)gridDim.x - 1) {
+      sched[0] = 0;
+      sched[1] = 0;
+      __threadfence();
+    }
+  }
+}
+
+// ---- fused sweep: host side ----
+PFN_cuTensorMapEncodeTiled_v12000 g_acenc = nullptr;
+std::once_flag g_acenc_once;
+PFN_cuTensorMapEncodeTiled_v12000 ac_encoder() {
+  std::call_once(g_acenc_once, [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_acenc = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    else
+      cudaGetLastError();
+  });
+  return g_acenc;
+}
+
+constexpr int kAcNTX[] = {128, 224};  // strip widths the autotuner tries (threads per CTA; a
+                                      // row box of the widest holds 224 + 2N + 3 <= 256 columns)
+constexpr int kAcNumNTX = 2;
+
+template <int N, int NTX>
+cudaError_t ac_launch_t(cudaStream_t st, int grid, const AcShot* shots, const CUtensorMap* maps,
+                        const int4* segs, int nseg, int* sched, float* state, const Coef& c,
+                        float dtdh, const float* wtab, int nbc, int wstride, int set, int* err) {
+  auto kern = k_uac_sweep<N, NTX>;
+  static std::once_flag once;
+  static cudaError_t attr = cudaSuccess;
+  std::call_once(once, [&] {
+    attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)AcShape<N, NTX>::smem());
+  });
+  if (attr != cudaSuccess) return attr;
+  kern<<<grid, NTX, AcShape<N, NTX>::smem(), st>>>(shots, maps, segs, nseg, sched, state, c, dtdh,
+                                                   dtdh, wtab, nbc, wstride, set, err);
+  return cudaGetLastError();
+}
+
+template <int N, int NTX>
+int ac_resident() {
+  int nb = 0, dev = 0, nsm = 148;
+  if (cudaFuncSetAttribute(k_uac_sweep<N, NTX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)AcShape<N, NTX>::smem()) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_uac_sweep<N, NTX>, NTX,
+                                                    AcShape<N, NTX>::smem()) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  return nb * nsm;
+}
+
+// Dispatch over (N, strip width): the launch, the resident CTA count, the strip's
+// output columns and the box widths of its tensor maps.
+struct AcForm {
+  int resident = 0, txo = 0, xw = 0, cw = 0;
+};
+template <int N, int NTX>
+AcForm ac_form_t() {
+  using S = AcShape<N, NTX>;
+  return AcForm{ac_resident<N, NTX>(), S::TXO, S::XW, S::CW};
+}
+AcForm ac_form(int N, int k) {
+#define FOMO_ACF(NN)                                                       \
+  case NN:                                                                 \
+    return k == 0 ? ac_form_t<NN, 128>() : ac_form_t<NN, 224>();
+  switch (N) { FOMO_ACF(2) FOMO_ACF(3) FOMO_ACF(4) FOMO_ACF(5) }
+#undef FOMO_ACF
+  return AcForm{};
+}
+cudaError_t ac_launch(int N, int k, cudaStream_t st, int grid, const AcShot* shots,
+                      const CUtensorMap* maps, const int4* segs, int nseg, int* sched,
+                      float* state, const Coef& c, float dtdh, const float* wtab, int nbc,
+                      int wstride, int set, int* err) {
+#define FOMO_ACL(NN)                                                                          \
+  case NN:                                                                                    \
+    return k == 0 ? ac_launch_t<NN, 128>(st, grid, shots, maps, segs, nseg, sched, state, c, \
+                                         dtdh, wtab, nbc, wstride, set, err)                  \
+                  : ac_launch_t<NN, 224>(st, grid, shots, maps, segs, nseg, sched, state, c, \
+                                         dtdh, wtab, nbc, wstride, set, err);
+  switch (N) { FOMO_ACL(2) FOMO_ACL(3) FOMO_ACL(4) FOMO_ACL(5) }
+#undef FOMO_ACL
+  return cudaErrorInvalidValue;
+}
+
+CUresult ac_encode(CUtensorMap* m, const float* base, int nx, int nz, int ld, long long plane,
+                   int nplanes, int bw, int bp) {
+  cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)nz, (cuuint64_t)nplanes};
+  cuuint64_t strides[2] = {(cuuint64_t)ld * 4, (cuuint64_t)plane * 4};
+  cuuint32_t box[3] = {(cuuint32_t)bw, 1, (cuuint32_t)bp};
+  cuuint32_t es[3] = {1, 1, 1};
+  return ac_encoder()(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims,
+                      strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                      CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
 }
 
 struct Tile {
@@ -272,6 +710,13 @@ int run_uneven(fomo_ctx* ctx, float dh, float dt, int nt, int nbc, int fd_order,
   const size_t o_tab = ar.take<UShot>(ns);
   const size_t o_tiles = ar.take<int>(max_tiles);
   const size_t o_w = ar.take<float>(wt_ref.size());
+  // fused sweep: shot table, five tensor maps per shot, segment list, counter
+  long long max_seg = 3LL * 4096;
+  for (int s = 0; s < ns; ++s) max_seg += (tab[s].nx + 63) / 64;
+  const size_t o_ashot = ar.take<AcShot>(ns);
+  const size_t o_maps = ar.take<CUtensorMap>((size_t)kAcMaps * ns);
+  const size_t o_segs = ar.take<int4>(max_seg);
+  const size_t o_sched = ar.take<int>(2);
   int rc;
   if ((rc = ensure_workspace(ctx, ar.off))) return rc;
   float* d_state = ws_ptr<float>(ctx, o_state);
@@ -310,6 +755,102 @@ int run_uneven(fomo_ctx* ctx, float dh, float dt, int nt, int nbc, int fd_order,
 
   Coef c;
   for (int l = 0; l < 5; ++l) c.a[l] = kFD[N][l];
+
+  // ---- fused single sweep (the default from order 4): strip width autotuned ----
+  const char* env_sweep = std::getenv("FOMO_UNEVEN_SWEEP");
+  const bool fused = N >= 2 && ac_encoder() && !std::getenv("FOMO_UNEVEN_TILE") &&
+                     !(opts && opts->kernel == FOMO_KERNEL_TWO_PHASE);
+  AcShot* d_ashot = ws_ptr<AcShot>(ctx, o_ashot);
+  CUtensorMap* d_maps = ws_ptr<CUtensorMap>(ctx, o_maps);
+  int4* d_segs = ws_ptr<int4>(ctx, o_segs);
+  int* d_sched = ws_ptr<int>(ctx, o_sched);
+  int a_grid = 0, a_nseg = 0, a_k = -1;
+  // Builds the tables of strip width kAcNTX[k]; returns FOMO_OK or a negative
+  // code, and a_grid = 0 when that width does not fit an SM.
+  auto ac_build = [&](int k) -> int {
+    const AcForm f = ac_form(N, k);
+    a_grid = 0;
+    if (f.resident < 1) return FOMO_OK;
+    std::vector<AcShot> at(ns);
+    std::vector<CUtensorMap> mh((size_t)kAcMaps * ns);
+    std::vector<int4> sg;
+    for (int s = 0; s < ns; ++s) {
+      const UShot& u = tab[s];
+      at[s] = AcShot{u.st, u.mat, u.plane, u.nx, u.nz, u.ld, 0, u.q, u.qt, u.qxt, 0.0f};
+      const float* bs = d_state + u.st;
+      const float* bm = d_mat + u.mat;
+      CUresult r = ac_encode(&mh[kAcMaps * s + 0], bs, u.nx, u.nz, u.ld, u.plane, 6, f.xw, 1);
+      if (r == CUDA_SUCCESS) r = ac_encode(&mh[kAcMaps * s + 1], bs, u.nx, u.nz, u.ld, u.plane, 6, f.cw, 1);
+      if (r == CUDA_SUCCESS) r = ac_encode(&mh[kAcMaps * s + 2], bs, u.nx, u.nz, u.ld, u.plane, 6, f.cw, 2);
+      if (r == CUDA_SUCCESS) r = ac_encode(&mh[kAcMaps * s + 3], bm, u.nx, u.nz, u.ld, u.plane, 3, f.cw, 1);
+      if (r == CUDA_SUCCESS) r = ac_encode(&mh[kAcMaps * s + 4], bm, u.nx, u.nz, u.ld, u.plane, 3, f.cw, 2);
+      if (r != CUDA_SUCCESS) return fail(ctx, FOMO_ECUDA, "uneven sweep: tensor map encoding failed");
+      for (int x0 = 0; x0 < u.nx; x0 += f.txo) sg.push_back(make_int4(s, x0, 0, u.nz));
+    }
+    // the last wave of strips is cut into four z chunks (chunk-major) so that
+    // the persistent CTAs finish together
+    a_grid = std::min<int>(f.resident, (int)sg.size());
+    const int L = std::min<int>(a_grid, (int)sg.size());
+    std::vector<int4> tail(sg.end() - L, sg.end());
+    sg.resize(sg.size() - L);
+    for (int k2 = 0; k2 < 4; ++k2)
+      for (const int4& e : tail) {
+        const int za = (int)((long long)e.w * k2 / 4), zb = (int)((long long)e.w * (k2 + 1) / 4);
+        if (zb > za) sg.push_back(make_int4(e.x, e.y, za, zb));
+      }
+    if ((long long)sg.size() > max_seg) return fail(ctx, FOMO_ECUDA, "uneven sweep: segment table");
+    a_nseg = (int)sg.size();
+    FOMO_CU(ctx, cudaMemcpyAsync(d_ashot, at.data(), sizeof(AcShot) * ns, cudaMemcpyHostToDevice, st));
+    FOMO_CU(ctx, cudaMemcpyAsync(d_maps, mh.data(), sizeof(CUtensorMap) * mh.size(),
+                                 cudaMemcpyHostToDevice, st));
+    FOMO_CU(ctx, cudaMemcpyAsync(d_segs, sg.data(), sizeof(int4) * sg.size(), cudaMemcpyHostToDevice, st));
+    FOMO_CU(ctx, cudaMemsetAsync(d_sched, 0, 2 * sizeof(int), st));
+    FOMO_CU(ctx, cudaStreamSynchronize(st));  // host tables change before the next build
+    return FOMO_OK;
+  };
+  auto ac_step = [&](cudaStream_t s2, int set) {
+    return ac_launch(N, a_k, s2, a_grid, d_ashot, d_maps, d_segs, a_nseg, d_sched, d_state, c,
+                     dtdh, d_w, zone, wstride, set, ctx->d_flag);
+  };
+  if (fused) {
+    FOMO_CU(ctx, cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), st));
+    int pin = -1;
+    if (env_sweep)
+      for (int k = 0; k < kAcNumNTX; ++k)
+        if (std::atoi(env_sweep) == kAcNTX[k]) pin = k;
+    const UKey key{-N, ns, cells};  // negative order: the fused form's cache entries
+    if (pin < 0) {
+      std::lock_guard<std::mutex> lk(g_umu);
+      auto it = g_utune.find(key);
+      if (it != g_utune.end()) pin = it->second;
+    }
+    if (pin < 0) {  // time each strip width on three steps of the zero state
+      FOMO_CU(ctx, cudaMemsetAsync(d_state, 0, 4 * off_state, st));
+      float best = 1e30f;
+      for (int k = 0; k < kAcNumNTX; ++k) {
+        if ((rc = ac_build(k))) return rc;
+        if (a_grid < 1) continue;
+        a_k = k;
+        FOMO_CU(ctx, ac_step(st, 0));
+        FOMO_CU(ctx, cudaEventRecord(ctx->ev0, st));
+        for (int r = 0; r < 3; ++r) FOMO_CU(ctx, ac_step(st, r & 1));
+        FOMO_CU(ctx, cudaEventRecord(ctx->ev1, st));
+        FOMO_CU(ctx, cudaEventSynchronize(ctx->ev1));
+        float ms = 0.0f;
+        FOMO_CU(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+        if (ms < best) {
+          best = ms;
+          pin = k;
+        }
+      }
+      if (pin < 0) return fail(ctx, FOMO_ECUDA, "uneven sweep: no strip width fits an SM");
+      std::lock_guard<std::mutex> lk(g_umu);
+      g_utune[key] = pin;
+    }
+    if ((rc = ac_build(pin))) return rc;
+    if (a_grid < 1) return fail(ctx, FOMO_ECUDA, "uneven sweep: the strip width does not fit an SM");
+    a_k = pin;
+  }
   std::vector<int> tile_shot;
   auto upload_tiles = [&](int k) -> int {
     tiles_for(kTiles[k], tile_shot);
@@ -320,7 +861,7 @@ int run_uneven(fomo_ctx* ctx, float dh, float dt, int nt, int nbc, int fd_order,
     return FOMO_OK;
   };
 
-  if (tsel < 0) {  // time each tile shape on three steps of the zero state
+  if (!fused && tsel < 0) {  // time each tile shape on three steps of the zero state
     FOMO_CU(ctx, cudaMemsetAsync(d_state, 0, 4 * off_state, st));
     float best = 1e30f;
     for (int k = 0; k < kNumTiles; ++k) {
@@ -344,9 +885,13 @@ int run_uneven(fomo_ctx* ctx, float dh, float dt, int nt, int nbc, int fd_order,
     std::lock_guard<std::mutex> lk(g_umu);
     g_utune[key] = tsel;
   }
-  if ((rc = upload_tiles(tsel))) return rc;
+  if (!fused && (rc = upload_tiles(tsel))) return rc;
+  if (fused) {  // the inject / record kernel reads the shot table
+    FOMO_CU(ctx, cudaMemcpyAsync(d_tab, tab.data(), sizeof(UShot) * ns, cudaMemcpyHostToDevice, st));
+    FOMO_CU(ctx, cudaStreamSynchronize(st));
+  }
   const int nblk = (int)tile_shot.size();
-  const Tile t = kTiles[tsel];
+  const Tile t = fused ? Tile{0, 0} : kTiles[tsel];
 
   // ---- zero state, capture the whole run, replay it once ----
   FOMO_CU(ctx, cudaMemsetAsync(d_state, 0, 4 * off_state, st));
@@ -360,7 +905,17 @@ int run_uneven(fomo_ctx* ctx, float dh, float dt, int nt, int nbc, int fd_order,
   FOMO_CU(ctx, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
   for (int it = 1; it <= nt; ++it) {
     const int A = (it - 1) & 1;
-    launch_step_n(N, cs, nblk, t, d_tab, d_tiles, d_state, d_mat, c, dtdh, d_w, zone, wstride, A);
+    if (fused) {
+      const cudaError_t e = ac_step(cs, A);
+      if (e != cudaSuccess) {
+        cudaGraph_t g0 = nullptr;
+        cudaStreamEndCapture(cs, &g0);
+        if (g0) cudaGraphDestroy(g0);
+        return cuda_fail(ctx, e, "uneven sweep launch");
+      }
+    } else {
+      launch_step_n(N, cs, nblk, t, d_tab, d_tiles, d_state, d_mat, c, dtdh, d_w, zone, wstride, A);
+    }
     k_uinject_record<<<ns, 256, 0, cs>>>(d_tab, d_state, d_src, d_wav, d_rec, d_seis, it, nt, 1 - A);
   }
   cudaError_t ce = cudaStreamEndCapture(cs, &graph);
@@ -379,6 +934,11 @@ int run_uneven(fomo_ctx* ctx, float dh, float dt, int nt, int nbc, int fd_order,
   if (ce != cudaSuccess) return cuda_fail(ctx, ce, "uneven-batch graph launch");
   float ms = 0.0f;
   FOMO_CU(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  if (fused) {
+    int hflag = 0;
+    FOMO_CU(ctx, cudaMemcpy(&hflag, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost));
+    if (hflag) return fail(ctx, FOMO_ECUDA, "uneven sweep: a bounded TMA wait timed out");
+  }
 
   // ---- seismograms back to each shot's buffers ----
   for (int s = 0; s < ns; ++s) {
@@ -398,9 +958,9 @@ int run_uneven(fomo_ctx* ctx, float dh, float dt, int nt, int nbc, int fd_order,
     // acoustic: vx, vz, p read and written + bx, bz, kappa read = 9 words per cell
     stats->alg_bytes = 36.0 * (double)cells * nt;
     stats->n_shots = ns;
-    stats->gpu_launches = 3 * nt;
-    stats->kernel = FOMO_KERNEL_TWO_PHASE;
-    stats->sweep_config = t.bx * 1000 + t.by;
+    stats->gpu_launches = (fused ? 2 : 3) * nt;
+    stats->kernel = fused ? FOMO_KERNEL_SINGLE_SWEEP : FOMO_KERNEL_TWO_PHASE;
+    stats->sweep_config = fused ? kAcNTX[a_k] * 1000 : t.bx * 1000 + t.by;
   }
   return FOMO_OK;
 }

@@ -485,7 +485,8 @@ class Acoustic2DUnevenResult(NamedTuple):
 
 def acoustic2d_uneven(vps, rhos, dh, dt, nt, f0, *, sx, sz, rx, rz, nbc: int = 50,
                       fd_order: int = 8, v_ref=None, wavelet=None,
-                      scale_source_by_dt: bool = False, device: int = 0) -> Acoustic2DUnevenResult:
+                      scale_source_by_dt: bool = False, device: int = 0,
+                      kernel: int = 0) -> Acoustic2DUnevenResult:
     """Many acoustic2d shots whose models differ in size, stepped together.
 
     ``vps``/``rhos``: one (nx_s, nz_s) model per shot; ``sx``/``sz``: per shot
@@ -493,6 +494,9 @@ def acoustic2d_uneven(vps, rhos, dh, dt, nt, f0, *, sx, sz, rx, rz, nbc: int = 5
     receiver indices; ``v_ref``: None (each shot's min positive vp), a number,
     or one value per shot.  Each shot's seismograms equal ``acoustic2d`` on
     that shot (equations/acoustic2d/acoustic2d.jl:47-192) bit for bit.
+    ``kernel``: 0 = the fused single sweep from order 4 (one launch per step
+    for all shots), 1 = velocity and pressure kernels per step.  ``stats.tile``
+    is (threads per strip, 0) for the sweep, the (x, z) block for two kernels.
     """
     ns = len(vps)
     if ns == 0 or len(rhos) != ns or len(sx) != ns or len(sz) != ns or len(rx) != ns \
@@ -533,7 +537,7 @@ def acoustic2d_uneven(vps, rhos, dh, dt, nt, f0, *, sx, sz, rx, rz, nbc: int = 5
         results.append(tuple(seis))
     st = L.Stats()
     ctx = L.context(device)
-    o = _opts()
+    o = _opts(kernel)
     ctx.check(L.lib().fomo_acoustic2d_uneven(ctx.handle, float(dh), float(dt), int(nt), int(nbc),
                                              int(fd_order), ns, descs, C.byref(o), C.byref(st)))
     _remember(st)
