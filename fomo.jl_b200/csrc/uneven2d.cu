@@ -143,7 +143,7 @@ struct AcShot {
   float q, qt, qxt, unused2;
 };
 constexpr int kAcMaps = 5;  // per shot: state x-halo row, state row, state 2 rows, material row, 2 rows
-constexpr int kAcR = 6;     // TMA slots
+constexpr int kAcR = 4;     // TMA slots (two rows each)
 constexpr int kAcVK = 8;    // vx'' ring rows
 constexpr int kAcWt = 256;  // weight-table entries per kind staged in shared memory
 
@@ -154,17 +154,18 @@ struct AcShape {
   static constexpr int TXO = NTX - 2 * N - 2;            // output columns per strip
   static constexpr int XW = (NTX + 2 * N + 3 + 3) & ~3;  // p row with x halos (+3 alignment)
   static constexpr int CW = (NTX + 3 + 3) & ~3;          // row of the strip (+3 alignment)
-  static constexpr int S_PX = 0;                          // p, row zv, x halos
-  static constexpr int S_PW = S_PX + ac_al32(XW);         // p, row zv + N (z window entry)
-  static constexpr int S_AV = S_PW + ac_al32(CW);         // vx, vz, row zv
-  static constexpr int S_MB = S_AV + ac_al32(2 * CW);     // bx, bz, row zv
-  static constexpr int S_AP = S_MB + ac_al32(2 * CW);     // p, row zp
-  static constexpr int S_KP = S_AP + ac_al32(CW);         // kappa, row zp
-  static constexpr int SLOT = S_KP + ac_al32(CW);
-  static constexpr unsigned BYTES = 4u * (XW + 7 * CW);
+  // one slot = the boxes of one iteration (two rows each; [plane][row][x])
+  static constexpr int S_PX = 0;                          // p, rows zv, zv+1, x halos
+  static constexpr int S_PW = S_PX + ac_al32(2 * XW);     // p, rows zv+N, zv+N+1 (z window)
+  static constexpr int S_AV = S_PW + ac_al32(2 * CW);     // vx, vz, rows zv, zv+1
+  static constexpr int S_MB = S_AV + ac_al32(4 * CW);     // bx, bz, rows zv, zv+1
+  static constexpr int S_AP = S_MB + ac_al32(4 * CW);     // p, rows zp, zp+1
+  static constexpr int S_KP = S_AP + ac_al32(2 * CW);     // kappa, rows zp, zp+1
+  static constexpr int SLOT = S_KP + ac_al32(2 * CW);
+  static constexpr unsigned BYTES = 4u * (2 * XW + 14 * CW);
   static_assert(XW <= 256 && CW <= 256, "a TMA box row holds at most 256 elements");
   static constexpr size_t smem() {
-    return (size_t)kAcR * SLOT * 4 + (size_t)(6 + 3 + kAcVK) * NTX * 4 + 3 * kAcWt * 4 +
+    return (size_t)kAcR * SLOT * 4 + (size_t)(12 + 6 + kAcVK) * NTX * 4 + 3 * kAcWt * 4 +
            (size_t)kAcR * 8;
   }
 };
@@ -227,14 +228,21 @@ __global__ void __launch_bounds__(NTX, NTX <= 128 ? 4 : 2) k_uac_sweep(const AcS
                                                  const float* __restrict__ wtab, int nbc,
                                                  int wstride, int set, int* __restrict__ err) {
   using S = AcShape<N, NTX>;
-  static_assert(N >= 2, "the pressure front trails the velocity front by N + 1 >= 3 rows");
-  constexpr int R = kAcR, D = N + 1, VK = kAcVK;
-  static_assert(D + 1 < VK, "vx'' ring depth");
+  // Two rows per iteration.  The pressure rows trail the velocity rows by D:
+  // their vz'' window (own registers) must be finished one iteration earlier
+  // (D >= N + 2) and their vx'' rows, which other threads write after the
+  // barrier, two iterations earlier (D >= 5).
+  constexpr int R = kAcR, D = (N + 2 > 5 ? N + 2 : 5), VK = kAcVK;
+  constexpr int WV = D + N + 1;  // vz'' window: rows zp - N .. zv
+  // vx'' ring: rows written after one barrier and rows read before the next
+  // never share an entry (D mod VK not in 2..4), and a row read is not yet
+  // replaced (VK > D - 2)
+  static_assert(VK > D - 2 && D % VK != 2 && D % VK != 3 && D % VK != 4, "vx'' ring depth");
   extern __shared__ __align__(128) float sm[];
   float* slots = sm;
-  float* vt = sm + R * S::SLOT;  // v' tile ring [3 rows][vx, vz][NTX]
-  float* pt = vt + 6 * NTX;      // p' tile ring [3 rows][NTX]
-  float* vr = pt + 3 * NTX;      // vx'' rows [VK][NTX]
+  float* vt = sm + R * S::SLOT;  // v' tile ring [3 iterations][2 rows][vx, vz][NTX]
+  float* pt = vt + 12 * NTX;     // p' tile ring [3 iterations][2 rows][NTX]
+  float* vr = pt + 6 * NTX;      // vx'' rows [VK][NTX]
   float* s_wt = vr + VK * NTX;   // weight ramps of vx, vz, p [3][kAcWt]
   uint64_t* bars = reinterpret_cast<uint64_t*>(s_wt + 3 * kAcWt);
   __shared__ int s_next;
@@ -258,7 +266,6 @@ __global__ void __launch_bounds__(NTX, NTX <= 128 ? 4 : 2) k_uac_sweep(const AcS
   uint32_t ph = 0;
   long long gk = 0, ok_upto = 0, issued = 0;
   bool live = true;
-  float* const vr_end = vr + VK * NTX;
   for (;;) {
     __syncthreads();  // the previous segment's readers are done with every slot and ring
     if (t == 0) s_next = atomicAdd(&sched[0], 1);
@@ -274,8 +281,9 @@ __global__ void __launch_bounds__(NTX, NTX <= 128 ? 4 : 2) k_uac_sweep(const AcS
     const int x = xl + t;
     const int bxc = xl & ~3, shc = xl - bxc;
     const int bxh = (xl - N) & ~3, shh = xl - bxh;
-    const int zs = z0 - N - 2;            // first velocity row
-    const int nit = z1 - z0 + D + N + 3;  // velocity rows zs .. z1 + D
+    const int zs = z0 - N - 2;  // first velocity row
+    // the last iteration finishes pressure row z1 - 1 (zp >= z1 - 1)
+    const int nit = (z1 - 1 + D - zs + 1) / 2 + 1;
     const HabcDev h{sh.q, sh.qt, sh.qxt, nbc, wstride, wtab};
     const float* A = state + sh.st + (long long)set * 3 * sh.plane;
     float* B = state + sh.st + (long long)(1 - set) * 3 * sh.plane;
@@ -290,7 +298,7 @@ __global__ void __launch_bounds__(NTX, NTX <= 128 ? 4 : 2) k_uac_sweep(const AcS
     auto issue = [&](int i, int slot) {
       float* s = slots + slot * S::SLOT;
       uint64_t* bar = &bars[slot];
-      const int zv = zs + i, zp = zv - D;
+      const int zv = zs + 2 * i, zp = zv - D;
       tma::mbar_expect_tx(bar, S::BYTES);
       ac_load_3d(s + S::S_PX, mp + 0, bxh, zv, fa + 2, bar);
       ac_load_3d(s + S::S_PW, mp + 1, bxc, zv + N, fa + 2, bar);
@@ -308,110 +316,138 @@ __global__ void __launch_bounds__(NTX, NTX <= 128 ? 4 : 2) k_uac_sweep(const AcS
       }
       issued = gk + min(R, nit);
     }
-    // z windows (length 2N + 3): in phase k of the three-row cycle the window of
-    // the current row is w[k .. k + 2N]; after phase 2 it moves down three rows.
-    // wp: p rows zv - N .. zv + N (velocity); wv: vz'' rows zp - N .. zp + N.
-    float wp[2 * N + 3], wv[2 * N + 3];
+    // z windows: wp[k] = p row zv - N + k (k < 2N + 2), for the velocity's z
+    // derivative; wv[k] = vz'' row zp - N + k (k < WV), for the pressure's.
+    float wp[2 * N + 2], wv[WV];
     {
       const float* pa = A + 2 * sh.plane;
 #pragma unroll
       for (int k = 0; k < 2 * N; ++k) {
         const int z = zs - N + k;
         wp[k] = (x >= 0 && x < nx && z >= 0 && z < nz) ? __ldg(pa + (long long)z * ld + x) : 0.0f;
-        wv[k] = 0.0f;
       }
-    }
-    // v', A.v, p', A.p of the last three rows, indexed by phase
-    float VX[3], VZ[3], AX[3], AZ[3], PP[3], AP[3];
 #pragma unroll
-    for (int k = 0; k < 3; ++k) VX[k] = VZ[k] = AX[k] = AZ[k] = PP[k] = AP[k] = 0.0f;
+      for (int k = 0; k < WV; ++k) wv[k] = 0.0f;
+    }
+    // v', A.v, p', A.p of this iteration's two rows [phase][row]; the other
+    // phase holds the previous iteration's
+    float VX[2][2], VZ[2][2], AX[2][2], AZ[2][2], PP[2][2], AP[2][2];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b) VX[a][b] = VZ[a][b] = AX[a][b] = AZ[a][b] = PP[a][b] = AP[a][b] = 0.0f;
     const int ce = t + shc;
     const float* s = slots + q * S::SLOT;  // boxes of the current iteration
     const float* sp = s;                    // ... and of the previous one
     int qp = q, qp2 = q;
-    float* vrw = vr + ((zs - 1) & (VK - 1)) * NTX + t;      // vx'' row zv - 1 (written)
-    const float* vrr = vr + ((zs - D) & (VK - 1)) * NTX + t;  // vx'' row zp (read)
-    int ov = (zs - 1) * ld + x;      // output offset of row zv - 1
-    int op = (zs - D - 1) * ld + x;  // ... and of row zp - 1
+    int ts = 0, tsp = 0;  // tile-ring entries of this and the previous iteration
+    int ov = (zs - 1) * ld + x;      // output offset of v'' row zv - 1
+    int op = (zs - D - 1) * ld + x;  // ... and of p'' row zp - 1
     auto body = [&](auto P, int i) {
-      constexpr int p = decltype(P)::value, p1 = (p + 2) % 3, p2 = (p + 1) % 3;
-      const int zv = zs + i, zp = zv - D;
+      constexpr int p = decltype(P)::value, o = 1 - p;
+      const int zv = zs + 2 * i, zp = zv - D;
       if (live) {
         live = tma::mbar_wait_bounded(&bars[q], ph, err);
         if (live) ok_upto = gk + i + 1;
       }
-      float(&wpw)[2 * N + 1] = *reinterpret_cast<float(*)[2 * N + 1]>(&wp[p]);
-      float(&wvw)[2 * N + 1] = *reinterpret_cast<float(*)[2 * N + 1]>(&wv[p]);
-      wpw[2 * N] = s[S::S_PW + ce];
-      // velocity update, row zv (acoustic2d/fused_kernels.jl:27-63)
-      AX[p] = VX[p] = s[S::S_AV + ce];
-      AZ[p] = VZ[p] = s[S::S_AV + S::CW + ce];
-      if (x_in && zv >= N && zv < nz - N) {
-        const float dpdx = ac_sdm<N>(s + S::S_PX + t + shh, c);
-        const float dpdz = ac_wdp<N>(wpw, c);
-        VX[p] = __fmaf_rn(__fmul_rn(s[S::S_MB + ce], dtx), dpdx, VX[p]);
-        VZ[p] = __fmaf_rn(__fmul_rn(s[S::S_MB + S::CW + ce], dtz), dpdz, VZ[p]);
+      wp[2 * N] = s[S::S_PW + ce];
+      wp[2 * N + 1] = s[S::S_PW + S::CW + ce];
+      float* vrow = vt + ts * 4 * NTX + t;  // [row][vx, vz][NTX]
+      float* prow = pt + ts * 2 * NTX + t;
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        // velocity update, row zv + r (acoustic2d/fused_kernels.jl:27-63)
+        AX[p][r] = VX[p][r] = s[S::S_AV + r * S::CW + ce];
+        AZ[p][r] = VZ[p][r] = s[S::S_AV + (2 + r) * S::CW + ce];
+        if (x_in && zv + r >= N && zv + r < nz - N) {
+          const float dpdx = ac_sdm<N>(s + S::S_PX + r * S::XW + t + shh, c);
+          const float dpdz = ac_wdp<N>(*reinterpret_cast<const float(*)[2 * N + 1]>(&wp[r]), c);
+          VX[p][r] = __fmaf_rn(__fmul_rn(s[S::S_MB + r * S::CW + ce], dtx), dpdx, VX[p][r]);
+          VZ[p][r] = __fmaf_rn(__fmul_rn(s[S::S_MB + (2 + r) * S::CW + ce], dtz), dpdz, VZ[p][r]);
+        }
+        // pressure update, row zp + r (fused_kernels.jl:86-114)
+        AP[p][r] = PP[p][r] = s[S::S_AP + r * S::CW + ce];
+        if (p_lane && x_in && zp + r >= N && zp + r < nz - N) {
+          const float dvxdx = ac_sdp<N>(vr + ((zp + r) & (VK - 1)) * NTX + t, c);
+          const float dvzdz = ac_wdm<N>(*reinterpret_cast<const float(*)[2 * N + 1]>(&wv[r]), c);
+          PP[p][r] = __fmaf_rn(s[S::S_KP + r * S::CW + ce],
+                               __fmaf_rn(dvxdx, dtx, __fmul_rn(dvzdz, dtz)), PP[p][r]);
+        }
+        vrow[r * 2 * NTX] = VX[p][r];
+        vrow[r * 2 * NTX + NTX] = VZ[p][r];
+        prow[r * NTX] = PP[p][r];
       }
-      // pressure update, row zp (fused_kernels.jl:86-114)
-      AP[p] = PP[p] = s[S::S_AP + ce];
-      if (p_lane && x_in && zp >= N && zp < nz - N) {
-        const float dvxdx = ac_sdp<N>(vrr, c);
-        const float dvzdz = ac_wdm<N>(wvw, c);
-        PP[p] = __fmaf_rn(s[S::S_KP + ce], __fmaf_rn(dvxdx, dtx, __fmul_rn(dvzdz, dtz)), PP[p]);
-      }
-      vt[p * 2 * NTX + t] = VX[p];
-      vt[p * 2 * NTX + NTX + t] = VZ[p];
-      pt[p * NTX + t] = PP[p];
-      __syncthreads();  // rows zv (v') and zp (p') are complete; the slot of i-2 is free
+      __syncthreads();  // rows zv, zv+1 (v') and zp, zp+1 (p') are complete
       if (t == 0 && live && i >= 2 && i + R - 2 < nit) {
         tma::fence_proxy_async();
         issue(i + R - 2, qp2);
         issued = gk + i + R - 1;
       }
-      // v'' of row zv - 1 (kernels_det.jl:22-57 on the velocity frame)
       if (i >= 1) {
-        const int zq = zv - 1;
-        float ux = VX[p1], uz = VZ[p1];
-        if (v_lane && fx && zq >= 1 && zq <= nz - 2) {
-          const int sz = zq <= nbc ? 1 : (zq >= nz - 1 - nbc ? -1 : 0);
-          if (sx | sz) {
-            const int dist = min(xdist, min(zq, nz - 1 - zq));
-            const float* vrow = vt + p1 * 2 * NTX + t;
-            const float* arow = sp + S::S_AV + ce;
-            ux = ac_higdon(h, weight(0, dist), sx, sz, ux, AX[p1], vrow[sx], arow[sx],
-                           sz > 0 ? VX[p] : VX[p2], sz > 0 ? AX[p] : AX[p2]);
-            uz = ac_higdon(h, weight(1, dist), sx, sz, uz, AZ[p1], vrow[NTX + sx],
-                           arow[S::CW + sx], sz > 0 ? VZ[p] : VZ[p2], sz > 0 ? AZ[p] : AZ[p2]);
+        const float* vprev = vt + tsp * 4 * NTX + t;
+        const float* pprev = pt + tsp * 2 * NTX + t;
+        // v'' of rows zv - 1 (r = 0) and zv (r = 1) (kernels_det.jl:22-57)
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+          const int zq = zv - 1 + r;
+          // the row, its upper (zq - 1) and lower (zq + 1) neighbours
+          const float fcx = r ? VX[p][0] : VX[o][1], fcz = r ? VZ[p][0] : VZ[o][1];
+          const float ocx = r ? AX[p][0] : AX[o][1], ocz = r ? AZ[p][0] : AZ[o][1];
+          float ux = fcx, uz = fcz;
+          if (v_lane && fx && zq >= 1 && zq <= nz - 2) {
+            const int sz = zq <= nbc ? 1 : (zq >= nz - 1 - nbc ? -1 : 0);
+            if (sx | sz) {
+              const int dist = min(xdist, min(zq, nz - 1 - zq));
+              const float* vrw = r ? vrow : vprev + 2 * NTX;  // v' of row zq
+              const float* arw = r ? s + S::S_AV + ce : sp + S::S_AV + S::CW + ce;  // A.v of row zq
+              const float dnx = r ? VX[p][1] : VX[p][0], upx = r ? VX[o][1] : VX[o][0];
+              const float dnz = r ? VZ[p][1] : VZ[p][0], upz = r ? VZ[o][1] : VZ[o][0];
+              const float adx = r ? AX[p][1] : AX[p][0], aux = r ? AX[o][1] : AX[o][0];
+              const float adz = r ? AZ[p][1] : AZ[p][0], auz = r ? AZ[o][1] : AZ[o][0];
+              ux = ac_higdon(h, weight(0, dist), sx, sz, ux, ocx, vrw[sx], arw[sx],
+                             sz > 0 ? dnx : upx, sz > 0 ? adx : aux);
+              uz = ac_higdon(h, weight(1, dist), sx, sz, uz, ocz, vrw[NTX + sx],
+                             arw[2 * S::CW + sx], sz > 0 ? dnz : upz, sz > 0 ? adz : auz);
+            }
+          }
+          vr[(zq & (VK - 1)) * NTX + t] = ux;
+          wv[D + N - 1 + r] = uz;
+          if (v_out && zq >= z0 && zq < z1) {
+            B[ov + r * ld] = ux;
+            B[pl + ov + r * ld] = uz;
           }
         }
-        *vrw = ux;
-        wvw[2 * N] = uz;
-        if (v_out && zq >= z0 && zq < z1) {
-          B[ov] = ux;
-          B[pl + ov] = uz;
-        }
-      }
-      // p'' of row zp - 1
-      if (i >= 1 && o_lane) {
-        const int zq = zp - 1;
-        float u = PP[p1];
-        if (fx && zq >= 1 && zq <= nz - 2) {
-          const int sz = zq <= nbc ? 1 : (zq >= nz - 1 - nbc ? -1 : 0);
-          if (sx | sz) {
-            const int dist = min(xdist, min(zq, nz - 1 - zq));
-            u = ac_higdon(h, weight(2, dist), sx, sz, u, AP[p1], pt[p1 * NTX + t + sx],
-                          sp[S::S_AP + ce + sx], sz > 0 ? PP[p] : PP[p2], sz > 0 ? AP[p] : AP[p2]);
+        // p'' of rows zp - 1 (r = 0) and zp (r = 1)
+        if (o_lane) {
+#pragma unroll
+          for (int r = 0; r < 2; ++r) {
+            const int zq = zp - 1 + r;
+            float u = r ? PP[p][0] : PP[o][1];
+            if (fx && zq >= 1 && zq <= nz - 2) {
+              const int sz = zq <= nbc ? 1 : (zq >= nz - 1 - nbc ? -1 : 0);
+              if (sx | sz) {
+                const int dist = min(xdist, min(zq, nz - 1 - zq));
+                const float* prw = r ? prow : pprev + NTX;
+                const float* arw = r ? s + S::S_AP + ce : sp + S::S_AP + S::CW + ce;
+                const float dn = r ? PP[p][1] : PP[p][0], up = r ? PP[o][1] : PP[o][0];
+                const float ad = r ? AP[p][1] : AP[p][0], au = r ? AP[o][1] : AP[o][0];
+                u = ac_higdon(h, weight(2, dist), sx, sz, u, r ? AP[p][0] : AP[o][1], prw[sx],
+                              arw[sx], sz > 0 ? dn : up, sz > 0 ? ad : au);
+              }
+            }
+            if (x < nx && zq >= z0 && zq < z1) B[2 * pl + op + r * ld] = u;
           }
         }
-        if (x < nx && zq >= z0 && zq < z1) B[2 * pl + op] = u;
       }
-      // advance rings, offsets and slots
-      vrw += NTX;
-      if (vrw >= vr_end) vrw -= VK * NTX;
-      vrr += NTX;
-      if (vrr >= vr_end) vrr -= VK * NTX;
-      ov += ld;
-      op += ld;
+      // advance: windows, tile ring, offsets, slots
+#pragma unroll
+      for (int k = 0; k < 2 * N; ++k) wp[k] = wp[k + 2];
+#pragma unroll
+      for (int k = 0; k + 2 < WV; ++k) wv[k] = wv[k + 2];
+      tsp = ts;
+      ts = ts == 2 ? 0 : ts + 1;
+      ov += 2 * ld;
+      op += 2 * ld;
       sp = s;
       qp2 = qp;
       qp = q;
@@ -427,14 +463,7 @@ __global__ void __launch_bounds__(NTX, NTX <= 128 ? 4 : 2) k_uac_sweep(const AcS
       body(std::integral_constant<int, 0>{}, i);
       if (++i >= nit) break;
       body(std::integral_constant<int, 1>{}, i);
-      if (++i >= nit) break;
-      body(std::integral_constant<int, 2>{}, i);
       ++i;
-#pragma unroll
-      for (int k = 0; k < 2 * N; ++k) {
-        wp[k] = wp[k + 3];
-        wv[k] = wv[k + 3];
-      }
     }
     gk += nit;
   }
@@ -541,7 +570,7 @@ CUresult ac_encode(CUtensorMap* m, const float* base, int nx, int nz, int ld, lo
                    int nplanes, int bw, int bp) {
   cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)nz, (cuuint64_t)nplanes};
   cuuint64_t strides[2] = {(cuuint64_t)ld * 4, (cuuint64_t)plane * 4};
-  cuuint32_t box[3] = {(cuuint32_t)bw, 1, (cuuint32_t)bp};
+  cuuint32_t box[3] = {(cuuint32_t)bw, 2, (cuuint32_t)bp};  // two rows per iteration
   cuuint32_t es[3] = {1, 1, 1};
   return ac_encoder()(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims,
                       strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
