@@ -814,10 +814,17 @@ int run_uneven(fomo_ctx* ctx, float dh, float dt, int nt, int nbc, int fd_order,
       if (r == CUDA_SUCCESS) r = ac_encode(&mh[kAcMaps * s + 3], bm, u.nx, u.nz, u.ld, u.plane, 3, f.cw, 1);
       if (r == CUDA_SUCCESS) r = ac_encode(&mh[kAcMaps * s + 4], bm, u.nx, u.nz, u.ld, u.plane, 3, f.cw, 2);
       if (r != CUDA_SUCCESS) return fail(ctx, FOMO_ECUDA, "uneven sweep: tensor map encoding failed");
-      for (int x0 = 0; x0 < u.nx; x0 += f.txo) sg.push_back(make_int4(s, x0, 0, u.nz));
     }
-    // the last wave of strips is cut into four z chunks (chunk-major) so that
-    // the persistent CTAs finish together
+    // Strips in order of decreasing height (the longest segments first, a
+    // shot's strips side by side so that neighbours share halo rows in L2); the
+    // last wave of strips is cut into four z chunks (chunk-major) so that the
+    // persistent CTAs finish together.
+    std::vector<int> order(ns);
+    for (int s = 0; s < ns; ++s) order[s] = s;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return tab[a].nz > tab[b].nz; });
+    for (int s : order)
+      for (int x0 = 0; x0 < tab[s].nx; x0 += f.txo) sg.push_back(make_int4(s, x0, 0, tab[s].nz));
     a_grid = std::min<int>(f.resident, (int)sg.size());
     const int L = std::min<int>(a_grid, (int)sg.size());
     std::vector<int4> tail(sg.end() - L, sg.end());
