@@ -199,7 +199,12 @@ __global__ void __launch_bounds__(kNT, 1)
     const int bxh = (x0 - N) & ~3, shh = x0 - bxh;
     const int nit = z1 - z0 + 2;
     const bool out_ok = own_out && x < g.nx && y < g.ny;
-    const bool in_xy = x >= N && x < g.nx - N && y >= N && y < g.ny - N;
+    // The ring rows (warps 0 and 15) only feed the y-side Higdon terms of the
+    // tile's first / last output row: the back band's (neighbour y - 1) and the
+    // front band's (neighbour y + 1).  Elsewhere those warps skip the update.
+    const bool ring_idle = (r == 0 && !(y0 + 1 >= g.ny - 1 - g.nbc)) ||
+                           (r == kTY - 1 && !(y0 + kOY <= g.nbc));
+    const bool in_xy = x >= N && x < g.nx - N && y >= N && y < g.ny - N && !ring_idle;
     // x / y part of the frame classification (kernels_3d.jl:117-150)
     const int sx = x <= g.nbc ? 1 : (x >= g.nx - 1 - g.nbc ? -1 : 0);
     const int sy = y <= g.nbc ? 1 : (y >= g.ny - 1 - g.nbc ? -1 : 0);
