@@ -174,11 +174,19 @@ def _check_numerics(vmax, vmin_disp, dh, dt, f0, fd_order, centered=False):
 
 
 def _min_pos(a) -> np.float32:
-    a = np.asarray(a, dtype=np.float32)
-    pos = a[a > 0]
-    if pos.size == 0:
+    """minimum(vp[vp .> 0]): scanned in memory order, in chunks (a boolean index
+    of a column-major volume would walk it in row-major order)."""
+    flat = np.asarray(a, dtype=np.float32).ravel(order="K")
+    best = np.float32(np.inf)
+    step = 1 << 22
+    for i in range(0, flat.size, step):
+        c = flat[i:i + step]
+        c = c[c > 0]
+        if c.size:
+            best = min(best, np.float32(c.min()))
+    if not np.isfinite(best):
         raise ArgumentError("model has no positive velocity")
-    return np.float32(pos.min())
+    return np.float32(best)
 
 
 def _f32F(a) -> np.ndarray:
