@@ -17,6 +17,7 @@ Secondary workloads (one JSON line each, same keys; not the default line):
     --workload uneven         64 acoustic shots on grids of uneven size (graph run)
     --workload elastic3d      elastic3d 400x400x300, nbc 40, order 8 (nt from --nt;
                               --grid3d / --kernel3d: other sizes and kernel forms)
+    --workload acoustic3d     acoustic3d on the same model and grid
     --workload readme         steps/s on the grids of Fomo's published throughput table
     --workload sponge         Fomo's HABC-vs-sponge benchmark (acoustic and elastic 401x401)
     --workload coupled        coupled2d on the grids of Fomo's two coupled2d demos
@@ -452,25 +453,29 @@ def secondary(args):
         h2d = sum(2 * v.nbytes for v in c["vps"])
         d2h = sum(3 * r.size * c["nt"] * 4 for r in c["rx"])
         dtype = "f32"
-    elif args.workload == "elastic3d":
+    elif args.workload in ("elastic3d", "acoustic3d"):
         from fomo_b200.synthetic import elastic3d_config
 
+        el = args.workload == "elastic3d"
         g3 = [int(v) for v in args.grid3d.split(",")]
         c = elastic3d_config(*g3)
         nt = args.nt if args.nt != 3000 else 200
         pads = [v + 2 * (c["nbc"] + c["fd_order"] // 2) for v in g3]
-        desc = (f"elastic3d: {g3[0]}x{g3[1]}x{g3[2]} (padded {pads[0]}x{pads[1]}x{pads[2]}), dh 10 m, "
-                f"dt 0.8 ms, nt {nt} of 2500, order 8, nbc 40, 3D GRF vp, vacuum top, "
+        desc = (f"{args.workload}: {g3[0]}x{g3[1]}x{g3[2]} (padded {pads[0]}x{pads[1]}x{pads[2]}), "
+                f"dh 10 m, dt 0.8 ms, nt {nt} of 2500, order 8, nbc 40, 3D GRF vp, vacuum top, "
                 f"{c['rx'].size} receivers")
+        kw3 = dict(sx=c["sx"], sy=c["sy"], sz=c["sz"], rx=c["rx"], ry=c["ry"], rz=c["rz"],
+                   nbc=c["nbc"], fd_order=c["fd_order"], device=local, kernel=args.kernel3d)
 
         def run():
-            r = F.elastic3d(c["vp"], c["vs"], c["rho"], c["dh"], c["dt"], nt, c["f0"], sx=c["sx"],
-                            sy=c["sy"], sz=c["sz"], rx=c["rx"], ry=c["ry"], rz=c["rz"], nbc=c["nbc"],
-                            fd_order=c["fd_order"], device=local, kernel=args.kernel3d)
+            if el:
+                r = F.elastic3d(c["vp"], c["vs"], c["rho"], c["dh"], c["dt"], nt, c["f0"], **kw3)
+            else:
+                r = F.acoustic3d(c["vp"], c["rho"], c["dh"], c["dt"], nt, c["f0"], **kw3)
             s = F.api.last_stats
             return r, s.kernel_time_s, s.cell_updates, s.alg_bytes, s.gpu_launches
         unit, metric, per = "Gcell-updates/s", "Gcell-updates/s", None
-        h2d = 3 * c["vp"].nbytes
+        h2d = (3 if el else 2) * c["vp"].nbytes
         d2h = 3 * c["rx"].size * nt * 4
         dtype = "f32"
     else:  # elastic-fp16
@@ -524,7 +529,7 @@ def secondary(args):
                          "kernel": "whole time loop (library CUDA events)"},
             "gpu_launches": launches, "clocks": clk.summary()}
     if rank == 0 and not os.environ.get("FOMO_BENCH_NO_CPU"):
-        nt_run = c["nt"] if args.workload != "elastic3d" else nt
+        nt_run = c["nt"] if args.workload not in ("elastic3d", "acoustic3d") else nt
         line["l2_vs_fp64"] = secondary_l2(args.workload, c, res, nt_run)
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -570,7 +575,7 @@ def secondary_l2(workload, c, r, nt):
                "bitwise_vs_fp32_oracle": bool(np.array_equal(p, o32["seis_p"][:, :, 0])),
                "tolerance": 1e-5, "sample": f"shot {s} ({c['vps'][s].shape[0]}x"
                                             f"{c['vps'][s].shape[1]}), all {nt} steps"}
-    else:  # elastic3d on a reduced grid of the same configuration
+    else:  # elastic3d / acoustic3d on a reduced grid of the same configuration
         from fomo_b200.synthetic import elastic3d_config
 
         c3 = elastic3d_config(64, 64, 48)
@@ -578,9 +583,14 @@ def secondary_l2(workload, c, r, nt):
         w = F.ricker_wavelet(c3["f0"], c3["dt"], k)
         kw = dict(sx=c3["sx"], sy=c3["sy"], sz=c3["sz"], rx=c3["rx"], ry=c3["ry"], rz=c3["rz"],
                   nbc=c3["nbc"], fd_order=c3["fd_order"])
-        g = F.elastic3d(c3["vp"], c3["vs"], c3["rho"], c3["dh"], c3["dt"], k, c3["f0"], **kw)
-        o = O.elastic3d(c3["vp"], c3["vs"], c3["rho"], c3["dh"], c3["dt"], k,
-                        wavelet=w.reshape(1, -1), prec=64, **kw)
+        if workload == "elastic3d":
+            g = F.elastic3d(c3["vp"], c3["vs"], c3["rho"], c3["dh"], c3["dt"], k, c3["f0"], **kw)
+            o = O.elastic3d(c3["vp"], c3["vs"], c3["rho"], c3["dh"], c3["dt"], k,
+                            wavelet=w.reshape(1, -1), prec=64, **kw)
+        else:
+            g = F.acoustic3d(c3["vp"], c3["rho"], c3["dh"], c3["dt"], k, c3["f0"], **kw)
+            o = O.acoustic3d(c3["vp"], c3["rho"], c3["dh"], c3["dt"], k,
+                             wavelet=w.reshape(1, -1), prec=64, **kw)
         out = {"vz": _rel(g[2], o["seis_vz"]), "vx": _rel(g[0], o["seis_vx"]),
                "tolerance": 1e-5, "sample": f"64x64x48 interior, {k} steps, same dh/dt/order/nbc"}
     out["oracle"] = f"C++ restatement in FP64 ({time.perf_counter() - t0:.1f} s on the host)"
@@ -819,7 +829,7 @@ def main():
                     help="elastic3d workload: interior nx,ny,nz (smaller cases for profiling)")
     ap.add_argument("--kernel3d", type=int, default=0,
                     help="elastic3d workload: fomo_opts.kernel (0 auto, 1 per-cell, 2 fused, 3 z-march)")
-    ap.add_argument("--workload", choices=["elastic-batch", "elastic-fp16", "uneven", "elastic3d",
+    ap.add_argument("--workload", choices=["elastic-batch", "elastic-fp16", "uneven", "elastic3d", "acoustic3d",
                                            "readme", "sponge", "coupled"],
                     default="elastic-batch")
     args = ap.parse_args()

@@ -876,9 +876,9 @@ int run3d(fomo_ctx* ctx, bool elastic, const fomo_grid3d* gp, const float* vp, c
   // The fused TMA half steps (sweep3d.cu: update and Higdon boundary in one
   // pass each) are the default wherever they run; SINGLE_SWEEP requests them.
   const int kreq = opts ? opts->kernel : FOMO_KERNEL_AUTO;
-  const bool fused = elastic && (kreq == FOMO_KERNEL_AUTO || kreq == FOMO_KERNEL_SINGLE_SWEEP) &&
+  const bool fused = (kreq == FOMO_KERNEL_AUTO || kreq == FOMO_KERNEL_SINGLE_SWEEP) &&
                      fused3_supported(N);
-  if (elastic && kreq == FOMO_KERNEL_SINGLE_SWEEP && !fused)
+  if (kreq == FOMO_KERNEL_SINGLE_SWEEP && !fused)
     return fail(ctx, FOMO_EUNSUPPORTED, "fused 3D half steps need the TMA tensor-map encoder");
   const bool zm_vel = elastic && !fused && kreq != FOMO_KERNEL_TWO_PHASE;
   const bool zm_str = elastic && !fused && kreq == FOMO_KERNEL_ZMARCH;
@@ -899,7 +899,7 @@ int run3d(fomo_ctx* ctx, bool elastic, const fomo_grid3d* gp, const float* vp, c
   }
   Fused3Plan fp;
   if (fused) {
-    FOMO_CU(ctx, fused3_make_plan(fp, g, N, d_state, d_mat, ws_ptr<char>(ctx, o_bnd), st));
+    FOMO_CU(ctx, fused3_make_plan(fp, g, N, elastic, d_state, d_mat, ws_ptr<char>(ctx, o_bnd), st));
     FOMO_CU(ctx, cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), st));
   }
   int A = 0, B = 1, launches = 0;

@@ -64,10 +64,26 @@ struct F3 {
   static constexpr int S_MT = S_AT + al32(6 * C); // lam, l2m, mxy, mxz, myz [5][TY][CW]
   static constexpr int S_SLOT = S_MT + al32(5 * C);
   static constexpr unsigned S_BYTES = 4u * (3 * XY + 14 * C);
+  // acoustic velocity slot (floats)
+  static constexpr int A_AV = 0;                   // A.v [3][TY][CW]
+  static constexpr int A_PX = A_AV + al32(3 * C);  // p x-halo [TY][XW]
+  static constexpr int A_PY = A_PX + al32(X);      // p y-halo [YH][CW]
+  static constexpr int A_WN = A_PY + al32(Y);      // p at z+N [TY][CW]
+  static constexpr int A_MB = A_WN + al32(C);      // bx, by, bz [3][TY][CW]
+  static constexpr int A_SLOT = A_MB + al32(3 * C);
+  static constexpr unsigned A_BYTES = 4u * (7 * C + X + Y);
+  // acoustic pressure slot (floats)
+  static constexpr int P_AP = 0;                   // A.p [TY][CW]
+  static constexpr int P_VX = P_AP + al32(C);      // B.vx x-halo [TY][XW]
+  static constexpr int P_VY = P_VX + al32(X);      // B.vy y-halo [YH][CW]
+  static constexpr int P_WN = P_VY + al32(Y);      // B.vz at z+N [TY][CW]
+  static constexpr int P_KP = P_WN + al32(C);      // kappa [TY][CW]
+  static constexpr int P_SLOT = P_KP + al32(C);
+  static constexpr unsigned P_BYTES = 4u * (3 * C + X + Y);
 };
 
 struct F3Maps {
-  CUtensorMap c1, c3, c6, xh, yh, xyh, xyh3, m3, m5;
+  CUtensorMap c1, c3, c6, xh, yh, xyh, xyh3, m1, m3, m5;
 };
 
 __device__ __forceinline__ void load_4d(void* dst, const CUtensorMap* map, int x, int y, int z,
@@ -137,7 +153,7 @@ __device__ __forceinline__ float blend3(const HabcDev& h, const float* s_wt, int
 }  // namespace
 
 // ---------------------------------------------------------------------------
-// The march of one half step (velocity: STRESS = false; stress: true).
+// The march of one half step (PH below).
 // Iteration i of a segment [z0, z1) of a tile updates plane z = z0 - 1 + i
 // (i = 0 .. z1 - z0 + 1) and finishes plane z - 1.  TMA slot k (of R) holds the
 // boxes of one plane; a slot is refilled two iterations after its plane was
@@ -146,20 +162,27 @@ __device__ __forceinline__ float blend3(const HabcDev& h, const float* s_wt, int
 // updated values of every thread go to a three-plane tile ring in shared
 // memory for the neighbours' Higdon terms.
 // ---------------------------------------------------------------------------
-template <int N, int R, bool STRESS>
+// PH: 0 elastic velocity, 1 elastic stress, 2 acoustic velocity, 3 acoustic
+// pressure (acoustic3d/update_velocity.jl:16-53, update_pressure.jl:16-50).
+template <int N, int R, int PH>
 __global__ void __launch_bounds__(kNT, 1)
     k_el3_fused(const __grid_constant__ F3Maps mp, Geo3 g, Coef c, float dtdh, HabcDev h,
                 float* __restrict__ st, int A, int B, const int4* __restrict__ segs, int nseg,
                 int* __restrict__ sched, int* __restrict__ err) {
   using S = F3<N>;
-  constexpr int NF = STRESS ? 6 : 3;                  // fields updated
-  constexpr int SLOT = STRESS ? S::S_SLOT : S::V_SLOT;
-  constexpr unsigned BYTES = STRESS ? S::S_BYTES : S::V_BYTES;
-  constexpr int OLD = STRESS ? S::S_AT : S::V_AV;    // centre boxes of the old field group
-  constexpr int WIN = STRESS ? S::S_WN : S::V_WN;    // window boxes (plane z + N)
+  constexpr bool EL = PH < 2;                 // elastic (9 fields a set) or acoustic (4)
+  constexpr bool SECOND = PH == 1 || PH == 3;  // stress / pressure: reads B's velocities
+  constexpr int NSET = EL ? 9 : 4;
+  constexpr int NF = PH == 0 ? 3 : (PH == 1 ? 6 : (PH == 2 ? 3 : 1));  // fields updated
+  constexpr int SLOT = PH == 0 ? S::V_SLOT : (PH == 1 ? S::S_SLOT : (PH == 2 ? S::A_SLOT : S::P_SLOT));
+  constexpr unsigned BYTES =
+      PH == 0 ? S::V_BYTES : (PH == 1 ? S::S_BYTES : (PH == 2 ? S::A_BYTES : S::P_BYTES));
+  // centre boxes of the old field group, and the z-window entries (plane z + N)
+  constexpr int OLD = PH == 0 ? S::V_AV : (PH == 1 ? S::S_AT : (PH == 2 ? S::A_AV : S::P_AP));
+  constexpr int WIN = PH == 0 ? S::V_WN : (PH == 1 ? S::S_WN : (PH == 2 ? S::A_WN : S::P_WN));
   extern __shared__ __align__(128) float sm[];
   float* slots = sm;
-  constexpr int NK = STRESS ? 1 : 3;                // Higdon weight ramps used
+  constexpr int NK = SECOND ? 1 : 3;                // Higdon weight ramps used
   float* tring = sm + R * SLOT;  // [3 planes][NF][NT]
   float* s_wt = tring + 3 * NF * kNT;  // [NK][kWt]
   uint64_t* bars = reinterpret_cast<uint64_t*>(s_wt + NK * kWt);
@@ -171,14 +194,17 @@ __global__ void __launch_bounds__(kNT, 1)
     tma::mbar_init_fence();
   }
   for (int k = tid; k < NK * kWt; k += kNT) {
-    const int kind = STRESS ? 3 : k / kWt, d = k % kWt;
+    const int kind = SECOND ? 3 : k / kWt, d = k % kWt;
     s_wt[k] = d < h.wstride ? __ldg(h.wtab + kind * h.wstride + d) : 1.0f;
   }
-  // z-window fields: txz, tyz, tzz of A (velocity) or vx, vy, vz of B (stress)
-  const float* w0 = st + (long long)(STRESS ? B * 9 + 0 : A * 9 + 7) * g.vol;
-  const float* w1 = st + (long long)(STRESS ? B * 9 + 1 : A * 9 + 8) * g.vol;
-  const float* w2 = st + (long long)(STRESS ? B * 9 + 2 : A * 9 + 5) * g.vol;
-  float* ob = st + (long long)(B * 9 + (STRESS ? 3 : 0)) * g.vol;
+  // z-window fields: txz, tyz, tzz of A (elastic velocity), vx, vy, vz of B
+  // (stress), p of A (acoustic velocity), vz of B (pressure)
+  constexpr int NW = EL ? 3 : 1;
+  const int wf0 = PH == 0 ? A * 9 + 7 : (PH == 1 ? B * 9 : (PH == 2 ? A * 4 + 3 : B * 4 + 2));
+  const float* w0 = st + (long long)wf0 * g.vol;
+  const float* w1 = st + (long long)(PH == 0 ? A * 9 + 8 : B * 9 + 1) * g.vol;
+  const float* w2 = st + (long long)(PH == 0 ? A * 9 + 5 : B * 9 + 2) * g.vol;
+  float* ob = st + (long long)(B * NSET + (PH == 1 ? 3 : (PH == 3 ? 3 : 0))) * g.vol;
   int q = 0;             // slot of the current iteration
   uint32_t ph = 0;       // its mbarrier phase parity
   long long gk = 0;      // iterations so far (all segments)
@@ -216,7 +242,19 @@ __global__ void __launch_bounds__(kNT, 1)
       uint64_t* bar = &bars[slot];
       const int z = z0 - 1 + i;
       tma::mbar_expect_tx(bar, BYTES);
-      if constexpr (STRESS) {
+      if constexpr (PH == 3) {
+        load_4d(s + S::P_AP, &mp.c1, bxc, y0, z, A * 4 + 3, bar);
+        load_4d(s + S::P_VX, &mp.xh, bxh, y0, z, B * 4 + 0, bar);
+        load_4d(s + S::P_VY, &mp.yh, bxc, y0 - N, z, B * 4 + 1, bar);
+        load_4d(s + S::P_WN, &mp.c1, bxc, y0, z + N, B * 4 + 2, bar);
+        load_4d(s + S::P_KP, &mp.m1, bxc, y0, z, 3, bar);
+      } else if constexpr (PH == 2) {
+        load_4d(s + S::A_AV, &mp.c3, bxc, y0, z, A * 4, bar);
+        load_4d(s + S::A_PX, &mp.xh, bxh, y0, z, A * 4 + 3, bar);
+        load_4d(s + S::A_PY, &mp.yh, bxc, y0 - N, z, A * 4 + 3, bar);
+        load_4d(s + S::A_WN, &mp.c1, bxc, y0, z + N, A * 4 + 3, bar);
+        load_4d(s + S::A_MB, &mp.m3, bxc, y0, z, 0, bar);
+      } else if constexpr (PH == 1) {
         load_4d(s + S::S_V, &mp.xyh3, bxh, y0 - N, z, B * 9, bar);
         load_4d(s + S::S_WN, &mp.c3, bxc, y0, z + N, B * 9, bar);
         load_4d(s + S::S_AT, &mp.c6, bxc, y0, z, A * 9 + 3, bar);
@@ -254,8 +292,10 @@ __global__ void __launch_bounds__(kNT, 1)
     for (int k = 0; k < 2 * N; ++k) {
       const int z = z0 - 1 - N + k;
       wa[k] = ld3(g, w0, x, y, z);
-      wb[k] = ld3(g, w1, x, y, z);
-      wc[k] = ld3(g, w2, x, y, z);
+      if constexpr (NW == 3) {
+        wb[k] = ld3(g, w1, x, y, z);
+        wc[k] = ld3(g, w2, x, y, z);
+      }
     }
     float U[3][NF], O[3][NF];
 #pragma unroll
@@ -272,17 +312,31 @@ __global__ void __launch_bounds__(kNT, 1)
         if (live) ok_upto = gk + i + 1;
       }
       float(&wA)[2 * N + 1] = *reinterpret_cast<float(*)[2 * N + 1]>(&wa[p]);
-      float(&wB)[2 * N + 1] = *reinterpret_cast<float(*)[2 * N + 1]>(&wb[p]);
-      float(&wC)[2 * N + 1] = *reinterpret_cast<float(*)[2 * N + 1]>(&wc[p]);
+      [[maybe_unused]] float(&wB)[2 * N + 1] = *reinterpret_cast<float(*)[2 * N + 1]>(&wb[p]);
+      [[maybe_unused]] float(&wC)[2 * N + 1] = *reinterpret_cast<float(*)[2 * N + 1]>(&wc[p]);
       wA[2 * N] = s[WIN + ce];
-      wB[2 * N] = s[WIN + S::C + ce];
-      wC[2 * N] = s[WIN + 2 * S::C + ce];
+      if constexpr (NW == 3) {
+        wB[2 * N] = s[WIN + S::C + ce];
+        wC[2 * N] = s[WIN + 2 * S::C + ce];
+      }
       float(&o)[NF] = O[p];
       float(&u)[NF] = U[p];
 #pragma unroll
       for (int f = 0; f < NF; ++f) u[f] = o[f] = s[OLD + f * S::C + ce];
       if (in_xy && z >= N && z < g.nz - N) {
-        if constexpr (STRESS) {
+        if constexpr (PH == 3) {
+          const float dx = sdp<N, 1>(s + S::P_VX + r * S::XW + t + shh, c);
+          const float dy = sdp<N, kCW>(s + S::P_VY + (r + N) * kCW + t + shc, c);
+          const float dz = wdm<N>(wA, c);
+          u[0] = __fmaf_rn(__fmul_rn(s[S::P_KP + ce], dtdh), __fadd_rn(__fadd_rn(dx, dy), dz), o[0]);
+        } else if constexpr (PH == 2) {
+          const float dx = sdm<N, 1>(s + S::A_PX + r * S::XW + t + shh, c);
+          const float dy = sdm<N, kCW>(s + S::A_PY + (r + N) * kCW + t + shc, c);
+          const float dz = wdp<N>(wA, c);
+          u[0] = __fmaf_rn(__fmul_rn(s[S::A_MB + ce], dtdh), dx, o[0]);
+          u[1] = __fmaf_rn(__fmul_rn(s[S::A_MB + S::C + ce], dtdh), dy, o[1]);
+          u[2] = __fmaf_rn(__fmul_rn(s[S::A_MB + 2 * S::C + ce], dtdh), dz, o[2]);
+        } else if constexpr (PH == 1) {
           const float* pvx = s + S::S_V + (r + N) * S::XW + t + shh;
           const float* pvy = pvx + S::XY;
           const float* pvz = pvx + 2 * S::XY;
@@ -349,7 +403,7 @@ __global__ void __launch_bounds__(kNT, 1)
             if (sz)
               sum = __fadd_rn(sum, higdon_side(h, sz > 0 ? u[f] : u2[f], o1[f],
                                                sz > 0 ? o[f] : o2[f]));
-            vv[f] = blend3(h, s_wt + (STRESS ? 0 : f) * kWt, STRESS ? 3 : f, dist, nd, u1[f], sum);
+            vv[f] = blend3(h, s_wt + (SECOND ? 0 : f) * kWt, SECOND ? 3 : f, dist, nd, u1[f], sum);
           }
         }
         const long long oi = x + g.sy * y + g.sz * zq;
@@ -373,8 +427,10 @@ __global__ void __launch_bounds__(kNT, 1)
 #pragma unroll
       for (int k = 0; k < 2 * N; ++k) {
         wa[k] = wa[k + 3];
-        wb[k] = wb[k + 3];
-        wc[k] = wc[k + 3];
+        if constexpr (NW == 3) {
+          wb[k] = wb[k + 3];
+          wc[k] = wc[k + 3];
+        }
       }
     }
     gk += nit;
@@ -417,22 +473,23 @@ PFN_cuTensorMapEncodeTiled_v12000 encoder3() {
 constexpr size_t kMaxDynSmem3 = 227 * 1024;
 constexpr int kRing = 4;  // TMA slots per CTA (two planes in flight ahead of the update)
 
-template <int N, bool STRESS>
+template <int N, int PH>
 constexpr size_t smem_bytes3() {
-  return (size_t)kRing * (STRESS ? F3<N>::S_SLOT : F3<N>::V_SLOT) * 4 +
-         (size_t)3 * (STRESS ? 6 : 3) * kNT * 4 + (size_t)(STRESS ? 1 : 3) * kWt * 4 +
+  using S = F3<N>;
+  const int slot = PH == 0 ? S::V_SLOT : (PH == 1 ? S::S_SLOT : (PH == 2 ? S::A_SLOT : S::P_SLOT));
+  const int nf = PH == 0 ? 3 : (PH == 1 ? 6 : (PH == 2 ? 3 : 1));
+  const int nk = (PH == 1 || PH == 3) ? 1 : 3;
+  return (size_t)kRing * slot * 4 + (size_t)3 * nf * kNT * 4 + (size_t)nk * kWt * 4 +
          (size_t)kRing * 8;
 }
-static_assert(smem_bytes3<5, true>() + 1024 <= kMaxDynSmem3, "the widest stress plan fits an SM");
+static_assert(smem_bytes3<5, 1>() + 1024 <= kMaxDynSmem3, "the widest stress plan fits an SM");
 
-size_t smem_of(int N, bool stress) {
-  switch (N) {
-    case 1: return stress ? smem_bytes3<1, true>() : smem_bytes3<1, false>();
-    case 2: return stress ? smem_bytes3<2, true>() : smem_bytes3<2, false>();
-    case 3: return stress ? smem_bytes3<3, true>() : smem_bytes3<3, false>();
-    case 4: return stress ? smem_bytes3<4, true>() : smem_bytes3<4, false>();
-    default: return stress ? smem_bytes3<5, true>() : smem_bytes3<5, false>();
-  }
+size_t smem_of(int N, int ph) {
+#define FOMO_SM3(NN) \
+  case NN:           \
+    return ph == 0 ? smem_bytes3<NN, 0>() : ph == 1 ? smem_bytes3<NN, 1>() : ph == 2 ? smem_bytes3<NN, 2>() : smem_bytes3<NN, 3>();
+  switch (N) { FOMO_SM3(1) FOMO_SM3(2) FOMO_SM3(3) FOMO_SM3(4) default: FOMO_SM3(5) }
+#undef FOMO_SM3
 }
 int xw_of(int N) { return (2 * N + 38) & ~3; }
 
@@ -455,37 +512,38 @@ F3Maps maps_of(const Fused3Plan& p) {
   m.yh = p.yh;
   m.xyh = p.xyh;
   m.xyh3 = p.xyh3;
+  m.m1 = p.m1;
   m.m3 = p.m3;
   m.m5 = p.m5;
   return m;
 }
 
-template <int N, bool STRESS>
+template <int N, int PH>
 cudaError_t launch3(cudaStream_t st, const Fused3Plan& p, const Geo3& g, float* state, int A,
                     int B, const Coef& c, float dtdh, const HabcDev& h, int* err) {
-  auto kern = k_el3_fused<N, kRing, STRESS>;
+  auto kern = k_el3_fused<N, kRing, PH>;
   static std::once_flag once;
   static cudaError_t attr = cudaSuccess;
   std::call_once(once, [&] {
     attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem_bytes3<N, STRESS>());
+                                (int)smem_bytes3<N, PH>());
   });
   if (attr != cudaSuccess) return attr;
-  kern<<<p.grid, dim3(kTX, kTY), smem_bytes3<N, STRESS>(), st>>>(maps_of(p), g, c, dtdh, h, state,
+  kern<<<p.grid, dim3(kTX, kTY), smem_bytes3<N, PH>(), st>>>(maps_of(p), g, c, dtdh, h, state,
                                                                  A, B, p.d_segs, p.nseg, p.d_sched,
                                                                  err);
   return cudaGetLastError();
 }
 
-template <bool STRESS>
+template <int PH>
 cudaError_t launch_any(cudaStream_t st, const Fused3Plan& p, const Geo3& g, float* state, int A,
                        int B, const Coef& c, float dtdh, const HabcDev& h, int* err) {
   switch (p.N) {
-    case 1: return launch3<1, STRESS>(st, p, g, state, A, B, c, dtdh, h, err);
-    case 2: return launch3<2, STRESS>(st, p, g, state, A, B, c, dtdh, h, err);
-    case 3: return launch3<3, STRESS>(st, p, g, state, A, B, c, dtdh, h, err);
-    case 4: return launch3<4, STRESS>(st, p, g, state, A, B, c, dtdh, h, err);
-    case 5: return launch3<5, STRESS>(st, p, g, state, A, B, c, dtdh, h, err);
+    case 1: return launch3<1, PH>(st, p, g, state, A, B, c, dtdh, h, err);
+    case 2: return launch3<2, PH>(st, p, g, state, A, B, c, dtdh, h, err);
+    case 3: return launch3<3, PH>(st, p, g, state, A, B, c, dtdh, h, err);
+    case 4: return launch3<4, PH>(st, p, g, state, A, B, c, dtdh, h, err);
+    case 5: return launch3<5, PH>(st, p, g, state, A, B, c, dtdh, h, err);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -499,14 +557,15 @@ size_t fused3_table_bytes(const Geo3& g) {
   return (size_t)(ntiles + 4 * kMaxGrid3) * sizeof(int4) + 512;
 }
 
-cudaError_t fused3_make_plan(Fused3Plan& p, const Geo3& g, int N, float* state, const float* mat,
-                             void* d_table, cudaStream_t st) {
+cudaError_t fused3_make_plan(Fused3Plan& p, const Geo3& g, int N, bool elastic, float* state,
+                             const float* mat, void* d_table, cudaStream_t st) {
   if (!fused3_supported(N)) return cudaErrorNotSupported;
   p.N = N;
   p.ntx = (g.nx + kOX - 1) / kOX;
   p.nty = (g.ny + kOY - 1) / kOY;
-  p.smem_v = smem_of(N, false);
-  p.smem_s = smem_of(N, true);
+  p.elastic = elastic;
+  p.smem_v = smem_of(N, elastic ? 0 : 2);
+  p.smem_s = smem_of(N, elastic ? 1 : 3);
   int dev = 0, nsm = 148;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
@@ -548,26 +607,32 @@ cudaError_t fused3_make_plan(Fused3Plan& p, const Geo3& g, int N, float* state, 
   auto ok = [&](CUresult x) {
     if (x != CUDA_SUCCESS) r = x;
   };
-  ok(encode4(&p.c1, state, g, 18, kCW, kTY, 1));
-  ok(encode4(&p.c3, state, g, 18, kCW, kTY, 3));
-  ok(encode4(&p.c6, state, g, 18, kCW, kTY, 6));
-  ok(encode4(&p.xh, state, g, 18, XW, kTY, 1));
-  ok(encode4(&p.yh, state, g, 18, kCW, YH, 1));
-  ok(encode4(&p.xyh, state, g, 18, XW, YH, 1));
-  ok(encode4(&p.xyh3, state, g, 18, XW, YH, 3));
-  ok(encode4(&p.m3, mat, g, 8, kCW, kTY, 3));
-  ok(encode4(&p.m5, mat, g, 8, kCW, kTY, 5));
+  const int nst = elastic ? 18 : 8, nmat = elastic ? 8 : 4;  // field planes of both sets
+  ok(encode4(&p.c1, state, g, nst, kCW, kTY, 1));
+  ok(encode4(&p.c3, state, g, nst, kCW, kTY, 3));
+  ok(encode4(&p.xh, state, g, nst, XW, kTY, 1));
+  ok(encode4(&p.yh, state, g, nst, kCW, YH, 1));
+  ok(encode4(&p.m1, mat, g, nmat, kCW, kTY, 1));
+  ok(encode4(&p.m3, mat, g, nmat, kCW, kTY, 3));
+  if (elastic) {
+    ok(encode4(&p.c6, state, g, nst, kCW, kTY, 6));
+    ok(encode4(&p.xyh, state, g, nst, XW, YH, 1));
+    ok(encode4(&p.xyh3, state, g, nst, XW, YH, 3));
+    ok(encode4(&p.m5, mat, g, nmat, kCW, kTY, 5));
+  }
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
 cudaError_t fused3_velocity(cudaStream_t st, const Fused3Plan& p, const Geo3& g, float* state,
                             int A, int B, const Coef& c, float dtdh, const HabcDev& h, int* err) {
-  return launch_any<false>(st, p, g, state, A, B, c, dtdh, h, err);
+  return p.elastic ? launch_any<0>(st, p, g, state, A, B, c, dtdh, h, err)
+                   : launch_any<2>(st, p, g, state, A, B, c, dtdh, h, err);
 }
 
 cudaError_t fused3_stress(cudaStream_t st, const Fused3Plan& p, const Geo3& g, float* state,
                           int A, int B, const Coef& c, float dtdh, const HabcDev& h, int* err) {
-  return launch_any<true>(st, p, g, state, A, B, c, dtdh, h, err);
+  return p.elastic ? launch_any<1>(st, p, g, state, A, B, c, dtdh, h, err)
+                   : launch_any<3>(st, p, g, state, A, B, c, dtdh, h, err);
 }
 
 }  // namespace fomo

@@ -1,6 +1,6 @@
-// sweep3d.cuh -- 3D grid geometry and the fused, TMA-staged elastic3d half
-// steps (sweep3d.cu): each launch updates one field group (velocities or
-// stresses) and applies the Higdon boundary to it in the same pass.
+// sweep3d.cuh -- 3D grid geometry and the fused, TMA-staged 3D half steps
+// (sweep3d.cu): each launch updates one field group (velocities, or stresses /
+// pressure) and applies the Higdon boundary to it in the same pass.
 #pragma once
 #include <cuda.h>
 
@@ -24,6 +24,7 @@ struct Geo3 {
 // from a list through a counter in device memory.
 struct Fused3Plan {
   int N = 0;
+  bool elastic = true;           // elastic3d (9 fields a set) or acoustic3d (4)
   int ntx = 0, nty = 0;          // tiles in x and y
   int grid = 0;                  // persistent CTAs
   size_t smem_v = 0, smem_s = 0; // dynamic shared memory of the two kernels
@@ -32,21 +33,23 @@ struct Fused3Plan {
   int* d_sched = nullptr;        // [next segment, CTAs done]; zero between launches
   // tensor maps over the two field sets (4D: x, y, z, set * 9 + field) and the
   // materials (x, y, z, material)
-  CUtensorMap c1, c3, c6, xh, yh, xyh, xyh3, m3, m5;
+  CUtensorMap c1, c3, c6, xh, yh, xyh, xyh3, m1, m3, m5;
 };
 
 // Whether the fused form runs for half-stencil N (TMA tensor-map encoder present).
 bool fused3_supported(int N);
 // Device bytes of the segment table for grid g.
 size_t fused3_table_bytes(const Geo3& g);
-// Builds the plan for elastic state `state` (2 sets x 9 fields of g.vol
-// floats: vx vy vz txx tyy tzz txy txz tyz) and materials `mat` (8 volumes:
-// bx by bz lam l2m mxy mxz myz); d_table: fused3_table_bytes(g) bytes of
-// device memory, 256-byte aligned.  Synchronizes `st`.
-cudaError_t fused3_make_plan(Fused3Plan& p, const Geo3& g, int N, float* state, const float* mat,
-                             void* d_table, cudaStream_t st);
-// Velocity half step: set A -> B.v (update + Higdon).  Stress half step:
-// A.tau and B.v -> B.tau (update + Higdon).  err collects bounded-wait timeouts.
+// Builds the plan for the state `state` (2 sets x 9 fields of g.vol floats:
+// vx vy vz txx tyy tzz txy txz tyz; acoustic: 2 sets x vx vy vz p) and the
+// materials `mat` (bx by bz lam l2m mxy mxz myz; acoustic: bx by bz kappa);
+// d_table: fused3_table_bytes(g) bytes of device memory, 256-byte aligned.
+// Synchronizes `st`.
+cudaError_t fused3_make_plan(Fused3Plan& p, const Geo3& g, int N, bool elastic, float* state,
+                             const float* mat, void* d_table, cudaStream_t st);
+// Velocity half step: set A -> B.v (update + Higdon).  Stress / pressure half
+// step: A's stresses (pressure) and B.v -> B (update + Higdon).  err collects
+// bounded-wait timeouts.
 cudaError_t fused3_velocity(cudaStream_t st, const Fused3Plan& p, const Geo3& g, float* state,
                             int A, int B, const Coef& c, float dtdh, const HabcDev& h, int* err);
 cudaError_t fused3_stress(cudaStream_t st, const Fused3Plan& p, const Geo3& g, float* state,

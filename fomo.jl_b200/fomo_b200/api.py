@@ -615,15 +615,19 @@ def _run3d(elastic, vp, vs, rho, dh, dt, nt, f0, sx, sy, sz, rx, ry, rz, nbc, fd
 def acoustic3d(vp, rho, dh, dt, nt, f0, *, sx, sy, sz, rx, ry, rz, nbc: int = 50,
                fd_order: int = 8, snap_interval: int = 0, snap_plane="xz", snap_index: int = 0,
                v_ref=None, wavelet=None, device: int = 0,
-               final_state: Optional[np.ndarray] = None):
+               final_state: Optional[np.ndarray] = None, kernel: int = 0):
     """3D acoustic simulation (equations/acoustic3d/acoustic3d.jl:37-185).
 
     Returns ``(seis_vx, seis_vy, seis_vz, snaps)``; snapshots hold p on the
-    chosen plane.  The HABC is the reference's 3D Higdon formula evaluated in
-    two passes (deterministic; the reference updates in place).
+    chosen plane.  The HABC is the reference's 3D Higdon formula with
+    read-only inputs (deterministic; the reference updates in place).
+    ``kernel``: 0 or 2 = fused TMA half steps (update and Higdon boundary in
+    one pass each), 1 = per-cell updates and two Higdon passes (identical
+    results).
     """
     return _run3d(False, vp, None, rho, dh, dt, nt, f0, sx, sy, sz, rx, ry, rz, nbc, fd_order,
-                  snap_interval, snap_plane, snap_index, v_ref, wavelet, device, final_state)
+                  snap_interval, snap_plane, snap_index, v_ref, wavelet, device, final_state,
+                  kernel)
 
 
 def elastic3d(vp, vs, rho, dh, dt, nt, f0, *, sx, sy, sz, rx, ry, rz, nbc: int = 50,

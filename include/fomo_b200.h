@@ -68,12 +68,12 @@ extern "C" {
 #define FOMO_KERNEL_AUTO 0
 #define FOMO_KERNEL_TWO_PHASE 1    /* velocity sweep + stress sweep per step      */
 #define FOMO_KERNEL_SINGLE_SWEEP 2 /* one fused sweep per step (z-marching tiles); */
-                                   /* elastic3d: two TMA-staged half steps per step,  */
-                                   /* each with its Higdon boundary fused (AUTO's     */
-                                   /* pick, stats: SINGLE_SWEEP)                      */
-#define FOMO_KERNEL_ZMARCH 3       /* 3D: z-marching velocity and stress updates and  */
-                                   /* two-pass Higdon kernels; TWO_PHASE = per-cell   */
-                                   /* updates (acoustic3d: always per-cell)           */
+                                   /* 3D: two TMA-staged half steps per step, each    */
+                                   /* with its Higdon boundary fused (AUTO's pick,    */
+                                   /* stats: SINGLE_SWEEP)                            */
+#define FOMO_KERNEL_ZMARCH 3       /* elastic3d: z-marching velocity and stress       */
+                                   /* updates and two-pass Higdon kernels; TWO_PHASE  */
+                                   /* = per-cell updates and two-pass Higdon kernels  */
 #define FOMO_KERNEL_REPLICA 4      /* elastic2d(_batch): a CUDA C++ replica of the    */
                                    /* reference's CUDA.jl step (batch.jl:157-183:     */
                                    /* 8 launches, strip backups, frame scratch), a    */
