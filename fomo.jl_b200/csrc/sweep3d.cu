@@ -164,8 +164,10 @@ __device__ __forceinline__ float blend3(const HabcDev& h, const float* s_wt, int
 // ---------------------------------------------------------------------------
 // PH: 0 elastic velocity, 1 elastic stress, 2 acoustic velocity, 3 acoustic
 // pressure (acoustic3d/update_velocity.jl:16-53, update_pressure.jl:16-50).
+// The acoustic phases fit 64 registers a thread: two CTAs per SM where the
+// shared memory allows.
 template <int N, int R, int PH>
-__global__ void __launch_bounds__(kNT, 1)
+__global__ void __launch_bounds__(kNT, PH >= 2 ? 2 : 1)
     k_el3_fused(const __grid_constant__ F3Maps mp, Geo3 g, Coef c, float dtdh, HabcDev h,
                 float* __restrict__ st, int A, int B, const int4* __restrict__ segs, int nseg,
                 int* __restrict__ sched, int* __restrict__ err) {
@@ -518,18 +520,40 @@ F3Maps maps_of(const Fused3Plan& p) {
   return m;
 }
 
+// Sets the kernel's shared-memory limit once; returns its resident CTAs per SM
+// (0 if the query fails).
+template <int N, int PH>
+int prepare3() {
+  auto kern = k_el3_fused<N, kRing, PH>;
+  static std::once_flag once;
+  static int per_sm = 0;
+  std::call_once(once, [&] {
+    int nb = 0;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem_bytes3<N, PH>()) == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, kNT, smem_bytes3<N, PH>()) ==
+            cudaSuccess)
+      per_sm = nb;
+    else
+      cudaGetLastError();
+  });
+  return per_sm;
+}
+int per_sm3(int N, int ph) {
+#define FOMO_PS3(NN) \
+  case NN:           \
+    return ph == 0 ? prepare3<NN, 0>() : ph == 1 ? prepare3<NN, 1>() : ph == 2 ? prepare3<NN, 2>() : prepare3<NN, 3>();
+  switch (N) { FOMO_PS3(1) FOMO_PS3(2) FOMO_PS3(3) FOMO_PS3(4) default: FOMO_PS3(5) }
+#undef FOMO_PS3
+}
+
 template <int N, int PH>
 cudaError_t launch3(cudaStream_t st, const Fused3Plan& p, const Geo3& g, float* state, int A,
                     int B, const Coef& c, float dtdh, const HabcDev& h, int* err) {
   auto kern = k_el3_fused<N, kRing, PH>;
-  static std::once_flag once;
-  static cudaError_t attr = cudaSuccess;
-  std::call_once(once, [&] {
-    attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem_bytes3<N, PH>());
-  });
-  if (attr != cudaSuccess) return attr;
-  kern<<<p.grid, dim3(kTX, kTY), smem_bytes3<N, PH>(), st>>>(maps_of(p), g, c, dtdh, h, state,
+  if (prepare3<N, PH>() < 1) return cudaErrorInvalidConfiguration;
+  const int grid = (PH == 0 || PH == 2) ? p.grid_v : p.grid_s;
+  kern<<<grid, dim3(kTX, kTY), smem_bytes3<N, PH>(), st>>>(maps_of(p), g, c, dtdh, h, state,
                                                                  A, B, p.d_segs, p.nseg, p.d_sched,
                                                                  err);
   return cudaGetLastError();
@@ -571,17 +595,25 @@ cudaError_t fused3_make_plan(Fused3Plan& p, const Geo3& g, int N, bool elastic, 
   if (e != cudaSuccess) return e;
   e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   if (e != cudaSuccess) return e;
-  // One persistent CTA per SM (the plan holds an SM's registers and most of
-  // its shared memory), at least 16 planes of work each.  The segment list
+  // Persistent CTAs: one per SM for the elastic phases (a CTA holds an SM's
+  // registers and most of its shared memory), two for the acoustic ones where
+  // they fit; at least 16 planes of work each.  The segment list
   // runs through the tiles in order, whole z columns, so the tiles marching
   // side by side are neighbours and read each other's halo rows from L2; the
   // last wave of tiles is cut into four z chunks (chunk-major) so that the
   // CTAs finish together.
   const int ntiles = p.ntx * p.nty;
   const long long total = (long long)ntiles * g.nz;
-  const int G = (int)std::max(1LL, std::min<long long>({(long long)nsm, (long long)kMaxGrid3,
-                                                        total / 16}));
-  p.grid = G;
+  const int ph0 = elastic ? 0 : 2;
+  const int pv = per_sm3(N, ph0), ps = per_sm3(N, ph0 + 1);
+  if (pv < 1 || ps < 1) return cudaErrorInvalidConfiguration;
+  auto grid_of = [&](int per_sm) {
+    return (int)std::max(1LL, std::min<long long>({(long long)per_sm * nsm, (long long)kMaxGrid3,
+                                                   total / 16}));
+  };
+  p.grid_v = grid_of(pv);
+  p.grid_s = grid_of(ps);
+  const int G = std::max(p.grid_v, p.grid_s);
   const int L = std::min(ntiles, G), K = g.nz >= 64 ? 4 : 1;
   std::vector<int4> segs;
   segs.reserve((size_t)ntiles + 3 * (size_t)L);

@@ -20,13 +20,13 @@ struct Geo3 {
 // Work split of the fused half steps.  A CTA of 32 x 16 threads owns a tile of
 // 30 x 14 output columns plus a one-column ring on every side (the ring's
 // updated values feed the Higdon terms of the tile's edge cells) and marches
-// down z.  Persistent CTAs (one per SM) take segments {tile x, tile y, z0, z1}
-// from a list through a counter in device memory.
+// down z.  Persistent CTAs (one or two per SM) take segments {tile x, tile y,
+// z0, z1} from a list through a counter in device memory.
 struct Fused3Plan {
   int N = 0;
   bool elastic = true;           // elastic3d (9 fields a set) or acoustic3d (4)
   int ntx = 0, nty = 0;          // tiles in x and y
-  int grid = 0;                  // persistent CTAs
+  int grid_v = 0, grid_s = 0;    // persistent CTAs of the two half steps
   size_t smem_v = 0, smem_s = 0; // dynamic shared memory of the two kernels
   int4* d_segs = nullptr;        // segments in the order they are handed out
   int nseg = 0;
