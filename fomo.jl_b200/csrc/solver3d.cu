@@ -19,10 +19,11 @@
 
 namespace fomo {
 
-// Injection and recording of one 3D step (linear indices).  The injected
-// fields (p, or txx/tyy/tzz) are never the recorded ones (vx, vy, vz), so the
-// recording needs no ordering after the injection and runs over all blocks;
-// block 0 injects.
+// Injection and recording of one 3D step (linear indices; a negative index
+// is a point another z-slab holds, skipped here).  The injected fields (p, or
+// txx/tyy/tzz) are never the recorded ones (vx, vy, vz), so the recording
+// needs no ordering after the injection and runs over all blocks; block 0
+// injects.
 __global__ void k_inject_record3(int it, int nt, int n_src, const int* __restrict__ src_lin,
                                  const float* __restrict__ wav, float* inj0, float* inj1,
                                  float* inj2, int n_rec, const int* __restrict__ rec_lin,
@@ -32,6 +33,7 @@ __global__ void k_inject_record3(int it, int nt, int n_src, const int* __restric
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     for (int q = 0; q < n_src; ++q) {
       const long long p = src_lin[q];
+      if (p < 0) continue;
       const float w = wav[(long long)(it - 1) * n_src + q];
       inj0[p] = __fadd_rn(inj0[p], w);
       if (inj1) inj1[p] = __fadd_rn(inj1[p], w);
@@ -41,6 +43,7 @@ __global__ void k_inject_record3(int it, int nt, int n_src, const int* __restric
   const long long ob = (long long)n_rec * (it - 1);
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n_rec; r += gridDim.x * blockDim.x) {
     const long long p = rec_lin[r];
+    if (p < 0) continue;
     s0[ob + r] = rec0[p];
     s1[ob + r] = rec1[p];
     s2[ob + r] = rec2[p];
@@ -628,13 +631,16 @@ inline void habc3_passes(cudaStream_t st, unsigned fblocks, const Geo3& g, const
 // ---------------------------------------------------------------------------
 // device medium preparation (pad_array_3d.jl, elastic3d/medium.jl, acoustic3d/medium.jl)
 // ---------------------------------------------------------------------------
+// A raw (unpadded) model read through the edge-replicating padding; `a`
+// holds its planes from kz0 on (a z-slab may upload only the planes it needs).
 struct Raw3 {
   const float* a;
   int nx, ny, nz, pad;
+  int kz0;
   __device__ __forceinline__ float at(int x, int y, int z) const {
     const int ii = min(max(x - pad, 0), nx - 1), jj = min(max(y - pad, 0), ny - 1),
               kk = min(max(z - pad, 0), nz - 1);
-    return __ldg(a + ii + (long long)nx * (jj + (long long)ny * kk));
+    return __ldg(a + ii + (long long)nx * (jj + (long long)ny * (kk - kz0)));
   }
 };
 
@@ -650,14 +656,16 @@ __device__ __forceinline__ float harm4d(float m1, float m2, float m3, float m4) 
                                    __frcp_rn(m4)));
 }
 
+// Local plane zl of the volume is global padded plane z = zl + g.z0.
 __global__ void k_medium3d(int kind, Geo3 g, Raw3 vp, Raw3 vs, Raw3 rho, float* o0, float* o1,
                            float* o2, float* o3, float* o4, float* o5, float* o6, float* o7) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z * blockDim.z + threadIdx.z;
-  if (x >= g.nx || y >= g.ny || z >= g.nz) return;
-  const long long q = x + g.sy * y + g.sz * z;
-  const int xb = max(x, 1), yb = max(y, 1), zb = min(z, g.nz - 2);
+  const int zl = blockIdx.z * blockDim.z + threadIdx.z;
+  if (x >= g.nx || y >= g.ny || zl >= g.nz) return;
+  const long long q = x + g.sy * y + g.sz * zl;
+  const int z = zl + g.z0;
+  const int xb = max(x, 1), yb = max(y, 1), zb = min(z, g.gnz - 2);
   o0[q] = harm2d(rho.at(xb - 1, y, z), rho.at(xb, y, z));
   o1[q] = harm2d(rho.at(x, yb - 1, z), rho.at(x, yb, z));
   o2[q] = harm2d(rho.at(x, y, zb), rho.at(x, y, zb + 1));
@@ -748,6 +756,8 @@ int run3d(fomo_ctx* ctx, bool elastic, const fomo_grid3d* gp, const float* vp, c
   g.vol = g.sz * g.nz;
   g.M = M;
   g.nbc = pad - 1;
+  g.gnz = g.nz;
+  g.zhi = g.nz;
   if (g.vol > (1LL << 31) - 1) return fail(ctx, FOMO_EARG, "padded volume exceeds 2^31 cells");
   const long long nint = (long long)nx * ny * nz;
   const int si = (snap_index > 0 ? snap_index : ny / 2) + pad - 1;  // 0-based padded index
@@ -781,13 +791,7 @@ int run3d(fomo_ctx* ctx, bool elastic, const fomo_grid3d* gp, const float* vp, c
   }
   // weight ramps for offsets 0, .25, .5, .75 (habc_3d.jl:40-43)
   HabcHost hh = make_habc(pad, v_ref, gp->dt, gp->dh);
-  std::vector<float> wt3(4 * hh.wstride);
-  const double offs[4] = {0.0, 0.25, 0.5, 0.75};
-  for (int k = 0; k < 4; ++k)
-    for (int d = 0; d < hh.wstride; ++d) {
-      double w = ((double)d - offs[k]) / (double)(pad - 1);
-      wt3[k * hh.wstride + d] = (float)std::min(std::max(w, 0.0), 1.0);
-    }
+  const std::vector<float> wt3 = habc3_ramps(pad, hh.wstride);
 
   const int nfield = elastic ? 9 : 4;  // vx vy vz (txx tyy tzz txy txz tyz | p)
   const int nmat = elastic ? 8 : 4;
@@ -854,7 +858,8 @@ int run3d(fomo_ctx* ctx, bool elastic, const fomo_grid3d* gp, const float* vp, c
 
   dim3 blk(32, 4, 2), grd(cdiv(g.nx, 32), cdiv(g.ny, 4), cdiv(g.nz, 2));
   {
-    Raw3 a{d_vp, nx, ny, nz, pad}, s{elastic ? d_vs : d_vp, nx, ny, nz, pad}, r{d_rho, nx, ny, nz, pad};
+    Raw3 a{d_vp, nx, ny, nz, pad, 0}, s{elastic ? d_vs : d_vp, nx, ny, nz, pad, 0},
+        r{d_rho, nx, ny, nz, pad, 0};
     float* o[8];
     for (int k = 0; k < 8; ++k) o[k] = k < nmat ? d_mat + k * g.vol : nullptr;
     k_medium3d<<<grd, blk, 0, st>>>(elastic ? 0 : 1, g, a, s, r, o[0], o[1], o[2], o[3], o[4], o[5],
@@ -1058,6 +1063,34 @@ int run3d(fomo_ctx* ctx, bool elastic, const fomo_grid3d* gp, const float* vp, c
 }
 
 }  // namespace
+
+cudaError_t medium3d(cudaStream_t st, bool elastic, const Geo3& g, const float* vp,
+                     const float* vs, const float* rho, int nx, int ny, int nz, int pad, int kz0,
+                     float* mat) {
+  dim3 blk(32, 4, 2), grd(cdiv(g.nx, 32), cdiv(g.ny, 4), cdiv(g.nz, 2));
+  Raw3 a{vp, nx, ny, nz, pad, kz0}, s{elastic ? vs : vp, nx, ny, nz, pad, kz0},
+      r{rho, nx, ny, nz, pad, kz0};
+  const int nmat = elastic ? 8 : 4;
+  float* o[8];
+  for (int k = 0; k < 8; ++k) o[k] = k < nmat ? mat + k * g.vol : nullptr;
+  k_medium3d<<<grd, blk, 0, st>>>(elastic ? 0 : 1, g, a, s, r, o[0], o[1], o[2], o[3], o[4], o[5],
+                                  o[6], o[7]);
+  return cudaGetLastError();
+}
+
+cudaError_t inject_record3(cudaStream_t st, bool elastic, const Geo3& g, float* state, int B,
+                           int it, int nt, int n_src, const int* src_lin, const float* wav,
+                           int n_rec, const int* rec_lin, float* s0, float* s1, float* s2) {
+  const int nfield = elastic ? 9 : 4;
+  auto field = [&](int f) { return state + ((long long)B * nfield + f) * g.vol; };
+  const unsigned rec_blocks = (unsigned)std::min(1184, std::max(1, (n_rec + 255) / 256));
+  k_inject_record3<<<rec_blocks, 256, 0, st>>>(it, nt, n_src, src_lin, wav, field(3),
+                                               elastic ? field(4) : nullptr,
+                                               elastic ? field(5) : nullptr, n_rec, rec_lin,
+                                               field(0), field(1), field(2), s0, s1, s2);
+  return cudaGetLastError();
+}
+
 }  // namespace fomo
 
 using namespace fomo;

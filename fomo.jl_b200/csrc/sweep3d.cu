@@ -325,7 +325,7 @@ __global__ void __launch_bounds__(kNT, PH >= 2 ? 2 : 1)
       float(&u)[NF] = U[p];
 #pragma unroll
       for (int f = 0; f < NF; ++f) u[f] = o[f] = s[OLD + f * S::C + ce];
-      if (in_xy && z >= N && z < g.nz - N) {
+      if (in_xy && z + g.z0 >= N && z + g.z0 < g.gnz - N) {
         if constexpr (PH == 3) {
           const float dx = sdp<N, 1>(s + S::P_VX + r * S::XW + t + shh, c);
           const float dy = sdp<N, kCW>(s + S::P_VY + (r + N) * kCW + t + shc, c);
@@ -382,6 +382,7 @@ __global__ void __launch_bounds__(kNT, PH >= 2 ? 2 : 1)
       // finish plane z - 1: Higdon(updated, old) on frame cells, the update elsewhere
       const int zq = z - 1;
       if (i >= 1 && out_ok && zq >= z0) {
+        const int zg = zq + g.z0;  // global plane: frame classification
         const float(&u1)[NF] = U[p1];
         const float(&u2)[NF] = U[p2];
         const float(&o1)[NF] = O[p1];
@@ -389,10 +390,10 @@ __global__ void __launch_bounds__(kNT, PH >= 2 ? 2 : 1)
         float vv[NF];
 #pragma unroll
         for (int f = 0; f < NF; ++f) vv[f] = u1[f];
-        const int sz = zq <= g.nbc ? 1 : (zq >= g.nz - 1 - g.nbc ? -1 : 0);
-        const int nd = (fr_xy && zq >= 1 && zq <= g.nz - 2) ? nd_xy + (sz != 0) : 0;
+        const int sz = zg <= g.nbc ? 1 : (zg >= g.gnz - 1 - g.nbc ? -1 : 0);
+        const int nd = (fr_xy && zg >= 1 && zg <= g.gnz - 2) ? nd_xy + (sz != 0) : 0;
         if (nd > 0) {
-          const int dist = min(dist_xy, min(zq, g.nz - 1 - zq));
+          const int dist = min(dist_xy, min(zg, g.gnz - 1 - zg));
           const float* tp = tprev + tid;
           const float* ap = slots + qp * SLOT + OLD + ce;
 #pragma unroll
@@ -603,7 +604,10 @@ cudaError_t fused3_make_plan(Fused3Plan& p, const Geo3& g, int N, bool elastic, 
   // last wave of tiles is cut into four z chunks (chunk-major) so that the
   // CTAs finish together.
   const int ntiles = p.ntx * p.nty;
-  const long long total = (long long)ntiles * g.nz;
+  const int zlo = g.zlo, zhi = g.zhi, nzo = zhi - zlo;  // planes updated
+  if (zlo < 0 || zhi > g.nz || nzo < 1 || g.gnz < g.nz || g.z0 < 0 || g.z0 + g.nz > g.gnz)
+    return cudaErrorInvalidValue;
+  const long long total = (long long)ntiles * nzo;
   const int ph0 = elastic ? 0 : 2;
   const int pv = per_sm3(N, ph0), ps = per_sm3(N, ph0 + 1);
   if (pv < 1 || ps < 1) return cudaErrorInvalidConfiguration;
@@ -614,13 +618,13 @@ cudaError_t fused3_make_plan(Fused3Plan& p, const Geo3& g, int N, bool elastic, 
   p.grid_v = grid_of(pv);
   p.grid_s = grid_of(ps);
   const int G = std::max(p.grid_v, p.grid_s);
-  const int L = std::min(ntiles, G), K = g.nz >= 64 ? 4 : 1;
+  const int L = std::min(ntiles, G), K = nzo >= 64 ? 4 : 1;
   std::vector<int4> segs;
   segs.reserve((size_t)ntiles + 3 * (size_t)L);
   for (int tile = 0; tile < ntiles - L; ++tile)
-    segs.push_back(make_int4(tile % p.ntx, tile / p.ntx, 0, g.nz));
+    segs.push_back(make_int4(tile % p.ntx, tile / p.ntx, zlo, zhi));
   for (int k = 0; k < K; ++k) {
-    const int z0 = (int)((long long)g.nz * k / K), z1 = (int)((long long)g.nz * (k + 1) / K);
+    const int z0 = zlo + (int)((long long)nzo * k / K), z1 = zlo + (int)((long long)nzo * (k + 1) / K);
     for (int tile = ntiles - L; tile < ntiles; ++tile)
       segs.push_back(make_int4(tile % p.ntx, tile / p.ntx, z0, z1));
   }

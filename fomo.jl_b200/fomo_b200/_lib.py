@@ -35,7 +35,8 @@ EXPORTS = (
     "fomo_scalar2d_noalloc", "fomo_acoustic3d", "fomo_elastic3d", "fomo_acoustic2d_uneven",
     "fomo_corr_param_count", "fomo_corr_features", "fomo_corr_target", "fomo_corr_forward",
     "fomo_corr_gradients", "fomo_corr_adam", "fomo_scalar2d_snapshots", "fomo_scalar2d_corrected",
-    "fomo_coupled2d", "fomo_debug_coupled_medium",
+    "fomo_coupled2d", "fomo_debug_coupled_medium", "fomo_slab3d_layout_of", "fomo_slab3d_create",
+    "fomo_slab3d_step", "fomo_slab3d_seismograms", "fomo_slab3d_destroy",
 )
 
 

@@ -560,16 +560,24 @@ def acoustic2d_uneven(vps, rhos, dh, dt, nt, f0, *, sx, sz, rx, rz, nbc: int = 5
 _PLANES = {"xz": 0, "xy": 1, "yz": 2}
 
 
-def _run3d(elastic, vp, vs, rho, dh, dt, nt, f0, sx, sy, sz, rx, ry, rz, nbc, fd_order,
-           snap_interval, snap_plane, snap_index, v_ref, wavelet, device, final_state, kernel=0):
+class _Prep3(NamedTuple):
+    vp: np.ndarray
+    vs: Optional[np.ndarray]
+    rho: np.ndarray
+    grid: object      # L.Grid3D
+    acq: object       # L.Acq3D (points into the arrays below)
+    keep: tuple       # the acquisition arrays acq points into
+    n_rec: int
+
+
+def _prep3d(elastic, vp, vs, rho, dh, dt, nt, f0, sx, sy, sz, rx, ry, rz, nbc, fd_order, v_ref,
+            wavelet) -> _Prep3:
+    """Checked float32 / int32 arrays and the C structs of a 3D run."""
     vp, rho = _f32F(vp), _f32F(rho)
     vs = _f32F(vs) if elastic else None
     if vp.ndim != 3:
         raise ArgumentError("3D models are (nx, ny, nz) arrays")
     nx, ny, nz = vp.shape
-    plane = _PLANES.get(str(snap_plane).lstrip(":"))
-    if plane is None:
-        raise ArgumentError(f"snap_plane must be :xz, :xy or :yz, got {snap_plane}")
     if fd_order not in _FD:
         raise ValueError(f"Unsupported FD order: {fd_order}")
     sxv, syv, szv = (_i32F(a).ravel() for a in (sx, sy, sz))
@@ -580,22 +588,34 @@ def _run3d(elastic, vp, vs, rho, dh, dt, nt, f0, sx, sy, sz, rx, ry, rz, nbc, fd
                        ("ry", ryv, ny), ("rz", rzv, nz)):
         if not np.all((1 <= v) & (v <= n)):
             raise ArgumentError(f"{name} out of range 1..{n}")
-    if snap_index == 0:
-        snap_index = ny // 2  # acoustic3d.jl:50-52 (ny÷2 for every plane)
     dh, dt, f0 = np.float32(dh), np.float32(dt), np.float32(f0)
     v_ref = _min_pos(vp) if v_ref is None else np.float32(v_ref)
     w = _wavelet_row(wavelet, f0, dt, nt)
     # every source fires the one Ricker row (acoustic3d.jl:64-66)
     wm = np.asfortranarray(np.repeat(w[None, :], sxv.size, axis=0))
-    seis = [np.zeros((rxv.size, nt), dtype=np.float32, order="F") for _ in range(3)]
+    g = L.Grid3D(nx, ny, nz, float(dh), float(dt), int(nt), int(nbc), int(fd_order), float(v_ref))
+    acq = L.Acq3D(sxv.size, _ptr(sxv), _ptr(syv), _ptr(szv), _ptr(wm), rxv.size, _ptr(rxv),
+                  _ptr(ryv), _ptr(rzv))
+    return _Prep3(vp, vs, rho, g, acq, (sxv, syv, szv, rxv, ryv, rzv, wm), int(rxv.size))
+
+
+def _run3d(elastic, vp, vs, rho, dh, dt, nt, f0, sx, sy, sz, rx, ry, rz, nbc, fd_order,
+           snap_interval, snap_plane, snap_index, v_ref, wavelet, device, final_state, kernel=0):
+    plane = _PLANES.get(str(snap_plane).lstrip(":"))
+    if plane is None:
+        raise ArgumentError(f"snap_plane must be :xz, :xy or :yz, got {snap_plane}")
+    pr = _prep3d(elastic, vp, vs, rho, dh, dt, nt, f0, sx, sy, sz, rx, ry, rz, nbc, fd_order,
+                 v_ref, wavelet)
+    vp, vs, rho, g, acq = pr.vp, pr.vs, pr.rho, pr.grid, pr.acq
+    nx, ny, nz = vp.shape
+    if snap_index == 0:
+        snap_index = ny // 2  # acoustic3d.jl:50-52 (ny÷2 for every plane)
+    seis = [np.zeros((pr.n_rec, nt), dtype=np.float32, order="F") for _ in range(3)]
     nsnap = nt // snap_interval if snap_interval > 0 else 0
     shape = {0: (nx, nz), 1: (nx, ny), 2: (ny, nz)}[plane]
     snaps = np.zeros(shape + (nsnap,), dtype=np.float32, order="F") if nsnap else None
     st = L.Stats()
     ctx = L.context(device)
-    g = L.Grid3D(nx, ny, nz, float(dh), float(dt), int(nt), int(nbc), int(fd_order), float(v_ref))
-    acq = L.Acq3D(sxv.size, _ptr(sxv), _ptr(syv), _ptr(szv), _ptr(wm), rxv.size, _ptr(rxv),
-                  _ptr(ryv), _ptr(rzv))
     o = _opts(kernel, final_state)
     if elastic:
         rc = L.lib().fomo_elastic3d(ctx.handle, C.byref(g), _ptr(vp), _ptr(vs), _ptr(rho),

@@ -245,6 +245,71 @@ FOMO_API int fomo_elastic3d(fomo_ctx* ctx, const fomo_grid3d* g, const float* vp
                             int32_t snap_plane, int32_t snap_index, float* seis_vx, float* seis_vy,
                             float* seis_vz, float* snaps, const fomo_opts* opts, fomo_stats* stats);
 
+/* ---- z-slab decomposition of one 3D model ------------------------------------
+ * No reference counterpart: Fomo advances a 3D model on one device
+ * (equations/elastic3d/elastic3d.jl:37-162, acoustic3d/acoustic3d.jl:37-185).
+ * Here a model may be split into z-slabs, one per GPU.  Each slab advances
+ * with the fused half steps; between half steps the caller exchanges halo
+ * planes with the neighbouring slabs (contiguous plane blocks: NCCL send/recv,
+ * or device copies when several slabs share a device).  Every slab's owned
+ * planes and seismograms then equal the single-device run's bit for bit.
+ *
+ * Planes are global padded z indices 0 .. nzp-1 (nzp = nz + 2 (nbc + fd_order/2)).
+ * A slab owns [z_lo, z_hi) and holds [z_base, z_base + nz_local) =
+ * [max(z_lo - halo, 0), min(z_hi + halo, nzp)), halo = fd_order / 2.  Cuts
+ * between slabs lie in [cut_min, cut_max] = [pad + 1, nzp - pad - 1]
+ * (pad = nbc + fd_order / 2): clear of the z bands of the Higdon boundary and
+ * of the plane each band's z terms read, which would otherwise need the
+ * neighbour's half-step values.  A slab with a neighbour owns at least `halo`
+ * planes.
+ *
+ * Halo exchange after each half step of step it (1-based), set B = it % 2:
+ *   half 0 (velocity): elastic fields 0 1 2 (vx vy vz), acoustic field 2 (vz);
+ *   half 1 (stress / pressure, after injection and recording): elastic 7 8 5
+ *     (txz tyz tzz), acoustic 3 (p).
+ * Field f of set s is the volume state + (s * nfield + f) * plane * nz_local.
+ * A slab sends its first / last `halo` owned planes to the slab above / below
+ * and receives the `halo` planes next to its owned range.
+ *
+ * fomo_slab3d_layout_of: the slab's layout, or FOMO_EARG (message on ctx,
+ * which may be NULL) when the cut is not allowed.
+ * fomo_slab3d_create: vp, vs (elastic only), rho are the full HOST raw models
+ * (nx, ny, nz), of which the slab uploads the planes it needs; acq is the full
+ * HOST acquisition (points outside the owned planes are left to other slabs);
+ * g->v_ref <= 0 scans vp for min(vp > 0) as fomo_elastic3d does.  `state` is
+ * caller device memory of layout.state_floats floats (16-byte aligned), which
+ * the slab zeroes and keeps using until it is destroyed.  Kernels run on the
+ * context's stream (fomo_set_stream); ctx must outlive the slab.
+ * fomo_slab3d_step: half 0 velocity, half 1 stress / pressure then injection
+ * and recording, for step it (1..nt).
+ * fomo_slab3d_seismograms: waits for the stream, then copies the (n_rec, nt)
+ * seismograms to HOST arrays (receivers of other slabs read 0) and sets
+ * owned[r] = 1 for the receivers this slab records.  Reports FOMO_ECUDA if a
+ * bounded wait inside a half step timed out. */
+typedef struct fomo_slab3d fomo_slab3d;
+typedef struct fomo_slab3d_layout {
+  int32_t nxp, nyp, nzp;    /* padded global grid                             */
+  int32_t ld;               /* x pitch (floats)                               */
+  int64_t plane;            /* floats per plane (ld * nyp)                    */
+  int32_t z_lo, z_hi;       /* owned planes                                   */
+  int32_t z_base, nz_local; /* planes held                                    */
+  int32_t halo;             /* halo depth (fd_order / 2)                      */
+  int32_t nfield;           /* fields per set: 9 elastic, 4 acoustic          */
+  int32_t cut_min, cut_max; /* allowed cut planes                             */
+  int64_t state_floats;     /* 2 * nfield * plane * nz_local                  */
+} fomo_slab3d_layout;
+
+FOMO_API int fomo_slab3d_layout_of(fomo_ctx* ctx, int32_t elastic, const fomo_grid3d* g,
+                                   int32_t z_lo, int32_t z_hi, fomo_slab3d_layout* out);
+FOMO_API int fomo_slab3d_create(fomo_ctx* ctx, int32_t elastic, const fomo_grid3d* g,
+                                const float* vp, const float* vs, const float* rho,
+                                const fomo_acq3d* acq, int32_t z_lo, int32_t z_hi, float* state,
+                                fomo_slab3d** out);
+FOMO_API int fomo_slab3d_step(fomo_slab3d* slab, int32_t it, int32_t half);
+FOMO_API int fomo_slab3d_seismograms(fomo_slab3d* slab, float* seis_vx, float* seis_vy,
+                                     float* seis_vz, uint8_t* owned);
+FOMO_API void fomo_slab3d_destroy(fomo_slab3d* slab);
+
 /* ---- learned coarse-grid corrector ------------------------------------------
  * No reference counterpart.  A 3-layer 3x3 CNN (6 -> 16 -> 16 -> 1 channels,
  * bias-free, ReLU between layers; BF16 tensor-core implicit GEMM with FP32
