@@ -18,6 +18,10 @@ Secondary workloads (one JSON line each, same keys; not the default line):
     --workload elastic3d      elastic3d 400x400x300, nbc 40, order 8 (nt from --nt;
                               --grid3d / --kernel3d: other sizes and kernel forms)
     --workload acoustic3d     acoustic3d on the same model and grid
+    --slabs K                 (with elastic3d / acoustic3d) the same model split into z-slabs
+                              through fomo_b200.slabs3d: K slabs sharing one GPU, or under
+                              torchrun one slab per rank with NCCL halo exchange (strong
+                              scaling; the multi-GPU form has not been run here)
     --workload readme         steps/s on the grids of Fomo's published throughput table
     --workload sponge         Fomo's HABC-vs-sponge benchmark (acoustic and elastic 401x401)
     --workload coupled        coupled2d on the grids of Fomo's two coupled2d demos
@@ -537,6 +541,90 @@ def secondary(args):
         print(json.dumps(line), flush=True)
 
 
+def slabs_bench(args):
+    """elastic3d / acoustic3d over z-slabs (fomo_b200.slabs3d).  `value`: padded
+    cell-updates of the whole model / the slowest rank's device time of the time
+    loop (CUDA events around the half steps and halo exchanges); `e2e`: the same
+    over the whole call (slab set-up from host arrays, seismograms back)."""
+    import datetime
+    import warnings
+
+    import torch
+    import torch.distributed as dist
+
+    from fomo_b200 import slabs3d
+    from fomo_b200.synthetic import elastic3d_config
+
+    warnings.simplefilter("ignore")
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://",
+                                timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    stream = torch.cuda.current_stream()
+    peak, peak_kind = _peaks()
+    el = args.workload == "elastic3d"
+    g3 = [int(v) for v in args.grid3d.split(",")]
+    c = elastic3d_config(*g3)
+    nt = args.nt if args.nt != 3000 else 200
+    n = world if world > 1 else args.slabs
+    pads = [v + 2 * (c["nbc"] + c["fd_order"] // 2) for v in g3]
+    cells = float(np.prod(pads)) * nt
+    desc = (f"{args.workload}: {g3[0]}x{g3[1]}x{g3[2]} (padded {pads[0]}x{pads[1]}x{pads[2]}), "
+            f"dh 10 m, dt 0.8 ms, nt {nt} of 2500, order 8, nbc 40, 3D GRF vp, vacuum top, "
+            f"{c['rx'].size} receivers; {n} z-slabs "
+            + ("one per GPU, NCCL halo exchange" if world > 1 else "on one GPU, device-copy halos"))
+    kw = dict(sx=c["sx"], sy=c["sy"], sz=c["sz"], rx=c["rx"], ry=c["ry"], rz=c["rz"],
+              nbc=c["nbc"], fd_order=c["fd_order"], device=local, n_slabs=n)
+
+    def run():
+        if el:
+            slabs3d.elastic3d_slabs(c["vp"], c["vs"], c["rho"], c["dh"], c["dt"], nt, c["f0"], **kw)
+        else:
+            slabs3d.acoustic3d_slabs(c["vp"], c["rho"], c["dh"], c["dt"], nt, c["f0"], **kw)
+        return dict(slabs3d.last_run)
+
+    try:
+        for _ in range(args.warmup):
+            run()
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        loops, launches = [], 0
+        with ClockSampler(local) as clk:
+            if world > 1:
+                dist.barrier()
+            ev[0].record(stream)
+            for _ in range(args.steps):
+                lr = run()
+                loops.append(lr["loop_s"])
+                launches += lr["gpu_launches"]
+            ev[1].record(stream)
+            torch.cuda.synchronize()
+        wall = max_over_ranks(ev[0].elapsed_time(ev[1]) / args.steps * 1e-3, world, "cuda")
+        t = max_over_ranks(float(np.mean(loops)), world, "cuda")
+    finally:
+        if world > 1:
+            dist.destroy_process_group()
+    nfield, nmat = (9, 8) if el else (4, 4)
+    achieved = 4.0 * (2 * nfield + nmat) * cells / t / 1e9
+    line = {"metric": "Gcell-updates/s", "value": cells / t / 1e9, "unit": "Gcell-updates/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": desc, "secondary": args.workload + "-slabs", "slabs": n},
+            "e2e": {"value": cells / wall / 1e9, "unit": "Gcell-updates/s",
+                    "h2d_bytes_per_step": int((3 if el else 2) * c["vp"].nbytes),
+                    "d2h_bytes_per_step": int(3 * c["rx"].size * nt * 4)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak / max(world, 1), "traffic": None,
+                         "peak_kind": peak_kind,
+                         "kernel": "whole time loop incl. halo exchange (CUDA events)"},
+            "gpu_launches": launches, "clocks": clk.summary()}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def _rel(a, b):
     a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
@@ -831,6 +919,8 @@ def main():
                     help="elastic3d workload: interior nx,ny,nz (smaller cases for profiling)")
     ap.add_argument("--kernel3d", type=int, default=0,
                     help="elastic3d workload: fomo_opts.kernel (0 auto, 1 per-cell, 2 fused, 3 z-march)")
+    ap.add_argument("--slabs", type=int, default=0,
+                    help="elastic3d / acoustic3d: split the model into this many z-slabs")
     ap.add_argument("--workload", choices=["elastic-batch", "elastic-fp16", "uneven", "elastic3d", "acoustic3d",
                                            "readme", "sponge", "coupled"],
                     default="elastic-batch")
@@ -855,6 +945,13 @@ def main():
                               "are compared against its published RTX 3060 figures"}))
             return
         readme_grids(args)
+        return
+    if args.workload in ("elastic3d", "acoustic3d") and args.slabs > 0:
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no "
+                              "domain-decomposed 3D solver"}))
+            return
+        slabs_bench(args)
         return
     if args.workload != "elastic-batch":
         if args.impl == "reference":

@@ -31,6 +31,11 @@ import numpy as np
 
 from . import _lib as L
 
+# The last run's time loop in this process: {"loop_s": device seconds from the
+# first half step to the last exchange (CUDA events on the launching stream),
+# "slabs": slabs held here, "gpu_launches": library kernels launched}.
+last_run: dict = {}
+
 # fields of set B exchanged after half step `half` (0 velocity, 1 stress / pressure)
 HALO_FIELDS = {
     (True, 0): (0, 1, 2),
@@ -319,6 +324,28 @@ def _assemble(parts):
     return tuple(out)
 
 
+class _LoopTimer:
+    """Device time of a slab time loop into ``last_run``."""
+
+    def __init__(self, n_here, nt):
+        import torch
+
+        self.n_here, self.nt = n_here, nt
+        self.ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def __enter__(self):
+        self.ev[0].record()
+        return self
+
+    def __exit__(self, *exc):
+        if exc[0] is None:
+            self.ev[1].record()
+            self.ev[1].synchronize()
+            last_run.clear()
+            last_run.update(loop_s=self.ev[0].elapsed_time(self.ev[1]) * 1e-3, slabs=self.n_here,
+                            gpu_launches=3 * self.nt * self.n_here)
+
+
 def _run_slabs(elastic, args, n_slabs, cuts, device, group, final_state):
     import torch
     import torch.distributed as dist
@@ -345,7 +372,8 @@ def _run_slabs(elastic, args, n_slabs, cuts, device, group, final_state):
             slab = None
             try:
                 slab = Slab(ctx, elastic, prep, *cuts[k])
-                run_rank(slab, k, ranks, elastic, nt, group)
+                with _LoopTimer(1, nt):
+                    run_rank(slab, k, ranks, elastic, nt, group)
                 part = slab.seismograms()
                 if final_state is not None:
                     final_state.append((slab.z_lo, slab.z_hi, [
@@ -359,7 +387,8 @@ def _run_slabs(elastic, args, n_slabs, cuts, device, group, final_state):
         try:
             for lo, hi in cuts:
                 slabs.append(Slab(ctx, elastic, prep, lo, hi))
-            run_local(slabs, elastic, nt)
+            with _LoopTimer(len(slabs), nt):
+                run_local(slabs, elastic, nt)
             parts = [s.seismograms() for s in slabs]
             if final_state is not None:
                 for s in slabs:
