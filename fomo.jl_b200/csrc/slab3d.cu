@@ -206,11 +206,15 @@ int fomo_slab3d_create(fomo_ctx* ctx, int32_t elastic, const fomo_grid3d* gp, co
   const int kz0 = std::min(std::max(L.z_base - pad, 0), nz - 1);
   const int kz1 = std::min(std::max(L.z_base + L.nz_local - pad, 0), nz - 1);
   const long long nraw = (long long)nx * ny * (kz1 - kz0 + 1);
-  const size_t o_raw = ar.take<float>(3 * nraw);
   FOMO_CU(ctx, cudaSetDevice(ctx->device));
+  float* raw = nullptr;  // freed once the materials are built
   if (cudaMalloc(&s->mem, ar.off) != cudaSuccess) {
     cudaGetLastError();
     s->mem = nullptr;
+    return bail(fail(ctx, FOMO_ENOMEM, "z-slab: device allocation failed"));
+  }
+  if (cudaMalloc(&raw, sizeof(float) * 3 * nraw) != cudaSuccess) {
+    cudaGetLastError();
     return bail(fail(ctx, FOMO_ENOMEM, "z-slab: device allocation failed"));
   }
   char* base = static_cast<char*>(s->mem);
@@ -221,7 +225,6 @@ int fomo_slab3d_create(fomo_ctx* ctx, int32_t elastic, const fomo_grid3d* gp, co
   s->wav = reinterpret_cast<float*>(base + o_wav);
   s->seis = reinterpret_cast<float*>(base + o_seis);
   s->err = reinterpret_cast<int*>(base + o_err);
-  float* raw = reinterpret_cast<float*>(base + o_raw);
   cudaStream_t st = ctx->stream;
   const long long off = (long long)nx * ny * kz0;
   int rc = FOMO_OK;
@@ -250,10 +253,9 @@ int fomo_slab3d_create(fomo_ctx* ctx, int32_t elastic, const fomo_grid3d* gp, co
   if (rc == FOMO_OK)
     cu(fused3_make_plan(s->fp, g, N, elastic, state, s->mat, base + o_tab, st),
        "fused3_make_plan");  // synchronizes the stream: the host arrays above are free
-  if (rc != FOMO_OK) {
-    cudaStreamSynchronize(st);
-    return bail(rc);
-  }
+  if (rc != FOMO_OK) cudaStreamSynchronize(st);
+  cudaFree(raw);
+  if (rc != FOMO_OK) return bail(rc);
   for (int l = 0; l < 5; ++l) s->c.a[l] = kFD[N][l];
   s->h = HabcDev{hh.q, hh.qt, hh.qxt, hh.nbc, hh.wstride, s->wt};
   s->dtdh = gp->dt / gp->dh;
@@ -267,6 +269,7 @@ int fomo_slab3d_step(fomo_slab3d* s, int32_t it, int32_t half) {
   if (it < 1 || it > s->nt || (half != 0 && half != 1))
     return fail(ctx, FOMO_EARG, "slab step: it must be in 1..nt and half 0 or 1");
   const int A = (it + 1) & 1, B = it & 1;
+  FOMO_CU(ctx, cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
   if (half == 0) {
     FOMO_CU(ctx, fused3_velocity(st, s->fp, s->g, s->state, A, B, s->c, s->dtdh, s->h, s->err));
@@ -283,6 +286,7 @@ int fomo_slab3d_seismograms(fomo_slab3d* s, float* svx, float* svy, float* svz, 
   if (!s) return FOMO_EARG;
   fomo_ctx* ctx = s->ctx;
   cudaStream_t st = ctx->stream;
+  FOMO_CU(ctx, cudaSetDevice(ctx->device));
   FOMO_CU(ctx, cudaStreamSynchronize(st));
   int flag = 0;
   FOMO_CU(ctx, cudaMemcpy(&flag, s->err, sizeof(int), cudaMemcpyDeviceToHost));

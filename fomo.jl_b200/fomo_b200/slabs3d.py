@@ -358,11 +358,15 @@ def _run_slabs(elastic, args, n_slabs, cuts, device, group, final_state):
         dist.get_world_size(group) > 1)
     n = dist.get_world_size(group) if distributed else (
         len(cuts) if cuts is not None else int(n_slabs))
+    nzp, cut_min, cut_max, halo = grid_planes(prep.grid)
     if cuts is None:
-        nzp, cut_min, cut_max, halo = grid_planes(prep.grid)
         cuts = plan_cuts(nzp, cut_min, cut_max, halo, n)
+    cuts = [(int(a), int(b)) for a, b in cuts]
     if len(cuts) != n:
         raise ValueError(f"{len(cuts)} slab ranges for {n} slabs")
+    if cuts[0][0] != 0 or cuts[-1][1] != nzp or any(
+            cuts[k][1] != cuts[k + 1][0] for k in range(n - 1)):
+        raise ValueError(f"slab ranges must tile the padded planes 0..{nzp} in order: {cuts}")
     ctx = L.Context(device)
     with torch.cuda.device(device):
         ctx.use_torch_stream(torch.cuda.current_stream(device))

@@ -212,3 +212,14 @@ def test_run_rank_gloo_equals_whole(world, tmp_path):
             p.kill()
     assert [p.exitcode for p in procs] == [0] * world
     assert [(tmp_path / f"rank{r}").read_text() for r in range(world)] == ["ok"] * world
+
+
+def test_cuts_must_tile_the_grid():
+    # refused on the host, before any device work
+    nx, ny, nz = 12, 10, 40  # nbc 4, order 4: pad 6, 52 padded planes
+    vp = np.full((nx, ny, nz), 3000.0, dtype=np.float32, order="F")
+    kw = dict(sx=[6], sy=[5], sz=[3], rx=[2, 3], ry=[2, 2], rz=[3, 30], nbc=4, fd_order=4)
+    for cuts in ([(0, 20), (21, 52)], [(0, 20), (20, 50)], [(1, 20), (20, 52)],
+                 [(0, 30), (20, 52)]):
+        with pytest.raises(ValueError, match="tile the padded planes"):
+            S.acoustic3d_slabs(vp, vp, 10.0, 1e-3, 5, 15.0, cuts=cuts, **kw)
