@@ -44,13 +44,11 @@ namespace {
 __device__ __forceinline__ float2 p_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 p_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 p_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-__device__ __forceinline__ float2 p_sub(float2 a, float2 b) {
-  float2 d;
-  asm("{\n .reg .b64 ra, rb, rd;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n"
-      " sub.rn.f32x2 rd, ra, rb;\n mov.b64 {%0, %1}, rd;\n}"
-      : "=f"(d.x), "=f"(d.y)
-      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-  return d;
+// a - b as fma(-1, b, a): -1 * b is exact, so the fma rounds a - b once, as
+// sub.rn.f32x2 does (signed zeros included).  m1 = {-1, -1}, kept in a
+// register pair by the caller.
+__device__ __forceinline__ float2 p_sub(float2 m1, float2 a, float2 b) {
+  return __ffma2_rn(m1, b, a);
 }
 __device__ __forceinline__ float2 lo2(const float4& v) { return make_float2(v.x, v.y); }
 __device__ __forceinline__ float2 hi2(const float4& v) { return make_float2(v.z, v.w); }
@@ -125,6 +123,7 @@ __global__ void __launch_bounds__(2 * NV, MINB)
   k.nq = pinned(kp.nq);
   k.nqt = pinned(kp.nqt);
   k.nqxt = pinned(kp.nqxt);
+  const float2 m1 = pinned(make_float2(-1.0f, -1.0f));
   constexpr int NT = 2 * NV;
   constexpr int W = S::W, M = N, TN = S::TN, HV = S::HV;
   constexpr int NZ = S::NZ, NO = S::NO, LVV = S::LVV;
@@ -262,10 +261,10 @@ __global__ void __launch_bounds__(2 * NV, MINB)
 #pragma unroll
             for (int l = 1; l <= N; ++l) {
               const float2 a = k.a[l - 1];
-              dxx = p_fma(a, p_sub(rxx[l - 1], rxx[-l]), dxx);
-              dxzx = p_fma(a, p_sub(rxz[l], rxz[1 - l]), dxzx);
-              dxzz = p_fma(a, p_sub(wxz[rr + M + l - 1], wxz[rr + M - l]), dxzz);
-              dzz = p_fma(a, p_sub(wzz[rr + M + l], wzz[rr + M - l + 1]), dzz);
+              dxx = p_fma(a, p_sub(m1, rxx[l - 1], rxx[-l]), dxx);
+              dxzx = p_fma(a, p_sub(m1, rxz[l], rxz[1 - l]), dxzx);
+              dxzz = p_fma(a, p_sub(m1, wxz[rr + M + l - 1], wxz[rr + M - l]), dxzz);
+              dzz = p_fma(a, p_sub(m1, wzz[rr + M + l], wzz[rr + M - l + 1]), dzz);
             }
             float2 ux = s_v[(os * 4 + rr) * W + c];
             float2 uz = s_v[(os * 4 + 2 + rr) * W + c];
@@ -423,10 +422,10 @@ __global__ void __launch_bounds__(2 * NV, MINB)
 #pragma unroll
             for (int l = 1; l <= N; ++l) {
               const float2 a = k.a[l - 1];
-              dvxdx = p_fma(a, p_sub(rvx[l], rvx[1 - l]), dvxdx);
-              dvzdx = p_fma(a, p_sub(rvz[l - 1], rvz[-l]), dvzdx);
-              dvxdz = p_fma(a, p_sub(wvx[rr + M + l], wvx[rr + M - l + 1]), dvxdz);
-              dvzdz = p_fma(a, p_sub(wvz[rr + M + l - 1], wvz[rr + M - l]), dvzdz);
+              dvxdx = p_fma(a, p_sub(m1, rvx[l], rvx[1 - l]), dvxdx);
+              dvzdx = p_fma(a, p_sub(m1, rvz[l - 1], rvz[-l]), dvzdx);
+              dvxdz = p_fma(a, p_sub(m1, wvx[rr + M + l], wvx[rr + M - l + 1]), dvxdz);
+              dvzdz = p_fma(a, p_sub(m1, wvz[rr + M + l - 1], wvz[rr + M - l]), dvzdz);
             }
             float2 sxx = s_o[(os * 6 + 0 + rr) * W + c + TN];
             float2 szz = s_o[(os * 6 + 2 + rr) * W + c + TN];
