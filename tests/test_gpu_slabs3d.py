@@ -105,3 +105,21 @@ def test_slab_refuses_cut_in_higdon_band(fomo, slabs3d):
         with pytest.raises(FomoError, match="Higdon z bands"):
             slabs3d.elastic3d_slabs(vp, vs, rho, 10.0, 8e-4, 10, 25.0,
                                     cuts=[(0, c), (c, nz + 2 * pad)], **kw)
+
+
+def test_elastic3d_slabs_order2_one_plane_slab(fomo, slabs3d):
+    # halo 1: a slab owning a single plane takes both halos from two neighbours
+    nbc, fd_order, nz = 4, 2, 20
+    pad = nbc + fd_order // 2          # 5: cuts in [6, 24] of 30 planes
+    nzp = nz + 2 * pad
+    cuts = [(0, 6), (6, 7), (7, 24), (24, nzp)]
+    _check(fomo, slabs3d, True, fd_order, nbc, (26, 22, nz), 40, cuts=cuts, src_z=(2, 3))
+
+
+def test_acoustic3d_slabs_source_on_cut(fomo, slabs3d):
+    # order 6; the second source sits on the first plane of the second slab
+    nbc, fd_order, nz = 6, 6, 48
+    pad = nbc + fd_order // 2          # 9: 66 planes
+    cuts = [(0, 30), (30, 66)]
+    _check(fomo, slabs3d, False, fd_order, nbc, (34, 30, nz), 60, cuts=cuts,
+           src_z=(4, 30 - pad + 1))
