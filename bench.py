@@ -621,6 +621,8 @@ def slabs_bench(args):
                          "peak_kind": peak_kind,
                          "kernel": "whole time loop incl. halo exchange (CUDA events)"},
             "gpu_launches": launches, "clocks": clk.summary()}
+    if rank == 0 and not os.environ.get("FOMO_BENCH_NO_CPU"):
+        line["l2_vs_fp64"] = secondary_l2(args.workload, c, None, nt, slabs=max(n, 2))
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -630,13 +632,15 @@ def _rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
-def secondary_l2(workload, c, r, nt):
+def secondary_l2(workload, c, r, nt, slabs=0):
     """Error statement of a secondary line against the FP64 oracle of the same
     scheme: elastic-fp16 -- the middle shot's seismograms over the first
     min(nt, 1000) steps; uneven -- the smallest shot over its whole run (and
     whether it equals the FP32 oracle bit for bit); elastic3d -- a reduced grid
     (64x64x48 interior, the same dh, dt, order, nbc and model statistics, 150
-    steps), since the oracle cannot run the full volume in a bench."""
+    steps), since the oracle cannot run the full volume in a bench; with slabs > 0
+    that grid runs as that many z-slabs on this device, and the line also says
+    whether it equals the single-device run bit for bit."""
     from oracle import oracle as O
 
     import fomo_b200 as F
@@ -673,16 +677,31 @@ def secondary_l2(workload, c, r, nt):
         w = F.ricker_wavelet(c3["f0"], c3["dt"], k)
         kw = dict(sx=c3["sx"], sy=c3["sy"], sz=c3["sz"], rx=c3["rx"], ry=c3["ry"], rz=c3["rz"],
                   nbc=c3["nbc"], fd_order=c3["fd_order"])
+        from fomo_b200 import slabs3d
+
         if workload == "elastic3d":
             g = F.elastic3d(c3["vp"], c3["vs"], c3["rho"], c3["dh"], c3["dt"], k, c3["f0"], **kw)
             o = O.elastic3d(c3["vp"], c3["vs"], c3["rho"], c3["dh"], c3["dt"], k,
                             wavelet=w.reshape(1, -1), prec=64, **kw)
+            if slabs:
+                gs = slabs3d.elastic3d_slabs(c3["vp"], c3["vs"], c3["rho"], c3["dh"], c3["dt"], k,
+                                             c3["f0"], n_slabs=slabs, **kw)
         else:
             g = F.acoustic3d(c3["vp"], c3["rho"], c3["dh"], c3["dt"], k, c3["f0"], **kw)
             o = O.acoustic3d(c3["vp"], c3["rho"], c3["dh"], c3["dt"], k,
                              wavelet=w.reshape(1, -1), prec=64, **kw)
+            if slabs:
+                gs = slabs3d.acoustic3d_slabs(c3["vp"], c3["rho"], c3["dh"], c3["dt"], k, c3["f0"],
+                                              n_slabs=slabs, **kw)
+        sample = f"64x64x48 interior, {k} steps, same dh/dt/order/nbc"
+        if slabs:
+            same = all(np.array_equal(gs[q], g[q]) for q in range(3))
+            g = gs
+            sample += f", {slabs} z-slabs on one device"
         out = {"vz": _rel(g[2], o["seis_vz"]), "vx": _rel(g[0], o["seis_vx"]),
-               "tolerance": 1e-5, "sample": f"64x64x48 interior, {k} steps, same dh/dt/order/nbc"}
+               "tolerance": 1e-5, "sample": sample}
+        if slabs:
+            out["bitwise_vs_single_device"] = bool(same)
     out["oracle"] = f"C++ restatement in FP64 ({time.perf_counter() - t0:.1f} s on the host)"
     return out
 
