@@ -25,7 +25,7 @@ from __future__ import annotations
 
 import ctypes as C
 from dataclasses import dataclass
-from typing import Callable, Optional, Sequence
+from typing import Optional, Sequence
 
 import numpy as np
 
@@ -190,15 +190,13 @@ def run_local(slabs: Sequence[SlabLike], elastic: bool, nt: int, it0: int = 1) -
 
 
 def run_rank(slab: SlabLike, k: int, ranks: Sequence[int], elastic: bool, nt: int,
-             group=None, it0: int = 1, after_half: Optional[Callable[[], None]] = None) -> None:
+             group=None, it0: int = 1) -> None:
     """Steps it0..nt of slab k on this rank, exchanging halos with the neighbours."""
     n = len(ranks)
     regions = halo_regions(k, n, slab.z_lo, slab.z_hi, slab.z_base, slab.halo)
     for it in range(it0, nt + 1):
         for half in (0, 1):
             slab.step(it, half)
-            if after_half is not None:
-                after_half()
             exchange_dist(slab.state, slab.nfield, slab.nz_local, slab.plane, regions, ranks,
                           HALO_FIELDS[(elastic, half)], it % 2, group)
 
@@ -269,6 +267,12 @@ class Slab(SlabLike):
             _bind().fomo_slab3d_destroy(self.handle)
             self.handle = None
 
+    def __del__(self):  # pragma: no cover - interpreter shutdown order varies
+        try:
+            self.close()
+        except Exception:
+            pass
+
 
 def grid_planes(grid) -> tuple[int, int, int, int]:
     """(padded planes, lowest cut, highest cut, halo depth) of a 3D grid.
@@ -291,6 +295,8 @@ def gather_parts(part, k, n, ranks, group, dev):
 
     vx, vy, vz, owned = part
     n_rec, nt = vx.shape
+    if n_rec == 0:  # nothing recorded anywhere: no transfers
+        return _assemble([part]) if k == 0 else None
     if k != 0:
         mask = torch.from_numpy(owned.astype(np.uint8)).to(dev)
         dist.send(mask, ranks[0], group)
