@@ -31,13 +31,36 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait: gives up after 2^22 polls (about a second) and records the
-// failure in *err; the caller stops waiting on later phases as well.
+// The same with a suspend-time hint: the thread sleeps until the phase
+// completes or about `ns` nanoseconds pass, instead of returning after the
+// hardware's default time limit.
+__device__ __forceinline__ bool mbar_try_wait_for(uint64_t* bar, uint32_t parity, uint32_t ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(saddr(bar)), "r"(parity), "r"(ns)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Bounded wait: polls with a 1 ms suspend hint and gives up once about a
+// second has passed on the global timer, recording the failure in *err; the
+// caller stops waiting on later phases as well.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err) {
-  for (int spin = 0; spin < (1 << 22); ++spin)
-    if (mbar_try_wait(bar, parity)) return true;
-  atomicOr(err, 1);
-  return false;
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  while (!mbar_try_wait_for(bar, parity, 1000000u))
+    if (global_ns() - t0 > 1000000000ull) {
+      atomicOr(err, 1);
+      return false;
+    }
+  return true;
 }
 // Orders this thread's earlier generic-proxy shared-memory accesses before
 // the async-proxy (TMA) writes it issues next.
