@@ -31,49 +31,19 @@
 #include <mutex>
 
 #include "sweep2d.cuh"
+#include "tma.cuh"
 
 namespace fomo {
 namespace {
 
-__device__ __forceinline__ uint32_t s_addr(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_addr(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(s_addr(bar)),
-               "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(s_addr(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-__device__ __forceinline__ void fence_proxy_async() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
+// The shared mbarrier / TMA primitives (tma.cuh), bounded waits included.
+using tma::fence_proxy_async;
+using tma::mbar_expect_tx;
+using tma::mbar_init;
+using tma::mbar_wait_bounded;
 __device__ __forceinline__ void tma_load_3d(float* dst, const CUtensorMap* map, int x, int y,
                                             int z, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(s_addr(dst)),
-      "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(s_addr(bar))
-      : "memory");
-}
-
-// Bounded wait: gives up after 2^22 polls (about a second), records the failure.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err) {
-  for (int spin = 0; spin < (1 << 22); ++spin)
-    if (mbar_try_wait(bar, parity)) return true;
-  atomicOr(err, 1);
-  return false;
+  tma::load_3d(dst, map, x, y, z, bar);
 }
 
 constexpr int halo_x(int M) { return (2 * M + 2 + 3) & ~3; }  // stress x-halo, 16-byte aligned
@@ -148,7 +118,7 @@ __global__ void __launch_bounds__(NT) k_el_sweep(const __grid_constant__ CUtenso
   auto wsm = [&](int kind, int dist) { return dist < h.wstride ? swt[kind * h.wstride + dist] : 1.0f; };
   if (t == 0) {
     for (int k = 0; k < NSLOT; ++k) mbar_init(&bars[k], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    tma::mbar_init_fence();
   }
   __syncthreads();
 
@@ -533,7 +503,7 @@ __global__ void __launch_bounds__(kX2Threads, 1)
   for (int k = tid; k < 3 * h.wstride; k += kX2Threads) s_wt[k] = __ldg(h.wtab + k);
   if (tid == 0) {
     for (int k = 0; k < NPT; ++k) mbar_init(&bars[k], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    tma::mbar_init_fence();
   }
   __syncthreads();
   auto wsm = [&](int kind, int dist) {
@@ -892,7 +862,7 @@ __global__ void __launch_bounds__(kRWThreads, 2)
   for (int k = tid; k < 3 * h.wstride; k += kRWThreads) s_wt[k] = __ldg(h.wtab + k);
   if (tid == 0) {
     for (int k = 0; k < NO; ++k) mbar_init(&bars[k], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    tma::mbar_init_fence();
   }
   __syncthreads();
   auto wsm = [&](int kind, int dist) {
@@ -1314,7 +1284,7 @@ __global__ void __launch_bounds__(NT, 256 / NT)
   for (int k = tid; k < 3 * h.wstride; k += NT) s_wt[k] = __ldg(h.wtab + k);
   if (tid == 0) {
     for (int k = 0; k < NO; ++k) mbar_init(&bars[k], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    tma::mbar_init_fence();
   }
   __syncthreads();
   auto wsm = [&](int kind, int dist) {
@@ -1761,7 +1731,7 @@ __global__ void __launch_bounds__(2 * NV, MINB)
   for (int k = tid; k < 3 * h.wstride; k += NT) s_wt[k] = __ldg(h.wtab + k);
   if (tid == 0) {
     for (int k = 0; k < NO; ++k) mbar_init(&bars[k], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    tma::mbar_init_fence();
   }
   __syncthreads();
   auto wsm = [&](int kind, int dist) {
